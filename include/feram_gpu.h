@@ -1,0 +1,259 @@
+/*
+ * feram_gpu.h -- C-ABI of the B200-native feram molecular-dynamics step.
+ *
+ * The reference (t-nissie/feram, Fortran 90 + OpenMP + FFTW) evaluates one
+ * MD time step of the first-principles effective Hamiltonian through the
+ * subroutines mirror_force_mirror, dVddi_*, nose_poincare and leapfrog, all
+ * of which take the derived types Param_type / Coord_type / Energy_type by
+ * reference.  Those types are not interoperable, so this header replaces
+ * them with plain C structs and an opaque device context.  A Fortran caller
+ * binds every function below with ISO_C_BINDING (see
+ * fortran/feram_gpu_iface.F90); arrays cross the boundary as plain host
+ * pointers in the reference's own padded, column-major layout:
+ *
+ *   real field  (ncomp, 0:2*(Lx/2+1)-1, 0:Ly+padding_y-1, 0:Lz-1)
+ *   complex     (ncomp, 0:Lx/2,         0:Ly+padding_y-1, 0:Lz-1)
+ *   k table     (3, 3,  0:Lx/2,         0:Ly+padding_y-1, 0:Lz-1)
+ *
+ * (coord_module.F:91-93,139-141,247,256).  Only physical points are read
+ * or written; padding is left untouched.
+ *
+ * Every function returns an int status (FG_OK = 0).  The library never
+ * calls exit(); the text of the last error of a context is available from
+ * fg_last_error().  One context per host thread; calls on one context are
+ * not re-entrant; different contexts are independent.
+ */
+#ifndef FERAM_GPU_H
+#define FERAM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FG_RELAXOR_MAX 3
+#define FG_FILENAME_LEN 300
+
+/* status codes */
+enum {
+  FG_OK = 0,
+  FG_ERR_ARG = 1,          /* invalid argument or parameter combination   */
+  FG_ERR_CUDA = 2,         /* CUDA runtime error                           */
+  FG_ERR_NAN = 3,          /* NaN or Inf found in a reduction              */
+  FG_ERR_TIMEOUT = 4,      /* a bounded device-side wait ran out           */
+  FG_ERR_UNSUPPORTED = 5,  /* input outside what this build implements     */
+  FG_ERR_IO = 6,           /* file could not be read or parsed             */
+  FG_ERR_STATE = 7         /* call order (e.g. no tables uploaded yet)     */
+};
+
+/* bulk_or_film (param_module.F:255-263) */
+enum { FG_BULK = 0, FG_FILM = 1, FG_EPIT = 2, FG_E110 = 3 };
+/* method (param_module.F:33) */
+enum { FG_METHOD_MD = 0, FG_METHOD_VS = 1, FG_METHOD_LF = 2, FG_METHOD_HL = 3 };
+/* E_wave_type (wave_module.F:180-220) */
+enum {
+  FG_WAVE_NONE = 0, FG_WAVE_TRIANGULAR_COS = 1, FG_WAVE_TRIANGULAR_SIN = 2,
+  FG_WAVE_RAMPING_ON = 3, FG_WAVE_RAMPING_OFF = 4, FG_WAVE_OTHER = 5
+};
+/* arithmetic of the device path */
+enum {
+  FG_PREC_FP64 = 0,   /* every field, FFT and force in FP64                  */
+  FG_PREC_MIXED = 1   /* FP32 fields/FFT/forces; FP64 thermostat, strain,
+                         energy accumulation                                 */
+};
+
+/*
+ * Param_type (param_module.F:8-111), the members the MD step reads.
+ * Units as in the reference: Angstrom, eV, ps, e, V/Angstrom.
+ */
+typedef struct fg_params {
+  /* method, temperature, masses */
+  int    method;                         /* FG_METHOD_*                    */
+  int    continue_run;                   /* 'continue' tag                 */
+  double GPa[3];
+  double kelvin;
+  double mass_dipo[FG_RELAXOR_MAX];      /* eV A^-2 ps^2                   */
+  double mass_acou[FG_RELAXOR_MAX];      /* <= 0: acoustic field relaxed    */
+  double Q_Nose;
+  /* geometry */
+  int    bulk_or_film;                   /* FG_BULK ... FG_E110            */
+  int    Lx, Ly, Lz;
+  int    gap_id;
+  int    padding_y;
+  double gap_dipole_u[3];
+  double a0;
+  double epi_strain;
+  /* time steps */
+  double dt;
+  int    n_thermalize, n_average, n_E_wave_period;
+  int    n_coord_freq, n_hl_freq, n_hysteresis_loop_continue;
+  /* external field */
+  double external_E_field[3];
+  int    E_wave_type;                    /* FG_WAVE_*                      */
+  /* on-site polynomial, per relaxor species */
+  double P_kappa2[FG_RELAXOR_MAX], P_alpha[FG_RELAXOR_MAX], P_gamma[FG_RELAXOR_MAX];
+  double P_k1[FG_RELAXOR_MAX], P_k2[FG_RELAXOR_MAX], P_k3[FG_RELAXOR_MAX], P_k4[FG_RELAXOR_MAX];
+  /* inter-site */
+  double j[7];
+  /* elastic constants and coupling */
+  double B11, B12, B44, B1xx, B1yy, B4yz, modulation_constant;
+  /* dipoles */
+  int    seed[2];
+  double init_dipo_avg[3], init_dipo_dev[3], k_stripe[3];
+  double Z_star[FG_RELAXOR_MAX];
+  double epsilon_inf;
+  double kappa;                          /* Ewald kappa; <= 0 -> default   */
+  int    plot_dispersion, output_polarization;
+  double delta_e, delta_e_acou;
+  int    verbose;
+  /* output directories: "" (cwd) or "never" */
+  char   coord_directory[FG_FILENAME_LEN];
+  char   slice_directory[FG_FILENAME_LEN];
+  char   distribution_directory[FG_FILENAME_LEN];
+  char   filename[FG_FILENAME_LEN];      /* basename of the .feram file    */
+  /* derived by fg_make_param (make_Param, param_module.F:452-480) */
+  int    N;
+  double Ninv, dt_2;
+  int    n_freedom;
+  double unit_cell_volume;
+  double pNa03[3];
+  double temperature_eV;
+  double target_kinetic_energy;
+  int    E_field_always_zero;
+} fg_params;
+
+/* Energy_type (energy_module.F:7-23), same member order; eV per supercell */
+typedef struct fg_energy {
+  double acou_kinetic;
+  double dipo_kinetic;
+  double short_range;
+  double long_range;
+  double dipole_E_field;
+  double unharmonic;
+  double homo_strain;
+  double homo_coupling;
+  double inho_strain;
+  double inho_coupling;
+  double inho_modulation;
+  double total;
+  double H_Nose_Poincare;
+} fg_energy;
+
+/* Running sums of add_to_Average (average_module.F:57-128) */
+typedef struct fg_average {
+  fg_energy energy;       /* sum of per-step energies                       */
+  double e2;              /* sum of total^2                                 */
+  double dipo_kinetic_true;
+  double strain[6];
+  double u[3], uu[6];     /* sum of (masked) sum_R u, and of (sum u)(sum u)  */
+  double p[3], pp[6];     /* same for Z* u                                   */
+  int    n_steps;
+} fg_average;
+
+typedef struct fg_ctx fg_ctx;
+
+/* ---- host-side mirror of param_module.F --------------------------------- */
+
+/* Defaults of read_Param (param_module.F:129-194). */
+void fg_default_param(fg_params* p);
+/* read_Param (param_module.F:114-450): parse a .feram file.  Unknown tags,
+   bad bulk_or_film, acoustic_mass_amu with method 'md' and n_E_wave_period
+   not divisible by 4 are errors (FG_ERR_IO), as in the reference's stops.
+   errbuf (may be NULL) receives a one-line message. */
+int  fg_read_param(const char* path, fg_params* p, char* errbuf, int errlen);
+/* make_Param (param_module.F:452-480): derived constants and geometry checks. */
+int  fg_make_param(fg_params* p, char* errbuf, int errlen);
+/* wave (wave_module.F:162-221): external field added at step i_step. */
+int  fg_wave(int wave_type, int i_step, int n_thermalize, int period,
+             const double amplitude[3], double out[3]);
+/* Marsaglia-Tsang uni64 (marsaglia_tsang_uni64_module.f:133-168) and the
+   Box-Muller normal_dist (:179-202), process-global like the reference's
+   SAVE variables.  fg_uni64_seed returns the running seed count (1.0, 2.0, ..). */
+double fg_uni64_seed(int seed1, int seed2);
+double fg_uni64(void);
+double fg_normal_dist_seed(int seed1, int seed2);
+double fg_normal_dist(double mu, double sigma);
+/* initialize_dipoR (initialize-dipoR.F:41-56), no-.restart branch: seeded
+   Gaussian u in the reference's draw order (alpha outer, z, y, x inner),
+   stripe sign flips, p = 0.  Arrays in the padded Fortran layout. */
+int  fg_init_dipoR_host(const fg_params* p, double* dipoR, double* dipoP);
+
+/* ---- device context ------------------------------------------------------ */
+
+/* Replaces alloc_Coord (coord_module.F:67-432): validates p, allocates the
+   device state for one supercell on the current CUDA device. */
+int  fg_create(const fg_params* p, int precision, fg_ctx** out);
+void fg_destroy(fg_ctx* ctx);
+const char* fg_last_error(const fg_ctx* ctx);
+/* cudaStream_t of the context, as void* (for event timing by the caller). */
+void* fg_stream(fg_ctx* ctx);
+
+/* Device-built k-space tables: replaces dipole_dipole (dipole-dipole.F:6-57:
+   Ewald long range + short-range stencil) and elastic (elastic.F:7-237).
+   The inhomogeneous elastic tables (inhomo_K, its Cholesky factor,
+   inhomo_coup2_K) are analytic in k and evaluated inside the k-space kernel. */
+int  fg_build_tables(fg_ctx* ctx);
+/* Tables computed by the reference's own setup (feram_common.F:82-83),
+   Fortran layout (3,3,0:Lx/2,0:Ly+padding_y-1,0:Lz-1), real*8.  The short-
+   range table must be the standard feram stencil (checked to 1e-9). */
+int  fg_upload_tables(fg_ctx* ctx, const double* short_range, const double* long_range);
+/* c_k_modulation_k (elastic.F:183-226), complex*16 (3,0:Lx/2,...); NULL clears. */
+int  fg_upload_modulation(fg_ctx* ctx, const double* c_k_modulation_k);
+/* .modulation real-space field modulation_R (scalar padded field); the FFT and
+   c_k = modulation_constant * k * modulation_k are done on the device. */
+int  fg_set_modulation_R(fg_ctx* ctx, const double* modulation_R);
+/* Long-range table as built on the device, Fortran layout, eV/A^2 (testing). */
+int  fg_get_long_range(fg_ctx* ctx, double* long_range);
+
+/* ---- state --------------------------------------------------------------- */
+
+/* Coord_type members (coord_module.F:18,25,26,48,53).  dipoR/dipoP/dVddi are
+   real fields with 3 components; dVddi may be NULL. */
+int  fg_set_state(fg_ctx* ctx, const double* dipoR, const double* dipoP,
+                  double s_Nose, double pi_Nose, double H0);
+int  fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi,
+                  double strain[6], double* s_Nose, double* pi_Nose, double* H0);
+int  fg_set_thermostat(fg_ctx* ctx, double s_Nose, double pi_Nose, double H0);
+/* acouK (complex, 3 comps) of the last force evaluation, Fortran layout. */
+int  fg_get_acouK(fg_ctx* ctx, double* acouK);
+/* Uniform external field E(R) = E (initialize_E_field.F:139-146,
+   molecular-dynamics.F:223-233 with no .localfield). */
+int  fg_set_uniform_E(fg_ctx* ctx, const double E[3]);
+
+/* ---- the hot path -------------------------------------------------------- */
+
+/* mirror_force_mirror (mirror_force_mirror.F:6-89): dVddi, strain, acouK and
+   every potential-energy member of e (kinetic members untouched). */
+int  fg_mirror_force_mirror(fg_ctx* ctx, fg_energy* e);
+/* nose_poincare (nose-poincare.F:10-78): one Nose-Poincare step.  e must hold
+   the energies of the previous call on entry (the reference reads them). */
+int  fg_nose_poincare(fg_ctx* ctx, fg_energy* e);
+/* leapfrog (leapfrog.F:9-157), acoustic mass <= 0, delta_e = 0. */
+int  fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step);
+/* kinetic_energy_dipo (kinetic_energy_dipo.F:14-28). */
+int  fg_kinetic_energy_dipo(fg_ctx* ctx, double* ke);
+/* Nose_Poincare_Hamiltonian (energy_module.F:128-148), e->H_Nose_Poincare. */
+int  fg_nose_poincare_hamiltonian(fg_ctx* ctx, fg_energy* e);
+/* add_to_Average (average_module.F:75-128) reductions, on the device. */
+int  fg_average_accumulate(fg_ctx* ctx, const fg_energy* e, fg_average* avg);
+/* c%dipoRavg += c%dipoR (molecular-dynamics.F:301-305), on the device. */
+int  fg_dipoRavg_accumulate(fg_ctx* ctx);
+int  fg_get_dipoRavg(fg_ctx* ctx, double* dipoRavg);
+
+/* Run n_steps of the method of p (md or lf) on the device as one CUDA graph
+   per step; the energies of the last step are returned in e. */
+int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
+
+/* ---- host driver ----------------------------------------------------------
+   feram_common + molecular_dynamics (feram_common.F:9-119,
+   molecular-dynamics.F:10-160) replayed on the host through the calls above:
+   reads <path>.feram, builds tables on the device, initialises u with
+   uni64, runs n_thermalize + n_average steps and writes <filename>.avg and
+   <filename>.log in the reference's formats.  t_sim receives the stepping
+   time in seconds (the reference's t_simulation). */
+int  fg_feram_run(const char* path, int precision, fg_average* avg_out,
+                  double* t_sim, char* errbuf, int errlen);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FERAM_GPU_H */
