@@ -1,0 +1,216 @@
+"""feram_b200 -- B200-native MD step of feram's effective Hamiltonian.
+
+The product is the C-ABI shared library ``libferam_gpu.so`` (declared in
+``include/feram_gpu.h``).  This module is the Python view of that interface
+for tests and benchmarks: ``Context`` wraps one ``fg_ctx`` and its methods
+carry the names of the reference subroutines they replace
+(``mirror_force_mirror``, ``nose_poincare``, ``leapfrog``,
+``kinetic_energy_dipo`` ...).  Arrays are numpy views of the reference's
+padded Fortran layout (see ``_capi.real_field``).  Every call goes to the
+device; there is no CPU fallback, and a missing library raises ``OSError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+
+import numpy as np
+
+from . import _capi
+from ._capi import (FG_PREC_FP64, FG_PREC_MIXED, FG_OK, fg_average, fg_energy, fg_params,
+                    complex_field, dptr, k_table, physical, real_field)
+
+__all__ = ["Context", "FeramError", "read_param", "make_param", "params_from_text", "default_params",
+           "FG_PREC_FP64", "FG_PREC_MIXED", "fg_energy", "fg_average", "fg_params",
+           "real_field", "complex_field", "k_table", "physical", "lib"]
+
+lib = _capi.lib
+
+
+class FeramError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _err(buf) -> str:
+    return buf.value.decode(errors="replace")
+
+
+def default_params() -> fg_params:
+    p = fg_params()
+    lib().fg_default_param(C.byref(p))
+    return p
+
+
+def read_param(path: str) -> fg_params:
+    """read_Param (param_module.F:114-450) on the host."""
+    p = fg_params()
+    eb = C.create_string_buffer(512)
+    rc = lib().fg_read_param(os.fsencode(path), C.byref(p), eb, 512)
+    if rc:
+        raise FeramError(rc, _err(eb))
+    return p
+
+
+def make_param(p: fg_params) -> fg_params:
+    """make_Param (param_module.F:452-480), in place."""
+    eb = C.create_string_buffer(512)
+    rc = lib().fg_make_param(C.byref(p), eb, 512)
+    if rc:
+        raise FeramError(rc, _err(eb))
+    return p
+
+
+def params_from_text(text: str, name: str = "input") -> fg_params:
+    """Parse .feram text (through a temporary file) and make the derived constants."""
+    with tempfile.TemporaryDirectory() as d:
+        fn = os.path.join(d, name + ".feram")
+        with open(fn, "w") as f:
+            f.write(text)
+        p = read_param(fn)
+    return make_param(p)
+
+
+class Context:
+    """One supercell on the current CUDA device (alloc_Coord + Coord_type)."""
+
+    def __init__(self, params: fg_params, precision: int = FG_PREC_FP64):
+        self.p = params
+        self.precision = precision
+        self._h = C.c_void_p()
+        rc = lib().fg_create(C.byref(params), precision, C.byref(self._h))
+        if rc:
+            msg = self.last_error()
+            self.close()
+            raise FeramError(rc, msg)
+
+    # -- plumbing
+    def last_error(self) -> str:
+        if not self._h:
+            return "no context"
+        r = lib().fg_last_error(self._h)
+        return r.decode() if r else ""
+
+    def _check(self, rc):
+        if rc != FG_OK:
+            raise FeramError(rc, self.last_error())
+
+    def close(self):
+        if self._h:
+            lib().fg_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return lib().fg_stream(self._h)
+
+    # -- setup
+    def build_tables(self):
+        self._check(lib().fg_build_tables(self._h))
+
+    def upload_tables(self, short_range: np.ndarray, long_range: np.ndarray):
+        self._check(lib().fg_upload_tables(self._h, dptr(short_range), dptr(long_range)))
+
+    def upload_modulation(self, c_k_modulation_k: np.ndarray | None):
+        a = None if c_k_modulation_k is None else np.ascontiguousarray(c_k_modulation_k).view(np.float64)
+        self._check(lib().fg_upload_modulation(self._h, dptr(a)))
+
+    def set_modulation_R(self, modulation_R: np.ndarray):
+        self._check(lib().fg_set_modulation_R(self._h, dptr(modulation_R)))
+
+    def get_long_range(self) -> np.ndarray:
+        t = k_table(self.p)
+        self._check(lib().fg_get_long_range(self._h, dptr(t)))
+        return t
+
+    # -- FFTs (plan_r2c_3_out / plan_c2r_3_out)
+    def fft_r2c3(self, field: np.ndarray) -> np.ndarray:
+        out = complex_field(self.p)
+        self._check(lib().fg_fft_r2c3(self._h, dptr(field), dptr(out.view(np.float64))))
+        return out
+
+    def fft_c2r3(self, spec: np.ndarray) -> np.ndarray:
+        out = real_field(self.p)
+        s = np.ascontiguousarray(spec, dtype=np.complex128)
+        self._check(lib().fg_fft_c2r3(self._h, dptr(s.view(np.float64)), dptr(out)))
+        return out
+
+    # -- state
+    def set_state(self, dipoR=None, dipoP=None, s=1.0, pi=0.0, H0=0.0):
+        self._check(lib().fg_set_state(self._h, dptr(dipoR), dptr(dipoP), s, pi, H0))
+
+    def set_thermostat(self, s, pi, H0):
+        self._check(lib().fg_set_thermostat(self._h, s, pi, H0))
+
+    def get_state(self) -> dict:
+        u, q, f = real_field(self.p), real_field(self.p), real_field(self.p)
+        strain = np.zeros(6)
+        s, pi, H0 = C.c_double(), C.c_double(), C.c_double()
+        self._check(lib().fg_get_state(self._h, dptr(u), dptr(q), dptr(f), dptr(strain),
+                                       C.byref(s), C.byref(pi), C.byref(H0)))
+        return dict(dipoR=u, dipoP=q, dVddi=f, strain=strain, s=s.value, pi=pi.value, H0=H0.value)
+
+    def get_acouK(self) -> np.ndarray:
+        a = complex_field(self.p)
+        self._check(lib().fg_get_acouK(self._h, dptr(a.view(np.float64))))
+        return a
+
+    def set_uniform_E(self, E):
+        e = np.ascontiguousarray(E, dtype=np.float64)
+        self._check(lib().fg_set_uniform_E(self._h, dptr(e)))
+
+    # -- hot path (reference subroutine names)
+    def mirror_force_mirror(self, e: fg_energy | None = None) -> fg_energy:
+        e = e if e is not None else fg_energy()
+        self._check(lib().fg_mirror_force_mirror(self._h, C.byref(e)))
+        return e
+
+    def nose_poincare(self, e: fg_energy) -> fg_energy:
+        self._check(lib().fg_nose_poincare(self._h, C.byref(e)))
+        return e
+
+    def leapfrog(self, e: fg_energy, i_step: int) -> fg_energy:
+        self._check(lib().fg_leapfrog(self._h, C.byref(e), i_step))
+        return e
+
+    def kinetic_energy_dipo(self) -> float:
+        v = C.c_double()
+        self._check(lib().fg_kinetic_energy_dipo(self._h, C.byref(v)))
+        return v.value
+
+    def nose_poincare_hamiltonian(self, e: fg_energy) -> fg_energy:
+        self._check(lib().fg_nose_poincare_hamiltonian(self._h, C.byref(e)))
+        return e
+
+    def average_accumulate(self, e: fg_energy, avg: fg_average):
+        self._check(lib().fg_average_accumulate(self._h, C.byref(e), C.byref(avg)))
+
+    def run_steps(self, n: int, e: fg_energy | None = None) -> fg_energy:
+        e = e if e is not None else fg_energy()
+        self._check(lib().fg_run_steps(self._h, n, C.byref(e)))
+        return e
+
+
+def feram_run(path: str, precision: int = FG_PREC_FP64):
+    """feram_common + molecular_dynamics for one .feram file (writes .avg/.log)."""
+    avg = fg_average()
+    t = C.c_double()
+    eb = C.create_string_buffer(512)
+    rc = lib().fg_feram_run(os.fsencode(path), precision, C.byref(avg), C.byref(t), eb, 512)
+    if rc:
+        raise FeramError(rc, _err(eb))
+    return avg, t.value

@@ -111,7 +111,9 @@ def physical(a: np.ndarray, p) -> np.ndarray:
 
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libferam_gpu.so")
+# FERAM_B200_LIB=checked selects the bounds-checked build of the same sources
+LIB_PATH = os.path.join(_HERE, "libferam_gpu_checked.so" if os.environ.get("FERAM_B200_LIB") == "checked"
+                        else "libferam_gpu.so")
 _lib = None
 
 
@@ -146,6 +148,8 @@ def lib() -> C.CDLL:
         "fg_upload_modulation": (C.c_int, [vp, dp]),
         "fg_set_modulation_R": (C.c_int, [vp, dp]),
         "fg_get_long_range": (C.c_int, [vp, dp]),
+        "fg_fft_r2c3": (C.c_int, [vp, dp, dp]),
+        "fg_fft_c2r3": (C.c_int, [vp, dp, dp]),
         "fg_set_state": (C.c_int, [vp, dp, dp, C.c_double, C.c_double, C.c_double]),
         "fg_get_state": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
         "fg_set_thermostat": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
@@ -160,6 +164,9 @@ def lib() -> C.CDLL:
         "fg_dipoRavg_accumulate": (C.c_int, [vp]),
         "fg_get_dipoRavg": (C.c_int, [vp, dp]),
         "fg_run_steps": (C.c_int, [vp, C.c_int, P(fg_energy)]),
+        "fg_time_steps": (C.c_int, [vp, C.c_int, dp]),
+        "fg_profile_step": (C.c_int, [vp, C.c_int, dp]),
+        "fg_profile_name": (C.c_char_p, [C.c_int]),
         "fg_feram_run": (C.c_int, [C.c_char_p, C.c_int, P(fg_average), dp, C.c_char_p, C.c_int]),
     }
     for name, (res, args) in sig.items():
@@ -177,4 +184,4 @@ def exported_symbols() -> list[str]:
     import re
     hdr = os.path.join(os.path.dirname(_HERE), "include", "feram_gpu.h")
     text = open(hdr).read()
-    return sorted(set(re.findall(r"\b(fg_[a-z0-9_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(fg_[A-Za-z0-9_]+)\s*\(", text)))

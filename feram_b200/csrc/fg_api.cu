@@ -1,0 +1,1242 @@
+// fg_api.cu -- the C-ABI of include/feram_gpu.h on one B200.
+//
+// One fg_ctx owns the device state of one supercell (coord_module.F's
+// Coord_type), the k-space tables, the FFT plans and a CUDA stream.  Each
+// MD step is a CUDA graph of ~12 kernels whose scalars (Nose-Poincare s, pi,
+// H0, strain, energies) live in device memory, so a step never waits on the
+// host; the host reads the 13 energies back once per call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/feram_gpu.h"
+#include "fg_kernels.cuh"
+
+using namespace fg;
+
+namespace {
+
+constexpr int kThreadsFFT = 512;
+constexpr int kThreadsElem = 256;
+
+int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// DIF stage radices, largest first (8, 4, 2, then 3 and 5).
+bool make_plan(int n, FftPlan* P) {
+  P->n = n;
+  P->nst = 0;
+  int m = n;
+  while (m % 8 == 0) { P->r[P->nst++] = 8; m /= 8; }
+  while (m % 4 == 0) { P->r[P->nst++] = 4; m /= 4; }
+  while (m % 2 == 0) { P->r[P->nst++] = 2; m /= 2; }
+  while (m % 3 == 0) { if (P->nst >= FFT_MAX_STAGES) return false; P->r[P->nst++] = 3; m /= 3; }
+  while (m % 5 == 0) { if (P->nst >= FFT_MAX_STAGES) return false; P->r[P->nst++] = 5; m /= 5; }
+  return m == 1 && P->nst <= FFT_MAX_STAGES;
+}
+
+// slot -> frequency of the DIF output (digit reversal)
+std::vector<int> digit_reversal(const FftPlan& P) {
+  std::vector<int> rev(P.n);
+  for (int p = 0; p < P.n; ++p) {
+    int q = p, k = 0, mult = 1, span = P.n;
+    for (int st = 0; st < P.nst; ++st) {
+      span /= P.r[st];
+      int s = q / span;
+      q -= s * span;
+      k += s * mult;
+      mult *= P.r[st];
+    }
+    rev[p] = k;
+  }
+  return rev;
+}
+
+// exp(-2 pi i k / n), k = 0..n-1, from long-double sin/cos of the reduced angle
+template <typename T>
+std::vector<cplx<T>> twiddles(int n) {
+  std::vector<cplx<T>> w(n);
+  for (int k = 0; k < n; ++k) {
+    long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+    w[k] = mk<cplx<T>>((T)std::cos(a), (T)std::sin(a));
+  }
+  return w;
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct fg_ctx {
+  fg_params P;
+  int prec = FG_PREC_FP64;
+  std::string err;
+  Geom g{};
+  FftPlan px{}, py{}, pz{};
+  int cw = 8, ntx = 1;        // z tile of the MD k-space kernel
+  int cw6 = 8, ntx6 = 1;      // z tile of the table build (6 FP64 comps)
+  int cw1 = 8, ntx1 = 1;      // z tile of the modulation FFT (1 FP64 comp)
+  int smem_xy = 0, smem_xy64 = 0, smem_z = 0, smem_z3 = 0, smem_z6 = 0, smem_z1 = 0;
+  int grid_elem = 1;
+  cudaStream_t stream = nullptr;
+  // fields (T = float or double)
+  void* u = nullptr;
+  void* p = nullptr;
+  void* F = nullptr;
+  void* spec = nullptr;   // 9 complex spectra
+  void* rwork = nullptr;  // 9 real fields
+  void* dtab = nullptr;   // 6 per table slot
+  void* ckmod = nullptr;  // 3 complex per table slot
+  void* acouK = nullptr;  // 3 complex per table slot
+  void* twx = nullptr;
+  void* twm = nullptr;
+  void* twy = nullptr;
+  void* twz = nullptr;
+  // FP64 twiddles for table construction
+  cplx<double>* twx64 = nullptr;
+  cplx<double>* twm64 = nullptr;
+  cplx<double>* twy64 = nullptr;
+  cplx<double>* twz64 = nullptr;
+  double* L64 = nullptr;  // long-range table (FP64, table slots)
+  int* revx = nullptr;
+  int* revy = nullptr;
+  int* revz = nullptr;
+  int* posm = nullptr;
+  double* kvx = nullptr;
+  double* kvy = nullptr;
+  double* kvz = nullptr;
+  double2* trx = nullptr;
+  double2* try_ = nullptr;
+  double2* trz = nullptr;
+  double* layer_minv = nullptr;
+  unsigned char* layer_sump = nullptr;
+  Phys* ph = nullptr;
+  Phys ph_host{};
+  DevScalars* sc = nullptr;
+  DevScalars* sc_host = nullptr;  // pinned
+  double* part_k = nullptr;
+  double* part_r = nullptr;
+  double* part_ke = nullptr;
+  double* part_avg = nullptr;
+  double* avg6 = nullptr;
+  double* staging = nullptr;      // padded Fortran-layout FP64 (3 components)
+  size_t staging_n = 0;
+  double* dipoRavg = nullptr;     // FP64 accumulator [3][nsite]
+  std::vector<int> h_revx, h_revy, h_revz;
+  cudaGraphExec_t g_np = nullptr, g_lf = nullptr, g_force = nullptr;
+  bool tables_ready = false;
+  bool force_fresh = false;
+  bool store_acouK = false;
+  double n_sum_p = 0;
+  int NXP = 0, NYP = 0;
+  bool bulk_or_film_mirror() const { return P.bulk_or_film == FG_FILM || P.bulk_or_film == FG_EPIT; }
+  size_t real_bytes = 0;
+};
+
+namespace {
+
+int fail(fg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(ctx, FG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));          \
+  } while (0)
+
+#define CKL()                                                                                     \
+  do {                                                                                            \
+    cudaError_t e_ = cudaGetLastError();                                                          \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(ctx, FG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_));     \
+  } while (0)
+
+template <typename T>
+KMaps kmaps(const fg_ctx* c) {
+  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz};
+}
+
+int check_device_error(fg_ctx* ctx) {
+#if FG_BOUNDS_CHECK
+  DevError de{};
+  CK(cudaMemcpyFromSymbol(&de, fg::g_fg_err, sizeof(de)));
+  if (de.code != 0) {
+    char b[128];
+    std::snprintf(b, sizeof(b), "device bounds check %d failed at index %lld", de.code, de.idx);
+    return fail(ctx, FG_ERR_CUDA, b);
+  }
+#else
+  (void)ctx;
+#endif
+  return FG_OK;
+}
+
+// ----------------------------------------------------------- force pipeline
+template <typename T>
+int enqueue_force(fg_ctx* ctx) {
+  const Geom& g = ctx->g;
+  cudaStream_t st = ctx->stream;
+  T* u = (T*)ctx->u;
+  if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
+    k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(u, g, ctx->P.gap_id);
+    CKL();
+  }
+  k_xy_fwd<T, SRC_U9><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
+      u, (cplx<T>*)ctx->spec, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm,
+      (const cplx<T>*)ctx->twy, ctx->posm, 0);
+  CKL();
+  k_z_kspace<T><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z, st>>>(
+      (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod,
+      ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr, g, ctx->pz, (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph,
+      ctx->part_k, ctx->sc, ctx->cw);
+  CKL();
+  k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->ntx * g.Ly);
+  CKL();
+  k_xy_inv<T><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
+      (const cplx<T>*)ctx->spec, (T*)ctx->rwork, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
+      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
+  CKL();
+  k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
+                                                         ctx->part_r);
+  CKL();
+  k_force_energies<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_r, ctx->grid_elem);
+  CKL();
+  if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
+    k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
+    CKL();
+  }
+  return FG_OK;
+}
+
+template <typename T>
+int enqueue_kick(fg_ctx* ctx, const double* coef) {
+  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (const T*)ctx->F, coef, ctx->g,
+                                                               ctx->layer_minv, ctx->layer_sump, ctx->part_ke);
+  CKL();
+  return FG_OK;
+}
+
+template <typename T>
+int enqueue_drift(fg_ctx* ctx, const double* coef) {
+  k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->u, (const T*)ctx->p, coef, ctx->g,
+                                                                ctx->layer_minv);
+  CKL();
+  return FG_OK;
+}
+
+// nose_poincare (nose-poincare.F:24-75)
+template <typename T>
+int enqueue_np(fg_ctx* ctx) {
+  int rc;
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef))) return rc;  // (35a)
+  k_np_pre<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+  CKL();
+  if ((rc = enqueue_drift<T>(ctx, &ctx->sc->drift_coef))) return rc;  // (35d)
+  if ((rc = enqueue_force<T>(ctx))) return rc;
+  k_np_post<<<1, 32, 0, ctx->stream>>>(ctx->ph, ctx->sc);
+  CKL();
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef))) return rc;  // (35f)
+  k_np_final<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+  CKL();
+  return FG_OK;
+}
+
+// leapfrog (leapfrog.F:103-151), i_step != 0
+template <typename T>
+int enqueue_lf(fg_ctx* ctx) {
+  int rc;
+  if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
+  if ((rc = enqueue_force<T>(ctx))) return rc;
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->lf_dt))) return rc;
+  k_lf_final<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+  CKL();
+  return FG_OK;
+}
+
+// Capture fn into a CUDA graph executable (once per context).
+template <typename Fn>
+int capture(fg_ctx* ctx, cudaGraphExec_t* out, Fn fn) {
+  if (*out) return FG_OK;
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = fn();
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return FG_OK;
+}
+
+int run_graph(fg_ctx* ctx, cudaGraphExec_t* gx, int which) {
+  int rc = FG_OK;
+  if (which == 0) {
+    rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_force<float>(ctx) : enqueue_force<double>(ctx); });
+  } else if (which == 1) {
+    rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_np<float>(ctx) : enqueue_np<double>(ctx); });
+  } else {
+    rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_lf<float>(ctx) : enqueue_lf<double>(ctx); });
+  }
+  if (rc) return rc;
+  CK(cudaGraphLaunch(*gx, ctx->stream));
+  return FG_OK;
+}
+
+int pull_scalars(fg_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->sc_host, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  int rc = check_device_error(ctx);
+  if (rc) return rc;
+  if (ctx->sc_host->status == FG_ERR_NAN) return fail(ctx, FG_ERR_NAN, "non-finite energy in a device reduction");
+  return FG_OK;
+}
+
+int push_scalars(fg_ctx* ctx) {
+  CK(cudaMemcpyAsync(ctx->sc, ctx->sc_host, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FG_OK;
+}
+
+void energy_out(const DevScalars* s, fg_energy* e, bool potential_only) {
+  double* d = &e->acou_kinetic;
+  for (int i = 0; i < E_COUNT; ++i) {
+    if (potential_only && (i < E_SHORT || i > E_IM)) continue;
+    d[i] = s->e[i];
+  }
+}
+
+template <typename T>
+void* dalloc(fg_ctx* ctx, size_t n, int* rc) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *rc = fail(ctx, FG_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return nullptr;
+  }
+  return p;
+}
+
+template <typename V>
+int upload(fg_ctx* ctx, void** dst, const std::vector<V>& v) {
+  CK(cudaMalloc(dst, v.size() * sizeof(V)));
+  CK(cudaMemcpy(*dst, v.data(), v.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return FG_OK;
+}
+
+// host analytic k vectors and trig tables
+double kvec_wrapped(int i, int L, double a0) {  // elastic.F:81-85
+  double k = (double)i / L;
+  if (k > 0.5) k = k - 1.0;
+  return k * 6.28318530717958647693 / a0;
+}
+
+int validate(const fg_params* p, std::string* why) {
+  if (p->N != p->Lx * p->Ly * p->Lz || p->N <= 0) { *why = "parameters not made (call fg_make_param)"; return FG_ERR_ARG; }
+  if (p->Lx % 2 != 0 || p->Lx < 4) { *why = "Lx must be even and >= 4"; return FG_ERR_UNSUPPORTED; }
+  if (p->Ly < 3 || p->Lz < 3) { *why = "Ly and Lz must be >= 3"; return FG_ERR_UNSUPPORTED; }
+  if (p->method != FG_METHOD_MD && p->method != FG_METHOD_LF) { *why = "only methods 'md' and 'lf' run on the device"; return FG_ERR_UNSUPPORTED; }
+  if (p->mass_acou[0] > 0.0) { *why = "acoustic-displacement MD (acoustic_mass_amu) is not implemented on the device"; return FG_ERR_UNSUPPORTED; }
+  if (p->delta_e != 0.0 || p->delta_e_acou != 0.0) { *why = "delta_e heat pumping is not implemented on the device"; return FG_ERR_UNSUPPORTED; }
+  if (p->dt <= 0.0) { *why = "dt must be positive"; return FG_ERR_ARG; }
+  if (p->method == FG_METHOD_MD && p->Q_Nose <= 0.0) { *why = "Q_Nose must be positive"; return FG_ERR_ARG; }
+  return FG_OK;
+}
+
+template <typename T>
+int create_impl(fg_ctx* ctx) {
+  const fg_params& P = ctx->P;
+  Geom& g = ctx->g;
+  g.Lx = P.Lx;
+  g.Ly = P.Ly;
+  g.Lz = P.Lz;
+  g.m = P.Lx / 2;
+  g.NKX = g.m + 1;
+  g.KXP = (g.NKX + 15) / 16 * 16;
+  g.plane_r = (long long)g.Lx * g.Ly;
+  g.plane_c = (long long)g.Ly * g.KXP;
+  g.nsite = (long long)g.Lx * g.Ly * g.Lz;
+  g.ncplx = (long long)g.Lz * g.plane_c;
+  g.nkpos = (long long)g.Ly * g.Lz * g.KXP;
+  ctx->NXP = 2 * (P.Lx / 2 + 1);
+  ctx->NYP = P.Ly + P.padding_y;
+  if (!make_plan(g.m, &ctx->px) || !make_plan(g.Ly, &ctx->py) || !make_plan(g.Lz, &ctx->pz))
+    return fail(ctx, FG_ERR_UNSUPPORTED, "L/2 (x), Ly and Lz must factor into 2, 3 and 5");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  int smem_max = 0, nsm = 0;
+  CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  smem_max -= 4096;  // static shared memory of the block reductions
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  ctx->smem_xy = (int)(sizeof(cplx<T>) * g.Ly * (g.m + 1));
+  ctx->smem_xy64 = (int)(sizeof(cplx<double>) * g.Ly * (g.m + 1));
+  if (ctx->smem_xy > smem_max || ctx->smem_xy64 > smem_max)
+    return fail(ctx, FG_ERR_UNSUPPORTED, "an x-y plane of the supercell does not fit in shared memory");
+  auto pick_cw = [&](int nc, size_t esz, int cwmax) {
+    int cw = cwmax;
+    while (cw > 1 && (size_t)nc * g.Lz * cw * esz > (size_t)smem_max) cw /= 2;
+    return cw;
+  };
+  ctx->cw = pick_cw(9, sizeof(cplx<T>), sizeof(T) == 4 ? 16 : 8);
+  ctx->cw6 = pick_cw(6, sizeof(cplx<double>), 8);
+  ctx->cw1 = pick_cw(1, sizeof(cplx<double>), 8);
+  if ((size_t)9 * g.Lz * ctx->cw * sizeof(cplx<T>) > (size_t)smem_max)
+    return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
+  ctx->ntx = div_up(g.NKX, ctx->cw);
+  ctx->ntx6 = div_up(g.NKX, ctx->cw6);
+  ctx->ntx1 = div_up(g.NKX, ctx->cw1);
+  ctx->smem_z = (int)(9 * (size_t)g.Lz * ctx->cw * sizeof(cplx<T>));
+  ctx->smem_z3 = (int)(3 * (size_t)g.Lz * ctx->cw * sizeof(cplx<T>));
+  ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->cw6 * sizeof(cplx<double>));
+  ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->cw1 * sizeof(cplx<double>));
+  ctx->grid_elem = std::max(1, std::min(div_up(g.nsite, kThreadsElem), nsm * 8));
+  CK(cudaFuncSetAttribute(k_xy_fwd<T, SRC_U9>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy));
+  CK(cudaFuncSetAttribute(k_xy_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy));
+  CK(cudaFuncSetAttribute(k_z_kspace<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z));
+  CK(cudaFuncSetAttribute(k_xy_fwd<T, SRC_FIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy));
+  CK(cudaFuncSetAttribute(k_z_pass<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z3));
+  CK(cudaFuncSetAttribute(k_z_pass<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z3));
+  CK(cudaFuncSetAttribute(k_xy_fwd<double, SRC_FIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy64));
+  CK(cudaFuncSetAttribute(k_z_ewald_pack<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z6));
+  CK(cudaFuncSetAttribute(k_z_modulation_pack<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z1));
+  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+
+  // slot maps
+  std::vector<int> revm = digit_reversal(ctx->px);
+  std::vector<int> posm(g.m);
+  for (int s = 0; s < g.m; ++s) posm[revm[s]] = s;
+  ctx->h_revx.resize(g.NKX);
+  for (int s = 0; s < g.m; ++s) ctx->h_revx[s] = revm[s];
+  ctx->h_revx[g.m] = g.m;
+  ctx->h_revy = digit_reversal(ctx->py);
+  ctx->h_revz = digit_reversal(ctx->pz);
+  int rc;
+  if ((rc = upload(ctx, (void**)&ctx->revx, ctx->h_revx))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->revy, ctx->h_revy))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->revz, ctx->h_revz))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->posm, posm))) return rc;
+  // twiddles
+  if ((rc = upload(ctx, &ctx->twx, twiddles<T>(g.Lx)))) return rc;
+  if ((rc = upload(ctx, &ctx->twm, twiddles<T>(g.m)))) return rc;
+  if ((rc = upload(ctx, &ctx->twy, twiddles<T>(g.Ly)))) return rc;
+  if ((rc = upload(ctx, &ctx->twz, twiddles<T>(g.Lz)))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->twx64, twiddles<double>(g.Lx)))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->twm64, twiddles<double>(g.m)))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->twy64, twiddles<double>(g.Ly)))) return rc;
+  if ((rc = upload(ctx, (void**)&ctx->twz64, twiddles<double>(g.Lz)))) return rc;
+  // wavevectors and trig tables (true-k indexed)
+  {
+    std::vector<double> kx(g.NKX), ky(g.Ly), kz(g.Lz);
+    for (int i = 0; i < g.NKX; ++i) kx[i] = (double)i / P.Lx * 6.28318530717958647693 / P.a0;  // elastic.F:87
+    for (int i = 0; i < g.Ly; ++i) ky[i] = kvec_wrapped(i, P.Ly, P.a0);
+    for (int i = 0; i < g.Lz; ++i) kz[i] = kvec_wrapped(i, P.Lz, P.a0);
+    auto trig = [](int n, int L) {
+      std::vector<double2> t(n);
+      for (int i = 0; i < n; ++i) {
+        long double a = 2.0L * 3.14159265358979323846264338327950288L * (long double)i / (long double)L;
+        t[i] = make_double2((double)std::cos(a), (double)std::sin(a));
+      }
+      return t;
+    };
+    if ((rc = upload(ctx, (void**)&ctx->kvx, kx))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->kvy, ky))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->kvz, kz))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->trx, trig(g.NKX, P.Lx)))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->try_, trig(g.Ly, P.Ly)))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->trz, trig(g.Lz, P.Lz)))) return rc;
+  }
+  // per-layer masses and masks (alloc_Coord, read_defects_u.F:52-69)
+  {
+    std::vector<double> minv(g.Lz, 1.0 / P.mass_dipo[0]);
+    std::vector<unsigned char> sump(g.Lz, 1);
+    if (P.bulk_or_film == FG_FILM || P.bulk_or_film == FG_EPIT)
+      for (int z = (P.Lz + 1) / 2; z < P.Lz; ++z) sump[z] = 0;
+    if (P.gap_id > 0) {
+      minv[0] = 0.0;
+      sump[0] = 0;
+      if (P.gap_id == 2) {
+        minv[P.Lz / 2] = 0.0;
+        sump[P.Lz / 2] = 0;
+      }
+    }
+    double n = 0;
+    for (int z = 0; z < g.Lz; ++z) n += sump[z] ? (double)g.plane_r : 0.0;
+    ctx->n_sum_p = n;
+    if ((rc = upload(ctx, (void**)&ctx->layer_minv, minv))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->layer_sump, sump))) return rc;
+  }
+  // physics constants (elastic.F:26-75, dVddi-unharmonic.F:28-32)
+  {
+    Phys& h = ctx->ph_host;
+    std::memset(&h, 0, sizeof(h));
+    h.N = P.N;
+    h.Ninv = P.Ninv;
+    for (int i = 0; i < 7; ++i) h.j[i] = P.j[i];
+    h.kap2x2 = P.P_kappa2[0] * 2;
+    h.P_alpha = P.P_alpha[0];
+    h.P_gamma = P.P_gamma[0];
+    h.P_k1 = P.P_k1[0];
+    h.P_k2 = P.P_k2[0];
+    h.P_k3 = P.P_k3[0];
+    h.P_k4 = P.P_k4[0];
+    h.fa2g = 4 * P.P_alpha[0] + 2 * P.P_gamma[0];
+    h.tg = 2 * P.P_gamma[0];
+    h.sk = 6 * P.P_k1[0] + 2 * P.P_k2[0];
+    h.tk2 = 2 * P.P_k2[0];
+    h.fk = 4 * P.P_k2[0] - 2 * P.P_k3[0];
+    h.B11 = P.B11;
+    h.B12 = P.B12;
+    h.B44 = P.B44;
+    for (int i = 0; i < 3; ++i) h.HC2[i][i] = P.B1xx / 2;
+    for (int i = 3; i < 6; ++i) h.HC2[i][i] = P.B4yz;
+    h.HC2[0][1] = h.HC2[0][2] = h.HC2[1][2] = h.HC2[1][0] = h.HC2[2][0] = h.HC2[2][1] = P.B1yy / 2;
+    for (int i = 0; i < 3; ++i) h.H[i][i] = P.B11 * P.N;
+    for (int i = 3; i < 6; ++i) h.H[i][i] = P.B44 * P.N;
+    h.H[0][1] = h.H[0][2] = h.H[1][2] = h.H[1][0] = h.H[2][0] = h.H[2][1] = P.B12 * P.N;
+    for (int jj = 0; jj < 6; ++jj) {
+      double s = 0.0;
+      for (int k = 0; k < jj; ++k) s += h.HG[jj][k] * h.HG[jj][k];
+      h.HG[jj][jj] = std::sqrt(h.H[jj][jj] - s);
+      h.HG_inv[jj] = 1.0 / h.HG[jj][jj];
+      for (int i = jj + 1; i < 6; ++i) {
+        double t = 0.0;
+        for (int k = 0; k < jj; ++k) t += h.HG[i][k] * h.HG[jj][k];
+        h.HG[i][jj] = (h.H[i][jj] - t) * h.HG_inv[jj];
+      }
+    }
+    for (int i = 0; i < 3; ++i) h.pNa03[i] = P.pNa03[i];
+    h.epi_strain = P.epi_strain;
+    h.bulk_or_film = P.bulk_or_film;
+    h.Zstar = P.Z_star[0];
+    h.dt = P.dt;
+    h.dt_2 = P.dt_2;
+    h.Q = P.Q_Nose;
+    h.nf_kT = (double)P.n_freedom * P.temperature_eV;
+    h.threeN_kT = (double)(3 * (long long)P.N) * P.temperature_eV;
+    h.n_sum_p = ctx->n_sum_p;
+    h.E_on = P.E_field_always_zero ? 0 : 1;
+    h.modulation_on = 0;
+    CK(cudaMalloc(&ctx->ph, sizeof(Phys)));
+    CK(cudaMemcpy(ctx->ph, &h, sizeof(Phys), cudaMemcpyHostToDevice));
+  }
+  // scalars
+  CK(cudaMalloc(&ctx->sc, sizeof(DevScalars)));
+  CK(cudaMallocHost(&ctx->sc_host, sizeof(DevScalars)));
+  std::memset(ctx->sc_host, 0, sizeof(DevScalars));
+  ctx->sc_host->s = 1.0;
+  ctx->sc_host->pi = 0.0;
+  ctx->sc_host->H0 = 0.0;
+  ctx->sc_host->lf_dt = P.dt;
+  ctx->sc_host->lf_dt_2 = P.dt_2;
+  ctx->sc_host->kick_coef = P.dt_2 * 1.0;
+  CK(cudaMemcpy(ctx->sc, ctx->sc_host, sizeof(DevScalars), cudaMemcpyHostToDevice));
+  // fields
+  const size_t es = sizeof(T);
+  ctx->real_bytes = es * (size_t)g.nsite;
+  CK(cudaMalloc(&ctx->u, 3 * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->p, 3 * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->F, 3 * ctx->real_bytes));
+  CK(cudaMemset(ctx->u, 0, 3 * ctx->real_bytes));
+  CK(cudaMemset(ctx->p, 0, 3 * ctx->real_bytes));
+  CK(cudaMemset(ctx->F, 0, 3 * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->spec, 9 * sizeof(cplx<T>) * (size_t)g.ncplx));
+  CK(cudaMemset(ctx->spec, 0, 9 * sizeof(cplx<T>) * (size_t)g.ncplx));
+  CK(cudaMalloc(&ctx->rwork, 9 * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->dtab, 6 * es * (size_t)g.nkpos));
+  CK(cudaMemset(ctx->dtab, 0, 6 * es * (size_t)g.nkpos));
+  CK(cudaMalloc(&ctx->ckmod, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
+  CK(cudaMemset(ctx->ckmod, 0, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
+  CK(cudaMalloc(&ctx->acouK, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
+  CK(cudaMemset(ctx->acouK, 0, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
+  CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)ctx->ntx * g.Ly));
+  CK(cudaMalloc(&ctx->part_r, sizeof(double) * NQ_R * (size_t)ctx->grid_elem));
+  CK(cudaMalloc(&ctx->part_ke, sizeof(double) * (size_t)ctx->grid_elem));
+  CK(cudaMalloc(&ctx->part_avg, sizeof(double) * 6 * (size_t)ctx->grid_elem));
+  CK(cudaMalloc(&ctx->avg6, sizeof(double) * 6));
+  ctx->staging_n = (size_t)3 * ctx->NXP * ctx->NYP * P.Lz;
+  CK(cudaMalloc(&ctx->staging, sizeof(double) * ctx->staging_n));
+  CK(cudaMemset(ctx->staging, 0, sizeof(double) * ctx->staging_n));
+  return FG_OK;
+}
+
+template <typename T>
+int build_tables_impl(fg_ctx* ctx) {
+  const Geom& g = ctx->g;
+  const fg_params& P = ctx->P;
+  double* real6 = nullptr;
+  cplx<double>* spec6 = nullptr;
+  CK(cudaMalloc(&real6, sizeof(double) * 6 * (size_t)g.nsite));
+  CK(cudaMalloc(&spec6, sizeof(cplx<double>) * 6 * (size_t)g.ncplx));
+  if (!ctx->L64) CK(cudaMalloc(&ctx->L64, sizeof(double) * 6 * (size_t)g.nkpos));
+  const int max_x = 24 / P.Lx, max_y = 24 / P.Ly, max_z = 24 / P.Lz;  // dipole-dipole-long-range.F:98-100
+  k_ewald_real<<<std::max(1, div_up(g.nsite, 128)), 128, 0, ctx->stream>>>(real6, g, P.a0, P.kappa, max_x, max_y, max_z);
+  CKL();
+  k_xy_fwd<double, SRC_FIELD><<<dim3(g.Lz, 6), kThreadsFFT, ctx->smem_xy64, ctx->stream>>>(
+      real6, spec6, g, ctx->px, ctx->py, ctx->twx64, ctx->twm64, ctx->twy64, ctx->posm, 0);
+  CKL();
+  k_z_ewald_pack<T><<<dim3(ctx->ntx6, g.Ly), kThreadsFFT, ctx->smem_z6, ctx->stream>>>(
+      spec6, (T*)ctx->dtab, ctx->L64, g, ctx->pz, ctx->twz64, kmaps<T>(ctx), ctx->ph, P.a0, P.kappa, P.epsilon_inf,
+      max_x, max_y, max_z, ctx->cw6);
+  CKL();
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(real6);
+  cudaFree(spec6);
+  int rc = check_device_error(ctx);
+  if (rc) return rc;
+  ctx->tables_ready = true;
+  return FG_OK;
+}
+
+template <typename T>
+int set_modulation_R_impl(fg_ctx* ctx, const double* modR) {
+  const Geom& g = ctx->g;
+  double* r1 = nullptr;
+  cplx<double>* s1 = nullptr;
+  const size_t nin = (size_t)ctx->NXP * ctx->NYP * ctx->P.Lz;
+  CK(cudaMalloc(&r1, sizeof(double) * (size_t)g.nsite));
+  CK(cudaMalloc(&s1, sizeof(cplx<double>) * (size_t)g.ncplx));
+  CK(cudaMemcpyAsync(ctx->staging, modR, sizeof(double) * nin, cudaMemcpyHostToDevice, ctx->stream));
+  k_fortran_to_soa<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(r1, ctx->staging, g, 1, ctx->NXP, ctx->NYP);
+  CKL();
+  k_xy_fwd<double, SRC_FIELD><<<dim3(g.Lz, 1), kThreadsFFT, ctx->smem_xy64, ctx->stream>>>(
+      r1, s1, g, ctx->px, ctx->py, ctx->twx64, ctx->twm64, ctx->twy64, ctx->posm, 0);
+  CKL();
+  k_z_modulation_pack<T><<<dim3(ctx->ntx1, g.Ly), kThreadsFFT, ctx->smem_z1, ctx->stream>>>(
+      s1, (cplx<T>*)ctx->ckmod, g, ctx->pz, ctx->twz64, kmaps<T>(ctx), ctx->P.modulation_constant, ctx->cw1);
+  CKL();
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(r1);
+  cudaFree(s1);
+  return check_device_error(ctx);
+}
+
+// Fortran (a,b,kx,ky,kz) index of a (3,ncol,0:Lx/2,0:NYP-1,0:Lz-1) table
+inline size_t ftab(const fg_ctx* c, int ncol, int a, int b, int kx, int ky, int kz) {
+  return (size_t)a + 3 * (size_t)b + (size_t)3 * ncol * ((size_t)kx + (size_t)c->g.NKX * ((size_t)ky + (size_t)c->NYP * kz));
+}
+
+// Fortran (comp, kx, ky, kz) of a complex field, in doubles (re at 2i)
+inline size_t fcplx(const fg_ctx* c, int nc, int comp, int kx, int ky, int kz) {
+  return (size_t)comp + (size_t)nc * ((size_t)kx + (size_t)c->g.NKX * ((size_t)ky + (size_t)c->NYP * kz));
+}
+
+template <typename T>
+int upload_tables_impl(fg_ctx* ctx, const double* sr, const double* lr) {
+  const Geom& g = ctx->g;
+  const fg_params& P = ctx->P;
+  std::vector<T> D(6 * (size_t)g.nkpos, (T)0);
+  std::vector<double> L(6 * (size_t)g.nkpos, 0.0);
+  const int qa[6] = {0, 1, 2, 1, 2, 0}, qb[6] = {0, 1, 2, 2, 0, 1};
+  double smax = 0.0, sdiff = 0.0;
+  const double z2 = P.Z_star[0] * P.Z_star[0];
+  for (int ys = 0; ys < g.Ly; ++ys)
+    for (int zs = 0; zs < g.Lz; ++zs)
+      for (int col = 0; col < g.NKX; ++col) {
+        const int kx = ctx->h_revx[col], ky = ctx->h_revy[ys], kz = ctx->h_revz[zs];
+        const long double tw = 2.0L * 3.14159265358979323846264338327950288L;
+        double cc[3] = {(double)std::cos(tw * kx / P.Lx), (double)std::cos(tw * ky / P.Ly), (double)std::cos(tw * kz / P.Lz)};
+        double ss[3] = {(double)std::sin(tw * kx / P.Lx), (double)std::sin(tw * ky / P.Ly), (double)std::sin(tw * kz / P.Lz)};
+        double S[6];
+        short_range_k(P.j, P.P_kappa2[0] * 2, cc, ss, S);
+        const size_t tpos = ((size_t)ys * g.Lz + zs) * g.KXP + col;
+        for (int q = 0; q < 6; ++q) {
+          const double s = sr[ftab(ctx, 3, qa[q], qb[q], kx, ky, kz)];
+          const double l = lr[ftab(ctx, 3, qa[q], qb[q], kx, ky, kz)];
+          smax = std::max(smax, std::fabs(s));
+          sdiff = std::max(sdiff, std::fabs(s - S[q]));
+          D[tpos * 6 + q] = (T)((s + z2 * l) * P.Ninv);
+          L[tpos * 6 + q] = l;
+        }
+      }
+  if (sdiff > 1e-9 * std::max(1.0, smax)) {
+    char b[200];
+    std::snprintf(b, sizeof(b), "short_range table differs from the feram stencil by %.3e (max %.3e)", sdiff, smax);
+    return fail(ctx, FG_ERR_ARG, b);
+  }
+  CK(cudaMemcpy(ctx->dtab, D.data(), D.size() * sizeof(T), cudaMemcpyHostToDevice));
+  if (!ctx->L64) CK(cudaMalloc(&ctx->L64, sizeof(double) * 6 * (size_t)g.nkpos));
+  CK(cudaMemcpy(ctx->L64, L.data(), L.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ctx->tables_ready = true;
+  return FG_OK;
+}
+
+template <typename T>
+int upload_modulation_impl(fg_ctx* ctx, const double* ck) {
+  const Geom& g = ctx->g;
+  std::vector<cplx<T>> C(3 * (size_t)g.nkpos, mk<cplx<T>>((T)0, (T)0));
+  if (ck) {
+    for (int ys = 0; ys < g.Ly; ++ys)
+      for (int zs = 0; zs < g.Lz; ++zs)
+        for (int col = 0; col < g.NKX; ++col) {
+          const int kx = ctx->h_revx[col], ky = ctx->h_revy[ys], kz = ctx->h_revz[zs];
+          const size_t tpos = ((size_t)ys * g.Lz + zs) * g.KXP + col;
+          for (int a = 0; a < 3; ++a) {
+            const size_t f = fcplx(ctx, 3, a, kx, ky, kz);
+            C[tpos * 3 + a] = mk<cplx<T>>((T)ck[2 * f], (T)ck[2 * f + 1]);
+          }
+        }
+  }
+  CK(cudaMemcpy(ctx->ckmod, C.data(), C.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+  return FG_OK;
+}
+
+int set_modulation_flag(fg_ctx* ctx, int on) {
+  ctx->ph_host.modulation_on = on;
+  CK(cudaMemcpy(ctx->ph, &ctx->ph_host, sizeof(Phys), cudaMemcpyHostToDevice));
+  return FG_OK;
+}
+
+template <typename T>
+int set_field(fg_ctx* ctx, void* dst, const double* src) {
+  const size_t nin = (size_t)3 * ctx->NXP * ctx->NYP * ctx->P.Lz;
+  CK(cudaMemcpyAsync(ctx->staging, src, sizeof(double) * nin, cudaMemcpyHostToDevice, ctx->stream));
+  k_fortran_to_soa<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)dst, ctx->staging, ctx->g, 3, ctx->NXP,
+                                                                         ctx->NYP);
+  CKL();
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FG_OK;
+}
+
+template <typename T>
+int get_field(fg_ctx* ctx, double* dst, const void* src) {
+  const size_t nin = (size_t)3 * ctx->NXP * ctx->NYP * ctx->P.Lz;
+  k_soa_to_fortran<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(ctx->staging, (const T*)src, ctx->g, 3,
+                                                                         ctx->NXP, ctx->NYP);
+  CKL();
+  CK(cudaMemcpyAsync(dst, ctx->staging, sizeof(double) * nin, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FG_OK;
+}
+
+template <typename T>
+int get_acouK_impl(fg_ctx* ctx, double* out) {
+  const Geom& g = ctx->g;
+  std::vector<cplx<T>> A(3 * (size_t)g.nkpos);
+  CK(cudaMemcpy(A.data(), ctx->acouK, A.size() * sizeof(cplx<T>), cudaMemcpyDeviceToHost));
+  for (int ys = 0; ys < g.Ly; ++ys)
+    for (int zs = 0; zs < g.Lz; ++zs)
+      for (int col = 0; col < g.NKX; ++col) {
+        const int kx = ctx->h_revx[col], ky = ctx->h_revy[ys], kz = ctx->h_revz[zs];
+        const size_t tpos = ((size_t)ys * g.Lz + zs) * g.KXP + col;
+        for (int a = 0; a < 3; ++a) {
+          const size_t f = fcplx(ctx, 3, a, kx, ky, kz);
+          out[2 * f] = (double)A[tpos * 3 + a].x;
+          out[2 * f + 1] = (double)A[tpos * 3 + a].y;
+        }
+      }
+  return FG_OK;
+}
+
+// 3-component r2c / c2r of the reference's plan_r2c_3_out / plan_c2r_3_out
+// (coord_module.F:155-157,310-312) on the device FFT.
+template <typename T>
+int fft_r2c3_impl(fg_ctx* ctx, const double* in, double* out) {
+  const Geom& g = ctx->g;
+  int rc = set_field<T>(ctx, ctx->rwork, in);
+  if (rc) return rc;
+  k_xy_fwd<T, SRC_FIELD><<<dim3(g.Lz, 3), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
+      (const T*)ctx->rwork, (cplx<T>*)ctx->spec, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
+      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
+  CKL();
+  k_z_pass<T, false><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z3, ctx->stream>>>(
+      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->cw);
+  CKL();
+  std::vector<cplx<T>> S(3 * (size_t)g.ncplx);
+  CK(cudaMemcpyAsync(S.data(), ctx->spec, S.size() * sizeof(cplx<T>), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if ((rc = check_device_error(ctx))) return rc;
+  for (int c = 0; c < 3; ++c)
+    for (int zs = 0; zs < g.Lz; ++zs)
+      for (int ys = 0; ys < g.Ly; ++ys)
+        for (int col = 0; col < g.NKX; ++col) {
+          const int kx = ctx->h_revx[col], ky = ctx->h_revy[ys], kz = ctx->h_revz[zs];
+          const cplx<T> v = S[(size_t)c * g.ncplx + (size_t)zs * g.plane_c + (size_t)ys * g.KXP + col];
+          const size_t f = fcplx(ctx, 3, c, kx, ky, kz);
+          out[2 * f] = (double)v.x;
+          out[2 * f + 1] = (double)v.y;
+        }
+  ctx->force_fresh = false;
+  return FG_OK;
+}
+
+template <typename T>
+int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
+  const Geom& g = ctx->g;
+  std::vector<cplx<T>> S(3 * (size_t)g.ncplx, mk<cplx<T>>((T)0, (T)0));
+  for (int c = 0; c < 3; ++c)
+    for (int zs = 0; zs < g.Lz; ++zs)
+      for (int ys = 0; ys < g.Ly; ++ys)
+        for (int col = 0; col < g.NKX; ++col) {
+          const int kx = ctx->h_revx[col], ky = ctx->h_revy[ys], kz = ctx->h_revz[zs];
+          const size_t f = fcplx(ctx, 3, c, kx, ky, kz);
+          S[(size_t)c * g.ncplx + (size_t)zs * g.plane_c + (size_t)ys * g.KXP + col] = mk<cplx<T>>((T)in[2 * f], (T)in[2 * f + 1]);
+        }
+  CK(cudaMemcpyAsync(ctx->spec, S.data(), S.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, ctx->stream));
+  k_z_pass<T, true><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z3, ctx->stream>>>(
+      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->cw);
+  CKL();
+  k_xy_inv<T><<<dim3(g.Lz, 3), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
+      (const cplx<T>*)ctx->spec, (T*)ctx->rwork, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
+      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
+  CKL();
+  int rc = get_field<T>(ctx, out, ctx->rwork);
+  if (rc) return rc;
+  ctx->force_fresh = false;
+  return check_device_error(ctx);
+}
+
+int ensure_ready(fg_ctx* ctx) {
+  if (!ctx) return FG_ERR_ARG;
+  if (!ctx->tables_ready) return fail(ctx, FG_ERR_STATE, "no k-space tables: call fg_build_tables or fg_upload_tables");
+  return FG_OK;
+}
+
+int force_now(fg_ctx* ctx) {
+  int rc = run_graph(ctx, &ctx->g_force, 0);
+  if (rc) return rc;
+  ctx->force_fresh = true;
+  return FG_OK;
+}
+
+const char* kProfNames[FG_NPROF] = {"k_kick(35a)", "k_np_pre", "k_drift", "k_xy_fwd", "k_z_kspace",
+                                           "k_homo_strain", "k_xy_inv", "k_assemble", "k_force_energies",
+                                           "k_np_post", "k_kick(35f)", "k_np_final"};
+
+template <typename T>
+int profile_impl(fg_ctx* ctx, int reps, double* ms) {
+  const Geom& g = ctx->g;
+  cudaStream_t st = ctx->stream;
+  cudaEvent_t ev[FG_NPROF + 1];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  for (int k = 0; k < FG_NPROF; ++k) ms[k] = 0.0;
+  T* u = (T*)ctx->u;
+  for (int r = 0; r < reps; ++r) {
+    int k = 0;
+    CK(cudaEventRecord(ev[k], st));
+    k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->p, (const T*)ctx->F, &ctx->sc->kick_coef, g,
+                                                       ctx->layer_minv, ctx->layer_sump, ctx->part_ke);
+    CK(cudaEventRecord(ev[++k], st));
+    k_np_pre<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+    CK(cudaEventRecord(ev[++k], st));
+    k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(u, (const T*)ctx->p, &ctx->sc->drift_coef, g, ctx->layer_minv);
+    CK(cudaEventRecord(ev[++k], st));
+    k_xy_fwd<T, SRC_U9><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
+        u, (cplx<T>*)ctx->spec, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm,
+        (const cplx<T>*)ctx->twy, ctx->posm, 0);
+    CK(cudaEventRecord(ev[++k], st));
+    k_z_kspace<T><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z, st>>>(
+        (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, nullptr, g, ctx->pz,
+        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->cw);
+    CK(cudaEventRecord(ev[++k], st));
+    k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->ntx * g.Ly);
+    CK(cudaEventRecord(ev[++k], st));
+    k_xy_inv<T><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
+        (const cplx<T>*)ctx->spec, (T*)ctx->rwork, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
+        (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
+    CK(cudaEventRecord(ev[++k], st));
+    k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
+                                                           ctx->part_r);
+    CK(cudaEventRecord(ev[++k], st));
+    k_force_energies<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_r, ctx->grid_elem);
+    CK(cudaEventRecord(ev[++k], st));
+    k_np_post<<<1, 32, 0, st>>>(ctx->ph, ctx->sc);
+    CK(cudaEventRecord(ev[++k], st));
+    k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->p, (const T*)ctx->F, &ctx->sc->kick_coef, g,
+                                                       ctx->layer_minv, ctx->layer_sump, ctx->part_ke);
+    CK(cudaEventRecord(ev[++k], st));
+    k_np_final<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+    CK(cudaEventRecord(ev[++k], st));
+    CKL();
+    CK(cudaEventSynchronize(ev[FG_NPROF]));
+    for (int i = 0; i < FG_NPROF; ++i) {
+      float t = 0.0f;
+      CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      ms[i] += t / reps;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  return FG_OK;
+}
+
+}  // namespace
+
+// ================================================================== C-ABI ===
+extern "C" {
+
+int fg_create(const fg_params* p, int precision, fg_ctx** out) {
+  if (!p || !out) return FG_ERR_ARG;
+  *out = nullptr;
+  std::string why;
+  int rc = validate(p, &why);
+  fg_ctx* ctx = new fg_ctx();
+  ctx->P = *p;
+  ctx->prec = precision;
+  if (rc) {
+    ctx->err = why;
+    *out = ctx;  // returned so that fg_last_error can report; caller must destroy
+    return rc;
+  }
+  if (precision != FG_PREC_FP64 && precision != FG_PREC_MIXED) {
+    ctx->err = "unknown precision";
+    *out = ctx;
+    return FG_ERR_ARG;
+  }
+  rc = (precision == FG_PREC_MIXED) ? create_impl<float>(ctx) : create_impl<double>(ctx);
+  *out = ctx;
+  return rc;
+}
+
+void fg_destroy(fg_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->g_np) cudaGraphExecDestroy(ctx->g_np);
+  if (ctx->g_lf) cudaGraphExecDestroy(ctx->g_lf);
+  if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
+  void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
+                  ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->revx,
+                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
+                  ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
+                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+  if (ctx->sc_host) cudaFreeHost(ctx->sc_host);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* fg_last_error(const fg_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void* fg_stream(fg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int fg_build_tables(fg_ctx* ctx) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  ctx->force_fresh = false;
+  return ctx->prec == FG_PREC_MIXED ? build_tables_impl<float>(ctx) : build_tables_impl<double>(ctx);
+}
+
+int fg_upload_tables(fg_ctx* ctx, const double* short_range, const double* long_range) {
+  if (!ctx || !ctx->stream || !short_range || !long_range) return FG_ERR_ARG;
+  ctx->force_fresh = false;
+  return ctx->prec == FG_PREC_MIXED ? upload_tables_impl<float>(ctx, short_range, long_range)
+                                    : upload_tables_impl<double>(ctx, short_range, long_range);
+}
+
+int fg_upload_modulation(fg_ctx* ctx, const double* ck) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  int rc = ctx->prec == FG_PREC_MIXED ? upload_modulation_impl<float>(ctx, ck) : upload_modulation_impl<double>(ctx, ck);
+  if (rc) return rc;
+  ctx->force_fresh = false;
+  return set_modulation_flag(ctx, (ck && ctx->P.modulation_constant != 0.0) ? 1 : 0);
+}
+
+int fg_set_modulation_R(fg_ctx* ctx, const double* modR) {
+  if (!ctx || !ctx->stream || !modR) return FG_ERR_ARG;
+  if (ctx->P.modulation_constant == 0.0)
+    return fail(ctx, FG_ERR_ARG, "There is a .modulation file, but modulation_constant is zero.");  // elastic.F:207-210
+  int rc = ctx->prec == FG_PREC_MIXED ? set_modulation_R_impl<float>(ctx, modR) : set_modulation_R_impl<double>(ctx, modR);
+  if (rc) return rc;
+  ctx->force_fresh = false;
+  return set_modulation_flag(ctx, 1);
+}
+
+int fg_get_long_range(fg_ctx* ctx, double* lr) {
+  if (!ctx || !lr) return FG_ERR_ARG;
+  if (!ctx->L64) return fail(ctx, FG_ERR_STATE, "no long-range table");
+  const Geom& g = ctx->g;
+  std::vector<double> L(6 * (size_t)g.nkpos);
+  CK(cudaMemcpy(L.data(), ctx->L64, L.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  const int qa[6] = {0, 1, 2, 1, 2, 0}, qb[6] = {0, 1, 2, 2, 0, 1};
+  for (int ys = 0; ys < g.Ly; ++ys)
+    for (int zs = 0; zs < g.Lz; ++zs)
+      for (int col = 0; col < g.NKX; ++col) {
+        const int kx = ctx->h_revx[col], ky = ctx->h_revy[ys], kz = ctx->h_revz[zs];
+        const size_t tpos = ((size_t)ys * g.Lz + zs) * g.KXP + col;
+        for (int q = 0; q < 6; ++q) {
+          lr[ftab(ctx, 3, qa[q], qb[q], kx, ky, kz)] = L[tpos * 6 + q];
+          lr[ftab(ctx, 3, qb[q], qa[q], kx, ky, kz)] = L[tpos * 6 + q];
+        }
+      }
+  return FG_OK;
+}
+
+int fg_fft_r2c3(fg_ctx* ctx, const double* in, double* out) {
+  if (!ctx || !ctx->stream || !in || !out) return FG_ERR_ARG;
+  return ctx->prec == FG_PREC_MIXED ? fft_r2c3_impl<float>(ctx, in, out) : fft_r2c3_impl<double>(ctx, in, out);
+}
+
+int fg_fft_c2r3(fg_ctx* ctx, const double* in, double* out) {
+  if (!ctx || !ctx->stream || !in || !out) return FG_ERR_ARG;
+  return ctx->prec == FG_PREC_MIXED ? fft_c2r3_impl<float>(ctx, in, out) : fft_c2r3_impl<double>(ctx, in, out);
+}
+
+int fg_set_state(fg_ctx* ctx, const double* dipoR, const double* dipoP, double s, double pi, double H0) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  int rc;
+  if (dipoR) {
+    rc = ctx->prec == FG_PREC_MIXED ? set_field<float>(ctx, ctx->u, dipoR) : set_field<double>(ctx, ctx->u, dipoR);
+    if (rc) return rc;
+  }
+  if (dipoP) {
+    rc = ctx->prec == FG_PREC_MIXED ? set_field<float>(ctx, ctx->p, dipoP) : set_field<double>(ctx, ctx->p, dipoP);
+    if (rc) return rc;
+  }
+  if ((rc = pull_scalars(ctx))) return rc;
+  ctx->sc_host->s = s;
+  ctx->sc_host->pi = pi;
+  ctx->sc_host->H0 = H0;
+  ctx->sc_host->kick_coef = ctx->P.dt_2 * s;
+  if ((rc = push_scalars(ctx))) return rc;
+  ctx->force_fresh = false;
+  return FG_OK;
+}
+
+int fg_set_thermostat(fg_ctx* ctx, double s, double pi, double H0) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  int rc;
+  if ((rc = pull_scalars(ctx))) return rc;
+  ctx->sc_host->s = s;
+  ctx->sc_host->pi = pi;
+  ctx->sc_host->H0 = H0;
+  ctx->sc_host->kick_coef = ctx->P.dt_2 * s;
+  return push_scalars(ctx);
+}
+
+int fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi, double strain[6], double* s, double* pi,
+                 double* H0) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  int rc;
+  const bool f32 = ctx->prec == FG_PREC_MIXED;
+  if (dipoR && (rc = f32 ? get_field<float>(ctx, dipoR, ctx->u) : get_field<double>(ctx, dipoR, ctx->u))) return rc;
+  if (dipoP && (rc = f32 ? get_field<float>(ctx, dipoP, ctx->p) : get_field<double>(ctx, dipoP, ctx->p))) return rc;
+  if (dVddi && (rc = f32 ? get_field<float>(ctx, dVddi, ctx->F) : get_field<double>(ctx, dVddi, ctx->F))) return rc;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (strain)
+    for (int i = 0; i < 6; ++i) strain[i] = ctx->sc_host->strain[i];
+  if (s) *s = ctx->sc_host->s;
+  if (pi) *pi = ctx->sc_host->pi;
+  if (H0) *H0 = ctx->sc_host->H0;
+  return FG_OK;
+}
+
+int fg_get_acouK(fg_ctx* ctx, double* acouK) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (!acouK) return FG_ERR_ARG;
+  // re-evaluate the force of the current state with the acouK store enabled
+  ctx->store_acouK = true;
+  rc = ctx->prec == FG_PREC_MIXED ? enqueue_force<float>(ctx) : enqueue_force<double>(ctx);
+  ctx->store_acouK = false;
+  if (rc) return rc;
+  if ((rc = pull_scalars(ctx))) return rc;
+  ctx->force_fresh = true;
+  return ctx->prec == FG_PREC_MIXED ? get_acouK_impl<float>(ctx, acouK) : get_acouK_impl<double>(ctx, acouK);
+}
+
+int fg_set_uniform_E(fg_ctx* ctx, const double E[3]) {
+  if (!ctx || !ctx->stream || !E) return FG_ERR_ARG;
+  CK(cudaMemcpyAsync(ctx->sc->E, E, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->force_fresh = false;
+  return FG_OK;
+}
+
+int fg_mirror_force_mirror(fg_ctx* ctx, fg_energy* e) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if ((rc = force_now(ctx))) return rc;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (e) energy_out(ctx->sc_host, e, true);
+  return FG_OK;
+}
+
+int fg_nose_poincare(fg_ctx* ctx, fg_energy* e) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  if ((rc = run_graph(ctx, &ctx->g_np, 1))) return rc;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (e) energy_out(ctx->sc_host, e, false);
+  return FG_OK;
+}
+
+int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (i_step == 0) {  // leapfrog.F:89-102
+    if ((rc = force_now(ctx))) return rc;
+    const bool f32 = ctx->prec == FG_PREC_MIXED;
+    if ((rc = f32 ? enqueue_kick<float>(ctx, &ctx->sc->lf_dt_2) : enqueue_kick<double>(ctx, &ctx->sc->lf_dt_2))) return rc;
+    k_lf_final<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+    CKL();
+  } else {
+    if ((rc = run_graph(ctx, &ctx->g_lf, 2))) return rc;
+  }
+  ctx->force_fresh = true;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (e) {
+    e->dipo_kinetic = ctx->sc_host->e[E_DIPO];
+    for (int i = E_SHORT; i <= E_IM; ++i) (&e->acou_kinetic)[i] = ctx->sc_host->e[i];
+  }
+  return FG_OK;
+}
+
+int fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (ctx->P.method == FG_METHOD_MD && !ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  for (int i = 0; i < n_steps; ++i) {
+    if (ctx->P.method == FG_METHOD_MD) rc = run_graph(ctx, &ctx->g_np, 1);
+    else rc = run_graph(ctx, &ctx->g_lf, 2);
+    if (rc) return rc;
+  }
+  ctx->force_fresh = true;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (e) energy_out(ctx->sc_host, e, false);
+  return FG_OK;
+}
+
+int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (!ms || n_steps < 1) return FG_ERR_ARG;
+  if (ctx->P.method == FG_METHOD_MD && !ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  // make sure the graph exists before the timed region
+  cudaGraphExec_t* gx = ctx->P.method == FG_METHOD_MD ? &ctx->g_np : &ctx->g_lf;
+  const int which = ctx->P.method == FG_METHOD_MD ? 1 : 2;
+  if (!*gx) {
+    if ((rc = run_graph(ctx, gx, which))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaEventRecord(e0, ctx->stream));
+  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(*gx, ctx->stream));
+  CK(cudaEventRecord(e1, ctx->stream));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.0f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t;
+  ctx->force_fresh = true;
+  return pull_scalars(ctx);
+}
+
+const char* fg_profile_name(int i) { return (i >= 0 && i < FG_NPROF) ? kProfNames[i] : ""; }
+
+int fg_profile_step(fg_ctx* ctx, int reps, double* ms) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (!ms || reps < 1) return FG_ERR_ARG;
+  if (ctx->bulk_or_film_mirror()) return fail(ctx, FG_ERR_UNSUPPORTED, "profile covers the bulk step only");
+  if (!ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  rc = ctx->prec == FG_PREC_MIXED ? profile_impl<float>(ctx, reps, ms) : profile_impl<double>(ctx, reps, ms);
+  if (rc) return rc;
+  ctx->force_fresh = true;
+  return pull_scalars(ctx);
+}
+
+int fg_kinetic_energy_dipo(fg_ctx* ctx, double* ke) {
+  if (!ctx || !ctx->stream || !ke) return FG_ERR_ARG;
+  if (ctx->prec == FG_PREC_MIXED)
+    k_ke_only<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const float*)ctx->p, ctx->g, ctx->layer_minv,
+                                                                       ctx->layer_sump, ctx->part_ke);
+  else
+    k_ke_only<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const double*)ctx->p, ctx->g, ctx->layer_minv,
+                                                                        ctx->layer_sump, ctx->part_ke);
+  CKL();
+  k_ke_finish<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+  CKL();
+  int rc = pull_scalars(ctx);
+  if (rc) return rc;
+  *ke = ctx->sc_host->e[E_DIPO];
+  return FG_OK;
+}
+
+int fg_nose_poincare_hamiltonian(fg_ctx* ctx, fg_energy* e) {
+  if (!ctx || !e) return FG_ERR_ARG;
+  int rc = pull_scalars(ctx);
+  if (rc) return rc;
+  const DevScalars* s = ctx->sc_host;
+  const fg_params& P = ctx->P;
+  const double V = e->short_range + e->long_range + e->dipole_E_field + e->unharmonic + e->homo_strain +
+                   e->homo_coupling + e->inho_strain + e->inho_coupling + e->inho_modulation;
+  double h = e->dipo_kinetic / (s->s * s->s) + V + s->pi * s->pi / 2 / P.Q_Nose +
+             3 * P.N * P.temperature_eV * std::log(s->s) - s->H0;
+  e->H_Nose_Poincare = h * s->s;
+  return FG_OK;
+}
+
+int fg_average_accumulate(fg_ctx* ctx, const fg_energy* e, fg_average* avg) {
+  if (!ctx || !ctx->stream || !e || !avg) return FG_ERR_ARG;
+  if (ctx->prec == FG_PREC_MIXED)
+    k_avg_sums<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const float*)ctx->u, ctx->g, ctx->P.Z_star[0],
+                                                                        ctx->layer_sump, ctx->part_avg);
+  else
+    k_avg_sums<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const double*)ctx->u, ctx->g, ctx->P.Z_star[0],
+                                                                         ctx->layer_sump, ctx->part_avg);
+  CKL();
+  k_avg_finish<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->avg6, ctx->part_avg, ctx->grid_elem);
+  CKL();
+  double v[6];
+  CK(cudaMemcpyAsync(v, ctx->avg6, sizeof(v), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  int rc = pull_scalars(ctx);
+  if (rc) return rc;
+  // average_module.F:75-128
+  double* ae = &avg->energy.acou_kinetic;
+  const double* ee = &e->acou_kinetic;
+  for (int i = 0; i < E_COUNT; ++i) ae[i] += ee[i];
+  avg->e2 += e->total * e->total;
+  const double s = ctx->sc_host->s;
+  avg->dipo_kinetic_true += e->dipo_kinetic / (s * s);
+  for (int i = 0; i < 6; ++i) avg->strain[i] += ctx->sc_host->strain[i];
+  const double* ut = v;
+  const double* pt = v + 3;
+  for (int a = 0; a < 3; ++a) {
+    avg->u[a] += ut[a];
+    avg->p[a] += pt[a];
+  }
+  avg->uu[0] += ut[0] * ut[0]; avg->uu[1] += ut[1] * ut[1]; avg->uu[2] += ut[2] * ut[2];
+  avg->uu[3] += ut[1] * ut[2]; avg->uu[4] += ut[2] * ut[0]; avg->uu[5] += ut[0] * ut[1];
+  avg->pp[0] += pt[0] * pt[0]; avg->pp[1] += pt[1] * pt[1]; avg->pp[2] += pt[2] * pt[2];
+  avg->pp[3] += pt[1] * pt[2]; avg->pp[4] += pt[2] * pt[0]; avg->pp[5] += pt[0] * pt[1];
+  avg->n_steps += 1;
+  return FG_OK;
+}
+
+int fg_dipoRavg_accumulate(fg_ctx* ctx) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  const long long n = 3 * ctx->g.nsite;
+  if (!ctx->dipoRavg) {
+    CK(cudaMalloc(&ctx->dipoRavg, sizeof(double) * (size_t)n));
+    CK(cudaMemsetAsync(ctx->dipoRavg, 0, sizeof(double) * (size_t)n, ctx->stream));
+  }
+  if (ctx->prec == FG_PREC_MIXED)
+    k_accumulate<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(ctx->dipoRavg, (const float*)ctx->u, n);
+  else
+    k_accumulate<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(ctx->dipoRavg, (const double*)ctx->u, n);
+  CKL();
+  return FG_OK;
+}
+
+int fg_get_dipoRavg(fg_ctx* ctx, double* out) {
+  if (!ctx || !out) return FG_ERR_ARG;
+  if (!ctx->dipoRavg) return fail(ctx, FG_ERR_STATE, "dipoRavg was never accumulated");
+  return get_field<double>(ctx, out, ctx->dipoRavg);
+}
+
+}  // extern "C"

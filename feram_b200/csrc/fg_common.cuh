@@ -1,0 +1,59 @@
+// fg_common.cuh -- shared types and helpers of the B200 MD-step kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+// Bounds-checked builds (-DFG_BOUNDS_CHECK=1) test every shared-memory and
+// global index of the FFT and field kernels; an out-of-range access is
+// skipped and recorded in fg_dev_error (first offending index wins).
+#ifndef FG_BOUNDS_CHECK
+#define FG_BOUNDS_CHECK 0
+#endif
+
+namespace fg {
+
+// Complex numbers as float2 / double2 (8- and 16-byte aligned vector types).
+template <typename T> struct CT;
+template <> struct CT<float> { using type = float2; };
+template <> struct CT<double> { using type = double2; };
+template <typename T> using cplx = typename CT<T>::type;
+template <typename T> struct RT2;  // two reals packed (x even, y odd)
+template <> struct RT2<float> { using type = float2; };
+template <> struct RT2<double> { using type = double2; };
+
+template <typename C> __host__ __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) {
+  C r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// a * conj(b)
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
+  return mk<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <typename C, bool INV> __device__ __forceinline__ C mul_mi(C a) {
+  return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
+}
+
+// Device error record (bounds checks, non-finite reductions).  The library
+// is one translation unit, so this __device__ variable has one definition.
+struct DevError {
+  int code;  // 0 = none
+  int pad;
+  long long idx;
+};
+__device__ DevError g_fg_err;
+
+__device__ __forceinline__ void fg_record_error(int code, long long idx) {
+  if (atomicCAS(&g_fg_err.code, 0, code) == 0) g_fg_err.idx = idx;
+}
+
+}  // namespace fg

@@ -1,0 +1,1054 @@
+// fg_kernels.cuh -- device kernels of one feram MD step on B200.
+//
+// Device layout (chosen for the GPU, converted at the C-ABI boundary):
+//   real fields  u, p, F, work : [comp][z][y][x]            (x contiguous)
+//   spectra      spec          : [comp][z][ky_slot][kx_slot], row pitch KXP
+//   k tables     dtab, ckmod   : [ky_slot][kz_slot][kx_slot][entries]
+// Slots are the digit-reversed positions left by the in-place DIF FFT
+// stages (fft_smem.cuh); rev{x,y,z} give the true wavenumber of a slot.
+//
+// One force evaluation (mirror_force_mirror.F:6-89) is four passes:
+//   k_xy_fwd     per (z-plane, component): r2c along x + DIF along y of
+//                u and u (x) u (dipoFFT.F:19-44) -> spec
+//   k_z_kspace   per (kx tile, ky): DIF along z, every k-space operation
+//                (dipole-dipole multiply, inhomogeneous strain solve,
+//                energies), DIT along z
+//   k_xy_inv     per (z-plane, component): DIT along y + c2r along x
+//   k_assemble   per site: dipole-dipole + anharmonic + field + homogeneous
+//                and inhomogeneous strain coupling forces
+#pragma once
+#include "fft_smem.cuh"
+
+namespace fg {
+
+// energy slots, fg_energy member order (energy_module.F:7-23)
+enum {
+  E_ACOU = 0, E_DIPO, E_SHORT, E_LONG, E_DIPE, E_UNH, E_HS, E_HC, E_IS, E_IC, E_IM, E_TOT, E_HNP, E_COUNT
+};
+constexpr int NQ_K = 5;   // k-space partial sums per block
+constexpr int NQ_R = 2;   // real-space partial sums per block
+constexpr int RED_THREADS = 256;
+
+struct Geom {
+  int Lx, Ly, Lz, m, NKX, KXP;
+  long long plane_r;  // Lx*Ly
+  long long plane_c;  // Ly*KXP
+  long long nsite;    // Lx*Ly*Lz
+  long long ncplx;    // Lz*Ly*KXP
+  long long nkpos;    // Ly*Lz*KXP
+};
+
+// Constants of the Hamiltonian and integrators, resident on the device.
+struct Phys {
+  double N, Ninv;
+  double j[7], kap2x2;                       // short range (dipole-dipole-short-range.F)
+  double P_alpha, P_gamma, P_k1, P_k2, P_k3, P_k4;
+  double fa2g, tg, sk, tk2, fk;              // dVddi-unharmonic.F:28-32
+  double B11, B12, B44;
+  double HC2[6][6];                          // homogeneous_coupling_2 (elastic.F:60-75)
+  double H[6][6], HG[6][6], HG_inv[6];       // homogeneous, Cholesky (elastic.F:26-52)
+  double pNa03[3], epi_strain;
+  int bulk_or_film;
+  double Zstar;
+  double dt, dt_2, Q, nf_kT, threeN_kT;
+  double n_sum_p;
+  int E_on;
+  int modulation_on;
+};
+
+struct DevScalars {
+  double s, pi, H0, s_old;
+  double kick_coef;   // p <- p - kick_coef * F
+  double drift_coef;  // u <- u + drift_coef * p * m^-1
+  double lf_dt, lf_dt_2;
+  double e[E_COUNT];
+  double strain[6];
+  double w_hom[6];    // sum_i strain_i * HC2(i, j)
+  double didiK0[6];   // Re didiK(k = 0)
+  double E[3];        // uniform external field
+  double ke_sum;      // last masked sum p^2/m
+  int status;
+  int pad;
+};
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block-wide sum of NQ values; thread 0 writes part[blockid*NQ + q].
+// Fixed reduction order, so results are reproducible run to run.
+template <int NQ>
+__device__ void block_partials(double* v, double* part, long long blockid) {
+  __shared__ double red[32][NQ];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double s = warp_sum(v[q]);
+    if (lane == 0) red[wid][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    for (int q = 0; q < NQ; ++q) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += red[w][q];
+      part[blockid * NQ + q] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// Sum of part[b*NQ + q] over b in fixed order by one RED_THREADS block.
+__device__ double reduce_partials(const double* part, int nblk, int NQ, int q) {
+  __shared__ double red[RED_THREADS];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(long long)b * NQ + q];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// ------------------------------------------------------- analytic short range
+// S(k) of the 27-point stencil of dipole-dipole-short-range.F:35-83 (2 kappa2
+// on site, j1..j7 on the first three neighbour shells), evaluated from the
+// cosines and sines of theta_a = 2 pi k_a / L_a.  Valid for L_a >= 3.
+// Order: xx, yy, zz, yz, zx, xy.
+__host__ __device__ inline void short_range_k(const double* j, double kap2x2, const double c[3], const double s[3],
+                                              double S[6]) {
+  for (int a = 0; a < 3; ++a) {
+    const int b = (a + 1) % 3, g = (a + 2) % 3;
+    S[a] = kap2x2 + 2 * j[1] * c[a] + 2 * j[0] * (c[b] + c[g]) + 4 * j[3] * c[b] * c[g] +
+           4 * j[2] * c[a] * (c[b] + c[g]) + 8 * j[5] * c[0] * c[1] * c[2];
+  }
+  // off-diagonal (a, b) with third axis g: -4 j5 s_a s_b - 8 j7 s_a s_b c_g
+  S[3] = -4 * j[4] * s[1] * s[2] - 8 * j[6] * s[1] * s[2] * c[0];  // yz
+  S[4] = -4 * j[4] * s[2] * s[0] - 8 * j[6] * s[2] * s[0] * c[1];  // zx
+  S[5] = -4 * j[4] * s[0] * s[1] - 8 * j[6] * s[0] * s[1] * c[2];  // xy
+}
+
+// ------------------------------------------------------------------ k_xy_fwd
+enum { SRC_U9 = 0, SRC_FIELD = 1 };
+
+// Per (z-plane, component): load a real plane, DIF along x on Lx/2 complex
+// pairs, unpack to the Lx/2+1 bins of the real transform, DIF along y.
+// SRC_U9: component c of (u_x, u_y, u_z, u_x^2, u_y^2, u_z^2, u_y u_z,
+// u_z u_x, u_x u_y) from u (dipoFFT.F:19-44).  SRC_FIELD: component c of src.
+template <typename T, int MODE>
+__global__ void __launch_bounds__(512) k_xy_fwd(const T* __restrict__ src, cplx<T>* __restrict__ spec, Geom g,
+                                                FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
+                                                const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
+                                                const int* __restrict__ posm, int out_comp0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  using T2 = typename RT2<T>::type;
+  const int z = blockIdx.x, c = blockIdx.y;
+  const int m = g.m, RS = m + 1, Ly = g.Ly, Lx = g.Lx;
+  const int buf_len = Ly * RS;
+  const long long plane_off = (long long)z * g.plane_r;
+  for (int idx = threadIdx.x; idx < Ly * m; idx += blockDim.x) {
+    const int y = idx / m, jx = idx - y * m;
+    const long long o = plane_off + (long long)y * Lx + 2 * jx;
+    T2 v;
+    if (MODE == SRC_FIELD) {
+      v = *reinterpret_cast<const T2*>(src + (long long)c * g.nsite + o);
+    } else if (c < 3) {
+      v = *reinterpret_cast<const T2*>(src + (long long)c * g.nsite + o);
+    } else {
+      const T2 a = *reinterpret_cast<const T2*>(src + o);
+      const T2 b = *reinterpret_cast<const T2*>(src + g.nsite + o);
+      const T2 d = *reinterpret_cast<const T2*>(src + 2 * g.nsite + o);
+      switch (c) {
+        case 3: v.x = a.x * a.x; v.y = a.y * a.y; break;
+        case 4: v.x = b.x * b.x; v.y = b.y * b.y; break;
+        case 5: v.x = d.x * d.x; v.y = d.y * d.y; break;
+        case 6: v.x = b.x * d.x; v.y = b.y * d.y; break;
+        case 7: v.x = d.x * a.x; v.y = d.y * a.y; break;
+        default: v.x = a.x * b.x; v.y = a.y * b.y; break;
+      }
+    }
+    buf[y * RS + jx] = mk<cplx<T>>(v.x, v.y);
+  }
+  __syncthreads();
+  {
+    Batch B{Ly, 1, 0, RS, 1, false};
+    fft_forward<T>(buf, B, px, twm, buf_len);
+  }
+  // unpack: slot posm[k] holds Z(k) of the packed row; X(k) = E(k) + w^k O(k)
+  const int half = m / 2 + 1;
+  for (int idx = threadIdx.x; idx < Ly * half; idx += blockDim.x) {
+    const int y = idx / half, k = idx - y * half;
+    cplx<T>* row = buf + y * RS;
+    if (k == 0) {
+      const cplx<T> z0 = row[0];
+      row[0] = mk<cplx<T>>(z0.x + z0.y, (T)0);
+      row[m] = mk<cplx<T>>(z0.x - z0.y, (T)0);
+    } else {
+      const int k2 = m - k;
+      const int s1 = __ldg(&posm[k]), s2 = __ldg(&posm[k2]);
+      const cplx<T> a = row[s1], b = row[s2];
+      const cplx<T> w1 = __ldg(&twx[k]), w2 = __ldg(&twx[k2]);
+      // X(k) = 1/2 (a + conj b) - i/2 w1 (a - conj b)
+      const cplx<T> e1 = mk<cplx<T>>(a.x + b.x, a.y - b.y), d1 = mk<cplx<T>>(a.x - b.x, a.y + b.y);
+      const cplx<T> wd1 = cmul(w1, d1);
+      const cplx<T> X1 = mk<cplx<T>>((T)0.5 * (e1.x + wd1.y), (T)0.5 * (e1.y - wd1.x));
+      const cplx<T> e2 = mk<cplx<T>>(b.x + a.x, b.y - a.y), d2 = mk<cplx<T>>(b.x - a.x, b.y + a.y);
+      const cplx<T> wd2 = cmul(w2, d2);
+      const cplx<T> X2 = mk<cplx<T>>((T)0.5 * (e2.x + wd2.y), (T)0.5 * (e2.y - wd2.x));
+      row[s1] = X1;
+      if (s2 != s1) row[s2] = X2;
+    }
+  }
+  __syncthreads();
+  {
+    Batch B{RS, RS, 1, 0, RS, true};
+    fft_forward<T>(buf, B, py, twy, buf_len);
+  }
+  cplx<T>* dst = spec + (long long)(out_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
+  for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
+    const int y = idx / RS, col = idx - y * RS;
+    dst[(long long)y * g.KXP + col] = buf[idx];
+  }
+}
+
+// ------------------------------------------------------------------ k_xy_inv
+// Per (z-plane, component): DIT along y, repack the Lx/2+1 bins into Lx/2
+// complex pairs (imaginary parts of the kx = 0 and kx = Lx/2 bins dropped,
+// the half-complex convention of the reference's c2r), DIT along x, store
+// the real plane.  Output is unnormalised (Lx*Ly*Lz times the IDFT).
+template <typename T>
+__global__ void __launch_bounds__(512) k_xy_inv(const cplx<T>* __restrict__ spec, T* __restrict__ out, Geom g,
+                                                FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
+                                                const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
+                                                const int* __restrict__ posm, int in_comp0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  using T2 = typename RT2<T>::type;
+  const int z = blockIdx.x, c = blockIdx.y;
+  const int m = g.m, RS = m + 1, Ly = g.Ly, Lx = g.Lx;
+  const int buf_len = Ly * RS;
+  const cplx<T>* srcp = spec + (long long)(in_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
+  for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
+    const int y = idx / RS, col = idx - y * RS;
+    buf[idx] = srcp[(long long)y * g.KXP + col];
+  }
+  __syncthreads();
+  {
+    Batch B{RS, RS, 1, 0, RS, true};
+    fft_inverse<T>(buf, B, py, twy, buf_len);
+  }
+  const int half = m / 2 + 1;
+  for (int idx = threadIdx.x; idx < Ly * half; idx += blockDim.x) {
+    const int y = idx / half, k = idx - y * half;
+    cplx<T>* row = buf + y * RS;
+    if (k == 0) {
+      const T X0 = row[0].x, Xm = row[m].x;
+      row[0] = mk<cplx<T>>(X0 + Xm, X0 - Xm);
+    } else {
+      const int k2 = m - k;
+      const int s1 = __ldg(&posm[k]), s2 = __ldg(&posm[k2]);
+      const cplx<T> a = row[s1], b = row[s2];
+      const cplx<T> w1 = __ldg(&twx[k]), w2 = __ldg(&twx[k2]);
+      // Z(k) = (a + conj b) + i conj(w1) (a - conj b)
+      const cplx<T> e1 = mk<cplx<T>>(a.x + b.x, a.y - b.y), d1 = mk<cplx<T>>(a.x - b.x, a.y + b.y);
+      const cplx<T> wd1 = cmulc(d1, w1);
+      const cplx<T> Z1 = mk<cplx<T>>(e1.x - wd1.y, e1.y + wd1.x);
+      const cplx<T> e2 = mk<cplx<T>>(b.x + a.x, b.y - a.y), d2 = mk<cplx<T>>(b.x - a.x, b.y + a.y);
+      const cplx<T> wd2 = cmulc(d2, w2);
+      const cplx<T> Z2 = mk<cplx<T>>(e2.x - wd2.y, e2.y + wd2.x);
+      row[s1] = Z1;
+      if (s2 != s1) row[s2] = Z2;
+    }
+  }
+  __syncthreads();
+  {
+    Batch B{Ly, 1, 0, RS, 1, false};
+    fft_inverse<T>(buf, B, px, twm, buf_len);
+  }
+  T* dst = out + (long long)c * g.nsite + (long long)z * g.plane_r;
+  for (int idx = threadIdx.x; idx < Ly * m; idx += blockDim.x) {
+    const int y = idx / m, jx = idx - y * m;
+    const cplx<T> v = buf[y * RS + jx];
+    T2 w;
+    w.x = v.x;
+    w.y = v.y;
+    *reinterpret_cast<T2*>(dst + (long long)y * Lx + 2 * jx) = w;
+  }
+}
+
+// ------------------------------------------------- z tiles (shared helpers)
+// A tile is CW consecutive kx slots of one ky slot, all z, nc components,
+// held in shared memory as buf[c][z][cw].
+template <typename T>
+__device__ void z_tile_load(cplx<T>* buf, const cplx<T>* __restrict__ spec, const Geom& g, int nc, int CW, int col0,
+                            int yslot) {
+  const int Lz = g.Lz;
+  const int n = nc * Lz * CW;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    const int c = idx / (Lz * CW), rem = idx - c * Lz * CW;
+    const int z = rem / CW, cw = rem - z * CW;
+    const int col = col0 + cw;
+    cplx<T> v = mk<cplx<T>>((T)0, (T)0);
+    if (col < g.NKX) v = spec[(long long)c * g.ncplx + (long long)z * g.plane_c + (long long)yslot * g.KXP + col];
+    buf[idx] = v;
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__device__ void z_tile_store(const cplx<T>* buf, cplx<T>* __restrict__ spec, const Geom& g, int nc, int CW, int col0,
+                             int yslot) {
+  const int Lz = g.Lz;
+  const int n = nc * Lz * CW;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    const int c = idx / (Lz * CW), rem = idx - c * Lz * CW;
+    const int z = rem / CW, cw = rem - z * CW;
+    const int col = col0 + cw;
+    if (col < g.NKX) spec[(long long)c * g.ncplx + (long long)z * g.plane_c + (long long)yslot * g.KXP + col] = buf[idx];
+  }
+}
+
+// Wavevectors, trig tables and slot maps shared by the k-space kernels.
+struct KMaps {
+  const int* revx;     // kx slot -> kx
+  const int* revy;     // ky slot -> ky
+  const int* revz;     // kz slot -> kz
+  const double* kvx;   // k(1) of elastic.F:87 per kx
+  const double* kvy;   // k(2) per ky (wrapped to (-1/2, 1/2])
+  const double* kvz;   // k(3) per kz
+  const double2* trx;  // (cos, sin)(2 pi kx / Lx)
+  const double2* try_;
+  const double2* trz;
+};
+
+// Plain z pass of nc spectra in place: DIF (INV = false) or DIT (INV = true).
+template <typename T, bool INV>
+__global__ void __launch_bounds__(512) k_z_pass(cplx<T>* __restrict__ spec, Geom g, FftPlan pz,
+                                                const cplx<T>* __restrict__ twz, int nc, int CW) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
+  z_tile_load<T>(buf, spec, g, nc, CW, col0, yslot);
+  Batch B{nc * CW, CW, 1, g.Lz * CW, CW, true};
+  if (INV) fft_inverse<T>(buf, B, pz, twz, nc * g.Lz * CW);
+  else fft_forward<T>(buf, B, pz, twz, nc * g.Lz * CW);
+  z_tile_store<T>(buf, spec, g, nc, CW, col0, yslot);
+}
+
+// ------------------------------------------------------------------ k_z_kspace
+// Per (kx tile, ky slot): DIF along z of the nine spectra, then for every k
+//   F(k)     = D(k) uK(k),  D = (S + Z*^2 L)/N   (dVddi-dipole-dipole.F:20-36)
+//   acouK(k) = -K(k)^-1 (c_k_mod + coup2(k) didiK(k))  (optimize-inho-strain.F:28-58)
+//   inhoK(k) = k (x) acouK / N                        (dVddi_inho_coupling.F:91-108)
+// with K, its Cholesky factor and coup2 evaluated analytically
+// (elastic.F:79-180), and the half-spectrum energy sums of
+// dVddi-dipole-dipole.F:226-250 (by Parseval) and energy_module.F:150-240;
+// then DIT along z.  Slots 0..2 return F(k), slots 3..8 inhoK(k).
+template <typename T>
+__global__ void __launch_bounds__(512) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
+                                                  const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
+                                                  Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
+                                                  const Phys* __restrict__ ph, double* __restrict__ part,
+                                                  DevScalars* __restrict__ sc, int CW) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  const int Lz = g.Lz;
+  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
+  const int buf_len = 9 * Lz * CW;
+  z_tile_load<T>(buf, spec, g, 9, CW, col0, yslot);
+  {
+    Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
+    fft_forward<T>(buf, B, pz, twz, buf_len);
+  }
+  const double Ninv = ph->Ninv;
+  const int ky = __ldg(&km.revy[yslot]);
+  const double kv2 = __ldg(&km.kvy[ky]);
+  const double2 ty = __ldg(&km.try_[ky]);
+  double acc[NQ_K] = {0, 0, 0, 0, 0};
+  for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
+    const int zs = idx / CW, cw = idx - zs * CW;
+    const int col = col0 + cw;
+    if (col >= g.NKX) continue;
+    const int kx = __ldg(&km.revx[col]), kz = __ldg(&km.revz[zs]);
+    const double w1 = (kx == 0 || kx == g.m) ? 1.0 : 2.0;  // full-spectrum multiplicity
+    cplx<T> u[3], d[6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) u[a] = buf[(a * Lz + zs) * CW + cw];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) d[i] = buf[((3 + i) * Lz + zs) * CW + cw];
+    if (kx == 0 && ky == 0 && kz == 0) {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) sc->didiK0[i] = (double)d[i].x;
+    }
+    // ---- dipole-dipole
+    const long long tpos = ((long long)yslot * Lz + zs) * g.KXP + col;
+    const T* Dp = dtab + tpos * 6;
+    T D[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) D[q] = __ldg(&Dp[q]);
+    double qv[6];  // Re(conj(u_a) u_b): xx, yy, zz, yz, zx, xy
+    qv[0] = (double)u[0].x * u[0].x + (double)u[0].y * u[0].y;
+    qv[1] = (double)u[1].x * u[1].x + (double)u[1].y * u[1].y;
+    qv[2] = (double)u[2].x * u[2].x + (double)u[2].y * u[2].y;
+    qv[3] = (double)u[1].x * u[2].x + (double)u[1].y * u[2].y;
+    qv[4] = (double)u[2].x * u[0].x + (double)u[2].y * u[0].y;
+    qv[5] = (double)u[0].x * u[1].x + (double)u[0].y * u[1].y;
+    {
+      const double2 tx = __ldg(&km.trx[kx]), tz = __ldg(&km.trz[kz]);
+      const double cc[3] = {tx.x, ty.x, tz.x}, ss[3] = {tx.y, ty.y, tz.y};
+      double S[6];
+      short_range_k(ph->j, ph->kap2x2, cc, ss, S);
+      acc[0] += w1 * (S[0] * qv[0] + S[1] * qv[1] + S[2] * qv[2] + 2.0 * (S[3] * qv[3] + S[4] * qv[4] + S[5] * qv[5]));
+      acc[1] += w1 * ((double)D[0] * qv[0] + (double)D[1] * qv[1] + (double)D[2] * qv[2] +
+                      2.0 * ((double)D[3] * qv[3] + (double)D[4] * qv[4] + (double)D[5] * qv[5]));
+    }
+    cplx<T> F[3];
+    F[0] = mk<cplx<T>>(D[0] * u[0].x + D[5] * u[1].x + D[4] * u[2].x, D[0] * u[0].y + D[5] * u[1].y + D[4] * u[2].y);
+    F[1] = mk<cplx<T>>(D[5] * u[0].x + D[1] * u[1].x + D[3] * u[2].x, D[5] * u[0].y + D[1] * u[1].y + D[3] * u[2].y);
+    F[2] = mk<cplx<T>>(D[4] * u[0].x + D[3] * u[1].x + D[2] * u[2].x, D[4] * u[0].y + D[3] * u[1].y + D[2] * u[2].y);
+    // ---- inhomogeneous strain
+    const T k1 = (T)__ldg(&km.kvx[kx]), k2 = (T)kv2, k3 = (T)__ldg(&km.kvz[kz]);
+    const T kk[4] = {(T)0, k1, k2, k3};
+    const T B11 = (T)ph->B11, B12 = (T)ph->B12, B44 = (T)ph->B44;
+    T K[3][3];
+#pragma unroll
+    for (int b = 1; b <= 3; ++b) {
+      const int o1 = (b + 1) % 3 + 1, o2 = b % 3 + 1;
+#pragma unroll
+      for (int a = 1; a <= 3; ++a) {
+        if (a == b) K[a - 1][b - 1] = B11 * kk[a] * kk[a] + B44 * kk[o1] * kk[o1] + B44 * kk[o2] * kk[o2];
+        else K[a - 1][b - 1] = B12 * kk[a] * kk[b] + B44 * kk[a] * kk[b];
+      }
+    }
+    // coup2(a, i) (elastic.F:156-180)
+    const T hx = (T)(ph->HC2[0][0]), hy = (T)(ph->HC2[0][1]), h4 = (T)(ph->HC2[3][3]);
+    T C2[3][6];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int i = 0; i < 3; ++i) C2[a][i] = (a == i) ? kk[a + 1] * hx : kk[a + 1] * hy;
+    }
+    C2[0][3] = (T)0 * h4; C2[1][3] = k3 * h4; C2[2][3] = k2 * h4;
+    C2[0][4] = k3 * h4;   C2[1][4] = (T)0 * h4; C2[2][4] = k1 * h4;
+    C2[0][5] = k2 * h4;   C2[1][5] = k1 * h4; C2[2][5] = (T)0 * h4;
+    cplx<T> ck[3] = {mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0)};
+    if (ph->modulation_on) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) ck[a] = ckmod[tpos * 3 + a];
+    }
+    cplx<T> acou[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      cplx<T> s = mk<cplx<T>>((T)0, (T)0);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) s = mk<cplx<T>>(s.x + C2[a][i] * d[i].x, s.y + C2[a][i] * d[i].y);
+      acou[a] = mk<cplx<T>>(-ck[a].x - s.x, -ck[a].y - s.y);
+    }
+    if (kx == 0 && ky == 0 && kz == 0) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) acou[a] = mk<cplx<T>>((T)0, (T)0);  // inhomo_K_G(:,:,0,0,0) = 0
+    } else {
+      T G[3][3], Gi[3];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        T s = (T)0;
+#pragma unroll
+        for (int q = 0; q < b; ++q) s += G[b][q] * G[b][q];
+        G[b][b] = sqrt(K[b][b] - s);
+        Gi[b] = (T)1 / G[b][b];
+#pragma unroll
+        for (int a = b + 1; a < 3; ++a) {
+          T t = (T)0;
+#pragma unroll
+          for (int q = 0; q < b; ++q) t += G[a][q] * G[b][q];
+          G[a][b] = (K[a][b] - t) * Gi[b];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        cplx<T> t = mk<cplx<T>>((T)0, (T)0);
+#pragma unroll
+        for (int b = 0; b < a; ++b) t = mk<cplx<T>>(t.x + G[a][b] * acou[b].x, t.y + G[a][b] * acou[b].y);
+        acou[a] = mk<cplx<T>>((acou[a].x - t.x) * Gi[a], (acou[a].y - t.y) * Gi[a]);
+      }
+#pragma unroll
+      for (int a = 2; a >= 0; --a) {
+        cplx<T> t = mk<cplx<T>>((T)0, (T)0);
+#pragma unroll
+        for (int b = a + 1; b < 3; ++b) t = mk<cplx<T>>(t.x + acou[b].x * G[b][a], t.y + acou[b].y * G[b][a]);
+        acou[a] = mk<cplx<T>>((acou[a].x - t.x) * Gi[a], (acou[a].y - t.y) * Gi[a]);
+      }
+    }
+    {
+      const double w2 = 0.5 * w1;  // energy_module.F weights: 1/2 at kx = 0, Lx/2
+      double es = 0.0, ec = 0.0, em = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        // Re(conj(acou_a) * sum_b K_ab acou_b)
+        double rx = 0.0, ry = 0.0;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          rx += (double)K[a][b] * acou[b].x;
+          ry += (double)K[a][b] * acou[b].y;
+        }
+        es += (double)acou[a].x * rx + (double)acou[a].y * ry;
+        double cx = 0.0, cy = 0.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          cx += (double)C2[a][i] * d[i].x;
+          cy += (double)C2[a][i] * d[i].y;
+        }
+        ec += (double)acou[a].x * cx + (double)acou[a].y * cy;
+        em += (double)acou[a].x * ck[a].x + (double)acou[a].y * ck[a].y;
+      }
+      acc[2] += w2 * es;
+      acc[3] += w2 * ec;
+      acc[4] += w2 * em;
+    }
+    if (acouK_out) {
+#pragma unroll
+      for (int a = 0; a < 3; ++a) acouK_out[tpos * 3 + a] = acou[a];
+    }
+    const T ni = (T)Ninv;
+    d[0] = mk<cplx<T>>(k1 * acou[0].x * ni, k1 * acou[0].y * ni);
+    d[1] = mk<cplx<T>>(k2 * acou[1].x * ni, k2 * acou[1].y * ni);
+    d[2] = mk<cplx<T>>(k3 * acou[2].x * ni, k3 * acou[2].y * ni);
+    d[3] = mk<cplx<T>>((k3 * acou[1].x + k2 * acou[2].x) * ni, (k3 * acou[1].y + k2 * acou[2].y) * ni);
+    d[4] = mk<cplx<T>>((k1 * acou[2].x + k3 * acou[0].x) * ni, (k1 * acou[2].y + k3 * acou[0].y) * ni);
+    d[5] = mk<cplx<T>>((k2 * acou[0].x + k1 * acou[1].x) * ni, (k2 * acou[0].y + k1 * acou[1].y) * ni);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) buf[(a * Lz + zs) * CW + cw] = F[a];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) buf[((3 + i) * Lz + zs) * CW + cw] = d[i];
+  }
+  __syncthreads();
+  {
+    Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
+    fft_inverse<T>(buf, B, pz, twz, buf_len);
+  }
+  z_tile_store<T>(buf, spec, g, 9, CW, col0, yslot);
+  block_partials<NQ_K>(acc, part, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ------------------------------------------------------------------ k_assemble
+// Real-space force (dVddi) on every site:
+//   F = F_dd                                      (c2r of k_z_kspace slots 0..2)
+//     + anharmonic polynomial force               (dVddi-unharmonic.F:34-65)
+//     - Z* E                                      (mirror_force_mirror.F:42-50)
+//     + homogeneous strain coupling, w = strain B2 (dVddi-homo-coupling.F:209-237)
+//     + inhomogeneous strain coupling, w(R) = eta(R) B2 (dVddi_inho_coupling.F:114-142)
+// and the per-block sums of the anharmonic energy (:67-99) and Z* u.E.
+template <typename T>
+__global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
+                                                  T* __restrict__ F, Geom g, const Phys* __restrict__ ph,
+                                                  const DevScalars* __restrict__ sc, double* __restrict__ part) {
+  const long long ns = g.nsite;
+  const T fa2g = (T)ph->fa2g, tg = (T)ph->tg, sk = (T)ph->sk, tk2 = (T)ph->tk2, fk = (T)ph->fk, k4x8 = (T)(8 * ph->P_k4);
+  const double Pa = ph->P_alpha, Pg = ph->P_gamma, P1 = ph->P_k1, P2 = ph->P_k2, P3 = ph->P_k3, P4 = ph->P_k4;
+  T wh[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) wh[i] = (T)sc->w_hom[i];
+  T B2[6][6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i)
+#pragma unroll
+    for (int jj = 0; jj < 6; ++jj) B2[i][jj] = (T)ph->HC2[i][jj];
+  const int E_on = ph->E_on;
+  const T Zs = (T)ph->Zstar;
+  const T E0 = (T)sc->E[0], E1 = (T)sc->E[1], E2 = (T)sc->E[2];
+  double acc[NQ_R] = {0.0, 0.0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
+    const T ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
+    T f0 = rw[i], f1 = rw[ns + i], f2 = rw[2 * ns + i];
+    const T d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
+    const T uu = d0 + d1 + d2;
+    // 4th order
+    f0 = f0 + ux * (fa2g * uu - tg * d0);
+    f1 = f1 + uy * (fa2g * uu - tg * d1);
+    f2 = f2 + uz * (fa2g * uu - tg * d2);
+    // 6th and 8th order
+    const T uu2 = uu * uu, uu3 = uu2 * uu;
+    f0 = f0 + ux * (sk * uu2 + k4x8 * uu3 - tk2 * (d0 * d0) - fk * d1 * d2);
+    f1 = f1 + uy * (sk * uu2 + k4x8 * uu3 - tk2 * (d1 * d1) - fk * d2 * d0);
+    f2 = f2 + uz * (sk * uu2 + k4x8 * uu3 - tk2 * (d2 * d2) - fk * d0 * d1);
+    {
+      const double D0 = d0, D1 = d1, D2 = d2, U = uu;
+      acc[0] += Pa * (U * U) + Pg * (D0 * D1 + D1 * D2 + D2 * D0) + P1 * (U * U * U) +
+                P2 * ((D0 * D0) * (D1 + D2) + (D1 * D1) * (D2 + D0) + (D2 * D2) * (D0 + D1)) + P3 * D0 * D1 * D2 +
+                P4 * (U * U * U * U);
+    }
+    if (E_on) {
+      f0 = f0 - Zs * E0;
+      f1 = f1 - Zs * E1;
+      f2 = f2 - Zs * E2;
+      acc[1] += (double)Zs * ((double)ux * E0 + (double)uy * E1 + (double)uz * E2);
+    }
+    // homogeneous strain coupling
+    f0 = f0 + 2 * wh[0] * ux + wh[4] * uz + wh[5] * uy;
+    f1 = f1 + 2 * wh[1] * uy + wh[3] * uz + wh[5] * ux;
+    f2 = f2 + 2 * wh[2] * uz + wh[3] * uy + wh[4] * ux;
+    // inhomogeneous strain coupling (eta already carries 1/N)
+    T eta[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
+    T w[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q)
+      w[q] = eta[0] * B2[0][q] + eta[1] * B2[1][q] + eta[2] * B2[2][q] + eta[3] * B2[3][q] + eta[4] * B2[4][q] +
+             eta[5] * B2[5][q];
+    f0 = f0 + 2 * w[0] * ux + w[4] * uz + w[5] * uy;
+    f1 = f1 + 2 * w[1] * uy + w[3] * uz + w[5] * ux;
+    f2 = f2 + 2 * w[2] * uz + w[3] * uy + w[4] * ux;
+    F[i] = f0;
+    F[ns + i] = f1;
+    F[2 * ns + i] = f2;
+  }
+  block_partials<NQ_R>(acc, part, blockIdx.x);
+}
+
+// --------------------------------------------------------------- integrators
+// p <- p - coef * F on every site (nose-poincare.F:24-28,66-71, leapfrog.F:
+// 134-138) and the masked sum p^2 m^-1 of kinetic_energy_dipo.F:92-105.
+// Per-layer masses and sum_p masks (film halves, dead layers).
+template <typename T>
+__global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __restrict__ F, const double* coef, Geom g,
+                                              const double* __restrict__ layer_minv,
+                                              const unsigned char* __restrict__ layer_sump, double* __restrict__ part) {
+  const long long ns = g.nsite;
+  const T c = (T)(*coef);
+  double acc[1] = {0.0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(i / g.plane_r);
+    const T p0 = p[i] - c * F[i];
+    const T p1 = p[ns + i] - c * F[ns + i];
+    const T p2 = p[2 * ns + i] - c * F[2 * ns + i];
+    p[i] = p0;
+    p[ns + i] = p1;
+    p[2 * ns + i] = p2;
+    if (layer_sump[z]) {
+      const double mi = layer_minv[z];
+      acc[0] += (double)p0 * p0 * mi + (double)p1 * p1 * mi + (double)p2 * p2 * mi;
+    }
+  }
+  block_partials<1>(acc, part, blockIdx.x);
+}
+
+// u <- u + coef * p * m^-1 (nose-poincare.F:41-53, leapfrog.F:104-114)
+template <typename T>
+__global__ void __launch_bounds__(256) k_drift(T* __restrict__ u, const T* __restrict__ p, const double* coef, Geom g,
+                                               const double* __restrict__ layer_minv) {
+  const long long ns = g.nsite;
+  const double c = *coef;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(i / g.plane_r);
+    const T f = (T)(c * layer_minv[z]);
+    u[i] = u[i] + f * p[i];
+    u[ns + i] = u[ns + i] + f * p[ns + i];
+    u[2 * ns + i] = u[2 * ns + i] + f * p[2 * ns + i];
+  }
+}
+
+// Film mirror (mirror.F:9-36): layer z' = Lz-1-z (gap_id = 0) or Lz-z gets
+// (-f_x, -f_y, f_z) of layer z.
+template <typename T>
+__global__ void k_mirror(T* __restrict__ f, Geom g, int gap_id) {
+  const long long ns = g.nsite;
+  const int z0 = (gap_id == 0) ? 0 : 1;
+  const int z1 = (gap_id == 0) ? g.Lz / 2 : (g.Lz + 1) / 2;  // exclusive
+  const long long n = (long long)(z1 - z0) * g.plane_r;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int z = z0 + (int)(i / g.plane_r);
+    const long long r = i % g.plane_r;
+    const int zd = (gap_id == 0) ? g.Lz - 1 - z : g.Lz - z;
+    const long long s = (long long)z * g.plane_r + r, d = (long long)zd * g.plane_r + r;
+    f[d] = -f[s];
+    f[ns + d] = -f[ns + s];
+    f[2 * ns + d] = f[2 * ns + s];
+  }
+}
+
+// ------------------------------------------------------------ scalar kernels
+__device__ __forceinline__ double sum_potential(const double* e) {
+  return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
+}
+
+__device__ __forceinline__ void np_hamiltonian(const Phys* ph, DevScalars* sc) {  // energy_module.F:128-148
+  double* e = sc->e;
+  const double s = sc->s;
+  double h = e[E_DIPO] / (s * s) + sum_potential(e) + sc->pi * sc->pi / 2 / ph->Q + ph->threeN_kT * log(s) - sc->H0;
+  e[E_HNP] = h * s;
+}
+
+__device__ __forceinline__ void check_finite(DevScalars* sc, const double* v, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!isfinite(v[i])) sc->status = 3;  // FG_ERR_NAN
+}
+
+// After the k-space pass: k-space energies, homogeneous strain
+// (optimize-homo-strain.F:27-186) and w_hom for k_assemble.
+__global__ void __launch_bounds__(RED_THREADS) k_homo_strain(const Phys* __restrict__ ph, DevScalars* sc,
+                                                             const double* __restrict__ part_k, int nblk) {
+  double v[NQ_K];
+  for (int q = 0; q < NQ_K; ++q) v[q] = reduce_partials(part_k, nblk, NQ_K, q);
+  if (threadIdx.x != 0) return;
+  double* e = sc->e;
+  const double es = v[0] * ph->Ninv / 2;       // (1/2N) sum w' Re(uK* S uK)
+  const double edd = v[1] / 2;                 // (1/2)  sum w' Re(uK* D uK), D = (S + Z*^2 L)/N
+  e[E_SHORT] = es;
+  e[E_LONG] = edd - es;
+  e[E_IS] = v[2] * ph->Ninv;
+  e[E_IC] = v[3] * 2 * ph->Ninv;
+  e[E_IM] = ph->modulation_on ? v[4] * 2 * ph->Ninv : 0.0;
+  double hc2uu[6];
+  for (int i = 0; i < 6; ++i) {
+    double s = 0.0;
+    for (int jj = 0; jj < 6; ++jj) s += ph->HC2[i][jj] * sc->didiK0[jj];
+    hc2uu[i] = s;
+  }
+  for (int i = 0; i < 3; ++i) hc2uu[i] = hc2uu[i] + ph->pNa03[i];
+  double* st = sc->strain;
+  const double(*H)[6] = ph->H;
+  if (ph->bulk_or_film == 2) {  // epit
+    st[0] = ph->epi_strain;
+    st[1] = ph->epi_strain;
+    st[2] = (-(H[2][0] + H[2][1]) * ph->epi_strain - hc2uu[2]) / H[2][2];
+    st[3] = -hc2uu[3] / H[3][3];
+    st[4] = -hc2uu[4] / H[4][4];
+    st[5] = 0.0;
+  } else if (ph->bulk_or_film == 3) {  // e110
+    st[2] = ph->epi_strain;
+    st[3] = 0.0;
+    st[4] = 0.0;
+    double num = -(H[0][0] + H[1][1] + 2 * H[1][1]) * ph->epi_strain - (H[2][0] + H[2][1]) * st[2] - hc2uu[0] - hc2uu[1] +
+                 2 * hc2uu[5];
+    double den = H[0][0] + H[1][1] + 2 * H[1][0] + 4 * H[5][5];
+    double delta = num / den;
+    st[0] = ph->epi_strain + delta;
+    st[1] = ph->epi_strain + delta;
+    st[5] = -2 * delta;
+  } else {
+    for (int i = 0; i < 6; ++i) st[i] = -hc2uu[i];
+    for (int i = 0; i < 6; ++i) {
+      double t = 0.0;
+      for (int jj = 0; jj < i; ++jj) t = t + ph->HG[i][jj] * st[jj];
+      st[i] = (st[i] - t) * ph->HG_inv[i];
+    }
+    for (int i = 5; i >= 0; --i) {
+      double t = 0.0;
+      for (int jj = i + 1; jj < 6; ++jj) t = t + st[jj] * ph->HG[jj][i];
+      st[i] = (st[i] - t) * ph->HG_inv[i];
+    }
+  }
+  double hs = 0.0;
+  for (int i = 0; i < 6; ++i) {
+    double d = 0.0;
+    for (int jj = 0; jj < 6; ++jj) d += H[i][jj] * st[jj];
+    hs = hs + st[i] * d;
+  }
+  e[E_HS] = hs / 2;
+  double hc = 0.0;
+  for (int i = 0; i < 6; ++i) hc += st[i] * hc2uu[i];
+  e[E_HC] = hc;
+  for (int jj = 0; jj < 6; ++jj) {
+    double w = 0.0;
+    for (int i = 0; i < 6; ++i) w = w + st[i] * ph->HC2[i][jj];
+    sc->w_hom[jj] = w;
+  }
+}
+
+// After k_assemble: real-space energies.
+__global__ void __launch_bounds__(RED_THREADS) k_force_energies(const Phys* __restrict__ ph, DevScalars* sc,
+                                                                const double* __restrict__ part_r, int nblk) {
+  double v0 = reduce_partials(part_r, nblk, NQ_R, 0);
+  double v1 = reduce_partials(part_r, nblk, NQ_R, 1);
+  if (threadIdx.x != 0) return;
+  sc->e[E_UNH] = v0;
+  sc->e[E_DIPE] = ph->E_on ? -v1 : 0.0;
+  check_finite(sc, sc->e + E_SHORT, 9);
+}
+
+// kinetic_energy_dipo.F:106 from the kick partials
+__device__ __forceinline__ double ke_from(const Phys* ph, double sum) { return sum / ph->n_sum_p * ph->N / 2; }
+
+// Nose-Poincare, first half (nose-poincare.F:30-41): KE, (38), (35c).
+__global__ void __launch_bounds__(RED_THREADS) k_np_pre(const Phys* __restrict__ ph, DevScalars* sc,
+                                                        const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  double* e = sc->e;
+  sc->ke_sum = v;
+  e[E_DIPO] = ke_from(ph, v);
+  double s = sc->s;
+  double CB = ph->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - sc->H0;
+  CB = ph->dt_2 * CB - sc->pi;
+  sc->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * ph->dt / ph->Q));
+  sc->s_old = s;
+  sc->s = s * (1.0 + ph->dt_2 * sc->pi / ph->Q) / (1.0 - ph->dt_2 * sc->pi / ph->Q);
+  sc->drift_coef = ph->dt_2 * (1 / sc->s + 1 / sc->s_old);
+}
+
+// Nose-Poincare after the force (nose-poincare.F:60-66): H_NP, (35e).
+__global__ void k_np_post(const Phys* __restrict__ ph, DevScalars* sc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  np_hamiltonian(ph, sc);
+  const double s = sc->s;
+  const double delta_H = sc->e[E_HNP] / s;
+  sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] / (s * s) - ph->nf_kT) - ph->dt_2 * delta_H;
+  sc->kick_coef = ph->dt_2 * s;
+}
+
+// After the closing kick: KE, H_NP, total (nose-poincare.F:74-75,
+// molecular-dynamics.F:293).
+__global__ void __launch_bounds__(RED_THREADS) k_np_final(const Phys* __restrict__ ph, DevScalars* sc,
+                                                          const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  sc->ke_sum = v;
+  sc->e[E_DIPO] = ke_from(ph, v);
+  np_hamiltonian(ph, sc);
+  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
+  check_finite(sc, sc->e, E_COUNT);
+}
+
+// Leapfrog closing reduction (leapfrog.F:151) and total.
+__global__ void __launch_bounds__(RED_THREADS) k_lf_final(const Phys* __restrict__ ph, DevScalars* sc,
+                                                          const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  sc->ke_sum = v;
+  sc->e[E_DIPO] = ke_from(ph, v);
+  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
+  check_finite(sc, sc->e, E_COUNT);
+}
+
+// KE of the current momenta without changing them.
+template <typename T>
+__global__ void __launch_bounds__(256) k_ke_only(const T* __restrict__ p, Geom g, const double* __restrict__ layer_minv,
+                                                 const unsigned char* __restrict__ layer_sump, double* __restrict__ part) {
+  const long long ns = g.nsite;
+  double acc[1] = {0.0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(i / g.plane_r);
+    if (layer_sump[z]) {
+      const double mi = layer_minv[z];
+      const double p0 = p[i], p1 = p[ns + i], p2 = p[2 * ns + i];
+      acc[0] += p0 * p0 * mi + p1 * p1 * mi + p2 * p2 * mi;
+    }
+  }
+  block_partials<1>(acc, part, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_ke_finish(const Phys* __restrict__ ph, DevScalars* sc,
+                                                           const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  sc->ke_sum = v;
+  sc->e[E_DIPO] = ke_from(ph, v);
+}
+
+// add_to_Average reductions (average_module.F:86-121): masked sum of u and of
+// Z* u per component.  part[b*6 + q]: q = 0..2 sum u, 3..5 sum Z* u.
+template <typename T>
+__global__ void __launch_bounds__(256) k_avg_sums(const T* __restrict__ u, Geom g, double Zs,
+                                                  const unsigned char* __restrict__ layer_sump, double* __restrict__ part) {
+  const long long ns = g.nsite;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
+    const int z = (int)(i / g.plane_r);
+    if (!layer_sump[z]) continue;
+    const double a = u[i], b = u[ns + i], c = u[2 * ns + i];
+    acc[0] += a;
+    acc[1] += b;
+    acc[2] += c;
+    acc[3] += Zs * a;
+    acc[4] += Zs * b;
+    acc[5] += Zs * c;
+  }
+  block_partials<6>(acc, part, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_avg_finish(double* out6, const double* __restrict__ part, int nblk) {
+  for (int q = 0; q < 6; ++q) {
+    double v = reduce_partials(part, nblk, 6, q);
+    if (threadIdx.x == 0) out6[q] = v;
+  }
+}
+
+template <typename T>
+__global__ void k_accumulate(double* __restrict__ acc, const T* __restrict__ u, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc[i] += (double)u[i];
+}
+
+// ------------------------------------------------------- layout conversion
+// Padded column-major (nc, 0:NXP-1, 0:NYP-1, 0:Lz-1) FP64 <-> [nc][z][y][x] T.
+template <typename T>
+__global__ void k_fortran_to_soa(T* __restrict__ dst, const double* __restrict__ src, Geom g, int nc, int NXP, int NYP) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.nsite; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % g.Lx);
+    const long long r = i / g.Lx;
+    const int y = (int)(r % g.Ly), z = (int)(r / g.Ly);
+    const long long s = (long long)nc * ((long long)x + (long long)NXP * ((long long)y + (long long)NYP * z));
+    for (int c = 0; c < nc; ++c) dst[(long long)c * g.nsite + i] = (T)src[s + c];
+  }
+}
+
+template <typename T>
+__global__ void k_soa_to_fortran(double* __restrict__ dst, const T* __restrict__ src, Geom g, int nc, int NXP, int NYP) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.nsite; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % g.Lx);
+    const long long r = i / g.Lx;
+    const int y = (int)(r % g.Ly), z = (int)(r / g.Ly);
+    const long long s = (long long)nc * ((long long)x + (long long)NXP * ((long long)y + (long long)NYP * z));
+    for (int c = 0; c < nc; ++c) dst[s + c] = (double)src[(long long)c * g.nsite + i];
+  }
+}
+
+// ------------------------------------------------------- table construction
+// Real-space Ewald sum of dipole-dipole-long-range.F:106-149 per site:
+// self term at R = 0, images jz, jy, jx in -1-max..max, per element +B on
+// the diagonal then -rn_a rn_b C.  Output [6][z][y][x]: xx, yy, zz, yz, zx, xy.
+__global__ void k_ewald_real(double* __restrict__ out, Geom g, double a0, double kappa, int max_x, int max_y, int max_z) {
+  const double two_over_sqrtpi = 1.12837916709551257390;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.nsite; i += (long long)gridDim.x * blockDim.x) {
+    const int ix = (int)(i % g.Lx);
+    const long long r = i / g.Lx;
+    const int iy = (int)(r % g.Ly), iz = (int)(r / g.Ly);
+    double t[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (i == 0) {
+      const double self = -2 * two_over_sqrtpi * kappa * kappa * kappa / 3;
+      t[0][0] = t[1][1] = t[2][2] = self;
+    }
+    for (int jz = -1 - max_z; jz <= max_z; ++jz)
+      for (int jy = -1 - max_y; jy <= max_y; ++jy)
+        for (int jx = -1 - max_x; jx <= max_x; ++jx) {
+          if (jx == 0 && jy == 0 && jz == 0 && i == 0) continue;
+          const double rn[3] = {ix * a0 + jx * (g.Lx * a0), iy * a0 + jy * (g.Ly * a0), iz * a0 + jz * (g.Lz * a0)};
+          const double rr = rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2];
+          const double rnorm = sqrt(rr);
+          const double ec = erfc(kappa * rnorm), ex = exp(-kappa * kappa * rr);
+          const double B = ec / (rnorm * rr) + two_over_sqrtpi * kappa * ex / rr;
+          const double C = (3 * ec / (rnorm * rr) + two_over_sqrtpi * kappa * ex * (2 * kappa * kappa + 3 / rr)) / rr;
+#pragma unroll
+          for (int b = 0; b < 3; ++b)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              if (a == b) t[a][b] = t[a][b] + B;
+              t[a][b] = t[a][b] - rn[a] * rn[b] * C;
+            }
+        }
+    out[i] = t[0][0];
+    out[g.nsite + i] = t[1][1];
+    out[2 * g.nsite + i] = t[2][2];
+    out[3 * g.nsite + i] = t[1][2];
+    out[4 * g.nsite + i] = t[2][0];
+    out[5 * g.nsite + i] = t[0][1];
+  }
+}
+
+// Per (kx tile, ky slot) of the six forward-transformed real-space sums:
+// DIF along z, then L = (Re FFT + reciprocal sum) * Hartree*Bohr/eps_inf
+// (dipole-dipole-long-range.F:151-206), D = (S + Z*^2 L)/N in the table
+// layout, and L in FP64 for inspection.
+template <typename T>
+__global__ void __launch_bounds__(512) k_z_ewald_pack(const cplx<double>* __restrict__ spec, T* __restrict__ dtab,
+                                                      double* __restrict__ L64, Geom g, FftPlan pz,
+                                                      const cplx<double>* __restrict__ twz, KMaps km,
+                                                      const Phys* __restrict__ ph, double a0, double kappa,
+                                                      double eps_inf, int max_x, int max_y, int max_z, int CW) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem_raw);
+  const int Lz = g.Lz;
+  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
+  z_tile_load<double>(buf, spec, g, 6, CW, col0, yslot);
+  {
+    Batch B{6 * CW, CW, 1, Lz * CW, CW, true};
+    fft_forward<double>(buf, B, pz, twz, 6 * Lz * CW);
+  }
+  const double pi = 3.14159265358979323846;
+  const double four_pi_over_v = 4 * pi / (a0 * a0 * a0);
+  const double two_pi_over_a = 2 * pi / a0;
+  const double four_kappa2 = 4 * kappa * kappa;
+  const double scale = 14.399644 / eps_inf;  // HARTREE_BOHR (define.h:32)
+  const int ky = km.revy[yslot];
+  for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
+    const int zs = idx / CW, cw = idx - zs * CW;
+    const int col = col0 + cw;
+    if (col >= g.NKX) continue;
+    const int kx = km.revx[col], kz = km.revz[zs];
+    double k[3];
+    k[2] = (double)kz / g.Lz;
+    if (k[2] > 0.5) k[2] = k[2] - 1.0;
+    k[1] = (double)ky / g.Ly;
+    if (k[1] > 0.5) k[1] = k[1] - 1.0;
+    k[0] = (double)kx / g.Lx;
+    double Lt[6];
+    for (int q = 0; q < 6; ++q) Lt[q] = buf[(q * Lz + zs) * CW + cw].x;
+    const int qa[6] = {0, 1, 2, 1, 2, 0}, qb[6] = {0, 1, 2, 2, 0, 1};
+    for (int q = 0; q < 6; ++q) {
+      double t = Lt[q];
+      for (int nz = -max_z; nz <= max_z; ++nz) {
+        const double kG2 = two_pi_over_a * (k[2] + nz);
+        for (int ny = -max_y; ny <= max_y; ++ny) {
+          const double kG1 = two_pi_over_a * (k[1] + ny);
+          for (int nx = -max_x; nx <= max_x; ++nx) {
+            if (kx == 0 && ky == 0 && kz == 0 && nx == 0 && ny == 0 && nz == 0) continue;
+            const double kG0 = two_pi_over_a * (k[0] + nx);
+            const double kG[3] = {kG0, kG1, kG2};
+            const double kGkG = kG0 * kG0 + kG1 * kG1 + kG2 * kG2;
+            t = t + four_pi_over_v * kG[qa[q]] * kG[qb[q]] * exp(-kGkG / four_kappa2) / kGkG;
+          }
+        }
+      }
+      Lt[q] = t * scale;
+    }
+    const double2 tx = km.trx[kx], ty = km.try_[ky], tz = km.trz[kz];
+    const double cc[3] = {tx.x, ty.x, tz.x}, ss[3] = {tx.y, ty.y, tz.y};
+    double S[6];
+    short_range_k(ph->j, ph->kap2x2, cc, ss, S);
+    const long long tpos = ((long long)yslot * Lz + zs) * g.KXP + col;
+    const double z2 = ph->Zstar * ph->Zstar;
+    for (int q = 0; q < 6; ++q) {
+      dtab[tpos * 6 + q] = (T)((S[q] + z2 * Lt[q]) * ph->Ninv);
+      if (L64) L64[tpos * 6 + q] = Lt[q];
+    }
+  }
+}
+
+// c_k_modulation_k = modulation_constant * k * r2c(modulation_R) (elastic.F:212-225)
+template <typename T>
+__global__ void __launch_bounds__(512) k_z_modulation_pack(const cplx<double>* __restrict__ spec, cplx<T>* __restrict__ ck,
+                                                           Geom g, FftPlan pz, const cplx<double>* __restrict__ twz,
+                                                           KMaps km, double mod_const, int CW) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem_raw);
+  const int Lz = g.Lz;
+  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
+  z_tile_load<double>(buf, spec, g, 1, CW, col0, yslot);
+  {
+    Batch B{CW, CW, 1, Lz * CW, CW, true};
+    fft_forward<double>(buf, B, pz, twz, Lz * CW);
+  }
+  const int ky = km.revy[yslot];
+  for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
+    const int zs = idx / CW, cw = idx - zs * CW;
+    const int col = col0 + cw;
+    if (col >= g.NKX) continue;
+    const int kx = km.revx[col], kz = km.revz[zs];
+    const double kv[3] = {km.kvx[kx], km.kvy[ky], km.kvz[kz]};
+    const cplx<double> mk_ = buf[zs * CW + cw];
+    const long long tpos = ((long long)yslot * Lz + zs) * g.KXP + col;
+    for (int a = 0; a < 3; ++a)
+      ck[tpos * 3 + a] = mk<cplx<T>>((T)(mod_const * kv[a] * mk_.x), (T)(mod_const * kv[a] * mk_.y));
+  }
+}
+
+}  // namespace fg

@@ -15,8 +15,9 @@
  *   complex     (ncomp, 0:Lx/2,         0:Ly+padding_y-1, 0:Lz-1)
  *   k table     (3, 3,  0:Lx/2,         0:Ly+padding_y-1, 0:Lz-1)
  *
- * (coord_module.F:91-93,139-141,247,256).  Only physical points are read
- * or written; padding is left untouched.
+ * (coord_module.F:91-93,139-141,247,256).  Only physical points are read;
+ * real fields returned by the library carry zeros in their padding, as the
+ * reference's arrays do.
  *
  * Every function returns an int status (FG_OK = 0).  The library never
  * calls exit(); the text of the last error of a context is available from
@@ -204,6 +205,15 @@ int  fg_set_modulation_R(fg_ctx* ctx, const double* modulation_R);
 /* Long-range table as built on the device, Fortran layout, eV/A^2 (testing). */
 int  fg_get_long_range(fg_ctx* ctx, double* long_range);
 
+/* fftw_execute_dft_r2c(c%plan_r2c_3_out, in, out) (dipoFFT.F:108): batched
+   3D r2c of a 3-component real field into its half spectrum, unnormalised,
+   on the device FFT.  in: real field layout; out: complex*16 (3, 0:Lx/2, ...). */
+int  fg_fft_r2c3(fg_ctx* ctx, const double* in, double* out);
+/* fftw_execute_dft_c2r(c%plan_c2r_3_out, in, out) (dVddi-dipole-dipole.F:194):
+   the inverse, unnormalised; imaginary parts of the kx = 0 and kx = Lx/2
+   bins are ignored as by FFTW's half-complex convention.  in is not modified. */
+int  fg_fft_c2r3(fg_ctx* ctx, const double* in, double* out);
+
 /* ---- state --------------------------------------------------------------- */
 
 /* Coord_type members (coord_module.F:18,25,26,48,53).  dipoR/dipoP/dVddi are
@@ -242,6 +252,17 @@ int  fg_get_dipoRavg(fg_ctx* ctx, double* dipoRavg);
 /* Run n_steps of the method of p (md or lf) on the device as one CUDA graph
    per step; the energies of the last step are returned in e. */
 int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
+
+/* ---- measurement ----------------------------------------------------------
+   CUDA-event timing on the context's own stream (no host work in between). */
+#define FG_NPROF 12
+/* Time n_steps graph launches of the MD step of p's method; *ms = total. */
+int  fg_time_steps(fg_ctx* ctx, int n_steps, double* ms);
+/* One bulk Nose-Poincare step launched kernel by kernel with an event between
+   kernels, averaged over reps steps; ms[i] (i < FG_NPROF) per kernel, in the
+   order named by fg_profile_name(i).  The steps advance the state. */
+int  fg_profile_step(fg_ctx* ctx, int reps, double* ms);
+const char* fg_profile_name(int i);
 
 /* ---- host driver ----------------------------------------------------------
    feram_common + molecular_dynamics (feram_common.F:9-119,
