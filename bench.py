@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""MD site-steps/s of feram's Nose-Poincare step at 128^3 on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: bulk BaTiO3 effective Hamiltonian (the Zhong-Vanderbilt-Rabe
+parameter set of the reference's BaTiO3 cooling example), 128^3 supercell,
+300 K, dt = 2 fs, E_z = 100 kV/cm, Nose-Poincare (method 'md').  The initial
+dipoles are uni64-seeded Gaussians (sigma 0.03 A); one step = one full
+nose_poincare call (kick, thermostat, drift, force, kick).  The timed steps
+run as CUDA graphs on the library's own stream and are timed with CUDA
+events recorded on that stream; the working set (fields, spectra and tables,
+~0.3 GB in the mixed path) exceeds the 126 MB L2, so no flush is needed.
+
+Under torchrun each rank runs an independent replica on its own GPU (the
+reference's task-farm parallelism, replicas only); value is the whole-job
+rate and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MD site-steps/s at 128^3: mixed vs FP64 GPU (force err<=1e-6); % HBM peak"
+UNIT = "site-steps/s"
+L_DEFAULT = 128
+
+# BaTiO3, Zhong-Vanderbilt-Rabe effective-Hamiltonian parameters as used by
+# the reference's BaTiO3 cooling sweep and 64^3 benchmark input decks (eV,
+# Angstrom, ps).  The Nose-Poincare mass grows with the supercell: the 64^3
+# benchmark deck uses Q = 1.0, so Q = 1.0 * N / 64^3 here (8.0 at 128^3),
+# which keeps CB dt / Q of nose-poincare.F:36 far below 1.
+ZVR = dict(GPa=-5.0, mass_amu=39.0, Q_Nose_64=1.0, a0=3.94, dt=0.002,
+           P_kappa2=5.502, P_alpha=110.4, P_gamma=-163.1,
+           j=(-2.648, 3.894, 0.898, -0.789, 0.562, 0.358, 0.179),
+           B11=126.0, B12=44.9, B44=50.3, B1xx=-211.0, B1yy=-19.3, B4yz=-7.75,
+           Z_star=9.956, epsilon_inf=5.24)
+
+
+def make_params(L, kelvin=300.0, Ez=0.001, seed=(123456789, 987654321)):
+    import feram_b200 as fb
+    p = fb.default_params()
+    z = ZVR
+    p.method = 0
+    p.GPa[0] = p.GPa[1] = p.GPa[2] = z["GPa"]
+    p.kelvin = kelvin
+    for s in range(3):
+        p.mass_dipo[s] = z["mass_amu"] / 9648.53377163899
+        p.P_kappa2[s], p.P_alpha[s], p.P_gamma[s] = z["P_kappa2"], z["P_alpha"], z["P_gamma"]
+        p.Z_star[s] = z["Z_star"]
+        p.init_dipo_dev[s] = 0.03
+        p.init_dipo_avg[s] = 0.0
+    p.Q_Nose = z["Q_Nose_64"] * L ** 3 / 64 ** 3
+    p.a0, p.dt = z["a0"], z["dt"]
+    p.Lx = p.Ly = p.Lz = L
+    for i, v in enumerate(z["j"]):
+        p.j[i] = v
+    p.B11, p.B12, p.B44, p.B1xx, p.B1yy, p.B4yz = (z[k] for k in ("B11", "B12", "B44", "B1xx", "B1yy", "B4yz"))
+    p.epsilon_inf = z["epsilon_inf"]
+    p.external_E_field[2] = Ez
+    p.E_field_always_zero = 0 if Ez != 0.0 else 1
+    p.seed[0], p.seed[1] = seed
+    return fb.make_param(p)
+
+
+def initial_state(p):
+    from feram_b200 import _capi as A
+    u = A.real_field(p)
+    q = A.real_field(p)
+    assert A.lib().fg_init_dipoR_host(C.byref(p), A.dptr(u), A.dptr(q)) == 0
+    return u, q
+
+
+def prepare(ctx, p, u, q):
+    """initialize_dipoR's tail and molecular-dynamics.F:209-212 (H0)."""
+    ctx.set_state(u, q, 1.0, 0.0, 0.0)
+    ctx.set_uniform_E([p.external_E_field[0], p.external_E_field[1], p.external_E_field[2]])
+    e = ctx.mirror_force_mirror()
+    e.dipo_kinetic = ctx.kinetic_energy_dipo()
+    ctx.nose_poincare_hamiltonian(e)
+    H0 = e.H_Nose_Poincare
+    ctx.set_thermostat(1.0, 0.0, H0)
+    ctx.nose_poincare_hamiltonian(e)
+    return H0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.dev)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def kernel_bytes(p, esz):
+    """Compulsory DRAM bytes per launch of each kernel of one step (inputs
+    read once + outputs written once), esz = bytes per real."""
+    N = p.Lx * p.Ly * p.Lz
+    nk = (p.Lx // 2 + 1) * p.Ly * p.Lz  # half-spectrum points per component
+    c = 2 * esz
+    return {
+        "k_kick(35a)": 9 * N * esz, "k_drift": 9 * N * esz, "k_kick(35f)": 9 * N * esz,
+        "k_xy_fwd": 3 * N * esz + 9 * nk * c,
+        "k_z_kspace": 18 * nk * c + 6 * nk * esz,
+        "k_xy_inv": 9 * nk * c + 9 * N * esz,
+        "k_assemble": 15 * N * esz,
+    }
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes per kernel from the committed ncu summary, if any."""
+    try:
+        return json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic_128.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_baseline(p, budget_s=20.0):
+    """The oracle (FP64 C++/OpenMP restatement of the reference's CPU path)
+    on this host's cores: one NP step after setup, then as many more as fit
+    in the budget.  Bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    threads = os.cpu_count() or 1
+    oracle_lib.load().oracle_set_threads(threads)
+    u, q = initial_state(p)
+    o = oracle_lib.Oracle(p)
+    o.set_state(u, q)
+    o.set_uniform_E([p.external_E_field[0], p.external_E_field[1], p.external_E_field[2]])
+    e = o.force()
+    e.dipo_kinetic = o.kinetic_energy_dipo()
+    o.md(1, 0, 1, e)  # H0
+    t0 = time.perf_counter()
+    o.nose_poincare(e)
+    t1 = time.perf_counter()
+    n = 1 + max(0, int((budget_s - (t1 - t0)) / max(t1 - t0, 1e-6)))
+    n = min(n, 50)
+    for _ in range(n - 1):
+        o.nose_poincare(e)
+    t2 = time.perf_counter()
+    o.close()
+    return {"value": p.N * n / (t2 - t0), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} Nose-Poincare steps at {p.Lx}^3 after table setup (oracle/, FP64, OpenMP)"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU path (its C++ restatement, since
+    the Fortran/FFTW binary cannot be built here) on all host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    L = args.size
+    p = make_params(L)
+    budget = 120.0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    threads = os.cpu_count() or 1
+    oracle_lib.load().oracle_set_threads(threads)
+    u, q = initial_state(p)
+    o = oracle_lib.Oracle(p)
+    o.set_state(u, q)
+    o.set_uniform_E([0.0, 0.0, p.external_E_field[2]])
+    e = o.force()
+    e.dipo_kinetic = o.kinetic_energy_dipo()
+    o.md(1, 0, 1, e)
+    for _ in range(min(args.warmup, 1)):
+        o.nose_poincare(e)
+    t0 = time.perf_counter()
+    o.nose_poincare(e)
+    t1 = time.perf_counter()
+    n = max(1, min(args.steps, int(budget / max(t1 - t0, 1e-6))))
+    for _ in range(n - 1):
+        o.nose_poincare(e)
+    t2 = time.perf_counter()
+    value = p.N * n / (t2 - t0)
+    sample = f"{n} of {args.steps} requested Nose-Poincare steps at {L}^3 (FP64 C++/OpenMP restatement)"
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 * (t2 - t0) / n,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: uni64-seeded dipoles, BaTiO3 ZVR parameters",
+        "config": {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", type=int, default=L_DEFAULT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import feram_b200 as fb
+    from feram_b200 import _capi as A
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    L = args.size
+    p = make_params(L, seed=(123456789 + rank, 987654321))
+    u, q = initial_state(p)
+
+    # force error of the mixed path against the FP64 path on the same state
+    ctx64 = fb.Context(p, A.FG_PREC_FP64)
+    ctx64.build_tables()
+    ctxm = fb.Context(p, A.FG_PREC_MIXED)
+    ctxm.build_tables()
+    H0 = 0.0
+    for c in (ctx64, ctxm):
+        H0 = prepare(c, p, u, q)
+    f64 = ctx64.get_state()["dVddi"]
+    fmx = ctxm.get_state()["dVddi"]
+    d = A.physical(fmx, p) - A.physical(f64, p)
+    rms = float(np.sqrt(np.mean(np.sum(A.physical(f64, p) ** 2, axis=-1))))
+    dn = np.sqrt(np.sum(d ** 2, axis=-1))
+    ferr = {"max": float(dn.max() / rms), "rms": float(np.sqrt(np.mean(dn ** 2)) / rms)}
+
+    def timed(ctx, steps, warmup, sample_clocks):
+        ms = C.c_double()
+        ctx._check(A.lib().fg_time_steps(ctx._h, warmup, C.byref(ms)))
+        barrier()
+        sampler = ClockSampler(torch.cuda.current_device()) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        barrier()
+        ctx._check(A.lib().fg_time_steps(ctx._h, steps, C.byref(ms)))
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        return max_over_ranks(ms.value), clocks
+
+    ms_mixed, clocks = timed(ctxm, args.steps, args.warmup, True)
+    ms_fp64, _ = timed(ctx64, max(args.steps // 2, 10), args.warmup, False)
+    steps64 = max(args.steps // 2, 10)
+    value = p.N * args.steps * world / (ms_mixed / 1000.0)
+    value64 = p.N * steps64 * world / (ms_fp64 / 1000.0)
+
+    # per-kernel times of one step (events between kernels, same stream)
+    nprof = 12
+    prof = (C.c_double * nprof)()
+    ctxm._check(A.lib().fg_profile_step(ctxm._h, 20, prof))
+    names = [A.lib().fg_profile_name(i).decode() for i in range(nprof)]
+    kb = kernel_bytes(p, 4)
+    pk, pk_kind = peaks()
+    hbm = float(pk.get("hbm_gbs", 6650.0))
+    per_kernel = {}
+    for n, t in zip(names, prof):
+        ent = {"ms": t}
+        if n in kb and t > 0:
+            ent["GBps"] = kb[n] / (t * 1e-3) / 1e9
+            ent["frac"] = ent["GBps"] / hbm
+        per_kernel[n] = ent
+    dom = max((n for n in names if n in kb), key=lambda n: per_kernel[n]["ms"])
+    traffic = ncu_traffic().get(dom)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": per_kernel[dom]["GBps"], "peak": hbm, "unit": "GB/s",
+                "frac": per_kernel[dom]["frac"], "peak_kind": pk_kind,
+                "algorithmic_bytes": kb[dom], "traffic": traffic}
+    ms_step = ms_mixed / args.steps
+    step_roofline = {"algorithmic_bytes_per_site_step": 264, "achieved_GBps": 264 * p.N / (ms_step * 1e-3) / 1e9,
+                     "frac": 264 * p.N / (ms_step * 1e-3) / 1e9 / hbm,
+                     "fp64_frac": 528 * p.N / (ms_fp64 / steps64 * 1e-3) / 1e9 / hbm}
+
+    # e2e through the public C-ABI with host buffers: upload the state from
+    # pinned memory, K reference-style per-step calls (field H2D, energies
+    # D2H), download u, p and dVddi.
+    keep = []
+
+    def pin(a):
+        t = torch.from_numpy(a).pin_memory()
+        keep.append(t)
+        return t.numpy()
+
+    hu, hq = pin(u.copy()), pin(q.copy())
+    out_u, out_q, out_f = pin(A.real_field(p)), pin(A.real_field(p)), pin(A.real_field(p))
+    E = np.array([0.0, 0.0, p.external_E_field[2]])
+    e = fb.fg_energy()
+    k_e2e = max(args.steps // 4, 10)
+    barrier()
+    t0 = time.perf_counter()
+    ctxm.set_state(hu, hq, 1.0, 0.0, H0)
+    ctxm.mirror_force_mirror(e)
+    for i in range(k_e2e):
+        ctxm.set_uniform_E(E)
+        ctxm.nose_poincare(e)
+    strain = np.zeros(6)
+    s_, pi_, h0_ = C.c_double(), C.c_double(), C.c_double()
+    ctxm._check(A.lib().fg_get_state(ctxm._h, A.dptr(out_u), A.dptr(out_q), A.dptr(out_f), A.dptr(strain),
+                                     C.byref(s_), C.byref(pi_), C.byref(h0_)))
+    barrier()
+    t1 = time.perf_counter()
+    t_e2e = max_over_ranks(t1 - t0)
+    field_bytes = u.nbytes
+    e2e = {"value": p.N * k_e2e * world / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": (2 * field_bytes + 24 * k_e2e) / k_e2e,
+           "d2h_bytes_per_step": (3 * field_bytes + 48 + C.sizeof(A.fg_energy) * k_e2e) / k_e2e,
+           "steps": k_e2e, "includes": "fg_set_state + fg_mirror_force_mirror + K x (fg_set_uniform_E, "
+                                       "fg_nose_poincare) + fg_get_state"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(p)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (fields, FFT, forces); f64 thermostat, strain, energy sums",
+        "data": "synthetic: uni64-seeded dipoles (sigma 0.03 A), BaTiO3 ZVR parameters",
+        "config": {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm",
+                   "sites": p.N, "precision": "mixed", "parallelism": f"replicas x{world}",
+                   "l2": "working set > 126 MB L2, no flush"},
+        "fp64": {"value": value64, "ms_per_step": ms_fp64 / steps64, "steps": steps64},
+        "mixed_over_fp64": value / value64,
+        "force_err_mixed_vs_fp64": ferr,
+        "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
+        "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": 12 * args.steps,
+    }
+    ctxm.close()
+    ctx64.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -299,6 +299,8 @@ int pull_scalars(fg_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->stream));
   int rc = check_device_error(ctx);
   if (rc) return rc;
+  if (ctx->sc_host->status == 10)
+    return fail(ctx, FG_ERR_NAN, "Nose-Poincare update (38): 1 - CB dt/Q < 0, Q_Nose is too small for this supercell");
   if (ctx->sc_host->status == FG_ERR_NAN) return fail(ctx, FG_ERR_NAN, "non-finite energy in a device reduction");
   return FG_OK;
 }

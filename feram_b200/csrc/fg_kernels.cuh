@@ -789,6 +789,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_np_pre(const Phys* __restrict__
   double s = sc->s;
   double CB = ph->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - sc->H0;
   CB = ph->dt_2 * CB - sc->pi;
+  if (1.0 - CB * ph->dt / ph->Q < 0.0) sc->status = 10;  // (38) has no real root: Q_Nose too small
   sc->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * ph->dt / ph->Q));
   sc->s_old = s;
   sc->s = s * (1.0 + ph->dt_2 * sc->pi / ph->Q) / (1.0 - ph->dt_2 * sc->pi / ph->Q);
