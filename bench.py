@@ -256,6 +256,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=L_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed-only", action="store_true",
+                    help="skip the FP64 context, the force-error check and e2e (small device footprint, for profiling)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -290,20 +292,21 @@ def main():
     p = make_params(L, seed=(123456789 + rank, 987654321))
     u, q = initial_state(p)
 
-    # force error of the mixed path against the FP64 path on the same state
-    ctx64 = fb.Context(p, A.FG_PREC_FP64)
-    ctx64.build_tables()
     ctxm = fb.Context(p, A.FG_PREC_MIXED)
     ctxm.build_tables()
-    H0 = 0.0
-    for c in (ctx64, ctxm):
-        H0 = prepare(c, p, u, q)
-    f64 = ctx64.get_state()["dVddi"]
-    fmx = ctxm.get_state()["dVddi"]
-    d = A.physical(fmx, p) - A.physical(f64, p)
-    rms = float(np.sqrt(np.mean(np.sum(A.physical(f64, p) ** 2, axis=-1))))
-    dn = np.sqrt(np.sum(d ** 2, axis=-1))
-    ferr = {"max": float(dn.max() / rms), "rms": float(np.sqrt(np.mean(dn ** 2)) / rms)}
+    H0 = prepare(ctxm, p, u, q)
+    ctx64, ferr = None, None
+    if not args.mixed_only:
+        # force error of the mixed path against the FP64 path on the same state
+        ctx64 = fb.Context(p, A.FG_PREC_FP64)
+        ctx64.build_tables()
+        prepare(ctx64, p, u, q)
+        f64 = ctx64.get_state()["dVddi"]
+        fmx = ctxm.get_state()["dVddi"]
+        d = A.physical(fmx, p) - A.physical(f64, p)
+        rms = float(np.sqrt(np.mean(np.sum(A.physical(f64, p) ** 2, axis=-1))))
+        dn = np.sqrt(np.sum(d ** 2, axis=-1))
+        ferr = {"max": float(dn.max() / rms), "rms": float(np.sqrt(np.mean(dn ** 2)) / rms)}
 
     def timed(ctx, steps, warmup, sample_clocks):
         ms = C.c_double()
@@ -320,10 +323,12 @@ def main():
         return max_over_ranks(ms.value), clocks
 
     ms_mixed, clocks = timed(ctxm, args.steps, args.warmup, True)
-    ms_fp64, _ = timed(ctx64, max(args.steps // 2, 10), args.warmup, False)
-    steps64 = max(args.steps // 2, 10)
     value = p.N * args.steps * world / (ms_mixed / 1000.0)
-    value64 = p.N * steps64 * world / (ms_fp64 / 1000.0)
+    steps64 = max(args.steps // 2, 10)
+    ms_fp64, value64 = None, None
+    if ctx64 is not None:
+        ms_fp64, _ = timed(ctx64, steps64, args.warmup, False)
+        value64 = p.N * steps64 * world / (ms_fp64 / 1000.0)
 
     # per-kernel times of one step (events between kernels, same stream)
     nprof = 12
@@ -348,43 +353,45 @@ def main():
     ms_step = ms_mixed / args.steps
     step_roofline = {"algorithmic_bytes_per_site_step": 264, "achieved_GBps": 264 * p.N / (ms_step * 1e-3) / 1e9,
                      "frac": 264 * p.N / (ms_step * 1e-3) / 1e9 / hbm,
-                     "fp64_frac": 528 * p.N / (ms_fp64 / steps64 * 1e-3) / 1e9 / hbm}
+                     "fp64_frac": (528 * p.N / (ms_fp64 / steps64 * 1e-3) / 1e9 / hbm) if ms_fp64 else None}
 
-    # e2e through the public C-ABI with host buffers: upload the state from
-    # pinned memory, K reference-style per-step calls (field H2D, energies
-    # D2H), download u, p and dVddi.
-    keep = []
+    e2e = None
+    if not args.mixed_only:
+        # e2e through the public C-ABI with host buffers: upload the state from
+        # pinned memory, K reference-style per-step calls (field H2D, energies
+        # D2H), download u, p and dVddi.
+        keep = []
 
-    def pin(a):
-        t = torch.from_numpy(a).pin_memory()
-        keep.append(t)
-        return t.numpy()
+        def pin(a):
+            t = torch.from_numpy(a).pin_memory()
+            keep.append(t)
+            return t.numpy()
 
-    hu, hq = pin(u.copy()), pin(q.copy())
-    out_u, out_q, out_f = pin(A.real_field(p)), pin(A.real_field(p)), pin(A.real_field(p))
-    E = np.array([0.0, 0.0, p.external_E_field[2]])
-    e = fb.fg_energy()
-    k_e2e = max(args.steps // 4, 10)
-    barrier()
-    t0 = time.perf_counter()
-    ctxm.set_state(hu, hq, 1.0, 0.0, H0)
-    ctxm.mirror_force_mirror(e)
-    for i in range(k_e2e):
-        ctxm.set_uniform_E(E)
-        ctxm.nose_poincare(e)
-    strain = np.zeros(6)
-    s_, pi_, h0_ = C.c_double(), C.c_double(), C.c_double()
-    ctxm._check(A.lib().fg_get_state(ctxm._h, A.dptr(out_u), A.dptr(out_q), A.dptr(out_f), A.dptr(strain),
-                                     C.byref(s_), C.byref(pi_), C.byref(h0_)))
-    barrier()
-    t1 = time.perf_counter()
-    t_e2e = max_over_ranks(t1 - t0)
-    field_bytes = u.nbytes
-    e2e = {"value": p.N * k_e2e * world / t_e2e, "unit": UNIT,
-           "h2d_bytes_per_step": (2 * field_bytes + 24 * k_e2e) / k_e2e,
-           "d2h_bytes_per_step": (3 * field_bytes + 48 + C.sizeof(A.fg_energy) * k_e2e) / k_e2e,
-           "steps": k_e2e, "includes": "fg_set_state + fg_mirror_force_mirror + K x (fg_set_uniform_E, "
-                                       "fg_nose_poincare) + fg_get_state"}
+        hu, hq = pin(u.copy()), pin(q.copy())
+        out_u, out_q, out_f = pin(A.real_field(p)), pin(A.real_field(p)), pin(A.real_field(p))
+        E = np.array([0.0, 0.0, p.external_E_field[2]])
+        e = fb.fg_energy()
+        k_e2e = max(args.steps // 4, 10)
+        barrier()
+        t0 = time.perf_counter()
+        ctxm.set_state(hu, hq, 1.0, 0.0, H0)
+        ctxm.mirror_force_mirror(e)
+        for i in range(k_e2e):
+            ctxm.set_uniform_E(E)
+            ctxm.nose_poincare(e)
+        strain = np.zeros(6)
+        s_, pi_, h0_ = C.c_double(), C.c_double(), C.c_double()
+        ctxm._check(A.lib().fg_get_state(ctxm._h, A.dptr(out_u), A.dptr(out_q), A.dptr(out_f), A.dptr(strain),
+                                         C.byref(s_), C.byref(pi_), C.byref(h0_)))
+        barrier()
+        t1 = time.perf_counter()
+        t_e2e = max_over_ranks(t1 - t0)
+        field_bytes = u.nbytes
+        e2e = {"value": p.N * k_e2e * world / t_e2e, "unit": UNIT,
+               "h2d_bytes_per_step": (2 * field_bytes + 24 * k_e2e) / k_e2e,
+               "d2h_bytes_per_step": (3 * field_bytes + 48 + C.sizeof(A.fg_energy) * k_e2e) / k_e2e,
+               "steps": k_e2e, "includes": "fg_set_state + fg_mirror_force_mirror + K x (fg_set_uniform_E, "
+                                           "fg_nose_poincare) + fg_get_state"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -398,15 +405,16 @@ def main():
         "config": {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm",
                    "sites": p.N, "precision": "mixed", "parallelism": f"replicas x{world}",
                    "l2": "working set > 126 MB L2, no flush"},
-        "fp64": {"value": value64, "ms_per_step": ms_fp64 / steps64, "steps": steps64},
-        "mixed_over_fp64": value / value64,
+        "fp64": {"value": value64, "ms_per_step": (ms_fp64 / steps64) if ms_fp64 else None, "steps": steps64},
+        "mixed_over_fp64": (value / value64) if value64 else None,
         "force_err_mixed_vs_fp64": ferr,
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": 12 * args.steps,
     }
     ctxm.close()
-    ctx64.close()
+    if ctx64 is not None:
+        ctx64.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

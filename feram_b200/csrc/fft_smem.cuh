@@ -94,6 +94,40 @@ struct Dft<T, 8, INV> {
 };
 
 template <typename T, bool INV>
+struct Dft<T, 16, INV> {
+  // 16 = 4 x 4: DFT-4 over q2 of x[q1 + 4 q2], twiddle w16^(q1 s2), DFT-4 over
+  // q1, result X[s2 + 4 s1].
+  static __device__ __forceinline__ void run(cplx<T>* v) {
+    const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173, h = (T)0.70710678118654752440;
+    const T sg = INV ? (T)1 : (T)-1;  // sign of the imaginary part of w16^k
+    cplx<T> a[4][4];
+#pragma unroll
+    for (int q1 = 0; q1 < 4; ++q1) {
+#pragma unroll
+      for (int q2 = 0; q2 < 4; ++q2) a[q1][q2] = v[q1 + 4 * q2];
+      Dft<T, 4, INV>::run(a[q1]);
+    }
+    auto tw = [](cplx<T> x, T cr, T ci) { return mk<cplx<T>>(x.x * cr - x.y * ci, x.x * ci + x.y * cr); };
+    a[1][1] = tw(a[1][1], c1, sg * s1);   // w^1
+    a[1][2] = tw(a[1][2], h, sg * h);     // w^2
+    a[1][3] = tw(a[1][3], s1, sg * c1);   // w^3
+    a[2][1] = tw(a[2][1], h, sg * h);     // w^2
+    a[2][2] = mul_mi<cplx<T>, INV>(a[2][2]);  // w^4
+    a[2][3] = tw(a[2][3], -h, sg * h);    // w^6
+    a[3][1] = tw(a[3][1], s1, sg * c1);   // w^3
+    a[3][2] = tw(a[3][2], -h, sg * h);    // w^6
+    a[3][3] = tw(a[3][3], -c1, -sg * s1); // w^9
+#pragma unroll
+    for (int s2 = 0; s2 < 4; ++s2) {
+      cplx<T> b[4] = {a[0][s2], a[1][s2], a[2][s2], a[3][s2]};
+      Dft<T, 4, INV>::run(b);
+#pragma unroll
+      for (int s1i = 0; s1i < 4; ++s1i) v[s2 + 4 * s1i] = b[s1i];
+    }
+  }
+};
+
+template <typename T, bool INV>
 struct Dft<T, 3, INV> {
   static __device__ __forceinline__ void run(cplx<T>* v) {
     const T s3 = (T)0.86602540378443864676;  // sin(2 pi / 3)
@@ -191,13 +225,14 @@ __device__ __forceinline__ void fft_stage_rt(int R, cplx<T>* buf, const Batch& B
     case 4: fft_stage<T, 4, INV>(buf, B, n, Ls, tw, buf_len); break;
     case 5: fft_stage<T, 5, INV>(buf, B, n, Ls, tw, buf_len); break;
     case 8: fft_stage<T, 8, INV>(buf, B, n, Ls, tw, buf_len); break;
+    case 16: fft_stage<T, 16, INV>(buf, B, n, Ls, tw, buf_len); break;
     default: break;
   }
 }
 
 // Full forward (DIF) transform of a batch; ends with __syncthreads().
 template <typename T>
-__device__ void fft_forward(cplx<T>* buf, const Batch& B, const FftPlan& P, const cplx<T>* tw, int buf_len) {
+__device__ __forceinline__ void fft_forward(cplx<T>* buf, const Batch& B, const FftPlan& P, const cplx<T>* tw, int buf_len) {
   int Ls = P.n;
   for (int st = 0; st < P.nst; ++st) {
     fft_stage_rt<T, false>(P.r[st], buf, B, P.n, Ls, tw, buf_len);
@@ -208,13 +243,99 @@ __device__ void fft_forward(cplx<T>* buf, const Batch& B, const FftPlan& P, cons
 
 // Full inverse (DIT) transform, digit-reversed in, natural out, unnormalised.
 template <typename T>
-__device__ void fft_inverse(cplx<T>* buf, const Batch& B, const FftPlan& P, const cplx<T>* tw, int buf_len) {
+__device__ __forceinline__ void fft_inverse(cplx<T>* buf, const Batch& B, const FftPlan& P, const cplx<T>* tw, int buf_len) {
   int Ls = 1;
   for (int st = P.nst - 1; st >= 0; --st) {
     Ls *= P.r[st];
     fft_stage_rt<T, true>(P.r[st], buf, B, P.n, Ls, tw, buf_len);
     __syncthreads();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Compile-time transforms for power-of-two lengths.  Same DIF/DIT algorithm
+// and slot order as above (the host builds its digit-reversal tables from
+// ct_radix), but every index is a compile-time expression, the radices are
+// 16 and 8 (two shared-memory stages for n <= 256), and twiddles come from a
+// shared-memory copy of the table.  Stage plans: 4:[4] 8:[8] 16:[16] 32:[8,4]
+// 64:[16,4] 128:[16,8] 256:[16,16] 512:[16,8,4].
+__host__ __device__ constexpr bool ct_supported(int n) {
+  return n == 4 || n == 8 || n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512;
+}
+__host__ __device__ constexpr int ct_nst(int n) { return n <= 16 ? 1 : (n <= 256 ? 2 : 3); }
+__host__ __device__ constexpr int ct_radix(int n, int st) {
+  return n <= 16 ? n
+       : n == 32 ? (st == 0 ? 8 : 4)
+       : n == 64 ? (st == 0 ? 16 : 4)
+       : n == 128 ? (st == 0 ? 16 : 8)
+       : n == 256 ? 16
+       : (st == 0 ? 16 : (st == 1 ? 8 : 4));
+}
+__host__ __device__ constexpr int ct_ls(int n, int st) {  // sub-transform length at stage st
+  return st == 0 ? n : ct_ls(n, st - 1) / ct_radix(n, st - 1);
+}
+
+// Compile-time batch layout (see Batch); consecutive threads take
+// consecutive transforms.
+template <int COUNT, int INNER, int ISTR, int OUTER, int ES>
+struct BatchCT {
+  static constexpr int count = COUNT, inner = INNER, istr = ISTR, outer = OUTER, es = ES;
+};
+
+template <typename T, int N, int LS, int R, bool INV, int NT, class B>
+__device__ __forceinline__ void ct_stage(cplx<T>* __restrict__ buf, const cplx<T>* __restrict__ tws) {
+  constexpr int S = LS / R, NB = N / R, TOTAL = B::count * NB, TWS = N / LS;
+  constexpr int STEP = S * B::es;
+#pragma unroll 2
+  for (int w = threadIdx.x; w < TOTAL; w += NT) {
+    const int t = w % B::count, j = w / B::count;
+    const int blk = j / S, b = j - blk * S;
+    const int base = (t / B::inner) * B::outer + (t % B::inner) * B::istr + (blk * LS + b) * B::es;
+    cplx<T> v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = buf[base + q * STEP];
+    if (!INV) {
+      Dft<T, R, false>::run(v);
+      if (S > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmul(v[q], tws[b * q * TWS]);
+      }
+    } else {
+      if (S > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], tws[b * q * TWS]);
+      }
+      Dft<T, R, true>::run(v);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) buf[base + q * STEP] = v[q];
+  }
+}
+
+template <typename T, int N, int ST, int NT, class B>
+__device__ __forceinline__ void ct_forward_from(cplx<T>* buf, const cplx<T>* tws) {
+  if constexpr (ST < ct_nst(N)) {
+    ct_stage<T, N, ct_ls(N, ST), ct_radix(N, ST), false, NT, B>(buf, tws);
+    __syncthreads();
+    ct_forward_from<T, N, ST + 1, NT, B>(buf, tws);
+  }
+}
+template <typename T, int N, int ST, int NT, class B>
+__device__ __forceinline__ void ct_inverse_from(cplx<T>* buf, const cplx<T>* tws) {
+  if constexpr (ST >= 0) {
+    ct_stage<T, N, ct_ls(N, ST), ct_radix(N, ST), true, NT, B>(buf, tws);
+    __syncthreads();
+    ct_inverse_from<T, N, ST - 1, NT, B>(buf, tws);
+  }
+}
+// Forward DIF / inverse DIT of a batch; both end with __syncthreads().
+template <typename T, int N, int NT, class B>
+__device__ __forceinline__ void ct_forward(cplx<T>* buf, const cplx<T>* tws) {
+  ct_forward_from<T, N, 0, NT, B>(buf, tws);
+}
+template <typename T, int N, int NT, class B>
+__device__ __forceinline__ void ct_inverse(cplx<T>* buf, const cplx<T>* tws) {
+  ct_inverse_from<T, N, ct_nst(N) - 1, NT, B>(buf, tws);
 }
 
 }  // namespace fg

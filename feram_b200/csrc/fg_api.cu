@@ -22,14 +22,21 @@ using namespace fg;
 namespace {
 
 constexpr int kThreadsFFT = 512;
+constexpr int kThreadsZ = 256;
 constexpr int kThreadsElem = 256;
 
 int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// DIF stage radices, largest first (8, 4, 2, then 3 and 5).
+// DIF stage radices: the compile-time plans of fft_smem.cuh for powers of
+// two, otherwise largest first (8, 4, 2, then 3 and 5).
 bool make_plan(int n, FftPlan* P) {
   P->n = n;
   P->nst = 0;
+  if (ct_supported(n)) {
+    P->nst = ct_nst(n);
+    for (int st = 0; st < P->nst; ++st) P->r[st] = ct_radix(n, st);
+    return true;
+  }
   int m = n;
   while (m % 8 == 0) { P->r[P->nst++] = 8; m /= 8; }
   while (m % 4 == 0) { P->r[P->nst++] = 4; m /= 4; }
@@ -81,9 +88,7 @@ struct fg_ctx {
   std::string err;
   Geom g{};
   FftPlan px{}, py{}, pz{};
-  int cw = 8, ntx = 1;        // z tile of the MD k-space kernel
-  int cw6 = 8, ntx6 = 1;      // z tile of the table build (6 FP64 comps)
-  int cw1 = 8, ntx1 = 1;      // z tile of the modulation FFT (1 FP64 comp)
+  ZTiles zt{}, zt6{}, zt1{};  // z tiles: MD k-space (9 comps, T), table build (6, FP64), modulation (1, FP64)
   int smem_xy = 0, smem_xy64 = 0, smem_z = 0, smem_z3 = 0, smem_z6 = 0, smem_z1 = 0;
   int grid_elem = 1;
   cudaStream_t stream = nullptr;
@@ -182,6 +187,74 @@ int check_device_error(fg_ctx* ctx) {
   return FG_OK;
 }
 
+// ------------------------------------------------ FFT kernel dispatch
+// Compile-time instances for the cubic power-of-two supercells 16^3..128^3
+// (m = Lx/2, Ly) = (8,16) .. (64,128) and Lz = 16..128; the runtime-plan
+// kernels take every other size.
+template <typename T, int MODE, class F>
+void with_xy_fwd(int m, int Ly, F f) {
+  if (m == 64 && Ly == 128) f(k_xy_fwd<T, MODE, 64, 128>);
+  else if (m == 32 && Ly == 64) f(k_xy_fwd<T, MODE, 32, 64>);
+  else if (m == 16 && Ly == 32) f(k_xy_fwd<T, MODE, 16, 32>);
+  else if (m == 8 && Ly == 16) f(k_xy_fwd<T, MODE, 8, 16>);
+  else f(k_xy_fwd<T, MODE, 0, 0>);
+}
+template <typename T, class F>
+void with_xy_inv(int m, int Ly, F f) {
+  if (m == 64 && Ly == 128) f(k_xy_inv<T, 64, 128>);
+  else if (m == 32 && Ly == 64) f(k_xy_inv<T, 32, 64>);
+  else if (m == 16 && Ly == 32) f(k_xy_inv<T, 16, 32>);
+  else if (m == 8 && Ly == 16) f(k_xy_inv<T, 8, 16>);
+  else f(k_xy_inv<T, 0, 0>);
+}
+template <typename T>
+constexpr int z_cw_cap() { return sizeof(T) == 4 ? 8 : 4; }
+template <typename T, class F>
+void with_z_kspace(int Lz, int cw, F f) {
+  constexpr int C = z_cw_cap<T>();
+  if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C>);
+  else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C>);
+  else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C>);
+  else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C>);
+  else f(k_z_kspace<T, 0, 0>);
+}
+
+template <typename T, int MODE>
+int launch_xy_fwd(fg_ctx* ctx, const T* src, cplx<T>* spec, int ncomp, int smem, const cplx<T>* twx,
+                  const cplx<T>* twm, const cplx<T>* twy) {
+  const Geom& g = ctx->g;
+  with_xy_fwd<T, MODE>(g.m, g.Ly, [&](auto kern) {
+    kern<<<dim3(g.Lz, ncomp), kThreadsFFT, smem, ctx->stream>>>(src, spec, g, ctx->px, ctx->py, twx, twm, twy,
+                                                                 ctx->posm, 0);
+  });
+  CKL();
+  return FG_OK;
+}
+
+template <typename T>
+int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp) {
+  const Geom& g = ctx->g;
+  with_xy_inv<T>(g.m, g.Ly, [&](auto kern) {
+    kern<<<dim3(g.Lz, ncomp), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
+        spec, out, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy,
+        ctx->posm, 0);
+  });
+  CKL();
+  return FG_OK;
+}
+
+template <typename T>
+int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
+  const Geom& g = ctx->g;
+  with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto kern) {
+    kern<<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z, ctx->stream>>>(
+        (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
+        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt);
+  });
+  CKL();
+  return FG_OK;
+}
+
 // ----------------------------------------------------------- force pipeline
 template <typename T>
 int enqueue_force(fg_ctx* ctx) {
@@ -192,21 +265,14 @@ int enqueue_force(fg_ctx* ctx) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(u, g, ctx->P.gap_id);
     CKL();
   }
-  k_xy_fwd<T, SRC_U9><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
-      u, (cplx<T>*)ctx->spec, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm,
-      (const cplx<T>*)ctx->twy, ctx->posm, 0);
+  int rc;
+  if ((rc = launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
+                                     (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy)))
+    return rc;
+  if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
+  k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
   CKL();
-  k_z_kspace<T><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z, st>>>(
-      (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod,
-      ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr, g, ctx->pz, (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph,
-      ctx->part_k, ctx->sc, ctx->cw);
-  CKL();
-  k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->ntx * g.Ly);
-  CKL();
-  k_xy_inv<T><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
-      (const cplx<T>*)ctx->spec, (T*)ctx->rwork, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
-      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
-  CKL();
+  if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9))) return rc;
   k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
                                                          ctx->part_r);
   CKL();
@@ -385,31 +451,43 @@ int create_impl(fg_ctx* ctx) {
   ctx->smem_xy64 = (int)(sizeof(cplx<double>) * g.Ly * (g.m + 1));
   if (ctx->smem_xy > smem_max || ctx->smem_xy64 > smem_max)
     return fail(ctx, FG_ERR_UNSUPPORTED, "an x-y plane of the supercell does not fit in shared memory");
-  auto pick_cw = [&](int nc, size_t esz, int cwmax) {
+  // z tiles: CW is the largest power of two <= cwmax dividing Lx/2 whose
+  // tile fits in shared memory
+  auto tiles = [&](int nc, size_t esz, int cwmax) {
+    ZTiles t{};
     int cw = cwmax;
-    while (cw > 1 && (size_t)nc * g.Lz * cw * esz > (size_t)smem_max) cw /= 2;
-    return cw;
+    while (cw > 1 && (g.m % cw != 0 || (size_t)nc * g.Lz * cw * esz > (size_t)smem_max)) cw /= 2;
+    t.CW = cw;
+    t.ntx = g.m / cw;
+    t.nreg = t.ntx * g.Ly;
+    t.nnyq = div_up(g.Ly, cw);
+    return t;
   };
-  ctx->cw = pick_cw(9, sizeof(cplx<T>), sizeof(T) == 4 ? 16 : 8);
-  ctx->cw6 = pick_cw(6, sizeof(cplx<double>), 8);
-  ctx->cw1 = pick_cw(1, sizeof(cplx<double>), 8);
-  if ((size_t)9 * g.Lz * ctx->cw * sizeof(cplx<T>) > (size_t)smem_max)
+  ctx->zt = tiles(9, sizeof(cplx<T>), sizeof(T) == 4 ? 8 : 4);
+  ctx->zt6 = tiles(6, sizeof(cplx<double>), 8);
+  ctx->zt1 = tiles(1, sizeof(cplx<double>), 8);
+  if ((size_t)9 * g.Lz * ctx->zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
     return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
-  ctx->ntx = div_up(g.NKX, ctx->cw);
-  ctx->ntx6 = div_up(g.NKX, ctx->cw6);
-  ctx->ntx1 = div_up(g.NKX, ctx->cw1);
-  ctx->smem_z = (int)(9 * (size_t)g.Lz * ctx->cw * sizeof(cplx<T>));
-  ctx->smem_z3 = (int)(3 * (size_t)g.Lz * ctx->cw * sizeof(cplx<T>));
-  ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->cw6 * sizeof(cplx<double>));
-  ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->cw1 * sizeof(cplx<double>));
+  ctx->smem_z = (int)(9 * (size_t)g.Lz * ctx->zt.CW * sizeof(cplx<T>));
+  ctx->smem_z3 = (int)(3 * (size_t)g.Lz * ctx->zt.CW * sizeof(cplx<T>));
+  ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->zt6.CW * sizeof(cplx<double>));
+  ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->zt1.CW * sizeof(cplx<double>));
   ctx->grid_elem = std::max(1, std::min(div_up(g.nsite, kThreadsElem), nsm * 8));
-  CK(cudaFuncSetAttribute(k_xy_fwd<T, SRC_U9>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy));
-  CK(cudaFuncSetAttribute(k_xy_inv<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy));
-  CK(cudaFuncSetAttribute(k_z_kspace<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z));
-  CK(cudaFuncSetAttribute(k_xy_fwd<T, SRC_FIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy));
+  {
+    cudaError_t ea = cudaSuccess;
+    auto setattr = [&](auto kern, int bytes) {
+      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      if (e != cudaSuccess) ea = e;
+    };
+    with_xy_fwd<T, SRC_U9>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
+    with_xy_fwd<T, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
+    with_xy_fwd<double, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy64); });
+    with_xy_inv<T>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
+    with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto k) { setattr(k, ctx->smem_z); });
+    if (ea != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
+  }
   CK(cudaFuncSetAttribute(k_z_pass<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z3));
   CK(cudaFuncSetAttribute(k_z_pass<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z3));
-  CK(cudaFuncSetAttribute(k_xy_fwd<double, SRC_FIELD>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_xy64));
   CK(cudaFuncSetAttribute(k_z_ewald_pack<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z6));
   CK(cudaFuncSetAttribute(k_z_modulation_pack<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z1));
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
@@ -561,7 +639,7 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaMemset(ctx->ckmod, 0, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
   CK(cudaMalloc(&ctx->acouK, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
   CK(cudaMemset(ctx->acouK, 0, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
-  CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)ctx->ntx * g.Ly));
+  CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)(ctx->zt.nreg + ctx->zt.nnyq)));
   CK(cudaMalloc(&ctx->part_r, sizeof(double) * NQ_R * (size_t)ctx->grid_elem));
   CK(cudaMalloc(&ctx->part_ke, sizeof(double) * (size_t)ctx->grid_elem));
   CK(cudaMalloc(&ctx->part_avg, sizeof(double) * 6 * (size_t)ctx->grid_elem));
@@ -584,12 +662,12 @@ int build_tables_impl(fg_ctx* ctx) {
   const int max_x = 24 / P.Lx, max_y = 24 / P.Ly, max_z = 24 / P.Lz;  // dipole-dipole-long-range.F:98-100
   k_ewald_real<<<std::max(1, div_up(g.nsite, 128)), 128, 0, ctx->stream>>>(real6, g, P.a0, P.kappa, max_x, max_y, max_z);
   CKL();
-  k_xy_fwd<double, SRC_FIELD><<<dim3(g.Lz, 6), kThreadsFFT, ctx->smem_xy64, ctx->stream>>>(
-      real6, spec6, g, ctx->px, ctx->py, ctx->twx64, ctx->twm64, ctx->twy64, ctx->posm, 0);
-  CKL();
-  k_z_ewald_pack<T><<<dim3(ctx->ntx6, g.Ly), kThreadsFFT, ctx->smem_z6, ctx->stream>>>(
+  int rc0 = launch_xy_fwd<double, SRC_FIELD>(ctx, real6, spec6, 6, ctx->smem_xy64, ctx->twx64, ctx->twm64,
+                                             ctx->twy64);
+  if (rc0) return rc0;
+  k_z_ewald_pack<T><<<ctx->zt6.nreg + ctx->zt6.nnyq, kThreadsZ, ctx->smem_z6, ctx->stream>>>(
       spec6, (T*)ctx->dtab, ctx->L64, g, ctx->pz, ctx->twz64, kmaps<T>(ctx), ctx->ph, P.a0, P.kappa, P.epsilon_inf,
-      max_x, max_y, max_z, ctx->cw6);
+      max_x, max_y, max_z, ctx->zt6);
   CKL();
   CK(cudaStreamSynchronize(ctx->stream));
   cudaFree(real6);
@@ -611,11 +689,10 @@ int set_modulation_R_impl(fg_ctx* ctx, const double* modR) {
   CK(cudaMemcpyAsync(ctx->staging, modR, sizeof(double) * nin, cudaMemcpyHostToDevice, ctx->stream));
   k_fortran_to_soa<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(r1, ctx->staging, g, 1, ctx->NXP, ctx->NYP);
   CKL();
-  k_xy_fwd<double, SRC_FIELD><<<dim3(g.Lz, 1), kThreadsFFT, ctx->smem_xy64, ctx->stream>>>(
-      r1, s1, g, ctx->px, ctx->py, ctx->twx64, ctx->twm64, ctx->twy64, ctx->posm, 0);
-  CKL();
-  k_z_modulation_pack<T><<<dim3(ctx->ntx1, g.Ly), kThreadsFFT, ctx->smem_z1, ctx->stream>>>(
-      s1, (cplx<T>*)ctx->ckmod, g, ctx->pz, ctx->twz64, kmaps<T>(ctx), ctx->P.modulation_constant, ctx->cw1);
+  int rc0 = launch_xy_fwd<double, SRC_FIELD>(ctx, r1, s1, 1, ctx->smem_xy64, ctx->twx64, ctx->twm64, ctx->twy64);
+  if (rc0) return rc0;
+  k_z_modulation_pack<T><<<ctx->zt1.nreg + ctx->zt1.nnyq, kThreadsZ, ctx->smem_z1, ctx->stream>>>(
+      s1, (cplx<T>*)ctx->ckmod, g, ctx->pz, ctx->twz64, kmaps<T>(ctx), ctx->P.modulation_constant, ctx->zt1);
   CKL();
   CK(cudaStreamSynchronize(ctx->stream));
   cudaFree(r1);
@@ -747,12 +824,12 @@ int fft_r2c3_impl(fg_ctx* ctx, const double* in, double* out) {
   const Geom& g = ctx->g;
   int rc = set_field<T>(ctx, ctx->rwork, in);
   if (rc) return rc;
-  k_xy_fwd<T, SRC_FIELD><<<dim3(g.Lz, 3), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
-      (const T*)ctx->rwork, (cplx<T>*)ctx->spec, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
-      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
-  CKL();
-  k_z_pass<T, false><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z3, ctx->stream>>>(
-      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->cw);
+  if ((rc = launch_xy_fwd<T, SRC_FIELD>(ctx, (const T*)ctx->rwork, (cplx<T>*)ctx->spec, 3, ctx->smem_xy,
+                                        (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm,
+                                        (const cplx<T>*)ctx->twy)))
+    return rc;
+  k_z_pass<T, false><<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z3, ctx->stream>>>(
+      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->zt);
   CKL();
   std::vector<cplx<T>> S(3 * (size_t)g.ncplx);
   CK(cudaMemcpyAsync(S.data(), ctx->spec, S.size() * sizeof(cplx<T>), cudaMemcpyDeviceToHost, ctx->stream));
@@ -785,14 +862,12 @@ int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
           S[(size_t)c * g.ncplx + (size_t)zs * g.plane_c + (size_t)ys * g.KXP + col] = mk<cplx<T>>((T)in[2 * f], (T)in[2 * f + 1]);
         }
   CK(cudaMemcpyAsync(ctx->spec, S.data(), S.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, ctx->stream));
-  k_z_pass<T, true><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z3, ctx->stream>>>(
-      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->cw);
+  k_z_pass<T, true><<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z3, ctx->stream>>>(
+      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->zt);
   CKL();
-  k_xy_inv<T><<<dim3(g.Lz, 3), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
-      (const cplx<T>*)ctx->spec, (T*)ctx->rwork, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
-      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
-  CKL();
-  int rc = get_field<T>(ctx, out, ctx->rwork);
+  int rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 3);
+  if (rc) return rc;
+  rc = get_field<T>(ctx, out, ctx->rwork);
   if (rc) return rc;
   ctx->force_fresh = false;
   return check_device_error(ctx);
@@ -833,19 +908,14 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     CK(cudaEventRecord(ev[++k], st));
     k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(u, (const T*)ctx->p, &ctx->sc->drift_coef, g, ctx->layer_minv);
     CK(cudaEventRecord(ev[++k], st));
-    k_xy_fwd<T, SRC_U9><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
-        u, (cplx<T>*)ctx->spec, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm,
-        (const cplx<T>*)ctx->twy, ctx->posm, 0);
+    launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
+                             (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy);
     CK(cudaEventRecord(ev[++k], st));
-    k_z_kspace<T><<<dim3(ctx->ntx, g.Ly), kThreadsFFT, ctx->smem_z, st>>>(
-        (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, nullptr, g, ctx->pz,
-        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->cw);
+    launch_z_kspace<T>(ctx, nullptr);
     CK(cudaEventRecord(ev[++k], st));
-    k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->ntx * g.Ly);
+    k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
     CK(cudaEventRecord(ev[++k], st));
-    k_xy_inv<T><<<dim3(g.Lz, 9), kThreadsFFT, ctx->smem_xy, st>>>(
-        (const cplx<T>*)ctx->spec, (T*)ctx->rwork, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx,
-        (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy, ctx->posm, 0);
+    launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9);
     CK(cudaEventRecord(ev[++k], st));
     k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
                                                            ctx->part_r);

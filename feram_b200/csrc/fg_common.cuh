@@ -43,6 +43,17 @@ template <typename C, bool INV> __device__ __forceinline__ C mul_mi(C a) {
   return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
 }
 
+// Asynchronous global -> shared copies (cp.async, sm_80+): many copies in
+// flight per thread without register staging; complete with cp_async_wait().
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if (BYTES == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+  else if (BYTES == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+  else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Device error record (bounds checks, non-finite reductions).  The library
 // is one translation unit, so this __device__ variable has one definition.
 struct DevError {

@@ -142,44 +142,78 @@ enum { SRC_U9 = 0, SRC_FIELD = 1 };
 // pairs, unpack to the Lx/2+1 bins of the real transform, DIF along y.
 // SRC_U9: component c of (u_x, u_y, u_z, u_x^2, u_y^2, u_z^2, u_y u_z,
 // u_z u_x, u_x u_y) from u (dipoFFT.F:19-44).  SRC_FIELD: component c of src.
-template <typename T, int MODE>
-__global__ void __launch_bounds__(512) k_xy_fwd(const T* __restrict__ src, cplx<T>* __restrict__ spec, Geom g,
+// MC, LYC > 0 select the compile-time transforms for m = Lx/2 = MC and
+// Ly = LYC (launched with exactly kXYThreads threads); 0 = runtime plans.
+constexpr int kXYThreads = 512;
+
+template <typename T, int MC, int LYC>
+__device__ __forceinline__ void xy_twiddles_to_smem(cplx<T>* tm, cplx<T>* ty, cplx<T>* tx, const cplx<T>* twm,
+                                                    const cplx<T>* twy, const cplx<T>* twx) {
+  if constexpr (MC > 0) {
+    for (int i = threadIdx.x; i < MC; i += blockDim.x) tm[i] = twm[i];
+    for (int i = threadIdx.x; i < LYC; i += blockDim.x) ty[i] = twy[i];
+    for (int i = threadIdx.x; i <= MC; i += blockDim.x) tx[i] = twx[i];
+  }
+}
+
+template <typename T, int MODE, int MC = 0, int LYC = 0>
+__global__ void __launch_bounds__(512, 2) k_xy_fwd(const T* __restrict__ src, cplx<T>* __restrict__ spec, Geom g,
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int out_comp0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
   using T2 = typename RT2<T>::type;
   const int z = blockIdx.x, c = blockIdx.y;
-  const int m = g.m, RS = m + 1, Ly = g.Ly, Lx = g.Lx;
+  const int m = MC > 0 ? MC : g.m, Ly = LYC > 0 ? LYC : g.Ly;
+  const int RS = m + 1, Lx = 2 * m;
   const int buf_len = Ly * RS;
+  xy_twiddles_to_smem<T, MC, LYC>(tws_m, tws_y, tws_x, twm, twy, twx);
+  const cplx<T>* twx_u = MC > 0 ? tws_x : twx;
   const long long plane_off = (long long)z * g.plane_r;
-  for (int idx = threadIdx.x; idx < Ly * m; idx += blockDim.x) {
-    const int y = idx / m, jx = idx - y * m;
-    const long long o = plane_off + (long long)y * Lx + 2 * jx;
-    T2 v;
-    if (MODE == SRC_FIELD) {
-      v = *reinterpret_cast<const T2*>(src + (long long)c * g.nsite + o);
-    } else if (c < 3) {
-      v = *reinterpret_cast<const T2*>(src + (long long)c * g.nsite + o);
-    } else {
-      const T2 a = *reinterpret_cast<const T2*>(src + o);
-      const T2 b = *reinterpret_cast<const T2*>(src + g.nsite + o);
-      const T2 d = *reinterpret_cast<const T2*>(src + 2 * g.nsite + o);
-      switch (c) {
-        case 3: v.x = a.x * a.x; v.y = a.y * a.y; break;
-        case 4: v.x = b.x * b.x; v.y = b.y * b.y; break;
-        case 5: v.x = d.x * d.x; v.y = d.y * d.y; break;
-        case 6: v.x = b.x * d.x; v.y = b.y * d.y; break;
-        case 7: v.x = d.x * a.x; v.y = d.y * a.y; break;
-        default: v.x = a.x * b.x; v.y = a.y * b.y; break;
+  const int total = Ly * m;
+  if (MODE == SRC_FIELD || c < 3) {
+    // plain component: asynchronous copies of packed (x even, x odd) pairs
+    const T* sp = src + (long long)c * g.nsite + plane_off;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+      const int y = idx / m, jx = idx - y * m;
+      cp_async<(int)sizeof(cplx<T>)>(&buf[y * RS + jx], sp + (long long)y * Lx + 2 * jx);
+    }
+    cp_async_wait();
+  } else {
+    // products: kLB independent loads in flight per thread, then compute
+    constexpr int kLB = 4;
+    for (int base = threadIdx.x; base < total; base += kLB * blockDim.x) {
+      T2 va[kLB], vb[kLB];
+#pragma unroll
+      for (int r = 0; r < kLB; ++r) {
+        const int idx = base + r * blockDim.x;
+        if (idx < total) {
+          const int y = idx / m, jx = idx - y * m;
+          const long long o = plane_off + (long long)y * Lx + 2 * jx;
+          const int ca = (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
+          const int cb = (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
+          va[r] = *reinterpret_cast<const T2*>(src + (long long)ca * g.nsite + o);
+          vb[r] = *reinterpret_cast<const T2*>(src + (long long)cb * g.nsite + o);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < kLB; ++r) {
+        const int idx = base + r * blockDim.x;
+        if (idx < total) {
+          const int y = idx / m, jx = idx - y * m;
+          buf[y * RS + jx] = mk<cplx<T>>(va[r].x * vb[r].x, va[r].y * vb[r].y);
+        }
       }
     }
-    buf[y * RS + jx] = mk<cplx<T>>(v.x, v.y);
   }
   __syncthreads();
-  {
-    Batch B{Ly, 1, 0, RS, 1, false};
+  // X pass; row stride RS = m+1 keeps the row-interleaved mapping bank-conflict free
+  if constexpr (MC > 0) {
+    ct_forward<T, MC, kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
+  } else {
+    Batch B{Ly, 1, 0, RS, 1, true};
     fft_forward<T>(buf, B, px, twm, buf_len);
   }
   // unpack: slot posm[k] holds Z(k) of the packed row; X(k) = E(k) + w^k O(k)
@@ -195,7 +229,7 @@ __global__ void __launch_bounds__(512) k_xy_fwd(const T* __restrict__ src, cplx<
       const int k2 = m - k;
       const int s1 = __ldg(&posm[k]), s2 = __ldg(&posm[k2]);
       const cplx<T> a = row[s1], b = row[s2];
-      const cplx<T> w1 = __ldg(&twx[k]), w2 = __ldg(&twx[k2]);
+      const cplx<T> w1 = twx_u[k], w2 = twx_u[k2];
       // X(k) = 1/2 (a + conj b) - i/2 w1 (a - conj b)
       const cplx<T> e1 = mk<cplx<T>>(a.x + b.x, a.y - b.y), d1 = mk<cplx<T>>(a.x - b.x, a.y + b.y);
       const cplx<T> wd1 = cmul(w1, d1);
@@ -208,7 +242,9 @@ __global__ void __launch_bounds__(512) k_xy_fwd(const T* __restrict__ src, cplx<
     }
   }
   __syncthreads();
-  {
+  if constexpr (MC > 0) {
+    ct_forward<T, LYC, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+  } else {
     Batch B{RS, RS, 1, 0, RS, true};
     fft_forward<T>(buf, B, py, twy, buf_len);
   }
@@ -224,24 +260,31 @@ __global__ void __launch_bounds__(512) k_xy_fwd(const T* __restrict__ src, cplx<
 // complex pairs (imaginary parts of the kx = 0 and kx = Lx/2 bins dropped,
 // the half-complex convention of the reference's c2r), DIT along x, store
 // the real plane.  Output is unnormalised (Lx*Ly*Lz times the IDFT).
-template <typename T>
-__global__ void __launch_bounds__(512) k_xy_inv(const cplx<T>* __restrict__ spec, T* __restrict__ out, Geom g,
+template <typename T, int MC = 0, int LYC = 0>
+__global__ void __launch_bounds__(512, 2) k_xy_inv(const cplx<T>* __restrict__ spec, T* __restrict__ out, Geom g,
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int in_comp0) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
   using T2 = typename RT2<T>::type;
   const int z = blockIdx.x, c = blockIdx.y;
-  const int m = g.m, RS = m + 1, Ly = g.Ly, Lx = g.Lx;
+  const int m = MC > 0 ? MC : g.m, Ly = LYC > 0 ? LYC : g.Ly;
+  const int RS = m + 1, Lx = 2 * m;
   const int buf_len = Ly * RS;
+  xy_twiddles_to_smem<T, MC, LYC>(tws_m, tws_y, tws_x, twm, twy, twx);
+  const cplx<T>* twx_u = MC > 0 ? tws_x : twx;
   const cplx<T>* srcp = spec + (long long)(in_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
   for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
     const int y = idx / RS, col = idx - y * RS;
-    buf[idx] = srcp[(long long)y * g.KXP + col];
+    cp_async<(int)sizeof(cplx<T>)>(&buf[idx], srcp + (long long)y * g.KXP + col);
   }
+  cp_async_wait();
   __syncthreads();
-  {
+  if constexpr (MC > 0) {
+    ct_inverse<T, LYC, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+  } else {
     Batch B{RS, RS, 1, 0, RS, true};
     fft_inverse<T>(buf, B, py, twy, buf_len);
   }
@@ -256,7 +299,7 @@ __global__ void __launch_bounds__(512) k_xy_inv(const cplx<T>* __restrict__ spec
       const int k2 = m - k;
       const int s1 = __ldg(&posm[k]), s2 = __ldg(&posm[k2]);
       const cplx<T> a = row[s1], b = row[s2];
-      const cplx<T> w1 = __ldg(&twx[k]), w2 = __ldg(&twx[k2]);
+      const cplx<T> w1 = twx_u[k], w2 = twx_u[k2];
       // Z(k) = (a + conj b) + i conj(w1) (a - conj b)
       const cplx<T> e1 = mk<cplx<T>>(a.x + b.x, a.y - b.y), d1 = mk<cplx<T>>(a.x - b.x, a.y + b.y);
       const cplx<T> wd1 = cmulc(d1, w1);
@@ -269,8 +312,10 @@ __global__ void __launch_bounds__(512) k_xy_inv(const cplx<T>* __restrict__ spec
     }
   }
   __syncthreads();
-  {
-    Batch B{Ly, 1, 0, RS, 1, false};
+  if constexpr (MC > 0) {
+    ct_inverse<T, MC, kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
+  } else {
+    Batch B{Ly, 1, 0, RS, 1, true};
     fft_inverse<T>(buf, B, px, twm, buf_len);
   }
   T* dst = out + (long long)c * g.nsite + (long long)z * g.plane_r;
@@ -285,34 +330,57 @@ __global__ void __launch_bounds__(512) k_xy_inv(const cplx<T>* __restrict__ spec
 }
 
 // ------------------------------------------------- z tiles (shared helpers)
-// A tile is CW consecutive kx slots of one ky slot, all z, nc components,
-// held in shared memory as buf[c][z][cw].
+// A z tile is CW pencils (kx slot, ky slot) with all z, nc components, held
+// in shared memory as buf[c][z][cw].  Blocks [0, nreg) take CW consecutive kx
+// slots of one ky slot (CW divides Lx/2); blocks [nreg, nreg + nnyq) take
+// the Nyquist slot kx = Lx/2 of CW consecutive ky slots.
+struct ZTiles {
+  int CW;
+  int ntx;   // regular tiles per ky slot (= (Lx/2) / CW)
+  int nreg;  // ntx * Ly
+  int nnyq;  // ceil(Ly / CW)
+};
+
+__device__ __forceinline__ bool tile_pencil(const ZTiles& zt, const Geom& g, int cw, int* col, int* yslot) {
+  const int b = blockIdx.x;
+  if (b < zt.nreg) {
+    *yslot = b / zt.ntx;
+    *col = (b - *yslot * zt.ntx) * zt.CW + cw;
+    return true;
+  }
+  *col = g.m;
+  *yslot = (b - zt.nreg) * zt.CW + cw;
+  return *yslot < g.Ly;
+}
+
 template <typename T>
-__device__ void z_tile_load(cplx<T>* buf, const cplx<T>* __restrict__ spec, const Geom& g, int nc, int CW, int col0,
-                            int yslot) {
-  const int Lz = g.Lz;
+__device__ void z_tile_load(cplx<T>* buf, const cplx<T>* __restrict__ spec, const Geom& g, const ZTiles& zt, int nc) {
+  const int Lz = g.Lz, CW = zt.CW;
   const int n = nc * Lz * CW;
   for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
     const int c = idx / (Lz * CW), rem = idx - c * Lz * CW;
     const int z = rem / CW, cw = rem - z * CW;
-    const int col = col0 + cw;
-    cplx<T> v = mk<cplx<T>>((T)0, (T)0);
-    if (col < g.NKX) v = spec[(long long)c * g.ncplx + (long long)z * g.plane_c + (long long)yslot * g.KXP + col];
-    buf[idx] = v;
+    int col, yslot;
+    if (tile_pencil(zt, g, cw, &col, &yslot))
+      cp_async<(int)sizeof(cplx<T>)>(&buf[idx], spec + (long long)c * g.ncplx + (long long)z * g.plane_c +
+                                                     (long long)yslot * g.KXP + col);
+    else
+      buf[idx] = mk<cplx<T>>((T)0, (T)0);
   }
+  cp_async_wait();
   __syncthreads();
 }
 
 template <typename T>
-__device__ void z_tile_store(const cplx<T>* buf, cplx<T>* __restrict__ spec, const Geom& g, int nc, int CW, int col0,
-                             int yslot) {
-  const int Lz = g.Lz;
+__device__ void z_tile_store(const cplx<T>* buf, cplx<T>* __restrict__ spec, const Geom& g, const ZTiles& zt, int nc) {
+  const int Lz = g.Lz, CW = zt.CW;
   const int n = nc * Lz * CW;
   for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
     const int c = idx / (Lz * CW), rem = idx - c * Lz * CW;
     const int z = rem / CW, cw = rem - z * CW;
-    const int col = col0 + cw;
-    if (col < g.NKX) spec[(long long)c * g.ncplx + (long long)z * g.plane_c + (long long)yslot * g.KXP + col] = buf[idx];
+    int col, yslot;
+    if (tile_pencil(zt, g, cw, &col, &yslot))
+      spec[(long long)c * g.ncplx + (long long)z * g.plane_c + (long long)yslot * g.KXP + col] = buf[idx];
   }
 }
 
@@ -331,16 +399,16 @@ struct KMaps {
 
 // Plain z pass of nc spectra in place: DIF (INV = false) or DIT (INV = true).
 template <typename T, bool INV>
-__global__ void __launch_bounds__(512) k_z_pass(cplx<T>* __restrict__ spec, Geom g, FftPlan pz,
-                                                const cplx<T>* __restrict__ twz, int nc, int CW) {
+__global__ void __launch_bounds__(256) k_z_pass(cplx<T>* __restrict__ spec, Geom g, FftPlan pz,
+                                                const cplx<T>* __restrict__ twz, int nc, ZTiles zt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
-  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
-  z_tile_load<T>(buf, spec, g, nc, CW, col0, yslot);
+  const int CW = zt.CW;
+  z_tile_load<T>(buf, spec, g, zt, nc);
   Batch B{nc * CW, CW, 1, g.Lz * CW, CW, true};
   if (INV) fft_inverse<T>(buf, B, pz, twz, nc * g.Lz * CW);
   else fft_forward<T>(buf, B, pz, twz, nc * g.Lz * CW);
-  z_tile_store<T>(buf, spec, g, nc, CW, col0, yslot);
+  z_tile_store<T>(buf, spec, g, zt, nc);
 }
 
 // ------------------------------------------------------------------ k_z_kspace
@@ -352,31 +420,39 @@ __global__ void __launch_bounds__(512) k_z_pass(cplx<T>* __restrict__ spec, Geom
 // (elastic.F:79-180), and the half-spectrum energy sums of
 // dVddi-dipole-dipole.F:226-250 (by Parseval) and energy_module.F:150-240;
 // then DIT along z.  Slots 0..2 return F(k), slots 3..8 inhoK(k).
-template <typename T>
-__global__ void __launch_bounds__(512) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
-                                                  const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
-                                                  Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
-                                                  const Phys* __restrict__ ph, double* __restrict__ part,
-                                                  DevScalars* __restrict__ sc, int CW) {
+// LZC, CWC > 0 select the compile-time z transforms (launched with exactly
+// kZThreads threads); 0 = runtime plan and tile width.
+constexpr int kZThreads = 256;
+
+template <typename T, int LZC = 0, int CWC = 0>
+__global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
+                                                     const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
+                                                     Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
+                                                     const Phys* __restrict__ ph, double* __restrict__ part,
+                                                     DevScalars* __restrict__ sc, ZTiles zt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
-  const int Lz = g.Lz;
-  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
+  __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
+  const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
   const int buf_len = 9 * Lz * CW;
-  z_tile_load<T>(buf, spec, g, 9, CW, col0, yslot);
-  {
+  if constexpr (LZC > 0)
+    for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws_z[i] = twz[i];
+  z_tile_load<T>(buf, spec, g, zt, 9);
+  if constexpr (LZC > 0) {
+    ct_forward<T, LZC, kZThreads, BatchCT<9 * CWC, CWC, 1, LZC * CWC, CWC>>(buf, tws_z);
+  } else {
     Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
     fft_forward<T>(buf, B, pz, twz, buf_len);
   }
   const double Ninv = ph->Ninv;
-  const int ky = __ldg(&km.revy[yslot]);
-  const double kv2 = __ldg(&km.kvy[ky]);
-  const double2 ty = __ldg(&km.try_[ky]);
   double acc[NQ_K] = {0, 0, 0, 0, 0};
   for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
     const int zs = idx / CW, cw = idx - zs * CW;
-    const int col = col0 + cw;
-    if (col >= g.NKX) continue;
+    int col, yslot;
+    if (!tile_pencil(zt, g, cw, &col, &yslot)) continue;
+    const int ky = __ldg(&km.revy[yslot]);
+    const double kv2 = __ldg(&km.kvy[ky]);
+    const double2 ty = __ldg(&km.try_[ky]);
     const int kx = __ldg(&km.revx[col]), kz = __ldg(&km.revz[zs]);
     const double w1 = (kx == 0 || kx == g.m) ? 1.0 : 2.0;  // full-spectrum multiplicity
     cplx<T> u[3], d[6];
@@ -530,12 +606,14 @@ __global__ void __launch_bounds__(512) k_z_kspace(cplx<T>* __restrict__ spec, co
     for (int i = 0; i < 6; ++i) buf[((3 + i) * Lz + zs) * CW + cw] = d[i];
   }
   __syncthreads();
-  {
+  if constexpr (LZC > 0) {
+    ct_inverse<T, LZC, kZThreads, BatchCT<9 * CWC, CWC, 1, LZC * CWC, CWC>>(buf, tws_z);
+  } else {
     Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
     fft_inverse<T>(buf, B, pz, twz, buf_len);
   }
-  z_tile_store<T>(buf, spec, g, 9, CW, col0, yslot);
-  block_partials<NQ_K>(acc, part, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+  z_tile_store<T>(buf, spec, g, zt, 9);
+  block_partials<NQ_K>(acc, part, blockIdx.x);
 }
 
 // ------------------------------------------------------------------ k_assemble
@@ -960,16 +1038,15 @@ __global__ void k_ewald_real(double* __restrict__ out, Geom g, double a0, double
 // (dipole-dipole-long-range.F:151-206), D = (S + Z*^2 L)/N in the table
 // layout, and L in FP64 for inspection.
 template <typename T>
-__global__ void __launch_bounds__(512) k_z_ewald_pack(const cplx<double>* __restrict__ spec, T* __restrict__ dtab,
+__global__ void __launch_bounds__(256) k_z_ewald_pack(const cplx<double>* __restrict__ spec, T* __restrict__ dtab,
                                                       double* __restrict__ L64, Geom g, FftPlan pz,
                                                       const cplx<double>* __restrict__ twz, KMaps km,
                                                       const Phys* __restrict__ ph, double a0, double kappa,
-                                                      double eps_inf, int max_x, int max_y, int max_z, int CW) {
+                                                      double eps_inf, int max_x, int max_y, int max_z, ZTiles zt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem_raw);
-  const int Lz = g.Lz;
-  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
-  z_tile_load<double>(buf, spec, g, 6, CW, col0, yslot);
+  const int Lz = g.Lz, CW = zt.CW;
+  z_tile_load<double>(buf, spec, g, zt, 6);
   {
     Batch B{6 * CW, CW, 1, Lz * CW, CW, true};
     fft_forward<double>(buf, B, pz, twz, 6 * Lz * CW);
@@ -979,11 +1056,11 @@ __global__ void __launch_bounds__(512) k_z_ewald_pack(const cplx<double>* __rest
   const double two_pi_over_a = 2 * pi / a0;
   const double four_kappa2 = 4 * kappa * kappa;
   const double scale = 14.399644 / eps_inf;  // HARTREE_BOHR (define.h:32)
-  const int ky = km.revy[yslot];
   for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
     const int zs = idx / CW, cw = idx - zs * CW;
-    const int col = col0 + cw;
-    if (col >= g.NKX) continue;
+    int col, yslot;
+    if (!tile_pencil(zt, g, cw, &col, &yslot)) continue;
+    const int ky = km.revy[yslot];
     const int kx = km.revx[col], kz = km.revz[zs];
     double k[3];
     k[2] = (double)kz / g.Lz;
@@ -1026,23 +1103,22 @@ __global__ void __launch_bounds__(512) k_z_ewald_pack(const cplx<double>* __rest
 
 // c_k_modulation_k = modulation_constant * k * r2c(modulation_R) (elastic.F:212-225)
 template <typename T>
-__global__ void __launch_bounds__(512) k_z_modulation_pack(const cplx<double>* __restrict__ spec, cplx<T>* __restrict__ ck,
+__global__ void __launch_bounds__(256) k_z_modulation_pack(const cplx<double>* __restrict__ spec, cplx<T>* __restrict__ ck,
                                                            Geom g, FftPlan pz, const cplx<double>* __restrict__ twz,
-                                                           KMaps km, double mod_const, int CW) {
+                                                           KMaps km, double mod_const, ZTiles zt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem_raw);
-  const int Lz = g.Lz;
-  const int col0 = blockIdx.x * CW, yslot = blockIdx.y;
-  z_tile_load<double>(buf, spec, g, 1, CW, col0, yslot);
+  const int Lz = g.Lz, CW = zt.CW;
+  z_tile_load<double>(buf, spec, g, zt, 1);
   {
     Batch B{CW, CW, 1, Lz * CW, CW, true};
     fft_forward<double>(buf, B, pz, twz, Lz * CW);
   }
-  const int ky = km.revy[yslot];
   for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
     const int zs = idx / CW, cw = idx - zs * CW;
-    const int col = col0 + cw;
-    if (col >= g.NKX) continue;
+    int col, yslot;
+    if (!tile_pencil(zt, g, cw, &col, &yslot)) continue;
+    const int ky = km.revy[yslot];
     const int kx = km.revx[col], kz = km.revz[zs];
     const double kv[3] = {km.kvx[kx], km.kvy[ky], km.kvz[kz]};
     const cplx<double> mk_ = buf[zs * CW + cw];
