@@ -131,6 +131,7 @@ struct fg_ctx {
   double* part_r = nullptr;
   double* part_ke = nullptr;
   double* part_avg = nullptr;
+  unsigned int* done = nullptr;   // last-block tickets: [0] kicks, [1] z k-space, [2] assemble
   double* avg6 = nullptr;
   double* staging = nullptr;      // padded Fortran-layout FP64 (3 components)
   size_t staging_n = 0;
@@ -249,7 +250,7 @@ int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
   with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto kern) {
     kern<<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z, ctx->stream>>>(
         (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
-        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt);
+        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, ctx->done + 1);
   });
   CKL();
   return FG_OK;
@@ -257,7 +258,7 @@ int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
 
 // ----------------------------------------------------------- force pipeline
 template <typename T>
-int enqueue_force(fg_ctx* ctx) {
+int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   T* u = (T*)ctx->u;
@@ -270,13 +271,9 @@ int enqueue_force(fg_ctx* ctx) {
                                      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy)))
     return rc;
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
-  k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
-  CKL();
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9))) return rc;
   k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
-                                                         ctx->part_r);
-  CKL();
-  k_force_energies<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_r, ctx->grid_elem);
+                                                         ctx->part_r, np_post ? TAIL_NP_POST : 1, ctx->done + 2);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
@@ -286,9 +283,10 @@ int enqueue_force(fg_ctx* ctx) {
 }
 
 template <typename T>
-int enqueue_kick(fg_ctx* ctx, const double* coef) {
+int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE) {
   k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (const T*)ctx->F, coef, ctx->g,
-                                                               ctx->layer_minv, ctx->layer_sump, ctx->part_ke);
+                                                               ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail,
+                                                               ctx->done, ctx->ph, ctx->sc);
   CKL();
   return FG_OK;
 }
@@ -301,20 +299,15 @@ int enqueue_drift(fg_ctx* ctx, const double* coef) {
   return FG_OK;
 }
 
-// nose_poincare (nose-poincare.F:24-75)
+// nose_poincare (nose-poincare.F:24-75): the scalar steps (38), (35c), (35e)
+// and the closing KE/H_NP run in the last block of the preceding kernel.
 template <typename T>
 int enqueue_np(fg_ctx* ctx) {
   int rc;
-  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef))) return rc;  // (35a)
-  k_np_pre<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
-  CKL();
-  if ((rc = enqueue_drift<T>(ctx, &ctx->sc->drift_coef))) return rc;  // (35d)
-  if ((rc = enqueue_force<T>(ctx))) return rc;
-  k_np_post<<<1, 32, 0, ctx->stream>>>(ctx->ph, ctx->sc);
-  CKL();
-  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef))) return rc;  // (35f)
-  k_np_final<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
-  CKL();
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_PRE))) return rc;  // (35a)
+  if ((rc = enqueue_drift<T>(ctx, &ctx->sc->drift_coef))) return rc;              // (35d)
+  if ((rc = enqueue_force<T>(ctx, true))) return rc;
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL))) return rc;  // (35f)
   return FG_OK;
 }
 
@@ -324,9 +317,7 @@ int enqueue_lf(fg_ctx* ctx) {
   int rc;
   if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
   if ((rc = enqueue_force<T>(ctx))) return rc;
-  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->lf_dt))) return rc;
-  k_lf_final<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
-  CKL();
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->lf_dt, TAIL_LF_FINAL))) return rc;
   return FG_OK;
 }
 
@@ -644,6 +635,8 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaMalloc(&ctx->part_ke, sizeof(double) * (size_t)ctx->grid_elem));
   CK(cudaMalloc(&ctx->part_avg, sizeof(double) * 6 * (size_t)ctx->grid_elem));
   CK(cudaMalloc(&ctx->avg6, sizeof(double) * 6));
+  CK(cudaMalloc(&ctx->done, sizeof(unsigned int) * 4));
+  CK(cudaMemset(ctx->done, 0, sizeof(unsigned int) * 4));
   ctx->staging_n = (size_t)3 * ctx->NXP * ctx->NYP * P.Lz;
   CK(cudaMalloc(&ctx->staging, sizeof(double) * ctx->staging_n));
   CK(cudaMemset(ctx->staging, 0, sizeof(double) * ctx->staging_n));
@@ -886,48 +879,35 @@ int force_now(fg_ctx* ctx) {
   return FG_OK;
 }
 
-const char* kProfNames[FG_NPROF] = {"k_kick(35a)", "k_np_pre", "k_drift", "k_xy_fwd", "k_z_kspace",
-                                           "k_homo_strain", "k_xy_inv", "k_assemble", "k_force_energies",
-                                           "k_np_post", "k_kick(35f)", "k_np_final"};
+const char* kProfNames[FG_NPROF] = {"k_kick(35a)+np_pre", "k_drift", "k_xy_fwd", "k_z_kspace+homo_strain",
+                                    "k_xy_inv", "k_assemble+energies+np_post", "k_kick(35f)+np_final"};
 
 template <typename T>
 int profile_impl(fg_ctx* ctx, int reps, double* ms) {
-  const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   cudaEvent_t ev[FG_NPROF + 1];
   for (auto& e : ev) CK(cudaEventCreate(&e));
   for (int k = 0; k < FG_NPROF; ++k) ms[k] = 0.0;
   T* u = (T*)ctx->u;
-  for (int r = 0; r < reps; ++r) {
+  int rc = FG_OK;
+  for (int r = 0; r < reps && rc == FG_OK; ++r) {
     int k = 0;
     CK(cudaEventRecord(ev[k], st));
-    k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->p, (const T*)ctx->F, &ctx->sc->kick_coef, g,
-                                                       ctx->layer_minv, ctx->layer_sump, ctx->part_ke);
+    rc |= enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_PRE);
     CK(cudaEventRecord(ev[++k], st));
-    k_np_pre<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+    rc |= enqueue_drift<T>(ctx, &ctx->sc->drift_coef);
     CK(cudaEventRecord(ev[++k], st));
-    k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(u, (const T*)ctx->p, &ctx->sc->drift_coef, g, ctx->layer_minv);
+    rc |= launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
+                                   (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy);
     CK(cudaEventRecord(ev[++k], st));
-    launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
-                             (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy);
+    rc |= launch_z_kspace<T>(ctx, nullptr);
     CK(cudaEventRecord(ev[++k], st));
-    launch_z_kspace<T>(ctx, nullptr);
+    rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9);
     CK(cudaEventRecord(ev[++k], st));
-    k_homo_strain<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
+    k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph,
+                                                           ctx->sc, ctx->part_r, TAIL_NP_POST, ctx->done + 2);
     CK(cudaEventRecord(ev[++k], st));
-    launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9);
-    CK(cudaEventRecord(ev[++k], st));
-    k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
-                                                           ctx->part_r);
-    CK(cudaEventRecord(ev[++k], st));
-    k_force_energies<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_r, ctx->grid_elem);
-    CK(cudaEventRecord(ev[++k], st));
-    k_np_post<<<1, 32, 0, st>>>(ctx->ph, ctx->sc);
-    CK(cudaEventRecord(ev[++k], st));
-    k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->p, (const T*)ctx->F, &ctx->sc->kick_coef, g,
-                                                       ctx->layer_minv, ctx->layer_sump, ctx->part_ke);
-    CK(cudaEventRecord(ev[++k], st));
-    k_np_final<<<1, RED_THREADS, 0, st>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
+    rc |= enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL);
     CK(cudaEventRecord(ev[++k], st));
     CKL();
     CK(cudaEventSynchronize(ev[FG_NPROF]));
@@ -938,7 +918,7 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     }
   }
   for (auto& e : ev) cudaEventDestroy(e);
-  return FG_OK;
+  return rc;
 }
 
 }  // namespace
@@ -979,7 +959,7 @@ void fg_destroy(fg_ctx* ctx) {
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->revx,
                   ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
-                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg};
+                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->sc_host) cudaFreeHost(ctx->sc_host);
@@ -1148,9 +1128,9 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
   if (i_step == 0) {  // leapfrog.F:89-102
     if ((rc = force_now(ctx))) return rc;
     const bool f32 = ctx->prec == FG_PREC_MIXED;
-    if ((rc = f32 ? enqueue_kick<float>(ctx, &ctx->sc->lf_dt_2) : enqueue_kick<double>(ctx, &ctx->sc->lf_dt_2))) return rc;
-    k_lf_final<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
-    CKL();
+    if ((rc = f32 ? enqueue_kick<float>(ctx, &ctx->sc->lf_dt_2, TAIL_LF_FINAL)
+                  : enqueue_kick<double>(ctx, &ctx->sc->lf_dt_2, TAIL_LF_FINAL)))
+      return rc;
   } else {
     if ((rc = run_graph(ctx, &ctx->g_lf, 2))) return rc;
   }

@@ -105,7 +105,7 @@ __device__ void block_partials(double* v, double* part, long long blockid) {
 __device__ double reduce_partials(const double* part, int nblk, int NQ, int q) {
   __shared__ double red[RED_THREADS];
   double s = 0.0;
-  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[(long long)b * NQ + q];
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(&part[(long long)b * NQ + q]);
   red[threadIdx.x] = s;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
@@ -115,6 +115,24 @@ __device__ double reduce_partials(const double* part, int nblk, int NQ, int q) {
   double r = red[0];
   __syncthreads();
   return r;
+}
+
+// Last-block-done: every block fences its writes and takes a ticket; the
+// block drawing the last ticket sees all of them and finishes the grid-wide
+// work (classic threadfence reduction, no waiting).  The counter is reset
+// for the next launch by that block.
+__device__ __forceinline__ bool is_last_block(unsigned int* counter) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned t = atomicAdd(counter, 1u);
+    last = (t == gridDim.x - 1);
+    if (last) *counter = 0u;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
 }
 
 // ------------------------------------------------------- analytic short range
@@ -353,35 +371,220 @@ __device__ __forceinline__ bool tile_pencil(const ZTiles& zt, const Geom& g, int
   return *yslot < g.Ly;
 }
 
-template <typename T>
-__device__ void z_tile_load(cplx<T>* buf, const cplx<T>* __restrict__ spec, const Geom& g, const ZTiles& zt, int nc) {
-  const int Lz = g.Lz, CW = zt.CW;
-  const int n = nc * Lz * CW;
-  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-    const int c = idx / (Lz * CW), rem = idx - c * Lz * CW;
-    const int z = rem / CW, cw = rem - z * CW;
-    int col, yslot;
-    if (tile_pencil(zt, g, cw, &col, &yslot))
-      cp_async<(int)sizeof(cplx<T>)>(&buf[idx], spec + (long long)c * g.ncplx + (long long)z * g.plane_c +
-                                                     (long long)yslot * g.KXP + col);
-    else
-      buf[idx] = mk<cplx<T>>((T)0, (T)0);
+// Threads own a fixed pencil cw = threadIdx.x % CW (blockDim is a multiple
+// of CW) and walk the tile rows r = c * Lz + z, so the pencil decode runs
+// once per thread and a row step is an add.  buf[r * CW + cw].
+template <typename T, int LZC = 0, int CWC = 0>
+__device__ __forceinline__ void z_tile_load(cplx<T>* buf, const cplx<T>* __restrict__ spec, const Geom& g,
+                                            const ZTiles& zt, int nc) {
+  const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
+  const int cw = threadIdx.x % CW, rstep = blockDim.x / CW;
+  int col, yslot;
+  const bool valid = tile_pencil(zt, g, cw, &col, &yslot);
+  const cplx<T>* base = spec + (valid ? (long long)yslot * g.KXP + col : 0);
+  for (int r = threadIdx.x / CW; r < nc * Lz; r += rstep) {
+    const int c = r / Lz, z = r - c * Lz;
+    cplx<T>* dst = &buf[r * CW + cw];
+    if (valid) cp_async<(int)sizeof(cplx<T>)>(dst, base + (long long)c * g.ncplx + (long long)z * g.plane_c);
+    else *dst = mk<cplx<T>>((T)0, (T)0);
   }
   cp_async_wait();
   __syncthreads();
 }
 
-template <typename T>
-__device__ void z_tile_store(const cplx<T>* buf, cplx<T>* __restrict__ spec, const Geom& g, const ZTiles& zt, int nc) {
-  const int Lz = g.Lz, CW = zt.CW;
-  const int n = nc * Lz * CW;
-  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-    const int c = idx / (Lz * CW), rem = idx - c * Lz * CW;
-    const int z = rem / CW, cw = rem - z * CW;
-    int col, yslot;
-    if (tile_pencil(zt, g, cw, &col, &yslot))
-      spec[(long long)c * g.ncplx + (long long)z * g.plane_c + (long long)yslot * g.KXP + col] = buf[idx];
+template <typename T, int LZC = 0, int CWC = 0>
+__device__ __forceinline__ void z_tile_store(const cplx<T>* buf, cplx<T>* __restrict__ spec, const Geom& g,
+                                             const ZTiles& zt, int nc) {
+  const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
+  const int cw = threadIdx.x % CW, rstep = blockDim.x / CW;
+  int col, yslot;
+  if (!tile_pencil(zt, g, cw, &col, &yslot)) return;
+  cplx<T>* base = spec + (long long)yslot * g.KXP + col;
+  for (int r = threadIdx.x / CW; r < nc * Lz; r += rstep) {
+    const int c = r / Lz, z = r - c * Lz;
+    base[(long long)c * g.ncplx + (long long)z * g.plane_c] = buf[r * CW + cw];
   }
+}
+
+// ------------------------------------------------------------ scalar kernels
+// Grid-wide scalar steps; each runs either as a single-block kernel or in the
+// last block of the kernel whose partial sums it reduces (tail).
+enum { TAIL_NONE = 0, TAIL_NP_PRE = 1, TAIL_NP_FINAL = 2, TAIL_LF_FINAL = 3, TAIL_NP_POST = 4 };
+
+__device__ __forceinline__ double sum_potential(const double* e) {
+  return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
+}
+
+__device__ __forceinline__ void np_hamiltonian(const Phys* ph, DevScalars* sc) {  // energy_module.F:128-148
+  double* e = sc->e;
+  const double s = sc->s;
+  double h = e[E_DIPO] / (s * s) + sum_potential(e) + sc->pi * sc->pi / 2 / ph->Q + ph->threeN_kT * log(s) - sc->H0;
+  e[E_HNP] = h * s;
+}
+
+__device__ __forceinline__ void check_finite(DevScalars* sc, const double* v, int n) {
+  for (int i = 0; i < n; ++i)
+    if (!isfinite(v[i])) sc->status = 3;  // FG_ERR_NAN
+}
+
+// After the k-space pass: k-space energies, homogeneous strain
+// (optimize-homo-strain.F:27-186) and w_hom for k_assemble.
+__device__ void homo_strain_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part_k,
+                                 int nblk) {
+  double v[NQ_K];
+  for (int q = 0; q < NQ_K; ++q) v[q] = reduce_partials(part_k, nblk, NQ_K, q);
+  if (threadIdx.x != 0) return;
+  double* e = sc->e;
+  const double es = v[0] * ph->Ninv / 2;       // (1/2N) sum w' Re(uK* S uK)
+  const double edd = v[1] / 2;                 // (1/2)  sum w' Re(uK* D uK), D = (S + Z*^2 L)/N
+  e[E_SHORT] = es;
+  e[E_LONG] = edd - es;
+  e[E_IS] = v[2] * ph->Ninv;
+  e[E_IC] = v[3] * 2 * ph->Ninv;
+  e[E_IM] = ph->modulation_on ? v[4] * 2 * ph->Ninv : 0.0;
+  double hc2uu[6];
+  for (int i = 0; i < 6; ++i) {
+    double s = 0.0;
+    for (int jj = 0; jj < 6; ++jj) s += ph->HC2[i][jj] * __ldcg(&sc->didiK0[jj]);
+    hc2uu[i] = s;
+  }
+  for (int i = 0; i < 3; ++i) hc2uu[i] = hc2uu[i] + ph->pNa03[i];
+  double* st = sc->strain;
+  const double(*H)[6] = ph->H;
+  if (ph->bulk_or_film == 2) {  // epit
+    st[0] = ph->epi_strain;
+    st[1] = ph->epi_strain;
+    st[2] = (-(H[2][0] + H[2][1]) * ph->epi_strain - hc2uu[2]) / H[2][2];
+    st[3] = -hc2uu[3] / H[3][3];
+    st[4] = -hc2uu[4] / H[4][4];
+    st[5] = 0.0;
+  } else if (ph->bulk_or_film == 3) {  // e110
+    st[2] = ph->epi_strain;
+    st[3] = 0.0;
+    st[4] = 0.0;
+    double num = -(H[0][0] + H[1][1] + 2 * H[1][1]) * ph->epi_strain - (H[2][0] + H[2][1]) * st[2] - hc2uu[0] - hc2uu[1] +
+                 2 * hc2uu[5];
+    double den = H[0][0] + H[1][1] + 2 * H[1][0] + 4 * H[5][5];
+    double delta = num / den;
+    st[0] = ph->epi_strain + delta;
+    st[1] = ph->epi_strain + delta;
+    st[5] = -2 * delta;
+  } else {
+    for (int i = 0; i < 6; ++i) st[i] = -hc2uu[i];
+    for (int i = 0; i < 6; ++i) {
+      double t = 0.0;
+      for (int jj = 0; jj < i; ++jj) t = t + ph->HG[i][jj] * st[jj];
+      st[i] = (st[i] - t) * ph->HG_inv[i];
+    }
+    for (int i = 5; i >= 0; --i) {
+      double t = 0.0;
+      for (int jj = i + 1; jj < 6; ++jj) t = t + st[jj] * ph->HG[jj][i];
+      st[i] = (st[i] - t) * ph->HG_inv[i];
+    }
+  }
+  double hs = 0.0;
+  for (int i = 0; i < 6; ++i) {
+    double d = 0.0;
+    for (int jj = 0; jj < 6; ++jj) d += H[i][jj] * st[jj];
+    hs = hs + st[i] * d;
+  }
+  e[E_HS] = hs / 2;
+  double hc = 0.0;
+  for (int i = 0; i < 6; ++i) hc += st[i] * hc2uu[i];
+  e[E_HC] = hc;
+  for (int jj = 0; jj < 6; ++jj) {
+    double w = 0.0;
+    for (int i = 0; i < 6; ++i) w = w + st[i] * ph->HC2[i][jj];
+    sc->w_hom[jj] = w;
+  }
+}
+
+// After k_assemble: real-space energies.
+__device__ void force_energies_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part_r,
+                                    int nblk) {
+  double v0 = reduce_partials(part_r, nblk, NQ_R, 0);
+  double v1 = reduce_partials(part_r, nblk, NQ_R, 1);
+  if (threadIdx.x != 0) return;
+  sc->e[E_UNH] = v0;
+  sc->e[E_DIPE] = ph->E_on ? -v1 : 0.0;
+  check_finite(sc, sc->e + E_SHORT, 9);
+}
+
+// kinetic_energy_dipo.F:106 from the kick partials
+__device__ __forceinline__ double ke_from(const Phys* ph, double sum) { return sum / ph->n_sum_p * ph->N / 2; }
+
+// Nose-Poincare, first half (nose-poincare.F:30-41): KE, (38), (35c).
+__device__ void np_pre_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  double* e = sc->e;
+  sc->ke_sum = v;
+  e[E_DIPO] = ke_from(ph, v);
+  double s = sc->s;
+  double CB = ph->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - sc->H0;
+  CB = ph->dt_2 * CB - sc->pi;
+  if (1.0 - CB * ph->dt / ph->Q < 0.0) sc->status = 10;  // (38) has no real root: Q_Nose too small
+  sc->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * ph->dt / ph->Q));
+  sc->s_old = s;
+  sc->s = s * (1.0 + ph->dt_2 * sc->pi / ph->Q) / (1.0 - ph->dt_2 * sc->pi / ph->Q);
+  sc->drift_coef = ph->dt_2 * (1 / sc->s + 1 / sc->s_old);
+}
+
+// Nose-Poincare after the force (nose-poincare.F:60-66): H_NP, (35e).
+// Thread 0 only.
+__device__ void np_post_body(const Phys* __restrict__ ph, DevScalars* sc) {
+  np_hamiltonian(ph, sc);
+  const double s = sc->s;
+  const double delta_H = sc->e[E_HNP] / s;
+  sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] / (s * s) - ph->nf_kT) - ph->dt_2 * delta_H;
+  sc->kick_coef = ph->dt_2 * s;
+}
+
+// After the closing kick: KE, H_NP, total (nose-poincare.F:74-75,
+// molecular-dynamics.F:293).
+__device__ void np_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  sc->ke_sum = v;
+  sc->e[E_DIPO] = ke_from(ph, v);
+  np_hamiltonian(ph, sc);
+  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
+  check_finite(sc, sc->e, E_COUNT);
+}
+
+// Leapfrog closing reduction (leapfrog.F:151) and total.
+__device__ void lf_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
+  double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x != 0) return;
+  sc->ke_sum = v;
+  sc->e[E_DIPO] = ke_from(ph, v);
+  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
+  check_finite(sc, sc->e, E_COUNT);
+}
+
+// Standalone launches of the tails (single block of RED_THREADS threads).
+__global__ void __launch_bounds__(RED_THREADS) k_homo_strain(const Phys* __restrict__ ph, DevScalars* sc,
+                                                             const double* __restrict__ part_k, int nblk) {
+  homo_strain_tail(ph, sc, part_k, nblk);
+}
+__global__ void __launch_bounds__(RED_THREADS) k_force_energies(const Phys* __restrict__ ph, DevScalars* sc,
+                                                                const double* __restrict__ part_r, int nblk) {
+  force_energies_tail(ph, sc, part_r, nblk);
+}
+__global__ void __launch_bounds__(RED_THREADS) k_np_pre(const Phys* __restrict__ ph, DevScalars* sc,
+                                                        const double* __restrict__ part, int nblk) {
+  np_pre_tail(ph, sc, part, nblk);
+}
+__global__ void k_np_post(const Phys* __restrict__ ph, DevScalars* sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) np_post_body(ph, sc);
+}
+__global__ void __launch_bounds__(RED_THREADS) k_np_final(const Phys* __restrict__ ph, DevScalars* sc,
+                                                          const double* __restrict__ part, int nblk) {
+  np_final_tail(ph, sc, part, nblk);
+}
+__global__ void __launch_bounds__(RED_THREADS) k_lf_final(const Phys* __restrict__ ph, DevScalars* sc,
+                                                          const double* __restrict__ part, int nblk) {
+  lf_final_tail(ph, sc, part, nblk);
 }
 
 // Wavevectors, trig tables and slot maps shared by the k-space kernels.
@@ -429,7 +632,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
                                                      const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
                                                      Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
                                                      const Phys* __restrict__ ph, double* __restrict__ part,
-                                                     DevScalars* __restrict__ sc, ZTiles zt) {
+                                                     DevScalars* sc, ZTiles zt, unsigned int* done) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
@@ -437,7 +640,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   const int buf_len = 9 * Lz * CW;
   if constexpr (LZC > 0)
     for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws_z[i] = twz[i];
-  z_tile_load<T>(buf, spec, g, zt, 9);
+  z_tile_load<T, LZC, CWC>(buf, spec, g, zt, 9);
   if constexpr (LZC > 0) {
     ct_forward<T, LZC, kZThreads, BatchCT<9 * CWC, CWC, 1, LZC * CWC, CWC>>(buf, tws_z);
   } else {
@@ -446,14 +649,19 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   }
   const double Ninv = ph->Ninv;
   double acc[NQ_K] = {0, 0, 0, 0, 0};
-  for (int idx = threadIdx.x; idx < Lz * CW; idx += blockDim.x) {
-    const int zs = idx / CW, cw = idx - zs * CW;
-    int col, yslot;
-    if (!tile_pencil(zt, g, cw, &col, &yslot)) continue;
-    const int ky = __ldg(&km.revy[yslot]);
-    const double kv2 = __ldg(&km.kvy[ky]);
-    const double2 ty = __ldg(&km.try_[ky]);
-    const int kx = __ldg(&km.revx[col]), kz = __ldg(&km.revz[zs]);
+  // this thread's pencil (fixed cw), decoded once
+  const int cw = threadIdx.x % CW;
+  int col = 0, yslot = 0;
+  const bool pencil_ok = tile_pencil(zt, g, cw, &col, &yslot);
+  const int ky = pencil_ok ? __ldg(&km.revy[yslot]) : 0;
+  const int kx = pencil_ok ? __ldg(&km.revx[col]) : 0;
+  const double kv2 = __ldg(&km.kvy[ky]);
+  const double2 ty = __ldg(&km.try_[ky]);
+  const double2 tx = __ldg(&km.trx[kx]);
+  const double kv1 = __ldg(&km.kvx[kx]);
+  const long long tpos0 = (long long)yslot * Lz * g.KXP + col;
+  for (int zs = threadIdx.x / CW; pencil_ok && zs < Lz; zs += blockDim.x / CW) {
+    const int kz = __ldg(&km.revz[zs]);
     const double w1 = (kx == 0 || kx == g.m) ? 1.0 : 2.0;  // full-spectrum multiplicity
     cplx<T> u[3], d[6];
 #pragma unroll
@@ -465,7 +673,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       for (int i = 0; i < 6; ++i) sc->didiK0[i] = (double)d[i].x;
     }
     // ---- dipole-dipole
-    const long long tpos = ((long long)yslot * Lz + zs) * g.KXP + col;
+    const long long tpos = tpos0 + (long long)zs * g.KXP;
     const T* Dp = dtab + tpos * 6;
     T D[6];
 #pragma unroll
@@ -478,7 +686,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     qv[4] = (double)u[2].x * u[0].x + (double)u[2].y * u[0].y;
     qv[5] = (double)u[0].x * u[1].x + (double)u[0].y * u[1].y;
     {
-      const double2 tx = __ldg(&km.trx[kx]), tz = __ldg(&km.trz[kz]);
+      const double2 tz = __ldg(&km.trz[kz]);
       const double cc[3] = {tx.x, ty.x, tz.x}, ss[3] = {tx.y, ty.y, tz.y};
       double S[6];
       short_range_k(ph->j, ph->kap2x2, cc, ss, S);
@@ -491,7 +699,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     F[1] = mk<cplx<T>>(D[5] * u[0].x + D[1] * u[1].x + D[3] * u[2].x, D[5] * u[0].y + D[1] * u[1].y + D[3] * u[2].y);
     F[2] = mk<cplx<T>>(D[4] * u[0].x + D[3] * u[1].x + D[2] * u[2].x, D[4] * u[0].y + D[3] * u[1].y + D[2] * u[2].y);
     // ---- inhomogeneous strain
-    const T k1 = (T)__ldg(&km.kvx[kx]), k2 = (T)kv2, k3 = (T)__ldg(&km.kvz[kz]);
+    const T k1 = (T)kv1, k2 = (T)kv2, k3 = (T)__ldg(&km.kvz[kz]);
     const T kk[4] = {(T)0, k1, k2, k3};
     const T B11 = (T)ph->B11, B12 = (T)ph->B12, B44 = (T)ph->B44;
     T K[3][3];
@@ -612,8 +820,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
     fft_inverse<T>(buf, B, pz, twz, buf_len);
   }
-  z_tile_store<T>(buf, spec, g, zt, 9);
+  z_tile_store<T, LZC, CWC>(buf, spec, g, zt, 9);
   block_partials<NQ_K>(acc, part, blockIdx.x);
+  if (done != nullptr && is_last_block(done)) homo_strain_tail(ph, sc, part, gridDim.x);
 }
 
 // ------------------------------------------------------------------ k_assemble
@@ -627,7 +836,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 template <typename T>
 __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
                                                   T* __restrict__ F, Geom g, const Phys* __restrict__ ph,
-                                                  const DevScalars* __restrict__ sc, double* __restrict__ part) {
+                                                  DevScalars* sc, double* __restrict__ part, int tail,
+                                                  unsigned int* done) {
   const long long ns = g.nsite;
   const T fa2g = (T)ph->fa2g, tg = (T)ph->tg, sk = (T)ph->sk, tk2 = (T)ph->tk2, fk = (T)ph->fk, k4x8 = (T)(8 * ph->P_k4);
   const double Pa = ph->P_alpha, Pg = ph->P_gamma, P1 = ph->P_k1, P2 = ph->P_k2, P3 = ph->P_k3, P4 = ph->P_k4;
@@ -690,6 +900,10 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
     F[2 * ns + i] = f2;
   }
   block_partials<NQ_R>(acc, part, blockIdx.x);
+  if (tail != TAIL_NONE && is_last_block(done)) {
+    force_energies_tail(ph, sc, part, gridDim.x);
+    if (tail == TAIL_NP_POST && threadIdx.x == 0) np_post_body(ph, sc);
+  }
 }
 
 // --------------------------------------------------------------- integrators
@@ -699,7 +913,9 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
 template <typename T>
 __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __restrict__ F, const double* coef, Geom g,
                                               const double* __restrict__ layer_minv,
-                                              const unsigned char* __restrict__ layer_sump, double* __restrict__ part) {
+                                              const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
+                                              int tail, unsigned int* done, const Phys* __restrict__ ph,
+                                              DevScalars* sc) {
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
@@ -717,6 +933,11 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
     }
   }
   block_partials<1>(acc, part, blockIdx.x);
+  if (tail != TAIL_NONE && is_last_block(done)) {
+    if (tail == TAIL_NP_PRE) np_pre_tail(ph, sc, part, gridDim.x);
+    else if (tail == TAIL_NP_FINAL) np_final_tail(ph, sc, part, gridDim.x);
+    else if (tail == TAIL_LF_FINAL) lf_final_tail(ph, sc, part, gridDim.x);
+  }
 }
 
 // u <- u + coef * p * m^-1 (nose-poincare.F:41-53, leapfrog.F:104-114)
@@ -751,161 +972,6 @@ __global__ void k_mirror(T* __restrict__ f, Geom g, int gap_id) {
     f[ns + d] = -f[ns + s];
     f[2 * ns + d] = f[2 * ns + s];
   }
-}
-
-// ------------------------------------------------------------ scalar kernels
-__device__ __forceinline__ double sum_potential(const double* e) {
-  return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
-}
-
-__device__ __forceinline__ void np_hamiltonian(const Phys* ph, DevScalars* sc) {  // energy_module.F:128-148
-  double* e = sc->e;
-  const double s = sc->s;
-  double h = e[E_DIPO] / (s * s) + sum_potential(e) + sc->pi * sc->pi / 2 / ph->Q + ph->threeN_kT * log(s) - sc->H0;
-  e[E_HNP] = h * s;
-}
-
-__device__ __forceinline__ void check_finite(DevScalars* sc, const double* v, int n) {
-  for (int i = 0; i < n; ++i)
-    if (!isfinite(v[i])) sc->status = 3;  // FG_ERR_NAN
-}
-
-// After the k-space pass: k-space energies, homogeneous strain
-// (optimize-homo-strain.F:27-186) and w_hom for k_assemble.
-__global__ void __launch_bounds__(RED_THREADS) k_homo_strain(const Phys* __restrict__ ph, DevScalars* sc,
-                                                             const double* __restrict__ part_k, int nblk) {
-  double v[NQ_K];
-  for (int q = 0; q < NQ_K; ++q) v[q] = reduce_partials(part_k, nblk, NQ_K, q);
-  if (threadIdx.x != 0) return;
-  double* e = sc->e;
-  const double es = v[0] * ph->Ninv / 2;       // (1/2N) sum w' Re(uK* S uK)
-  const double edd = v[1] / 2;                 // (1/2)  sum w' Re(uK* D uK), D = (S + Z*^2 L)/N
-  e[E_SHORT] = es;
-  e[E_LONG] = edd - es;
-  e[E_IS] = v[2] * ph->Ninv;
-  e[E_IC] = v[3] * 2 * ph->Ninv;
-  e[E_IM] = ph->modulation_on ? v[4] * 2 * ph->Ninv : 0.0;
-  double hc2uu[6];
-  for (int i = 0; i < 6; ++i) {
-    double s = 0.0;
-    for (int jj = 0; jj < 6; ++jj) s += ph->HC2[i][jj] * sc->didiK0[jj];
-    hc2uu[i] = s;
-  }
-  for (int i = 0; i < 3; ++i) hc2uu[i] = hc2uu[i] + ph->pNa03[i];
-  double* st = sc->strain;
-  const double(*H)[6] = ph->H;
-  if (ph->bulk_or_film == 2) {  // epit
-    st[0] = ph->epi_strain;
-    st[1] = ph->epi_strain;
-    st[2] = (-(H[2][0] + H[2][1]) * ph->epi_strain - hc2uu[2]) / H[2][2];
-    st[3] = -hc2uu[3] / H[3][3];
-    st[4] = -hc2uu[4] / H[4][4];
-    st[5] = 0.0;
-  } else if (ph->bulk_or_film == 3) {  // e110
-    st[2] = ph->epi_strain;
-    st[3] = 0.0;
-    st[4] = 0.0;
-    double num = -(H[0][0] + H[1][1] + 2 * H[1][1]) * ph->epi_strain - (H[2][0] + H[2][1]) * st[2] - hc2uu[0] - hc2uu[1] +
-                 2 * hc2uu[5];
-    double den = H[0][0] + H[1][1] + 2 * H[1][0] + 4 * H[5][5];
-    double delta = num / den;
-    st[0] = ph->epi_strain + delta;
-    st[1] = ph->epi_strain + delta;
-    st[5] = -2 * delta;
-  } else {
-    for (int i = 0; i < 6; ++i) st[i] = -hc2uu[i];
-    for (int i = 0; i < 6; ++i) {
-      double t = 0.0;
-      for (int jj = 0; jj < i; ++jj) t = t + ph->HG[i][jj] * st[jj];
-      st[i] = (st[i] - t) * ph->HG_inv[i];
-    }
-    for (int i = 5; i >= 0; --i) {
-      double t = 0.0;
-      for (int jj = i + 1; jj < 6; ++jj) t = t + st[jj] * ph->HG[jj][i];
-      st[i] = (st[i] - t) * ph->HG_inv[i];
-    }
-  }
-  double hs = 0.0;
-  for (int i = 0; i < 6; ++i) {
-    double d = 0.0;
-    for (int jj = 0; jj < 6; ++jj) d += H[i][jj] * st[jj];
-    hs = hs + st[i] * d;
-  }
-  e[E_HS] = hs / 2;
-  double hc = 0.0;
-  for (int i = 0; i < 6; ++i) hc += st[i] * hc2uu[i];
-  e[E_HC] = hc;
-  for (int jj = 0; jj < 6; ++jj) {
-    double w = 0.0;
-    for (int i = 0; i < 6; ++i) w = w + st[i] * ph->HC2[i][jj];
-    sc->w_hom[jj] = w;
-  }
-}
-
-// After k_assemble: real-space energies.
-__global__ void __launch_bounds__(RED_THREADS) k_force_energies(const Phys* __restrict__ ph, DevScalars* sc,
-                                                                const double* __restrict__ part_r, int nblk) {
-  double v0 = reduce_partials(part_r, nblk, NQ_R, 0);
-  double v1 = reduce_partials(part_r, nblk, NQ_R, 1);
-  if (threadIdx.x != 0) return;
-  sc->e[E_UNH] = v0;
-  sc->e[E_DIPE] = ph->E_on ? -v1 : 0.0;
-  check_finite(sc, sc->e + E_SHORT, 9);
-}
-
-// kinetic_energy_dipo.F:106 from the kick partials
-__device__ __forceinline__ double ke_from(const Phys* ph, double sum) { return sum / ph->n_sum_p * ph->N / 2; }
-
-// Nose-Poincare, first half (nose-poincare.F:30-41): KE, (38), (35c).
-__global__ void __launch_bounds__(RED_THREADS) k_np_pre(const Phys* __restrict__ ph, DevScalars* sc,
-                                                        const double* __restrict__ part, int nblk) {
-  double v = reduce_partials(part, nblk, 1, 0);
-  if (threadIdx.x != 0) return;
-  double* e = sc->e;
-  sc->ke_sum = v;
-  e[E_DIPO] = ke_from(ph, v);
-  double s = sc->s;
-  double CB = ph->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - sc->H0;
-  CB = ph->dt_2 * CB - sc->pi;
-  if (1.0 - CB * ph->dt / ph->Q < 0.0) sc->status = 10;  // (38) has no real root: Q_Nose too small
-  sc->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * ph->dt / ph->Q));
-  sc->s_old = s;
-  sc->s = s * (1.0 + ph->dt_2 * sc->pi / ph->Q) / (1.0 - ph->dt_2 * sc->pi / ph->Q);
-  sc->drift_coef = ph->dt_2 * (1 / sc->s + 1 / sc->s_old);
-}
-
-// Nose-Poincare after the force (nose-poincare.F:60-66): H_NP, (35e).
-__global__ void k_np_post(const Phys* __restrict__ ph, DevScalars* sc) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  np_hamiltonian(ph, sc);
-  const double s = sc->s;
-  const double delta_H = sc->e[E_HNP] / s;
-  sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] / (s * s) - ph->nf_kT) - ph->dt_2 * delta_H;
-  sc->kick_coef = ph->dt_2 * s;
-}
-
-// After the closing kick: KE, H_NP, total (nose-poincare.F:74-75,
-// molecular-dynamics.F:293).
-__global__ void __launch_bounds__(RED_THREADS) k_np_final(const Phys* __restrict__ ph, DevScalars* sc,
-                                                          const double* __restrict__ part, int nblk) {
-  double v = reduce_partials(part, nblk, 1, 0);
-  if (threadIdx.x != 0) return;
-  sc->ke_sum = v;
-  sc->e[E_DIPO] = ke_from(ph, v);
-  np_hamiltonian(ph, sc);
-  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
-  check_finite(sc, sc->e, E_COUNT);
-}
-
-// Leapfrog closing reduction (leapfrog.F:151) and total.
-__global__ void __launch_bounds__(RED_THREADS) k_lf_final(const Phys* __restrict__ ph, DevScalars* sc,
-                                                          const double* __restrict__ part, int nblk) {
-  double v = reduce_partials(part, nblk, 1, 0);
-  if (threadIdx.x != 0) return;
-  sc->ke_sum = v;
-  sc->e[E_DIPO] = ke_from(ph, v);
-  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
-  check_finite(sc, sc->e, E_COUNT);
 }
 
 // KE of the current momenta without changing them.

@@ -255,12 +255,13 @@ int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
 
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */
-#define FG_NPROF 12
+#define FG_NPROF 7
 /* Time n_steps graph launches of the MD step of p's method; *ms = total. */
 int  fg_time_steps(fg_ctx* ctx, int n_steps, double* ms);
-/* One bulk Nose-Poincare step launched kernel by kernel with an event between
-   kernels, averaged over reps steps; ms[i] (i < FG_NPROF) per kernel, in the
-   order named by fg_profile_name(i).  The steps advance the state. */
+/* One bulk Nose-Poincare step launched kernel by kernel (the same kernels as
+   the step's graph) with an event between kernels, averaged over reps steps;
+   ms[i] (i < FG_NPROF) per kernel, in the order named by fg_profile_name(i).
+   The steps advance the state. */
 int  fg_profile_step(fg_ctx* ctx, int reps, double* ms);
 const char* fg_profile_name(int i);
 
