@@ -833,71 +833,114 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 //     + homogeneous strain coupling, w = strain B2 (dVddi-homo-coupling.F:209-237)
 //     + inhomogeneous strain coupling, w(R) = eta(R) B2 (dVddi_inho_coupling.F:114-142)
 // and the per-block sums of the anharmonic energy (:67-99) and Z* u.E.
+// 16-byte vectors of consecutive sites of one component (4 floats or 2
+// doubles); used when a vector never straddles a z layer (plane % width == 0).
+template <typename T>
+struct alignas(16) V16 {
+  static constexpr int n = 16 / (int)sizeof(T);
+  T v[16 / sizeof(T)];
+};
+template <typename T>
+__device__ __forceinline__ V16<T> ldv(const T* p) { return *reinterpret_cast<const V16<T>*>(p); }
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V16<T>*>(p) = a; }
+
+template <typename T>
+struct AsmConst {
+  T fa2g, tg, sk, tk2, fk, k4x8;  // anharmonic force constants
+  T hx, hy, h4;                   // homogeneous_coupling_2: B1xx/2, B1yy/2, B4yz
+  T wh[6];                        // strain . B2
+  T Zs, E0, E1, E2;
+  double Pa, Pg, P1, P2, P3, P4;
+  int E_on;
+};
+
+// Force on one site from F_dd, u and eta (see k_assemble); acc += energies.
+template <typename T>
+__device__ __forceinline__ void assemble_site(const AsmConst<T>& k, T ux, T uy, T uz, T f0, T f1, T f2,
+                                              const T* eta, T& o0, T& o1, T& o2, double* acc) {
+  const T d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
+  const T uu = d0 + d1 + d2;
+  // 4th order
+  f0 = f0 + ux * (k.fa2g * uu - k.tg * d0);
+  f1 = f1 + uy * (k.fa2g * uu - k.tg * d1);
+  f2 = f2 + uz * (k.fa2g * uu - k.tg * d2);
+  // 6th and 8th order
+  const T uu2 = uu * uu, uu3 = uu2 * uu;
+  f0 = f0 + ux * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d0 * d0) - k.fk * d1 * d2);
+  f1 = f1 + uy * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d1 * d1) - k.fk * d2 * d0);
+  f2 = f2 + uz * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d2 * d2) - k.fk * d0 * d1);
+  {
+    const double D0 = d0, D1 = d1, D2 = d2, U = uu;
+    acc[0] += k.Pa * (U * U) + k.Pg * (D0 * D1 + D1 * D2 + D2 * D0) + k.P1 * (U * U * U) +
+              k.P2 * ((D0 * D0) * (D1 + D2) + (D1 * D1) * (D2 + D0) + (D2 * D2) * (D0 + D1)) + k.P3 * D0 * D1 * D2 +
+              k.P4 * (U * U * U * U);
+  }
+  if (k.E_on) {
+    f0 = f0 - k.Zs * k.E0;
+    f1 = f1 - k.Zs * k.E1;
+    f2 = f2 - k.Zs * k.E2;
+    acc[1] += (double)k.Zs * ((double)ux * k.E0 + (double)uy * k.E1 + (double)uz * k.E2);
+  }
+  // homogeneous strain coupling
+  f0 = f0 + 2 * k.wh[0] * ux + k.wh[4] * uz + k.wh[5] * uy;
+  f1 = f1 + 2 * k.wh[1] * uy + k.wh[3] * uz + k.wh[5] * ux;
+  f2 = f2 + 2 * k.wh[2] * uz + k.wh[3] * uy + k.wh[4] * ux;
+  // inhomogeneous strain coupling, w_q = sum_j eta_j B2(j, q) with the
+  // sparsity of homogeneous_coupling_2 (eta already carries 1/N)
+  const T w0 = k.hx * eta[0] + k.hy * (eta[1] + eta[2]);
+  const T w1 = k.hx * eta[1] + k.hy * (eta[0] + eta[2]);
+  const T w2 = k.hx * eta[2] + k.hy * (eta[0] + eta[1]);
+  const T w3 = k.h4 * eta[3], w4 = k.h4 * eta[4], w5 = k.h4 * eta[5];
+  o0 = f0 + 2 * w0 * ux + w4 * uz + w5 * uy;
+  o1 = f1 + 2 * w1 * uy + w3 * uz + w5 * ux;
+  o2 = f2 + 2 * w2 * uz + w3 * uy + w4 * ux;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
                                                   T* __restrict__ F, Geom g, const Phys* __restrict__ ph,
                                                   DevScalars* sc, double* __restrict__ part, int tail,
                                                   unsigned int* done) {
   const long long ns = g.nsite;
-  const T fa2g = (T)ph->fa2g, tg = (T)ph->tg, sk = (T)ph->sk, tk2 = (T)ph->tk2, fk = (T)ph->fk, k4x8 = (T)(8 * ph->P_k4);
-  const double Pa = ph->P_alpha, Pg = ph->P_gamma, P1 = ph->P_k1, P2 = ph->P_k2, P3 = ph->P_k3, P4 = ph->P_k4;
-  T wh[6];
+  AsmConst<T> k;
+  k.fa2g = (T)ph->fa2g; k.tg = (T)ph->tg; k.sk = (T)ph->sk; k.tk2 = (T)ph->tk2; k.fk = (T)ph->fk;
+  k.k4x8 = (T)(8 * ph->P_k4);
+  k.hx = (T)ph->HC2[0][0]; k.hy = (T)ph->HC2[0][1]; k.h4 = (T)ph->HC2[3][3];
 #pragma unroll
-  for (int i = 0; i < 6; ++i) wh[i] = (T)sc->w_hom[i];
-  T B2[6][6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i)
-#pragma unroll
-    for (int jj = 0; jj < 6; ++jj) B2[i][jj] = (T)ph->HC2[i][jj];
-  const int E_on = ph->E_on;
-  const T Zs = (T)ph->Zstar;
-  const T E0 = (T)sc->E[0], E1 = (T)sc->E[1], E2 = (T)sc->E[2];
+  for (int i = 0; i < 6; ++i) k.wh[i] = (T)sc->w_hom[i];
+  k.Zs = (T)ph->Zstar; k.E0 = (T)sc->E[0]; k.E1 = (T)sc->E[1]; k.E2 = (T)sc->E[2];
+  k.Pa = ph->P_alpha; k.Pg = ph->P_gamma; k.P1 = ph->P_k1; k.P2 = ph->P_k2; k.P3 = ph->P_k3; k.P4 = ph->P_k4;
+  k.E_on = ph->E_on;
   double acc[NQ_R] = {0.0, 0.0};
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
-    const T ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
-    T f0 = rw[i], f1 = rw[ns + i], f2 = rw[2 * ns + i];
-    const T d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
-    const T uu = d0 + d1 + d2;
-    // 4th order
-    f0 = f0 + ux * (fa2g * uu - tg * d0);
-    f1 = f1 + uy * (fa2g * uu - tg * d1);
-    f2 = f2 + uz * (fa2g * uu - tg * d2);
-    // 6th and 8th order
-    const T uu2 = uu * uu, uu3 = uu2 * uu;
-    f0 = f0 + ux * (sk * uu2 + k4x8 * uu3 - tk2 * (d0 * d0) - fk * d1 * d2);
-    f1 = f1 + uy * (sk * uu2 + k4x8 * uu3 - tk2 * (d1 * d1) - fk * d2 * d0);
-    f2 = f2 + uz * (sk * uu2 + k4x8 * uu3 - tk2 * (d2 * d2) - fk * d0 * d1);
-    {
-      const double D0 = d0, D1 = d1, D2 = d2, U = uu;
-      acc[0] += Pa * (U * U) + Pg * (D0 * D1 + D1 * D2 + D2 * D0) + P1 * (U * U * U) +
-                P2 * ((D0 * D0) * (D1 + D2) + (D1 * D1) * (D2 + D0) + (D2 * D2) * (D0 + D1)) + P3 * D0 * D1 * D2 +
-                P4 * (U * U * U * U);
-    }
-    if (E_on) {
-      f0 = f0 - Zs * E0;
-      f1 = f1 - Zs * E1;
-      f2 = f2 - Zs * E2;
-      acc[1] += (double)Zs * ((double)ux * E0 + (double)uy * E1 + (double)uz * E2);
-    }
-    // homogeneous strain coupling
-    f0 = f0 + 2 * wh[0] * ux + wh[4] * uz + wh[5] * uy;
-    f1 = f1 + 2 * wh[1] * uy + wh[3] * uz + wh[5] * ux;
-    f2 = f2 + 2 * wh[2] * uz + wh[3] * uy + wh[4] * ux;
-    // inhomogeneous strain coupling (eta already carries 1/N)
-    T eta[6];
+  constexpr int NV = V16<T>::n;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (g.plane_r % NV == 0) {
+    for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
+      const long long i = iv * NV;
+      const V16<T> ux = ldv(u + i), uy = ldv(u + ns + i), uz = ldv(u + 2 * ns + i);
+      const V16<T> a0 = ldv(rw + i), a1 = ldv(rw + ns + i), a2 = ldv(rw + 2 * ns + i);
+      V16<T> e[6];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
-    T w[6];
+      for (int q = 0; q < 6; ++q) e[q] = ldv(rw + (3 + q) * ns + i);
+      V16<T> o0, o1, o2;
 #pragma unroll
-    for (int q = 0; q < 6; ++q)
-      w[q] = eta[0] * B2[0][q] + eta[1] * B2[1][q] + eta[2] * B2[2][q] + eta[3] * B2[3][q] + eta[4] * B2[4][q] +
-             eta[5] * B2[5][q];
-    f0 = f0 + 2 * w[0] * ux + w[4] * uz + w[5] * uy;
-    f1 = f1 + 2 * w[1] * uy + w[3] * uz + w[5] * ux;
-    f2 = f2 + 2 * w[2] * uz + w[3] * uy + w[4] * ux;
-    F[i] = f0;
-    F[ns + i] = f1;
-    F[2 * ns + i] = f2;
+      for (int l = 0; l < NV; ++l) {
+        const T eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
+        assemble_site(k, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, o0.v[l], o1.v[l], o2.v[l], acc);
+      }
+      stv(F + i, o0);
+      stv(F + ns + i, o1);
+      stv(F + 2 * ns + i, o2);
+    }
+  } else {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+      T eta[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
+      assemble_site(k, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, F[i], F[ns + i],
+                    F[2 * ns + i], acc);
+    }
   }
   block_partials<NQ_R>(acc, part, blockIdx.x);
   if (tail != TAIL_NONE && is_last_block(done)) {
@@ -919,17 +962,40 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(i / g.plane_r);
-    const T p0 = p[i] - c * F[i];
-    const T p1 = p[ns + i] - c * F[ns + i];
-    const T p2 = p[2 * ns + i] - c * F[2 * ns + i];
-    p[i] = p0;
-    p[ns + i] = p1;
-    p[2 * ns + i] = p2;
-    if (layer_sump[z]) {
-      const double mi = layer_minv[z];
-      acc[0] += (double)p0 * p0 * mi + (double)p1 * p1 * mi + (double)p2 * p2 * mi;
+  constexpr int NV = V16<T>::n;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (g.plane_r % NV == 0) {
+    for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
+      const long long i = iv * NV;
+      const int z = (int)(i / g.plane_r);
+      V16<T> q0 = ldv(p + i), q1 = ldv(p + ns + i), q2 = ldv(p + 2 * ns + i);
+      const V16<T> f0 = ldv(F + i), f1 = ldv(F + ns + i), f2 = ldv(F + 2 * ns + i);
+      double ke = 0.0;
+#pragma unroll
+      for (int l = 0; l < NV; ++l) {
+        q0.v[l] = q0.v[l] - c * f0.v[l];
+        q1.v[l] = q1.v[l] - c * f1.v[l];
+        q2.v[l] = q2.v[l] - c * f2.v[l];
+        ke += (double)q0.v[l] * q0.v[l] + (double)q1.v[l] * q1.v[l] + (double)q2.v[l] * q2.v[l];
+      }
+      stv(p + i, q0);
+      stv(p + ns + i, q1);
+      stv(p + 2 * ns + i, q2);
+      if (layer_sump[z]) acc[0] += ke * layer_minv[z];
+    }
+  } else {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+      const int z = (int)(i / g.plane_r);
+      const T p0 = p[i] - c * F[i];
+      const T p1 = p[ns + i] - c * F[ns + i];
+      const T p2 = p[2 * ns + i] - c * F[2 * ns + i];
+      p[i] = p0;
+      p[ns + i] = p1;
+      p[2 * ns + i] = p2;
+      if (layer_sump[z]) {
+        const double mi = layer_minv[z];
+        acc[0] += (double)p0 * p0 * mi + (double)p1 * p1 * mi + (double)p2 * p2 * mi;
+      }
     }
   }
   block_partials<1>(acc, part, blockIdx.x);
@@ -946,12 +1012,29 @@ __global__ void __launch_bounds__(256) k_drift(T* __restrict__ u, const T* __res
                                                const double* __restrict__ layer_minv) {
   const long long ns = g.nsite;
   const double c = *coef;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
-    const int z = (int)(i / g.plane_r);
-    const T f = (T)(c * layer_minv[z]);
-    u[i] = u[i] + f * p[i];
-    u[ns + i] = u[ns + i] + f * p[ns + i];
-    u[2 * ns + i] = u[2 * ns + i] + f * p[2 * ns + i];
+  constexpr int NV = V16<T>::n;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (g.plane_r % NV == 0) {
+    for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
+      const long long i = iv * NV;
+      const T f = (T)(c * layer_minv[(int)(i / g.plane_r)]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        V16<T> x = ldv(u + a * ns + i);
+        const V16<T> q = ldv(p + a * ns + i);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) x.v[l] = x.v[l] + f * q.v[l];
+        stv(u + a * ns + i, x);
+      }
+    }
+  } else {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+      const int z = (int)(i / g.plane_r);
+      const T f = (T)(c * layer_minv[z]);
+      u[i] = u[i] + f * p[i];
+      u[ns + i] = u[ns + i] + f * p[ns + i];
+      u[2 * ns + i] = u[2 * ns + i] + f * p[2 * ns + i];
+    }
   }
 }
 
