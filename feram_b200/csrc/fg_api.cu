@@ -1099,7 +1099,9 @@ int fg_set_uniform_E(fg_ctx* ctx, const double E[3]) {
   if (!ctx || !ctx->stream || !E) return FG_ERR_ARG;
   CK(cudaMemcpyAsync(ctx->sc->E, E, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  ctx->force_fresh = false;
+  // The stored dVddi and energies stay those of the last evaluation, as
+  // c%dVddi does when molecular-dynamics.F:66-76 changes c%E_field between
+  // steps: the next force evaluation sees the new field.
   return FG_OK;
 }
 

@@ -273,7 +273,7 @@ contains
     call from_c_energy(q, e)
   end subroutine leapfrog_gpu
 
-  ! The per-step E-field update of molecular-dynamics.F:223-233 (uniform field)
+  ! The per-step E-field update of molecular-dynamics.F:66-76 (uniform field)
   subroutine gpu_set_field(E_field_add)
     real(c_double), intent(in) :: E_field_add(3)
     call check(fg_set_uniform_E(gctx, E_field_add), 'fg_set_uniform_E')

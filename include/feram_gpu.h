@@ -226,7 +226,9 @@ int  fg_set_thermostat(fg_ctx* ctx, double s_Nose, double pi_Nose, double H0);
 /* acouK (complex, 3 comps) of the last force evaluation, Fortran layout. */
 int  fg_get_acouK(fg_ctx* ctx, double* acouK);
 /* Uniform external field E(R) = E (initialize_E_field.F:139-146,
-   molecular-dynamics.F:223-233 with no .localfield). */
+   molecular-dynamics.F:66-76 with no .localfield).  dVddi and the energies
+   of the last force evaluation are kept; the next evaluation (inside the
+   next nose_poincare / leapfrog step) uses E, as in the reference. */
 int  fg_set_uniform_E(fg_ctx* ctx, const double E[3]);
 
 /* ---- the hot path -------------------------------------------------------- */

@@ -182,11 +182,16 @@ def test_leapfrog_steps_match_oracle(fg, prec):
     assert ru <= tol and max(ee.values()) <= tol, (ru, ee)
 
 
-def test_feram_run_matches_oracle_md(fg, tmp_path):
-    """The whole host driver (initialize_dipoR with uni64, H0, NP loop,
-    add_to_Average) against the oracle's molecular_dynamics."""
+WAVE = dict(external_E_field="0.0 0.0 0.002", E_wave_type="'triangular_cos'", n_E_wave_period="8")
+
+
+@pytest.mark.parametrize("extra", [{}, WAVE], ids=["static", "triangular_cos"])
+def test_feram_run_matches_oracle_md(fg, tmp_path, extra):
+    """The whole host driver (initialize_dipoR with uni64, H0, NP loop with
+    the per-step field of wave_module.F, add_to_Average) against the
+    oracle's molecular_dynamics."""
     text = helpers.deck("zzznp.feram", L="8 8 8", n_thermalize="10", n_average="10", verbose="1",
-                        n_coord_freq="100000", kelvin="280")
+                        n_coord_freq="100000", kelvin="280", **extra)
     (tmp_path / "run.feram").write_text(text)
     avg, tsim = fg.feram_run(str(tmp_path / "run.feram"), A.FG_PREC_FP64)
     p = fg.params_from_text(text, "run")
