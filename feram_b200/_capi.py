@@ -168,6 +168,8 @@ def lib() -> C.CDLL:
         "fg_profile_step": (C.c_int, [vp, C.c_int, dp]),
         "fg_profile_name": (C.c_char_p, [C.c_int]),
         "fg_feram_run": (C.c_int, [C.c_char_p, C.c_int, P(fg_average), dp, C.c_char_p, C.c_int]),
+        "fg_kinetic_energy_dipo_noalloc": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, dp, P(C.c_ubyte), vp, vp,
+                                                     C.c_char_p, C.c_int]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name, None)

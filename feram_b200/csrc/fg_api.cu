@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1294,3 +1295,106 @@ int fg_get_dipoRavg(fg_ctx* ctx, double* out) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free kinetic energy (no counterpart in the reference).
+//
+// Some callers cannot allocate device memory at the point where they want the
+// kinetic energy of a momentum field they already hold on the device: a
+// driver that runs the MD from its own device memory pool under a fixed
+// budget, or a host thread that must never enter the CUDA allocator.  This
+// entry point needs no fg_ctx and calls neither cudaMalloc nor cudaFree: the
+// block partial sums of k_ke_only and the per-layer mass and mask tables live
+// in one file-scope device array of fixed size.  Every call on a device uses
+// the same array, so two calls that overlap in time on one device (different
+// streams or host threads) overwrite each other's partials; the caller orders
+// them.  Nothing in the array has to start at zero: each call writes the
+// tables and every partial it reads before reading them.
+namespace {
+constexpr int kNoAllocPartials = 4096;  // >= blocks of one k_ke_only launch
+constexpr int kNoAllocMinv = kNoAllocPartials;                       // FG_NOALLOC_MAX_LZ doubles
+constexpr int kNoAllocMask = kNoAllocMinv + FG_NOALLOC_MAX_LZ;       // FG_NOALLOC_MAX_LZ bytes
+constexpr int kNoAllocDoubles = kNoAllocMask + FG_NOALLOC_MAX_LZ / 8;  // 5248 doubles = 41 KiB
+
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+  std::once_flag once;
+  cudaError_t status = cudaSuccess;
+  double* scratch = nullptr;  // device address of g_noalloc_scratch on this device
+  int nsm = 0;
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+// KE = sum p^2 m^-1 / n_sum_p * N / 2, the scaling of kinetic_energy_dipo.F:28
+__global__ void __launch_bounds__(RED_THREADS) k_ke_finish_out(const double* __restrict__ part, int nblk,
+                                                               double n_sum_p, double N, double* out) {
+  const double v = reduce_partials(part, nblk, 1, 0);
+  if (threadIdx.x == 0) *out = v / n_sum_p * N / 2;
+}
+
+int noalloc_fail(char* errbuf, int errlen, int rc, const char* msg) {
+  if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", msg);
+  return rc;
+}
+}  // namespace
+
+extern "C" int fg_kinetic_energy_dipo_noalloc(const double* dipoP, int Lx, int Ly, int Lz,
+                                              const double* layer_mass_inv, const unsigned char* layer_sum_p,
+                                              void* stream, double* ke, char* errbuf, int errlen) {
+  char msg[160];
+  if (!dipoP || !layer_mass_inv || !layer_sum_p || !ke)
+    return noalloc_fail(errbuf, errlen, FG_ERR_ARG, "fg_kinetic_energy_dipo_noalloc: null pointer argument");
+  if (Lx < 1 || Ly < 1 || Lz < 1)
+    return noalloc_fail(errbuf, errlen, FG_ERR_ARG, "fg_kinetic_energy_dipo_noalloc: Lx, Ly, Lz must be >= 1");
+  if (Lz > FG_NOALLOC_MAX_LZ) {
+    std::snprintf(msg, sizeof(msg), "fg_kinetic_energy_dipo_noalloc: Lz = %d exceeds FG_NOALLOC_MAX_LZ = %d", Lz,
+                  FG_NOALLOC_MAX_LZ);
+    return noalloc_fail(errbuf, errlen, FG_ERR_ARG, msg);
+  }
+  const long long plane = (long long)Lx * Ly;
+  long long counted = 0;
+  for (int z = 0; z < Lz; ++z) counted += layer_sum_p[z] ? 1 : 0;
+  if (counted == 0)
+    return noalloc_fail(errbuf, errlen, FG_ERR_ARG, "fg_kinetic_energy_dipo_noalloc: layer_sum_p counts no layer");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return noalloc_fail(errbuf, errlen, FG_ERR_UNSUPPORTED, "fg_kinetic_energy_dipo_noalloc: device index >= 64");
+  // one-time set-up on this device (it is current): the array's device address
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  std::call_once(d.once, [&d, dev]() {
+    void* ptr = nullptr;
+    d.status = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (d.status == cudaSuccess) d.status = cudaDeviceGetAttribute(&d.nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (d.status == cudaSuccess) d.scratch = static_cast<double*>(ptr);
+  });
+  if (d.status != cudaSuccess || !d.scratch) {
+    std::snprintf(msg, sizeof(msg), "fg_kinetic_energy_dipo_noalloc: set-up failed: %s",
+                  cudaGetErrorString(d.status));
+    return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, msg);
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  double* part = d.scratch;
+  double* minv = d.scratch + kNoAllocMinv;
+  unsigned char* mask = reinterpret_cast<unsigned char*>(d.scratch + kNoAllocMask);
+  e = cudaMemcpyAsync(minv, layer_mass_inv, sizeof(double) * (size_t)Lz, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mask, layer_sum_p, (size_t)Lz, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, cudaGetErrorString(e));
+  Geom g;
+  std::memset(&g, 0, sizeof(g));
+  g.Lx = Lx;
+  g.Ly = Ly;
+  g.Lz = Lz;
+  g.plane_r = plane;
+  g.nsite = plane * Lz;
+  const long long want = (g.nsite + kThreadsElem - 1) / kThreadsElem;
+  const int grid = (int)std::max(1LL, std::min({want, (long long)std::max(d.nsm, 1) * 8, (long long)kNoAllocPartials}));
+  k_ke_only<double><<<grid, kThreadsElem, 0, st>>>(dipoP, g, minv, mask, part);
+  k_ke_finish_out<<<1, RED_THREADS, 0, st>>>(part, grid, (double)(counted * plane), (double)g.nsite, ke);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, cudaGetErrorString(e));
+  return FG_OK;
+}

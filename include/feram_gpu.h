@@ -277,6 +277,31 @@ const char* fg_profile_name(int i);
 int  fg_feram_run(const char* path, int precision, fg_average* avg_out,
                   double* t_sim, char* errbuf, int errlen);
 
+/* ---- allocation-free entry point (no counterpart in the reference) -------
+   kinetic_energy_dipo (kinetic_energy_dipo.F:14-28) of a momentum field the
+   caller already holds in device memory, for callers that cannot allocate at
+   that point: a driver running the MD from its own device memory pool under
+   a fixed budget, or a host thread that must not enter the CUDA allocator.
+   It needs no fg_ctx and allocates nothing: its block partials and per-layer
+   tables live in one fixed device array of 5248 doubles (41 KiB) inside the
+   library.
+     dipoP           device, FP64, component-major [3][Lz][Ly][Lx], contiguous
+     layer_mass_inv  host, Lz values of m^-1 per z-layer
+     layer_sum_p     host, Lz flags of the sum_p mask (1 = layer counted)
+     stream          a cudaStream_t (NULL = the legacy default stream)
+     ke              device pointer; receives sum p^2 m^-1 * N / (2 n_sum_p),
+                     n_sum_p = Lx*Ly*(counted layers), when the stream gets there
+   Lz > FG_NOALLOC_MAX_LZ, a null pointer or a mask that counts no layer give
+   FG_ERR_ARG and a message in errbuf (may be NULL).  The first call on each
+   device does a one-time set-up (it looks up the array's device address) and
+   should come before any stream capture.  All calls on one device share the
+   array: calls that overlap in time (different streams or host threads) race,
+   and the caller must order them. */
+#define FG_NOALLOC_MAX_LZ 1024
+int  fg_kinetic_energy_dipo_noalloc(const double* dipoP, int Lx, int Ly, int Lz,
+                                    const double* layer_mass_inv, const unsigned char* layer_sum_p,
+                                    void* stream, double* ke, char* errbuf, int errlen);
+
 #ifdef __cplusplus
 }
 #endif
