@@ -154,11 +154,11 @@ def kernel_bytes(p, esz):
     nk = (p.Lx // 2 + 1) * p.Ly * p.Lz  # half-spectrum points per component
     c = 2 * esz
     return {
-        "k_kick(35a)+np_pre": 9 * N * esz, "k_drift": 9 * N * esz, "k_kick(35f)+np_final": 9 * N * esz,
+        "k_kick(35a)+np_pre": 9 * N * esz, "k_drift": 9 * N * esz, "k_kick(35f)+np_post+np_final": 9 * N * esz,
         "k_xy_fwd": 3 * N * esz + 9 * nk * c,
-        "k_z_kspace+homo_strain": 18 * nk * c + 6 * nk * esz,
-        "k_xy_inv": 9 * nk * c + 9 * N * esz,
-        "k_assemble+energies+np_post": 15 * N * esz,
+        "k_z_kspace": 18 * nk * c + 6 * nk * esz,
+        "k_xy_inv+homo_strain": 9 * nk * c + 9 * N * esz,
+        "k_assemble": 15 * N * esz,
     }
 
 

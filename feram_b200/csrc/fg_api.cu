@@ -233,25 +233,28 @@ int launch_xy_fwd(fg_ctx* ctx, const T* src, cplx<T>* spec, int ncomp, int smem,
   return FG_OK;
 }
 
+// strain_prologue: block (0, 0) also runs the k-space energies and the
+// homogeneous strain from the partials of the preceding k_z_kspace.
 template <typename T>
-int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp) {
+int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp, bool strain_prologue = false) {
   const Geom& g = ctx->g;
   with_xy_inv<T>(g.m, g.Ly, [&](auto kern) {
     kern<<<dim3(g.Lz, ncomp), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
         spec, out, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy,
-        ctx->posm, 0);
+        ctx->posm, 0, strain_prologue ? ctx->ph : nullptr, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
   });
   CKL();
   return FG_OK;
 }
 
+// The k-space partials are finished by the next k_xy_inv (strain prologue).
 template <typename T>
 int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
   const Geom& g = ctx->g;
   with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto kern) {
     kern<<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z, ctx->stream>>>(
         (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
-        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, ctx->done + 1);
+        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, nullptr);
   });
   CKL();
   return FG_OK;
@@ -272,9 +275,10 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
                                      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy)))
     return rc;
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
-  if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9))) return rc;
+  if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9, true))) return rc;
+  // np_post: the energies and (35e) are finished by the closing kick's block 0
   k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
-                                                         ctx->part_r, np_post ? TAIL_NP_POST : 1, ctx->done + 2);
+                                                         ctx->part_r, np_post ? TAIL_NONE : 1, ctx->done + 2);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
@@ -283,11 +287,13 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   return FG_OK;
 }
 
+// force_prologue: block 0 first finishes the preceding k_assemble (energies,
+// (35e)) from its partials.
 template <typename T>
-int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE) {
-  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (const T*)ctx->F, coef, ctx->g,
-                                                               ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail,
-                                                               ctx->done, ctx->ph, ctx->sc);
+int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE, bool force_prologue = false) {
+  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+      (T*)ctx->p, (const T*)ctx->F, coef, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail, ctx->done,
+      ctx->ph, ctx->sc, force_prologue ? ctx->part_r : nullptr, ctx->grid_elem);
   CKL();
   return FG_OK;
 }
@@ -300,15 +306,16 @@ int enqueue_drift(fg_ctx* ctx, const double* coef) {
   return FG_OK;
 }
 
-// nose_poincare (nose-poincare.F:24-75): the scalar steps (38), (35c), (35e)
-// and the closing KE/H_NP run in the last block of the preceding kernel.
+// nose_poincare (nose-poincare.F:24-75): (38) and (35c) run in the last
+// block of the opening kick, (35e) in block 0 of the closing kick, the
+// closing KE/H_NP in the last block of the closing kick.
 template <typename T>
 int enqueue_np(fg_ctx* ctx) {
   int rc;
   if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_PRE))) return rc;  // (35a)
   if ((rc = enqueue_drift<T>(ctx, &ctx->sc->drift_coef))) return rc;              // (35d)
   if ((rc = enqueue_force<T>(ctx, true))) return rc;
-  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL))) return rc;  // (35f)
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL, true))) return rc;  // (35f)
   return FG_OK;
 }
 
@@ -880,8 +887,8 @@ int force_now(fg_ctx* ctx) {
   return FG_OK;
 }
 
-const char* kProfNames[FG_NPROF] = {"k_kick(35a)+np_pre", "k_drift", "k_xy_fwd", "k_z_kspace+homo_strain",
-                                    "k_xy_inv", "k_assemble+energies+np_post", "k_kick(35f)+np_final"};
+const char* kProfNames[FG_NPROF] = {"k_kick(35a)+np_pre", "k_drift",    "k_xy_fwd", "k_z_kspace",
+                                    "k_xy_inv+homo_strain", "k_assemble", "k_kick(35f)+np_post+np_final"};
 
 template <typename T>
 int profile_impl(fg_ctx* ctx, int reps, double* ms) {
@@ -903,12 +910,12 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     CK(cudaEventRecord(ev[++k], st));
     rc |= launch_z_kspace<T>(ctx, nullptr);
     CK(cudaEventRecord(ev[++k], st));
-    rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9);
+    rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9, true);
     CK(cudaEventRecord(ev[++k], st));
     k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph,
-                                                           ctx->sc, ctx->part_r, TAIL_NP_POST, ctx->done + 2);
+                                                           ctx->sc, ctx->part_r, TAIL_NONE, ctx->done + 2);
     CK(cudaEventRecord(ev[++k], st));
-    rc |= enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL);
+    rc |= enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL, true);
     CK(cudaEventRecord(ev[++k], st));
     CKL();
     CK(cudaEventSynchronize(ev[FG_NPROF]));

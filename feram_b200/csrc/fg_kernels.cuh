@@ -117,15 +117,71 @@ __device__ double reduce_partials(const double* part, int nblk, int NQ, int q) {
   return r;
 }
 
-// Last-block-done: every block fences its writes and takes a ticket; the
-// block drawing the last ticket sees all of them and finishes the grid-wide
-// work (classic threadfence reduction, no waiting).  The counter is reset
-// for the next launch by that block.
+// The same sums for all NQ columns in one pass: each thread adds its
+// blocks in a fixed order, warps combine with shuffles, warps in order.
+// Every thread receives the NQ totals.
+template <int NQ>
+__device__ void reduce_partials_all(const double* __restrict__ part, int nblk, double (&out)[NQ]) {
+  __shared__ double red[32][NQ];
+  double s[NQ];
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) s[q] = 0.0;
+#pragma unroll 4
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) s[q] += __ldcg(&part[(long long)b * NQ + q]);
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    const double t = warp_sum(s[q]);
+    if (lane == 0) red[wid][q] = t;
+  }
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w][q];
+    out[q] = t;
+  }
+  __syncthreads();
+}
+
+// Scalar work of a tail: thread 0 runs body on shared-memory copies of the
+// constants and scalars, loaded and stored back by the whole block in one
+// round trip each (instead of a chain of dependent global loads and stores
+// by one thread).
+static_assert(sizeof(DevScalars) % 8 == 0, "DevScalars is copied as doubles");
+static_assert(sizeof(Phys) % 8 == 0, "Phys is copied as doubles");
+template <class F>
+__device__ __forceinline__ void scalar_tail(const Phys* __restrict__ ph, DevScalars* sc, F&& body) {
+  __shared__ Phys sph;
+  __shared__ DevScalars ssc;
+  constexpr int NP = (int)(sizeof(Phys) / 8), NS = (int)(sizeof(DevScalars) / 8);
+  for (int i = threadIdx.x; i < NP; i += blockDim.x)
+    reinterpret_cast<double*>(&sph)[i] = __ldg(reinterpret_cast<const double*>(ph) + i);
+  for (int i = threadIdx.x; i < NS; i += blockDim.x)
+    reinterpret_cast<double*>(&ssc)[i] = __ldcg(reinterpret_cast<const double*>(sc) + i);
+  __syncthreads();
+  if (threadIdx.x == 0) body(static_cast<const Phys*>(&sph), &ssc);
+  __syncthreads();
+  for (int i = threadIdx.x; i < NS; i += blockDim.x)
+    reinterpret_cast<double*>(sc)[i] = reinterpret_cast<const double*>(&ssc)[i];
+}
+
+// Last-block-done: thread 0 of every block fences the block's partials and
+// takes a ticket; the block drawing the last ticket sees all of them and
+// finishes the grid-wide work (classic threadfence reduction, no waiting).
+// The counter is reset for the next launch by that block.  Only thread 0
+// fences: the tails read nothing but the partials thread 0 wrote (and values
+// whose writers fence themselves), so the other threads retire without
+// waiting for their bulk stores to drain.
 __device__ __forceinline__ bool is_last_block(unsigned int* counter) {
   __shared__ bool last;
-  __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
+    __threadfence();
     const unsigned t = atomicAdd(counter, 1u);
     last = (t == gridDim.x - 1);
     if (last) *counter = 0u;
@@ -152,6 +208,9 @@ __host__ __device__ inline void short_range_k(const double* j, double kap2x2, co
   S[4] = -4 * j[4] * s[2] * s[0] - 8 * j[6] * s[2] * s[0] * c[1];  // zx
   S[5] = -4 * j[4] * s[0] * s[1] - 8 * j[6] * s[0] * s[1] * c[2];  // xy
 }
+
+__device__ __noinline__ void homo_strain_tail(const Phys* __restrict__ ph, DevScalars* sc,
+                                              const double* __restrict__ part_k, int nblk);
 
 // ------------------------------------------------------------------ k_xy_fwd
 enum { SRC_U9 = 0, SRC_FIELD = 1 };
@@ -282,7 +341,13 @@ template <typename T, int MC = 0, int LYC = 0>
 __global__ void __launch_bounds__(512, 2) k_xy_inv(const cplx<T>* __restrict__ spec, T* __restrict__ out, Geom g,
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
-                                                const int* __restrict__ posm, int in_comp0) {
+                                                const int* __restrict__ posm, int in_comp0,
+                                                const Phys* __restrict__ ph, DevScalars* sc,
+                                                const double* __restrict__ part_k, int nblk_k) {
+  // Block (0, 0) first finishes the k-space pass that wrote spec: its
+  // energies and the homogeneous strain, from k_z_kspace's block partials
+  // (nothing in this kernel needs them; k_assemble does).
+  if (ph != nullptr && blockIdx.x == 0 && blockIdx.y == 0) homo_strain_tail(ph, sc, part_k, nblk_k);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
@@ -359,15 +424,19 @@ struct ZTiles {
   int nnyq;  // ceil(Ly / CW)
 };
 
+// Blocks 0 .. nnyq-1 take the Nyquist tiles (kx = Lx/2 batched across ky,
+// one uncoalesced 8-byte access per element), the rest the regular tiles:
+// the slow tiles start first instead of trailing the grid.
 __device__ __forceinline__ bool tile_pencil(const ZTiles& zt, const Geom& g, int cw, int* col, int* yslot) {
   const int b = blockIdx.x;
-  if (b < zt.nreg) {
-    *yslot = b / zt.ntx;
-    *col = (b - *yslot * zt.ntx) * zt.CW + cw;
+  if (b >= zt.nnyq) {
+    const int r = b - zt.nnyq;
+    *yslot = r / zt.ntx;
+    *col = (r - *yslot * zt.ntx) * zt.CW + cw;
     return true;
   }
   *col = g.m;
-  *yslot = (b - zt.nreg) * zt.CW + cw;
+  *yslot = b * zt.CW + cw;
   return *yslot < g.Ly;
 }
 
@@ -429,106 +498,79 @@ __device__ __forceinline__ void check_finite(DevScalars* sc, const double* v, in
 
 // After the k-space pass: k-space energies, homogeneous strain
 // (optimize-homo-strain.F:27-186) and w_hom for k_assemble.
-__device__ void homo_strain_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part_k,
-                                 int nblk) {
+__device__ __noinline__ void homo_strain_tail(const Phys* __restrict__ ph, DevScalars* sc,
+                                              const double* __restrict__ part_k, int nblk) {
   double v[NQ_K];
-  for (int q = 0; q < NQ_K; ++q) v[q] = reduce_partials(part_k, nblk, NQ_K, q);
-  if (threadIdx.x != 0) return;
-  double* e = sc->e;
-  const double es = v[0] * ph->Ninv / 2;       // (1/2N) sum w' Re(uK* S uK)
-  const double edd = v[1] / 2;                 // (1/2)  sum w' Re(uK* D uK), D = (S + Z*^2 L)/N
-  e[E_SHORT] = es;
-  e[E_LONG] = edd - es;
-  e[E_IS] = v[2] * ph->Ninv;
-  e[E_IC] = v[3] * 2 * ph->Ninv;
-  e[E_IM] = ph->modulation_on ? v[4] * 2 * ph->Ninv : 0.0;
-  double hc2uu[6];
-  for (int i = 0; i < 6; ++i) {
-    double s = 0.0;
-    for (int jj = 0; jj < 6; ++jj) s += ph->HC2[i][jj] * __ldcg(&sc->didiK0[jj]);
-    hc2uu[i] = s;
-  }
-  for (int i = 0; i < 3; ++i) hc2uu[i] = hc2uu[i] + ph->pNa03[i];
-  double* st = sc->strain;
-  const double(*H)[6] = ph->H;
-  if (ph->bulk_or_film == 2) {  // epit
-    st[0] = ph->epi_strain;
-    st[1] = ph->epi_strain;
-    st[2] = (-(H[2][0] + H[2][1]) * ph->epi_strain - hc2uu[2]) / H[2][2];
-    st[3] = -hc2uu[3] / H[3][3];
-    st[4] = -hc2uu[4] / H[4][4];
-    st[5] = 0.0;
-  } else if (ph->bulk_or_film == 3) {  // e110
-    st[2] = ph->epi_strain;
-    st[3] = 0.0;
-    st[4] = 0.0;
-    double num = -(H[0][0] + H[1][1] + 2 * H[1][1]) * ph->epi_strain - (H[2][0] + H[2][1]) * st[2] - hc2uu[0] - hc2uu[1] +
-                 2 * hc2uu[5];
-    double den = H[0][0] + H[1][1] + 2 * H[1][0] + 4 * H[5][5];
-    double delta = num / den;
-    st[0] = ph->epi_strain + delta;
-    st[1] = ph->epi_strain + delta;
-    st[5] = -2 * delta;
-  } else {
-    for (int i = 0; i < 6; ++i) st[i] = -hc2uu[i];
+  reduce_partials_all<NQ_K>(part_k, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    double* e = S->e;
+    const double es = v[0] * P->Ninv / 2;  // (1/2N) sum w' Re(uK* S uK)
+    const double edd = v[1] / 2;           // (1/2)  sum w' Re(uK* D uK), D = (S + Z*^2 L)/N
+    e[E_SHORT] = es;
+    e[E_LONG] = edd - es;
+    e[E_IS] = v[2] * P->Ninv;
+    e[E_IC] = v[3] * 2 * P->Ninv;
+    e[E_IM] = P->modulation_on ? v[4] * 2 * P->Ninv : 0.0;
+    double hc2uu[6];
     for (int i = 0; i < 6; ++i) {
       double t = 0.0;
-      for (int jj = 0; jj < i; ++jj) t = t + ph->HG[i][jj] * st[jj];
-      st[i] = (st[i] - t) * ph->HG_inv[i];
+      for (int jj = 0; jj < 6; ++jj) t += P->HC2[i][jj] * S->didiK0[jj];
+      hc2uu[i] = t;
     }
-    for (int i = 5; i >= 0; --i) {
-      double t = 0.0;
-      for (int jj = i + 1; jj < 6; ++jj) t = t + st[jj] * ph->HG[jj][i];
-      st[i] = (st[i] - t) * ph->HG_inv[i];
+    for (int i = 0; i < 3; ++i) hc2uu[i] = hc2uu[i] + P->pNa03[i];
+    double* st = S->strain;
+    const double(*H)[6] = P->H;
+    if (P->bulk_or_film == 2) {  // epit
+      st[0] = P->epi_strain;
+      st[1] = P->epi_strain;
+      st[2] = (-(H[2][0] + H[2][1]) * P->epi_strain - hc2uu[2]) / H[2][2];
+      st[3] = -hc2uu[3] / H[3][3];
+      st[4] = -hc2uu[4] / H[4][4];
+      st[5] = 0.0;
+    } else if (P->bulk_or_film == 3) {  // e110
+      st[2] = P->epi_strain;
+      st[3] = 0.0;
+      st[4] = 0.0;
+      double num = -(H[0][0] + H[1][1] + 2 * H[1][1]) * P->epi_strain - (H[2][0] + H[2][1]) * st[2] - hc2uu[0] -
+                   hc2uu[1] + 2 * hc2uu[5];
+      double den = H[0][0] + H[1][1] + 2 * H[1][0] + 4 * H[5][5];
+      double delta = num / den;
+      st[0] = P->epi_strain + delta;
+      st[1] = P->epi_strain + delta;
+      st[5] = -2 * delta;
+    } else {
+      for (int i = 0; i < 6; ++i) st[i] = -hc2uu[i];
+      for (int i = 0; i < 6; ++i) {
+        double t = 0.0;
+        for (int jj = 0; jj < i; ++jj) t = t + P->HG[i][jj] * st[jj];
+        st[i] = (st[i] - t) * P->HG_inv[i];
+      }
+      for (int i = 5; i >= 0; --i) {
+        double t = 0.0;
+        for (int jj = i + 1; jj < 6; ++jj) t = t + st[jj] * P->HG[jj][i];
+        st[i] = (st[i] - t) * P->HG_inv[i];
+      }
     }
-  }
-  double hs = 0.0;
-  for (int i = 0; i < 6; ++i) {
-    double d = 0.0;
-    for (int jj = 0; jj < 6; ++jj) d += H[i][jj] * st[jj];
-    hs = hs + st[i] * d;
-  }
-  e[E_HS] = hs / 2;
-  double hc = 0.0;
-  for (int i = 0; i < 6; ++i) hc += st[i] * hc2uu[i];
-  e[E_HC] = hc;
-  for (int jj = 0; jj < 6; ++jj) {
-    double w = 0.0;
-    for (int i = 0; i < 6; ++i) w = w + st[i] * ph->HC2[i][jj];
-    sc->w_hom[jj] = w;
-  }
-}
-
-// After k_assemble: real-space energies.
-__device__ void force_energies_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part_r,
-                                    int nblk) {
-  double v0 = reduce_partials(part_r, nblk, NQ_R, 0);
-  double v1 = reduce_partials(part_r, nblk, NQ_R, 1);
-  if (threadIdx.x != 0) return;
-  sc->e[E_UNH] = v0;
-  sc->e[E_DIPE] = ph->E_on ? -v1 : 0.0;
-  check_finite(sc, sc->e + E_SHORT, 9);
+    double hs = 0.0;
+    for (int i = 0; i < 6; ++i) {
+      double d = 0.0;
+      for (int jj = 0; jj < 6; ++jj) d += H[i][jj] * st[jj];
+      hs = hs + st[i] * d;
+    }
+    e[E_HS] = hs / 2;
+    double hc = 0.0;
+    for (int i = 0; i < 6; ++i) hc += st[i] * hc2uu[i];
+    e[E_HC] = hc;
+    for (int jj = 0; jj < 6; ++jj) {
+      double w = 0.0;
+      for (int i = 0; i < 6; ++i) w = w + st[i] * P->HC2[i][jj];
+      S->w_hom[jj] = w;
+    }
+  });
 }
 
 // kinetic_energy_dipo.F:106 from the kick partials
 __device__ __forceinline__ double ke_from(const Phys* ph, double sum) { return sum / ph->n_sum_p * ph->N / 2; }
-
-// Nose-Poincare, first half (nose-poincare.F:30-41): KE, (38), (35c).
-__device__ void np_pre_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
-  double v = reduce_partials(part, nblk, 1, 0);
-  if (threadIdx.x != 0) return;
-  double* e = sc->e;
-  sc->ke_sum = v;
-  e[E_DIPO] = ke_from(ph, v);
-  double s = sc->s;
-  double CB = ph->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - sc->H0;
-  CB = ph->dt_2 * CB - sc->pi;
-  if (1.0 - CB * ph->dt / ph->Q < 0.0) sc->status = 10;  // (38) has no real root: Q_Nose too small
-  sc->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * ph->dt / ph->Q));
-  sc->s_old = s;
-  sc->s = s * (1.0 + ph->dt_2 * sc->pi / ph->Q) / (1.0 - ph->dt_2 * sc->pi / ph->Q);
-  sc->drift_coef = ph->dt_2 * (1 / sc->s + 1 / sc->s_old);
-}
 
 // Nose-Poincare after the force (nose-poincare.F:60-66): H_NP, (35e).
 // Thread 0 only.
@@ -537,29 +579,65 @@ __device__ void np_post_body(const Phys* __restrict__ ph, DevScalars* sc) {
   const double s = sc->s;
   const double delta_H = sc->e[E_HNP] / s;
   sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] / (s * s) - ph->nf_kT) - ph->dt_2 * delta_H;
-  sc->kick_coef = ph->dt_2 * s;
+}
+
+// After k_assemble: real-space energies, and with np_post the (35e) update.
+__device__ __noinline__ void force_energies_tail(const Phys* __restrict__ ph, DevScalars* sc,
+                                                 const double* __restrict__ part_r, int nblk, bool np_post) {
+  double v[NQ_R];
+  reduce_partials_all<NQ_R>(part_r, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    S->e[E_UNH] = v[0];
+    S->e[E_DIPE] = P->E_on ? -v[1] : 0.0;
+    check_finite(S, S->e + E_SHORT, 9);
+    if (np_post) np_post_body(P, S);
+  });
+}
+
+// Nose-Poincare, first half (nose-poincare.F:30-41): KE, (38), (35c).
+__device__ void np_pre_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
+  double v[1];
+  reduce_partials_all<1>(part, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    double* e = S->e;
+    S->ke_sum = v[0];
+    e[E_DIPO] = ke_from(P, v[0]);
+    const double s = S->s;
+    double CB = P->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - S->H0;
+    CB = P->dt_2 * CB - S->pi;
+    if (1.0 - CB * P->dt / P->Q < 0.0) S->status = 10;  // (38) has no real root: Q_Nose too small
+    S->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * P->dt / P->Q));
+    S->s_old = s;
+    S->s = s * (1.0 + P->dt_2 * S->pi / P->Q) / (1.0 - P->dt_2 * S->pi / P->Q);
+    S->drift_coef = P->dt_2 * (1 / S->s + 1 / S->s_old);
+    S->kick_coef = P->dt_2 * S->s;  // (35f) of this step and (35a) of the next
+  });
 }
 
 // After the closing kick: KE, H_NP, total (nose-poincare.F:74-75,
 // molecular-dynamics.F:293).
 __device__ void np_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
-  double v = reduce_partials(part, nblk, 1, 0);
-  if (threadIdx.x != 0) return;
-  sc->ke_sum = v;
-  sc->e[E_DIPO] = ke_from(ph, v);
-  np_hamiltonian(ph, sc);
-  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
-  check_finite(sc, sc->e, E_COUNT);
+  double v[1];
+  reduce_partials_all<1>(part, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    S->ke_sum = v[0];
+    S->e[E_DIPO] = ke_from(P, v[0]);
+    np_hamiltonian(P, S);
+    S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
+    check_finite(S, S->e, E_COUNT);
+  });
 }
 
 // Leapfrog closing reduction (leapfrog.F:151) and total.
 __device__ void lf_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
-  double v = reduce_partials(part, nblk, 1, 0);
-  if (threadIdx.x != 0) return;
-  sc->ke_sum = v;
-  sc->e[E_DIPO] = ke_from(ph, v);
-  sc->e[E_TOT] = sc->e[E_DIPO] / (sc->s * sc->s) + sc->e[E_ACOU] + sum_potential(sc->e);
-  check_finite(sc, sc->e, E_COUNT);
+  double v[1];
+  reduce_partials_all<1>(part, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    S->ke_sum = v[0];
+    S->e[E_DIPO] = ke_from(P, v[0]);
+    S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
+    check_finite(S, S->e, E_COUNT);
+  });
 }
 
 // Standalone launches of the tails (single block of RED_THREADS threads).
@@ -569,14 +647,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_homo_strain(const Phys* __restr
 }
 __global__ void __launch_bounds__(RED_THREADS) k_force_energies(const Phys* __restrict__ ph, DevScalars* sc,
                                                                 const double* __restrict__ part_r, int nblk) {
-  force_energies_tail(ph, sc, part_r, nblk);
+  force_energies_tail(ph, sc, part_r, nblk, false);
 }
 __global__ void __launch_bounds__(RED_THREADS) k_np_pre(const Phys* __restrict__ ph, DevScalars* sc,
                                                         const double* __restrict__ part, int nblk) {
   np_pre_tail(ph, sc, part, nblk);
-}
-__global__ void k_np_post(const Phys* __restrict__ ph, DevScalars* sc) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) np_post_body(ph, sc);
 }
 __global__ void __launch_bounds__(RED_THREADS) k_np_final(const Phys* __restrict__ ph, DevScalars* sc,
                                                           const double* __restrict__ part, int nblk) {
@@ -671,6 +746,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     if (kx == 0 && ky == 0 && kz == 0) {
 #pragma unroll
       for (int i = 0; i < 6; ++i) sc->didiK0[i] = (double)d[i].x;
+      __threadfence();  // read by homo_strain_tail in another block
     }
     // ---- dipole-dipole
     const long long tpos = tpos0 + (long long)zs * g.KXP;
@@ -943,10 +1019,7 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
     }
   }
   block_partials<NQ_R>(acc, part, blockIdx.x);
-  if (tail != TAIL_NONE && is_last_block(done)) {
-    force_energies_tail(ph, sc, part, gridDim.x);
-    if (tail == TAIL_NP_POST && threadIdx.x == 0) np_post_body(ph, sc);
-  }
+  if (tail != TAIL_NONE && is_last_block(done)) force_energies_tail(ph, sc, part, gridDim.x, tail == TAIL_NP_POST);
 }
 
 // --------------------------------------------------------------- integrators
@@ -958,7 +1031,11 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
                                               const double* __restrict__ layer_minv,
                                               const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
                                               int tail, unsigned int* done, const Phys* __restrict__ ph,
-                                              DevScalars* sc) {
+                                              DevScalars* sc, const double* __restrict__ part_r, int nblk_r) {
+  // Block 0 first finishes the preceding force evaluation (its energies and
+  // (35e)) from k_assemble's partials; the closing tail of this kick runs in
+  // the last block to arrive, which is after block 0.
+  if (part_r != nullptr && blockIdx.x == 0) force_energies_tail(ph, sc, part_r, nblk_r, true);
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
