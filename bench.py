@@ -154,7 +154,7 @@ def kernel_bytes(p, esz):
     nk = (p.Lx // 2 + 1) * p.Ly * p.Lz  # half-spectrum points per component
     c = 2 * esz
     return {
-        "k_kick(35a)+np_pre": 9 * N * esz, "k_drift": 9 * N * esz, "k_kick(35f)+np_post+np_final": 9 * N * esz,
+        "k_kick_drift(35a,35c)": 15 * N * esz, "k_kick_close(35e,35f)+np_tail": 9 * N * esz,
         "k_xy_fwd": 3 * N * esz + 9 * nk * c,
         "k_z_kspace": 18 * nk * c + 6 * nk * esz,
         "k_xy_inv+homo_strain": 9 * nk * c + 9 * N * esz,
@@ -331,7 +331,7 @@ def main():
         value64 = p.N * steps64 * world / (ms_fp64 / 1000.0)
 
     # per-kernel times of one step (events between kernels, same stream)
-    nprof = 7
+    nprof = A.FG_NPROF
     prof = (C.c_double * nprof)()
     ctxm._check(A.lib().fg_profile_step(ctxm._h, 20, prof))
     names = [A.lib().fg_profile_name(i).decode() for i in range(nprof)]
@@ -410,7 +410,7 @@ def main():
         "force_err_mixed_vs_fp64": ferr,
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-        "gpu_launches": 7 * args.steps,
+        "gpu_launches": A.FG_NPROF * args.steps,  # kernels per bulk NP step graph
     }
     ctxm.close()
     if ctx64 is not None:

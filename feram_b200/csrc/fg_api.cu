@@ -141,6 +141,7 @@ struct fg_ctx {
   cudaGraphExec_t g_np = nullptr, g_lf = nullptr, g_force = nullptr;
   bool tables_ready = false;
   bool force_fresh = false;
+  bool np_ready = false;  // DevScalars' pending half step matches the state
   bool store_acouK = false;
   double n_sum_p = 0;
   int NXP = 0, NYP = 0;
@@ -278,7 +279,8 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9, true))) return rc;
   // np_post: the energies and (35e) are finished by the closing kick's block 0
   k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
-                                                         ctx->part_r, np_post ? TAIL_NONE : 1, ctx->done + 2);
+                                                         ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
+                                                         ctx->done + 2);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
@@ -287,13 +289,11 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   return FG_OK;
 }
 
-// force_prologue: block 0 first finishes the preceding k_assemble (energies,
-// (35e)) from its partials.
 template <typename T>
-int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE, bool force_prologue = false) {
-  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
-      (T*)ctx->p, (const T*)ctx->F, coef, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail, ctx->done,
-      ctx->ph, ctx->sc, force_prologue ? ctx->part_r : nullptr, ctx->grid_elem);
+int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE) {
+  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (const T*)ctx->F, coef, ctx->g,
+                                                               ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail,
+                                                               ctx->done, ctx->ph, ctx->sc);
   CKL();
   return FG_OK;
 }
@@ -306,17 +306,38 @@ int enqueue_drift(fg_ctx* ctx, const double* coef) {
   return FG_OK;
 }
 
-// nose_poincare (nose-poincare.F:24-75): (38) and (35c) run in the last
-// block of the opening kick, (35e) in block 0 of the closing kick, the
-// closing KE/H_NP in the last block of the closing kick.
+template <typename T>
+int enqueue_kick_drift(fg_ctx* ctx) {
+  k_kick_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
+                                                                     ctx->sc, ctx->g, ctx->layer_minv);
+  CKL();
+  return FG_OK;
+}
+
+// prep: sums of the current state only (np_prepare)
+template <typename T, bool PREP>
+int enqueue_kick_close(fg_ctx* ctx) {
+  k_kick_close<T, PREP><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+      (T*)ctx->p, (const T*)ctx->F, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, ctx->done, ctx->ph,
+      ctx->sc, ctx->part_r, ctx->grid_elem);
+  CKL();
+  return FG_OK;
+}
+
+// nose_poincare (nose-poincare.F:24-75) as one graph of six kernels:
+//   k_kick_drift       (35a) + (35c) with the coefficients prepared by the
+//                      previous closing tail ((38) solved there)
+//   force              xy_fwd, z_kspace, xy_inv (+ homogeneous strain),
+//                      k_assemble (partials only)
+//   k_kick_close       block 0: energies, commit of the half step, (35e);
+//                      all: (35f) and the three kinetic sums; last block:
+//                      KE, H_NP of this step and the scalars of the next.
 template <typename T>
 int enqueue_np(fg_ctx* ctx) {
   int rc;
-  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_PRE))) return rc;  // (35a)
-  if ((rc = enqueue_drift<T>(ctx, &ctx->sc->drift_coef))) return rc;              // (35d)
+  if ((rc = enqueue_kick_drift<T>(ctx))) return rc;
   if ((rc = enqueue_force<T>(ctx, true))) return rc;
-  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL, true))) return rc;  // (35f)
-  return FG_OK;
+  return enqueue_kick_close<T, false>(ctx);
 }
 
 // leapfrog (leapfrog.F:103-151), i_step != 0
@@ -640,7 +661,7 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaMemset(ctx->acouK, 0, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
   CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)(ctx->zt.nreg + ctx->zt.nnyq)));
   CK(cudaMalloc(&ctx->part_r, sizeof(double) * NQ_R * (size_t)ctx->grid_elem));
-  CK(cudaMalloc(&ctx->part_ke, sizeof(double) * (size_t)ctx->grid_elem));
+  CK(cudaMalloc(&ctx->part_ke, sizeof(double) * 3 * (size_t)ctx->grid_elem));
   CK(cudaMalloc(&ctx->part_avg, sizeof(double) * 6 * (size_t)ctx->grid_elem));
   CK(cudaMalloc(&ctx->avg6, sizeof(double) * 6));
   CK(cudaMalloc(&ctx->done, sizeof(unsigned int) * 4));
@@ -847,6 +868,7 @@ int fft_r2c3_impl(fg_ctx* ctx, const double* in, double* out) {
           out[2 * f + 1] = (double)v.y;
         }
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return FG_OK;
 }
 
@@ -871,6 +893,7 @@ int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
   rc = get_field<T>(ctx, out, ctx->rwork);
   if (rc) return rc;
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return check_device_error(ctx);
 }
 
@@ -884,11 +907,29 @@ int force_now(fg_ctx* ctx) {
   int rc = run_graph(ctx, &ctx->g_force, 0);
   if (rc) return rc;
   ctx->force_fresh = true;
+  ctx->np_ready = false;
   return FG_OK;
 }
 
-const char* kProfNames[FG_NPROF] = {"k_kick(35a)+np_pre", "k_drift",    "k_xy_fwd", "k_z_kspace",
-                                    "k_xy_inv+homo_strain", "k_assemble", "k_kick(35f)+np_post+np_final"};
+// Scalars of the first half of the next Nose-Poincare step from the current
+// state (after the state, the thermostat or the force changed outside a step).
+int np_prepare(fg_ctx* ctx) {
+  int rc = ctx->prec == FG_PREC_MIXED ? enqueue_kick_close<float, true>(ctx) : enqueue_kick_close<double, true>(ctx);
+  if (rc) return rc;
+  ctx->np_ready = true;
+  return FG_OK;
+}
+
+// Everything a Nose-Poincare graph launch needs before it starts.
+int np_ready_for_step(fg_ctx* ctx) {
+  int rc;
+  if (!ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  if (!ctx->np_ready && (rc = np_prepare(ctx))) return rc;
+  return FG_OK;
+}
+
+const char* kProfNames[FG_NPROF] = {"k_kick_drift(35a,35c)", "k_xy_fwd", "k_z_kspace", "k_xy_inv+homo_strain",
+                                    "k_assemble", "k_kick_close(35e,35f)+np_tail"};
 
 template <typename T>
 int profile_impl(fg_ctx* ctx, int reps, double* ms) {
@@ -901,9 +942,7 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
   for (int r = 0; r < reps && rc == FG_OK; ++r) {
     int k = 0;
     CK(cudaEventRecord(ev[k], st));
-    rc |= enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_PRE);
-    CK(cudaEventRecord(ev[++k], st));
-    rc |= enqueue_drift<T>(ctx, &ctx->sc->drift_coef);
+    rc |= enqueue_kick_drift<T>(ctx);
     CK(cudaEventRecord(ev[++k], st));
     rc |= launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
                                    (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy);
@@ -915,7 +954,7 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph,
                                                            ctx->sc, ctx->part_r, TAIL_NONE, ctx->done + 2);
     CK(cudaEventRecord(ev[++k], st));
-    rc |= enqueue_kick<T>(ctx, &ctx->sc->kick_coef, TAIL_NP_FINAL, true);
+    rc |= enqueue_kick_close<T, false>(ctx);
     CK(cudaEventRecord(ev[++k], st));
     CKL();
     CK(cudaEventSynchronize(ev[FG_NPROF]));
@@ -982,12 +1021,14 @@ void* fg_stream(fg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 int fg_build_tables(fg_ctx* ctx) {
   if (!ctx || !ctx->stream) return FG_ERR_ARG;
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return ctx->prec == FG_PREC_MIXED ? build_tables_impl<float>(ctx) : build_tables_impl<double>(ctx);
 }
 
 int fg_upload_tables(fg_ctx* ctx, const double* short_range, const double* long_range) {
   if (!ctx || !ctx->stream || !short_range || !long_range) return FG_ERR_ARG;
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return ctx->prec == FG_PREC_MIXED ? upload_tables_impl<float>(ctx, short_range, long_range)
                                     : upload_tables_impl<double>(ctx, short_range, long_range);
 }
@@ -997,6 +1038,7 @@ int fg_upload_modulation(fg_ctx* ctx, const double* ck) {
   int rc = ctx->prec == FG_PREC_MIXED ? upload_modulation_impl<float>(ctx, ck) : upload_modulation_impl<double>(ctx, ck);
   if (rc) return rc;
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return set_modulation_flag(ctx, (ck && ctx->P.modulation_constant != 0.0) ? 1 : 0);
 }
 
@@ -1007,6 +1049,7 @@ int fg_set_modulation_R(fg_ctx* ctx, const double* modR) {
   int rc = ctx->prec == FG_PREC_MIXED ? set_modulation_R_impl<float>(ctx, modR) : set_modulation_R_impl<double>(ctx, modR);
   if (rc) return rc;
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return set_modulation_flag(ctx, 1);
 }
 
@@ -1058,6 +1101,7 @@ int fg_set_state(fg_ctx* ctx, const double* dipoR, const double* dipoP, double s
   ctx->sc_host->kick_coef = ctx->P.dt_2 * s;
   if ((rc = push_scalars(ctx))) return rc;
   ctx->force_fresh = false;
+  ctx->np_ready = false;
   return FG_OK;
 }
 
@@ -1069,6 +1113,7 @@ int fg_set_thermostat(fg_ctx* ctx, double s, double pi, double H0) {
   ctx->sc_host->pi = pi;
   ctx->sc_host->H0 = H0;
   ctx->sc_host->kick_coef = ctx->P.dt_2 * s;
+  ctx->np_ready = false;
   return push_scalars(ctx);
 }
 
@@ -1100,6 +1145,7 @@ int fg_get_acouK(fg_ctx* ctx, double* acouK) {
   if (rc) return rc;
   if ((rc = pull_scalars(ctx))) return rc;
   ctx->force_fresh = true;
+  ctx->np_ready = false;
   return ctx->prec == FG_PREC_MIXED ? get_acouK_impl<float>(ctx, acouK) : get_acouK_impl<double>(ctx, acouK);
 }
 
@@ -1125,8 +1171,9 @@ int fg_mirror_force_mirror(fg_ctx* ctx, fg_energy* e) {
 int fg_nose_poincare(fg_ctx* ctx, fg_energy* e) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
-  if (!ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  if ((rc = np_ready_for_step(ctx))) return rc;
   if ((rc = run_graph(ctx, &ctx->g_np, 1))) return rc;
+  ctx->np_ready = true;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) energy_out(ctx->sc_host, e, false);
   return FG_OK;
@@ -1145,6 +1192,7 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
     if ((rc = run_graph(ctx, &ctx->g_lf, 2))) return rc;
   }
   ctx->force_fresh = true;
+  ctx->np_ready = false;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) {
     e->dipo_kinetic = ctx->sc_host->e[E_DIPO];
@@ -1156,13 +1204,14 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
 int fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
-  if (ctx->P.method == FG_METHOD_MD && !ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  if (ctx->P.method == FG_METHOD_MD && (rc = np_ready_for_step(ctx))) return rc;
   for (int i = 0; i < n_steps; ++i) {
     if (ctx->P.method == FG_METHOD_MD) rc = run_graph(ctx, &ctx->g_np, 1);
     else rc = run_graph(ctx, &ctx->g_lf, 2);
     if (rc) return rc;
   }
   ctx->force_fresh = true;
+  ctx->np_ready = ctx->P.method == FG_METHOD_MD;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) energy_out(ctx->sc_host, e, false);
   return FG_OK;
@@ -1172,7 +1221,7 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
   if (!ms || n_steps < 1) return FG_ERR_ARG;
-  if (ctx->P.method == FG_METHOD_MD && !ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  if (ctx->P.method == FG_METHOD_MD && (rc = np_ready_for_step(ctx))) return rc;
   // make sure the graph exists before the timed region
   cudaGraphExec_t* gx = ctx->P.method == FG_METHOD_MD ? &ctx->g_np : &ctx->g_lf;
   const int which = ctx->P.method == FG_METHOD_MD ? 1 : 2;
@@ -1194,6 +1243,7 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
   cudaEventDestroy(e1);
   *ms = t;
   ctx->force_fresh = true;
+  ctx->np_ready = ctx->P.method == FG_METHOD_MD;
   return pull_scalars(ctx);
 }
 
@@ -1204,10 +1254,11 @@ int fg_profile_step(fg_ctx* ctx, int reps, double* ms) {
   if (rc) return rc;
   if (!ms || reps < 1) return FG_ERR_ARG;
   if (ctx->bulk_or_film_mirror()) return fail(ctx, FG_ERR_UNSUPPORTED, "profile covers the bulk step only");
-  if (!ctx->force_fresh && (rc = force_now(ctx))) return rc;
+  if ((rc = np_ready_for_step(ctx))) return rc;
   rc = ctx->prec == FG_PREC_MIXED ? profile_impl<float>(ctx, reps, ms) : profile_impl<double>(ctx, reps, ms);
   if (rc) return rc;
   ctx->force_fresh = true;
+  ctx->np_ready = true;
   return pull_scalars(ctx);
 }
 

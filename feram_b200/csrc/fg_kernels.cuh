@@ -67,6 +67,12 @@ struct DevScalars {
   double didiK0[6];   // Re didiK(k = 0)
   double E[3];        // uniform external field
   double ke_sum;      // last masked sum p^2/m
+  // Nose-Poincare half step (35a), (38), (35c) of the next step, prepared by
+  // the closing tail of the previous one (or by np_prepare) and committed by
+  // block 0 of the next closing kick: masked sum p^2/m and KE at the half
+  // step, pi_{n+1/2}, s_{n+1}, the drift coefficient and the (35f) kick
+  // coefficient dt/2 s_{n+1}.
+  double pend_ke_sum, pend_ke, pend_pi, pend_s, pend_drift, pend_kick_f;
   int status;
   int pad;
 };
@@ -478,7 +484,7 @@ __device__ __forceinline__ void z_tile_store(const cplx<T>* buf, cplx<T>* __rest
 // ------------------------------------------------------------ scalar kernels
 // Grid-wide scalar steps; each runs either as a single-block kernel or in the
 // last block of the kernel whose partial sums it reduces (tail).
-enum { TAIL_NONE = 0, TAIL_NP_PRE = 1, TAIL_NP_FINAL = 2, TAIL_LF_FINAL = 3, TAIL_NP_POST = 4 };
+enum { TAIL_NONE = 0, TAIL_ENERGIES = 1, TAIL_LF_FINAL = 3 };
 
 __device__ __forceinline__ double sum_potential(const double* e) {
   return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
@@ -581,50 +587,66 @@ __device__ void np_post_body(const Phys* __restrict__ ph, DevScalars* sc) {
   sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] / (s * s) - ph->nf_kT) - ph->dt_2 * delta_H;
 }
 
-// After k_assemble: real-space energies, and with np_post the (35e) update.
+// After k_assemble: real-space energies.  With np_close also the commit of
+// the prepared half step ((38), (35c): s, pi, KE at the half step) and the
+// (35e) update of pi, as the closing kick of a Nose-Poincare step needs.
 __device__ __noinline__ void force_energies_tail(const Phys* __restrict__ ph, DevScalars* sc,
-                                                 const double* __restrict__ part_r, int nblk, bool np_post) {
+                                                 const double* __restrict__ part_r, int nblk, bool np_close) {
   double v[NQ_R];
   reduce_partials_all<NQ_R>(part_r, nblk, v);
   scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
     S->e[E_UNH] = v[0];
     S->e[E_DIPE] = P->E_on ? -v[1] : 0.0;
     check_finite(S, S->e + E_SHORT, 9);
-    if (np_post) np_post_body(P, S);
+    if (np_close) {
+      S->s_old = S->s;
+      S->s = S->pend_s;
+      S->pi = S->pend_pi;
+      S->ke_sum = S->pend_ke_sum;
+      S->e[E_DIPO] = S->pend_ke;
+      S->drift_coef = S->pend_drift;
+      np_post_body(P, S);
+    }
   });
 }
 
-// Nose-Poincare, first half (nose-poincare.F:30-41): KE, (38), (35c).
-__device__ void np_pre_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
-  double v[1];
-  reduce_partials_all<1>(part, nblk, v);
+// Closing tail of a Nose-Poincare step.  part holds per block the masked
+// sums of p^2/m, p.F/m and F^2/m after the closing kick (35f).
+//  - step_done: KE, H_NP and total of the finished step (nose-poincare.F:
+//    74-75, molecular-dynamics.F:293);
+//  - always: the first half of the next step (nose-poincare.F:24-41) as far
+//    as it is scalar: its kick (35a) p - c F with c = dt/2 s has the kinetic
+//    sum  sum p^2/m - 2 c sum p.F/m + c^2 sum F^2/m,  which gives (38) pi,
+//    s_{n+1} and the drift coefficient of (35c) before any site is touched.
+//    They are kept pending (s and pi still report the finished step).
+__device__ __noinline__ void np_close_tail(const Phys* __restrict__ ph, DevScalars* sc,
+                                           const double* __restrict__ part, int nblk, bool step_done) {
+  double v[3];
+  reduce_partials_all<3>(part, nblk, v);
   scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
-    double* e = S->e;
-    S->ke_sum = v[0];
-    e[E_DIPO] = ke_from(P, v[0]);
+    if (step_done) {
+      S->ke_sum = v[0];
+      S->e[E_DIPO] = ke_from(P, v[0]);
+      np_hamiltonian(P, S);
+      S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
+      check_finite(S, S->e, E_COUNT);
+    }
     const double s = S->s;
-    double CB = P->nf_kT * (1.0 + log(s)) - e[E_DIPO] / (s * s) + sum_potential(e) - S->H0;
+    const double ca = P->dt_2 * s;
+    const double kh = v[0] - 2 * ca * v[1] + ca * ca * v[2];
+    const double ke = ke_from(P, kh);
+    double CB = P->nf_kT * (1.0 + log(s)) - ke / (s * s) + sum_potential(S->e) - S->H0;
     CB = P->dt_2 * CB - S->pi;
     if (1.0 - CB * P->dt / P->Q < 0.0) S->status = 10;  // (38) has no real root: Q_Nose too small
-    S->pi = -2 * CB / (1.0 + sqrt(1.0 - CB * P->dt / P->Q));
-    S->s_old = s;
-    S->s = s * (1.0 + P->dt_2 * S->pi / P->Q) / (1.0 - P->dt_2 * S->pi / P->Q);
-    S->drift_coef = P->dt_2 * (1 / S->s + 1 / S->s_old);
-    S->kick_coef = P->dt_2 * S->s;  // (35f) of this step and (35a) of the next
-  });
-}
-
-// After the closing kick: KE, H_NP, total (nose-poincare.F:74-75,
-// molecular-dynamics.F:293).
-__device__ void np_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
-  double v[1];
-  reduce_partials_all<1>(part, nblk, v);
-  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
-    S->ke_sum = v[0];
-    S->e[E_DIPO] = ke_from(P, v[0]);
-    np_hamiltonian(P, S);
-    S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
-    check_finite(S, S->e, E_COUNT);
+    const double pih = -2 * CB / (1.0 + sqrt(1.0 - CB * P->dt / P->Q));
+    const double sn = s * (1.0 + P->dt_2 * pih / P->Q) / (1.0 - P->dt_2 * pih / P->Q);
+    S->kick_coef = ca;
+    S->pend_ke_sum = kh;
+    S->pend_ke = ke;
+    S->pend_pi = pih;
+    S->pend_s = sn;
+    S->pend_drift = P->dt_2 * (1 / sn + 1 / s);
+    S->pend_kick_f = P->dt_2 * sn;
   });
 }
 
@@ -638,28 +660,6 @@ __device__ void lf_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const
     S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
     check_finite(S, S->e, E_COUNT);
   });
-}
-
-// Standalone launches of the tails (single block of RED_THREADS threads).
-__global__ void __launch_bounds__(RED_THREADS) k_homo_strain(const Phys* __restrict__ ph, DevScalars* sc,
-                                                             const double* __restrict__ part_k, int nblk) {
-  homo_strain_tail(ph, sc, part_k, nblk);
-}
-__global__ void __launch_bounds__(RED_THREADS) k_force_energies(const Phys* __restrict__ ph, DevScalars* sc,
-                                                                const double* __restrict__ part_r, int nblk) {
-  force_energies_tail(ph, sc, part_r, nblk, false);
-}
-__global__ void __launch_bounds__(RED_THREADS) k_np_pre(const Phys* __restrict__ ph, DevScalars* sc,
-                                                        const double* __restrict__ part, int nblk) {
-  np_pre_tail(ph, sc, part, nblk);
-}
-__global__ void __launch_bounds__(RED_THREADS) k_np_final(const Phys* __restrict__ ph, DevScalars* sc,
-                                                          const double* __restrict__ part, int nblk) {
-  np_final_tail(ph, sc, part, nblk);
-}
-__global__ void __launch_bounds__(RED_THREADS) k_lf_final(const Phys* __restrict__ ph, DevScalars* sc,
-                                                          const double* __restrict__ part, int nblk) {
-  lf_final_tail(ph, sc, part, nblk);
 }
 
 // Wavevectors, trig tables and slot maps shared by the k-space kernels.
@@ -1019,23 +1019,19 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
     }
   }
   block_partials<NQ_R>(acc, part, blockIdx.x);
-  if (tail != TAIL_NONE && is_last_block(done)) force_energies_tail(ph, sc, part, gridDim.x, tail == TAIL_NP_POST);
+  if (tail == TAIL_ENERGIES && is_last_block(done)) force_energies_tail(ph, sc, part, gridDim.x, false);
 }
 
 // --------------------------------------------------------------- integrators
-// p <- p - coef * F on every site (nose-poincare.F:24-28,66-71, leapfrog.F:
-// 134-138) and the masked sum p^2 m^-1 of kinetic_energy_dipo.F:92-105.
-// Per-layer masses and sum_p masks (film halves, dead layers).
+// p <- p - coef * F on every site (leapfrog.F:134-138) and the masked sum
+// p^2 m^-1 of kinetic_energy_dipo.F:92-105.  Per-layer masses and sum_p
+// masks (film halves, dead layers).
 template <typename T>
 __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __restrict__ F, const double* coef, Geom g,
                                               const double* __restrict__ layer_minv,
                                               const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
                                               int tail, unsigned int* done, const Phys* __restrict__ ph,
-                                              DevScalars* sc, const double* __restrict__ part_r, int nblk_r) {
-  // Block 0 first finishes the preceding force evaluation (its energies and
-  // (35e)) from k_assemble's partials; the closing tail of this kick runs in
-  // the last block to arrive, which is after block 0.
-  if (part_r != nullptr && blockIdx.x == 0) force_energies_tail(ph, sc, part_r, nblk_r, true);
+                                              DevScalars* sc) {
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
@@ -1076,11 +1072,124 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
     }
   }
   block_partials<1>(acc, part, blockIdx.x);
-  if (tail != TAIL_NONE && is_last_block(done)) {
-    if (tail == TAIL_NP_PRE) np_pre_tail(ph, sc, part, gridDim.x);
-    else if (tail == TAIL_NP_FINAL) np_final_tail(ph, sc, part, gridDim.x);
-    else if (tail == TAIL_LF_FINAL) lf_final_tail(ph, sc, part, gridDim.x);
+  if (tail == TAIL_LF_FINAL && is_last_block(done)) lf_final_tail(ph, sc, part, gridDim.x);
+}
+
+// Opening half of a Nose-Poincare step in one sweep: the kick (35a)
+// p <- p - kick_coef F and the drift (35c) u <- u + drift p m^-1
+// (nose-poincare.F:24-53).  Both coefficients come from the previous closing
+// tail, which already solved (38) with the kinetic energy of the kicked p.
+template <typename T>
+__global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __restrict__ u, const T* __restrict__ F,
+                                                    const DevScalars* __restrict__ sc, Geom g,
+                                                    const double* __restrict__ layer_minv) {
+  const long long ns = g.nsite;
+  const T ck = (T)sc->kick_coef;
+  const double cd = sc->pend_drift;
+  constexpr int NV = V16<T>::n;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (g.plane_r % NV == 0) {
+    for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
+      const long long i = iv * NV;
+      const T f = (T)(cd * layer_minv[(int)(i / g.plane_r)]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        V16<T> q = ldv(p + a * ns + i), x = ldv(u + a * ns + i);
+        const V16<T> y = ldv(F + a * ns + i);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          q.v[l] = q.v[l] - ck * y.v[l];
+          x.v[l] = x.v[l] + f * q.v[l];
+        }
+        stv(p + a * ns + i, q);
+        stv(u + a * ns + i, x);
+      }
+    }
+  } else {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+      const T f = (T)(cd * layer_minv[(int)(i / g.plane_r)]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const T q = p[a * ns + i] - ck * F[a * ns + i];
+        p[a * ns + i] = q;
+        u[a * ns + i] = u[a * ns + i] + f * q;
+      }
+    }
   }
+}
+
+// Closing kick of a Nose-Poincare step (35f), p <- p - dt/2 s_{n+1} F
+// (nose-poincare.F:66-71), with per-block masked sums of p^2/m, p.F/m and
+// F^2/m of the new p for np_close_tail.  Block 0 first finishes the force
+// evaluation of this step (energies from k_assemble's partials, commit of the
+// prepared half step, (35e)); the last block to arrive, after block 0, runs
+// np_close_tail.  PREP: no kick and no prologue; the sums of the current
+// state prepare the first step after the state or the thermostat was set.
+template <typename T, bool PREP>
+__global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* __restrict__ F, Geom g,
+                                                    const double* __restrict__ layer_minv,
+                                                    const unsigned char* __restrict__ layer_sump,
+                                                    double* __restrict__ part, unsigned int* done,
+                                                    const Phys* __restrict__ ph, DevScalars* sc,
+                                                    const double* __restrict__ part_r, int nblk_r) {
+  if (!PREP && blockIdx.x == 0) force_energies_tail(ph, sc, part_r, nblk_r, true);
+  const long long ns = g.nsite;
+  // pend_kick_f is not changed by block 0's commit
+  const T c = PREP ? (T)0 : (T)__ldcg(&sc->pend_kick_f);
+  double acc[3] = {0.0, 0.0, 0.0};
+  constexpr int NV = V16<T>::n;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (g.plane_r % NV == 0) {
+    for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
+      const long long i = iv * NV;
+      const int z = (int)(i / g.plane_r);
+      double pp = 0.0, pf = 0.0, ff = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        V16<T> q = ldv(p + a * ns + i);
+        const V16<T> y = ldv(F + a * ns + i);
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          if (!PREP) q.v[l] = q.v[l] - c * y.v[l];
+          pp += (double)q.v[l] * q.v[l];
+          pf += (double)q.v[l] * y.v[l];
+          ff += (double)y.v[l] * y.v[l];
+        }
+        if (!PREP) stv(p + a * ns + i, q);
+      }
+      if (layer_sump[z]) {
+        const double mi = layer_minv[z];
+        acc[0] += pp * mi;
+        acc[1] += pf * mi;
+        acc[2] += ff * mi;
+      }
+    }
+  } else {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+      const int z = (int)(i / g.plane_r);
+      double pp = 0.0, pf = 0.0, ff = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        T q = p[a * ns + i];
+        const T y = F[a * ns + i];
+        if (!PREP) {
+          q = q - c * y;
+          p[a * ns + i] = q;
+        }
+        pp += (double)q * q;
+        pf += (double)q * y;
+        ff += (double)y * y;
+      }
+      if (layer_sump[z]) {
+        const double mi = layer_minv[z];
+        acc[0] += pp * mi;
+        acc[1] += pf * mi;
+        acc[2] += ff * mi;
+      }
+    }
+  }
+  block_partials<3>(acc, part, blockIdx.x);
+  if (is_last_block(done)) np_close_tail(ph, sc, part, gridDim.x, !PREP);
 }
 
 // u <- u + coef * p * m^-1 (nose-poincare.F:41-53, leapfrog.F:104-114)

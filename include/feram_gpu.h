@@ -257,7 +257,7 @@ int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
 
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */
-#define FG_NPROF 7
+#define FG_NPROF 6
 /* Time n_steps graph launches of the MD step of p's method; *ms = total. */
 int  fg_time_steps(fg_ctx* ctx, int n_steps, double* ms);
 /* One bulk Nose-Poincare step launched kernel by kernel (the same kernels as
