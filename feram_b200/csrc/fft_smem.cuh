@@ -258,7 +258,9 @@ __device__ __forceinline__ void fft_inverse(cplx<T>* buf, const Batch& B, const 
 // ct_radix), but every index is a compile-time expression, the radices are
 // 16 and 8 (two shared-memory stages for n <= 256), and twiddles come from a
 // shared-memory copy of the table.  Stage plans: 4:[4] 8:[8] 16:[16] 32:[8,4]
-// 64:[16,4] 128:[16,8] 256:[16,16] 512:[16,8,4].
+// 64:[4,16] 128:[16,8] 256:[16,16] 512:[16,8,4].  64 starts with radix 4 so
+// that its first stage (16 butterflies per transform, elements 16 apart) can
+// read a 64-point row straight from global memory in 128-byte runs.
 __host__ __device__ constexpr bool ct_supported(int n) {
   return n == 4 || n == 8 || n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512;
 }
@@ -266,7 +268,7 @@ __host__ __device__ constexpr int ct_nst(int n) { return n <= 16 ? 1 : (n <= 256
 __host__ __device__ constexpr int ct_radix(int n, int st) {
   return n <= 16 ? n
        : n == 32 ? (st == 0 ? 8 : 4)
-       : n == 64 ? (st == 0 ? 16 : 4)
+       : n == 64 ? (st == 0 ? 4 : 16)
        : n == 128 ? (st == 0 ? 16 : 8)
        : n == 256 ? 16
        : (st == 0 ? 16 : (st == 1 ? 8 : 4));
@@ -286,7 +288,8 @@ template <typename T, int N, int LS, int R, bool INV, int NT, class B>
 __device__ __forceinline__ void ct_stage(cplx<T>* __restrict__ buf, const cplx<T>* __restrict__ tws) {
   constexpr int S = LS / R, NB = N / R, TOTAL = B::count * NB, TWS = N / LS;
   constexpr int STEP = S * B::es;
-#pragma unroll 2
+  constexpr int U = (R <= 8 || (sizeof(T) == 4 && NT <= 256)) ? 2 : 1;  // butterflies in flight per thread
+#pragma unroll U
   for (int w = threadIdx.x; w < TOTAL; w += NT) {
     const int t = w % B::count, j = w / B::count;
     const int blk = j / S, b = j - blk * S;
@@ -328,6 +331,63 @@ __device__ __forceinline__ void ct_inverse_from(cplx<T>* buf, const cplx<T>* tws
     ct_inverse_from<T, N, ST - 1, NT, B>(buf, tws);
   }
 }
+// Stages ST .. END-1 (forward) or ST down to END+1 (inverse), each followed
+// by __syncthreads().
+template <typename T, int N, int ST, int END, int NT, class B>
+__device__ __forceinline__ void ct_forward_range(cplx<T>* buf, const cplx<T>* tws) {
+  if constexpr (ST < END) {
+    ct_stage<T, N, ct_ls(N, ST), ct_radix(N, ST), false, NT, B>(buf, tws);
+    __syncthreads();
+    ct_forward_range<T, N, ST + 1, END, NT, B>(buf, tws);
+  }
+}
+template <typename T, int N, int ST, int END, int NT, class B>
+__device__ __forceinline__ void ct_inverse_range(cplx<T>* buf, const cplx<T>* tws) {
+  if constexpr (ST > END) {
+    ct_stage<T, N, ct_ls(N, ST), ct_radix(N, ST), true, NT, B>(buf, tws);
+    __syncthreads();
+    ct_inverse_range<T, N, ST - 1, END, NT, B>(buf, tws);
+  }
+}
+
+// One compile-time stage of a batch of COUNT transforms whose elements are
+// read through ld(t, e) and written through st(t, e, v) (t = transform,
+// e = element): the first or last stage of a pass fused with its global load
+// or store.  JFAST: consecutive threads take consecutive butterflies of one
+// transform (global rows whose butterflies run along the contiguous
+// direction); otherwise consecutive transforms, as ct_stage.  No barrier.
+template <typename T, int N, int ST, bool INV, int NT, int COUNT, bool JFAST, class LD, class SV>
+__device__ __forceinline__ void ct_stage_io(const LD& ld, const SV& st, const cplx<T>* __restrict__ tws) {
+  constexpr int LS = ct_ls(N, ST), R = ct_radix(N, ST);
+  constexpr int S = LS / R, NB = N / R, TOTAL = COUNT * NB, TWS = N / LS;
+  constexpr int U = 1;  // butterflies in flight per thread
+#pragma unroll U
+  for (int w = threadIdx.x; w < TOTAL; w += NT) {
+    const int t = JFAST ? w / NB : w % COUNT;
+    const int j = JFAST ? w - t * NB : w / COUNT;
+    const int blk = j / S, b = j - blk * S;
+    const int e0 = blk * LS + b;
+    cplx<T> v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) v[q] = ld(t, e0 + q * S);
+    if (!INV) {
+      Dft<T, R, false>::run(v);
+      if (S > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmul(v[q], tws[b * q * TWS]);
+      }
+    } else {
+      if (S > 1) {
+#pragma unroll
+        for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], tws[b * q * TWS]);
+      }
+      Dft<T, R, true>::run(v);
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) st(t, e0 + q * S, v[q]);
+  }
+}
+
 // Forward DIF / inverse DIT of a batch; both end with __syncthreads().
 template <typename T, int N, int NT, class B>
 __device__ __forceinline__ void ct_forward(cplx<T>* buf, const cplx<T>* tws) {

@@ -240,7 +240,7 @@ __device__ __forceinline__ void xy_twiddles_to_smem(cplx<T>* tm, cplx<T>* ty, cp
 }
 
 template <typename T, int MODE, int MC = 0, int LYC = 0>
-__global__ void __launch_bounds__(512, 2) k_xy_fwd(const T* __restrict__ src, cplx<T>* __restrict__ spec, Geom g,
+__global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T* __restrict__ src, cplx<T>* __restrict__ spec, Geom g,
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int out_comp0) {
@@ -256,7 +256,31 @@ __global__ void __launch_bounds__(512, 2) k_xy_fwd(const T* __restrict__ src, cp
   const cplx<T>* twx_u = MC > 0 ? tws_x : twx;
   const long long plane_off = (long long)z * g.plane_r;
   const int total = Ly * m;
-  if (MODE == SRC_FIELD || c < 3) {
+  if constexpr (MC > 0) {
+    // First x stage straight from the real rows (packed (x even, x odd)
+    // pairs, products formed on load), then the rest of the x pass.
+    const int ca = (MODE == SRC_FIELD || c < 3) ? c : (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
+    const int cb = (MODE == SRC_FIELD || c < 3) ? -1 : (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
+    const T* pa = src + (long long)ca * g.nsite + plane_off;
+    const T* pb = src + (long long)(cb < 0 ? ca : cb) * g.nsite + plane_off;
+    auto st = [&](int y, int e, const cplx<T>& v) { buf[y * (MC + 1) + e] = v; };
+    if (cb < 0) {
+      auto ld = [&](int y, int e) {
+        const T2 a = *reinterpret_cast<const T2*>(pa + (long long)y * (2 * MC) + 2 * e);
+        return mk<cplx<T>>(a.x, a.y);
+      };
+      ct_stage_io<T, MC, 0, false, kXYThreads, LYC, true>(ld, st, twm);
+    } else {
+      auto ld = [&](int y, int e) {
+        const long long o = (long long)y * (2 * MC) + 2 * e;
+        const T2 a = *reinterpret_cast<const T2*>(pa + o), b = *reinterpret_cast<const T2*>(pb + o);
+        return mk<cplx<T>>(a.x * b.x, a.y * b.y);
+      };
+      ct_stage_io<T, MC, 0, false, kXYThreads, LYC, true>(ld, st, twm);
+    }
+    __syncthreads();
+    ct_forward_range<T, MC, 1, ct_nst(MC), kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
+  } else if (MODE == SRC_FIELD || c < 3) {
     // plain component: asynchronous copies of packed (x even, x odd) pairs
     const T* sp = src + (long long)c * g.nsite + plane_off;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
@@ -291,11 +315,9 @@ __global__ void __launch_bounds__(512, 2) k_xy_fwd(const T* __restrict__ src, cp
       }
     }
   }
-  __syncthreads();
   // X pass; row stride RS = m+1 keeps the row-interleaved mapping bank-conflict free
-  if constexpr (MC > 0) {
-    ct_forward<T, MC, kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
-  } else {
+  if constexpr (MC == 0) {
+    __syncthreads();
     Batch B{Ly, 1, 0, RS, 1, true};
     fft_forward<T>(buf, B, px, twm, buf_len);
   }
@@ -325,16 +347,22 @@ __global__ void __launch_bounds__(512, 2) k_xy_fwd(const T* __restrict__ src, cp
     }
   }
   __syncthreads();
+  cplx<T>* dst = spec + (long long)(out_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
   if constexpr (MC > 0) {
-    ct_forward<T, LYC, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+    // y pass; its last stage writes the spectrum rows directly
+    constexpr int NSY = ct_nst(LYC);
+    ct_forward_range<T, LYC, 0, NSY - 1, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+    const long long kxp = g.KXP;
+    auto ld = [&](int col, int e) { return buf[col + e * (MC + 1)]; };
+    auto st = [&](int col, int e, const cplx<T>& v) { dst[(long long)e * kxp + col] = v; };
+    ct_stage_io<T, LYC, NSY - 1, false, kXYThreads, MC + 1, false>(ld, st, tws_y);
   } else {
     Batch B{RS, RS, 1, 0, RS, true};
     fft_forward<T>(buf, B, py, twy, buf_len);
-  }
-  cplx<T>* dst = spec + (long long)(out_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
-  for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
-    const int y = idx / RS, col = idx - y * RS;
-    dst[(long long)y * g.KXP + col] = buf[idx];
+    for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
+      const int y = idx / RS, col = idx - y * RS;
+      dst[(long long)y * g.KXP + col] = buf[idx];
+    }
   }
 }
 
@@ -344,7 +372,7 @@ __global__ void __launch_bounds__(512, 2) k_xy_fwd(const T* __restrict__ src, cp
 // the half-complex convention of the reference's c2r), DIT along x, store
 // the real plane.  Output is unnormalised (Lx*Ly*Lz times the IDFT).
 template <typename T, int MC = 0, int LYC = 0>
-__global__ void __launch_bounds__(512, 2) k_xy_inv(const cplx<T>* __restrict__ spec, T* __restrict__ out, Geom g,
+__global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cplx<T>* __restrict__ spec, T* __restrict__ out, Geom g,
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int in_comp0,
@@ -365,15 +393,23 @@ __global__ void __launch_bounds__(512, 2) k_xy_inv(const cplx<T>* __restrict__ s
   xy_twiddles_to_smem<T, MC, LYC>(tws_m, tws_y, tws_x, twm, twy, twx);
   const cplx<T>* twx_u = MC > 0 ? tws_x : twx;
   const cplx<T>* srcp = spec + (long long)(in_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
-  for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
-    const int y = idx / RS, col = idx - y * RS;
-    cp_async<(int)sizeof(cplx<T>)>(&buf[idx], srcp + (long long)y * g.KXP + col);
-  }
-  cp_async_wait();
-  __syncthreads();
   if constexpr (MC > 0) {
-    ct_inverse<T, LYC, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+    // y pass; its first stage (the last forward one, no twiddles) reads the
+    // spectrum rows directly
+    constexpr int NSY = ct_nst(LYC);
+    const long long kxp = g.KXP;
+    auto ld = [&](int col, int e) { return srcp[(long long)e * kxp + col]; };
+    auto st = [&](int col, int e, const cplx<T>& v) { buf[col + e * (MC + 1)] = v; };
+    ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, MC + 1, false>(ld, st, tws_y);
+    __syncthreads();
+    ct_inverse_range<T, LYC, NSY - 2, -1, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
   } else {
+    for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
+      const int y = idx / RS, col = idx - y * RS;
+      cp_async<(int)sizeof(cplx<T>)>(&buf[idx], srcp + (long long)y * g.KXP + col);
+    }
+    cp_async_wait();
+    __syncthreads();
     Batch B{RS, RS, 1, 0, RS, true};
     fft_inverse<T>(buf, B, py, twy, buf_len);
   }
@@ -401,20 +437,29 @@ __global__ void __launch_bounds__(512, 2) k_xy_inv(const cplx<T>* __restrict__ s
     }
   }
   __syncthreads();
+  T* dst = out + (long long)c * g.nsite + (long long)z * g.plane_r;
   if constexpr (MC > 0) {
-    ct_inverse<T, MC, kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
+    // x pass; its last stage (stage 0, DIT) writes the real rows directly
+    ct_inverse_range<T, MC, ct_nst(MC) - 1, 0, kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
+    auto ld = [&](int y, int e) { return buf[y * (MC + 1) + e]; };
+    auto st = [&](int y, int e, const cplx<T>& v) {
+      T2 w;
+      w.x = v.x;
+      w.y = v.y;
+      *reinterpret_cast<T2*>(dst + (long long)y * (2 * MC) + 2 * e) = w;
+    };
+    ct_stage_io<T, MC, 0, true, kXYThreads, LYC, true>(ld, st, tws_m);
   } else {
     Batch B{Ly, 1, 0, RS, 1, true};
     fft_inverse<T>(buf, B, px, twm, buf_len);
-  }
-  T* dst = out + (long long)c * g.nsite + (long long)z * g.plane_r;
-  for (int idx = threadIdx.x; idx < Ly * m; idx += blockDim.x) {
-    const int y = idx / m, jx = idx - y * m;
-    const cplx<T> v = buf[y * RS + jx];
-    T2 w;
-    w.x = v.x;
-    w.y = v.y;
-    *reinterpret_cast<T2*>(dst + (long long)y * Lx + 2 * jx) = w;
+    for (int idx = threadIdx.x; idx < Ly * m; idx += blockDim.x) {
+      const int y = idx / m, jx = idx - y * m;
+      const cplx<T> v = buf[y * RS + jx];
+      T2 w;
+      w.x = v.x;
+      w.y = v.y;
+      *reinterpret_cast<T2*>(dst + (long long)y * Lx + 2 * jx) = w;
+    }
   }
 }
 
