@@ -758,21 +758,35 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
   const int buf_len = 9 * Lz * CW;
-  if constexpr (LZC > 0)
-    for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws_z[i] = twz[i];
-  z_tile_load<T, LZC, CWC>(buf, spec, g, zt, 9);
+  // this thread's pencil: every butterfly it takes belongs to pencil
+  // threadIdx.x % CW (the batch and the block size are multiples of CW)
+  const int cwp = threadIdx.x % CW;
+  int colp = 0, ysp = 0;
+  const bool okp = tile_pencil(zt, g, cwp, &colp, &ysp);
+  cplx<T>* gp = spec + (okp ? (long long)ysp * g.KXP + colp : 0);
+  using BZ = BatchCT<9 * (CWC > 0 ? CWC : 1), (CWC > 0 ? CWC : 1), 1, (LZC > 0 ? LZC : 1) * (CWC > 0 ? CWC : 1),
+                     (CWC > 0 ? CWC : 1)>;
   if constexpr (LZC > 0) {
-    ct_forward<T, LZC, kZThreads, BatchCT<9 * CWC, CWC, 1, LZC * CWC, CWC>>(buf, tws_z);
+    for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws_z[i] = twz[i];
+    // first z stage straight from the spectrum (zeros for the pencils past
+    // Ly of the last Nyquist tile)
+    auto ld = [&](int t, int e) {
+      return okp ? gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] : mk<cplx<T>>((T)0, (T)0);
+    };
+    auto st = [&](int t, int e, const cplx<T>& v) { buf[(t / CWC) * (LZC * CWC) + (t % CWC) + e * CWC] = v; };
+    ct_stage_io<T, LZC, 0, false, kZThreads, 9 * CWC, false>(ld, st, twz);
+    __syncthreads();
+    ct_forward_range<T, LZC, 1, ct_nst(LZC), kZThreads, BZ>(buf, tws_z);
   } else {
+    z_tile_load<T, LZC, CWC>(buf, spec, g, zt, 9);
     Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
     fft_forward<T>(buf, B, pz, twz, buf_len);
   }
   const double Ninv = ph->Ninv;
   double acc[NQ_K] = {0, 0, 0, 0, 0};
   // this thread's pencil (fixed cw), decoded once
-  const int cw = threadIdx.x % CW;
-  int col = 0, yslot = 0;
-  const bool pencil_ok = tile_pencil(zt, g, cw, &col, &yslot);
+  const int cw = cwp, col = colp, yslot = ysp;
+  const bool pencil_ok = okp;
   const int ky = pencil_ok ? __ldg(&km.revy[yslot]) : 0;
   const int kx = pencil_ok ? __ldg(&km.revx[col]) : 0;
   const double kv2 = __ldg(&km.kvy[ky]);
@@ -936,12 +950,18 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   }
   __syncthreads();
   if constexpr (LZC > 0) {
-    ct_inverse<T, LZC, kZThreads, BatchCT<9 * CWC, CWC, 1, LZC * CWC, CWC>>(buf, tws_z);
+    ct_inverse_range<T, LZC, ct_nst(LZC) - 1, 0, kZThreads, BZ>(buf, tws_z);
+    // last z stage straight to the spectrum
+    auto ld = [&](int t, int e) { return buf[(t / CWC) * (LZC * CWC) + (t % CWC) + e * CWC]; };
+    auto st = [&](int t, int e, const cplx<T>& v) {
+      if (okp) gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] = v;
+    };
+    ct_stage_io<T, LZC, 0, true, kZThreads, 9 * CWC, false>(ld, st, tws_z);
   } else {
     Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
     fft_inverse<T>(buf, B, pz, twz, buf_len);
+    z_tile_store<T, LZC, CWC>(buf, spec, g, zt, 9);
   }
-  z_tile_store<T, LZC, CWC>(buf, spec, g, zt, 9);
   block_partials<NQ_K>(acc, part, blockIdx.x);
   if (done != nullptr && is_last_block(done)) homo_strain_tail(ph, sc, part, gridDim.x);
 }
