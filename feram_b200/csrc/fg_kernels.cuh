@@ -323,8 +323,9 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
   }
   // unpack: slot posm[k] holds Z(k) of the packed row; X(k) = E(k) + w^k O(k)
   const int half = m / 2 + 1;
+  // lanes run along y (same k): conflict-free rows, uniform posm and twiddle
   for (int idx = threadIdx.x; idx < Ly * half; idx += blockDim.x) {
-    const int y = idx / half, k = idx - y * half;
+    const int k = idx / Ly, y = idx - k * Ly;
     cplx<T>* row = buf + y * RS;
     if (k == 0) {
       const cplx<T> z0 = row[0];
@@ -414,8 +415,9 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
     fft_inverse<T>(buf, B, py, twy, buf_len);
   }
   const int half = m / 2 + 1;
+  // lanes run along y (same k): conflict-free rows, uniform posm and twiddle
   for (int idx = threadIdx.x; idx < Ly * half; idx += blockDim.x) {
-    const int y = idx / half, k = idx - y * half;
+    const int k = idx / Ly, y = idx - k * Ly;
     cplx<T>* row = buf + y * RS;
     if (k == 0) {
       const T X0 = row[0].x, Xm = row[m].x;
