@@ -465,7 +465,7 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaGetDevice(&dev));
   int smem_max = 0, nsm = 0;
   CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  smem_max -= 4096;  // static shared memory of the block reductions
+  smem_max -= 8192;  // static shared memory: twiddles, block reductions, scalar tails
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   ctx->smem_xy = (int)(sizeof(cplx<T>) * g.Ly * (g.m + 1));
   ctx->smem_xy64 = (int)(sizeof(cplx<double>) * g.Ly * (g.m + 1));
@@ -488,7 +488,7 @@ int create_impl(fg_ctx* ctx) {
   ctx->zt1 = tiles(1, sizeof(cplx<double>), 8);
   if ((size_t)9 * g.Lz * ctx->zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
     return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
-  ctx->smem_z = (int)(9 * (size_t)g.Lz * ctx->zt.CW * sizeof(cplx<T>));
+  ctx->smem_z = (int)(9 * ((size_t)g.Lz * ctx->zt.CW + kZPad<T>) * sizeof(cplx<T>));
   ctx->smem_z3 = (int)(3 * (size_t)g.Lz * ctx->zt.CW * sizeof(cplx<T>));
   ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->zt6.CW * sizeof(cplx<double>));
   ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->zt1.CW * sizeof(cplx<double>));

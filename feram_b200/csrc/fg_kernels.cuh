@@ -748,6 +748,9 @@ __global__ void __launch_bounds__(256) k_z_pass(cplx<T>* __restrict__ spec, Geom
 // LZC, CWC > 0 select the compile-time z transforms (launched with exactly
 // kZThreads threads); 0 = runtime plan and tile width.
 constexpr int kZThreads = 256;
+// Component padding of the compile-time z tile, in complex values (64 bytes).
+template <typename T>
+constexpr int kZPad = 64 / (int)sizeof(cplx<T>);
 
 template <typename T, int LZC = 0, int CWC = 0>
 __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
@@ -760,14 +763,17 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
   const int buf_len = 9 * Lz * CW;
+  // component stride of the tile; the compile-time path pads it by 64 bytes
+  // so that the 4 components a warp spans fall on different banks
+  const int ZS = LZC > 0 ? LZC * CWC + kZPad<T> : Lz * CW;
   // this thread's pencil: every butterfly it takes belongs to pencil
   // threadIdx.x % CW (the batch and the block size are multiples of CW)
   const int cwp = threadIdx.x % CW;
   int colp = 0, ysp = 0;
   const bool okp = tile_pencil(zt, g, cwp, &colp, &ysp);
   cplx<T>* gp = spec + (okp ? (long long)ysp * g.KXP + colp : 0);
-  using BZ = BatchCT<9 * (CWC > 0 ? CWC : 1), (CWC > 0 ? CWC : 1), 1, (LZC > 0 ? LZC : 1) * (CWC > 0 ? CWC : 1),
-                     (CWC > 0 ? CWC : 1)>;
+  using BZ = BatchCT<9 * (CWC > 0 ? CWC : 1), (CWC > 0 ? CWC : 1), 1,
+                     (LZC > 0 ? LZC : 1) * (CWC > 0 ? CWC : 1) + kZPad<T>, (CWC > 0 ? CWC : 1)>;
   if constexpr (LZC > 0) {
     for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws_z[i] = twz[i];
     // first z stage straight from the spectrum (zeros for the pencils past
@@ -775,7 +781,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     auto ld = [&](int t, int e) {
       return okp ? gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] : mk<cplx<T>>((T)0, (T)0);
     };
-    auto st = [&](int t, int e, const cplx<T>& v) { buf[(t / CWC) * (LZC * CWC) + (t % CWC) + e * CWC] = v; };
+    auto st = [&](int t, int e, const cplx<T>& v) { buf[(t / CWC) * ZS + (t % CWC) + e * CWC] = v; };
     ct_stage_io<T, LZC, 0, false, kZThreads, 9 * CWC, false>(ld, st, twz);
     __syncthreads();
     ct_forward_range<T, LZC, 1, ct_nst(LZC), kZThreads, BZ>(buf, tws_z);
@@ -801,9 +807,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     const double w1 = (kx == 0 || kx == g.m) ? 1.0 : 2.0;  // full-spectrum multiplicity
     cplx<T> u[3], d[6];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) u[a] = buf[(a * Lz + zs) * CW + cw];
+    for (int a = 0; a < 3; ++a) u[a] = buf[a * ZS + zs * CW + cw];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) d[i] = buf[((3 + i) * Lz + zs) * CW + cw];
+    for (int i = 0; i < 6; ++i) d[i] = buf[(3 + i) * ZS + zs * CW + cw];
     if (kx == 0 && ky == 0 && kz == 0) {
 #pragma unroll
       for (int i = 0; i < 6; ++i) sc->didiK0[i] = (double)d[i].x;
@@ -946,15 +952,15 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     d[4] = mk<cplx<T>>((k1 * acou[2].x + k3 * acou[0].x) * ni, (k1 * acou[2].y + k3 * acou[0].y) * ni);
     d[5] = mk<cplx<T>>((k2 * acou[0].x + k1 * acou[1].x) * ni, (k2 * acou[0].y + k1 * acou[1].y) * ni);
 #pragma unroll
-    for (int a = 0; a < 3; ++a) buf[(a * Lz + zs) * CW + cw] = F[a];
+    for (int a = 0; a < 3; ++a) buf[a * ZS + zs * CW + cw] = F[a];
 #pragma unroll
-    for (int i = 0; i < 6; ++i) buf[((3 + i) * Lz + zs) * CW + cw] = d[i];
+    for (int i = 0; i < 6; ++i) buf[(3 + i) * ZS + zs * CW + cw] = d[i];
   }
   __syncthreads();
   if constexpr (LZC > 0) {
     ct_inverse_range<T, LZC, ct_nst(LZC) - 1, 0, kZThreads, BZ>(buf, tws_z);
     // last z stage straight to the spectrum
-    auto ld = [&](int t, int e) { return buf[(t / CWC) * (LZC * CWC) + (t % CWC) + e * CWC]; };
+    auto ld = [&](int t, int e) { return buf[(t / CWC) * ZS + (t % CWC) + e * CWC]; };
     auto st = [&](int t, int e, const cplx<T>& v) {
       if (okp) gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] = v;
     };
