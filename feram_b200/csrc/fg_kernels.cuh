@@ -817,10 +817,15 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     }
     // ---- dipole-dipole
     const long long tpos = tpos0 + (long long)zs * g.KXP;
-    const T* Dp = dtab + tpos * 6;
+    using T2 = typename RT2<T>::type;
+    const T2* Dp = reinterpret_cast<const T2*>(dtab + tpos * 6);  // 6 T per k: 2 T-aligned pairs
     T D[6];
 #pragma unroll
-    for (int q = 0; q < 6; ++q) D[q] = __ldg(&Dp[q]);
+    for (int q = 0; q < 3; ++q) {
+      const T2 v = __ldg(&Dp[q]);
+      D[2 * q] = v.x;
+      D[2 * q + 1] = v.y;
+    }
     double qv[6];  // Re(conj(u_a) u_b): xx, yy, zz, yz, zx, xy
     qv[0] = (double)u[0].x * u[0].x + (double)u[0].y * u[0].y;
     qv[1] = (double)u[1].x * u[1].x + (double)u[1].y * u[1].y;
@@ -871,72 +876,45 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 #pragma unroll
       for (int a = 0; a < 3; ++a) ck[a] = ckmod[tpos * 3 + a];
     }
-    cplx<T> acou[3];
+    // rhs = -(c_k_mod + coup2 . didiK)  (optimize-inho-strain.F:28-45)
+    cplx<T> cs[3], acou[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      cplx<T> s = mk<cplx<T>>((T)0, (T)0);
+      cplx<T> t = mk<cplx<T>>((T)0, (T)0);
 #pragma unroll
-      for (int i = 0; i < 6; ++i) s = mk<cplx<T>>(s.x + C2[a][i] * d[i].x, s.y + C2[a][i] * d[i].y);
-      acou[a] = mk<cplx<T>>(-ck[a].x - s.x, -ck[a].y - s.y);
+      for (int i = 0; i < 6; ++i) t = mk<cplx<T>>(t.x + C2[a][i] * d[i].x, t.y + C2[a][i] * d[i].y);
+      cs[a] = t;
     }
     if (kx == 0 && ky == 0 && kz == 0) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) acou[a] = mk<cplx<T>>((T)0, (T)0);  // inhomo_K_G(:,:,0,0,0) = 0
     } else {
-      T G[3][3], Gi[3];
+      // K acou = rhs with K symmetric positive definite: adjugate over the
+      // determinant (the reference factorises K by Cholesky, elastic.F:
+      // 110-125; the solution is the same up to rounding)
+      const T c00 = K[1][1] * K[2][2] - K[1][2] * K[1][2], c11 = K[0][0] * K[2][2] - K[0][2] * K[0][2];
+      const T c22 = K[0][0] * K[1][1] - K[0][1] * K[0][1], c01 = K[0][2] * K[1][2] - K[0][1] * K[2][2];
+      const T c02 = K[0][1] * K[1][2] - K[0][2] * K[1][1], c12 = K[0][1] * K[0][2] - K[0][0] * K[1][2];
+      const T inv = (T)1 / (K[0][0] * c00 + K[0][1] * c01 + K[0][2] * c02);
+      cplx<T> r[3];
 #pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        T s = (T)0;
-#pragma unroll
-        for (int q = 0; q < b; ++q) s += G[b][q] * G[b][q];
-        G[b][b] = sqrt(K[b][b] - s);
-        Gi[b] = (T)1 / G[b][b];
-#pragma unroll
-        for (int a = b + 1; a < 3; ++a) {
-          T t = (T)0;
-#pragma unroll
-          for (int q = 0; q < b; ++q) t += G[a][q] * G[b][q];
-          G[a][b] = (K[a][b] - t) * Gi[b];
-        }
-      }
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        cplx<T> t = mk<cplx<T>>((T)0, (T)0);
-#pragma unroll
-        for (int b = 0; b < a; ++b) t = mk<cplx<T>>(t.x + G[a][b] * acou[b].x, t.y + G[a][b] * acou[b].y);
-        acou[a] = mk<cplx<T>>((acou[a].x - t.x) * Gi[a], (acou[a].y - t.y) * Gi[a]);
-      }
-#pragma unroll
-      for (int a = 2; a >= 0; --a) {
-        cplx<T> t = mk<cplx<T>>((T)0, (T)0);
-#pragma unroll
-        for (int b = a + 1; b < 3; ++b) t = mk<cplx<T>>(t.x + acou[b].x * G[b][a], t.y + acou[b].y * G[b][a]);
-        acou[a] = mk<cplx<T>>((acou[a].x - t.x) * Gi[a], (acou[a].y - t.y) * Gi[a]);
-      }
+      for (int a = 0; a < 3; ++a) r[a] = mk<cplx<T>>((-ck[a].x - cs[a].x) * inv, (-ck[a].y - cs[a].y) * inv);
+      acou[0] = mk<cplx<T>>(c00 * r[0].x + c01 * r[1].x + c02 * r[2].x, c00 * r[0].y + c01 * r[1].y + c02 * r[2].y);
+      acou[1] = mk<cplx<T>>(c01 * r[0].x + c11 * r[1].x + c12 * r[2].x, c01 * r[0].y + c11 * r[1].y + c12 * r[2].y);
+      acou[2] = mk<cplx<T>>(c02 * r[0].x + c12 * r[1].x + c22 * r[2].x, c02 * r[0].y + c12 * r[1].y + c22 * r[2].y);
     }
     {
+      // coupling Re(acou* . coup2 didiK), modulation Re(acou* . c_k); the
+      // strain energy Re(acou* K acou) = -(coupling + modulation) because
+      // K acou = -(c_k + coup2 didiK)
       const double w2 = 0.5 * w1;  // energy_module.F weights: 1/2 at kx = 0, Lx/2
-      double es = 0.0, ec = 0.0, em = 0.0;
+      double ec = 0.0, em = 0.0;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        // Re(conj(acou_a) * sum_b K_ab acou_b)
-        double rx = 0.0, ry = 0.0;
-#pragma unroll
-        for (int b = 0; b < 3; ++b) {
-          rx += (double)K[a][b] * acou[b].x;
-          ry += (double)K[a][b] * acou[b].y;
-        }
-        es += (double)acou[a].x * rx + (double)acou[a].y * ry;
-        double cx = 0.0, cy = 0.0;
-#pragma unroll
-        for (int i = 0; i < 6; ++i) {
-          cx += (double)C2[a][i] * d[i].x;
-          cy += (double)C2[a][i] * d[i].y;
-        }
-        ec += (double)acou[a].x * cx + (double)acou[a].y * cy;
+        ec += (double)acou[a].x * cs[a].x + (double)acou[a].y * cs[a].y;
         em += (double)acou[a].x * ck[a].x + (double)acou[a].y * ck[a].y;
       }
-      acc[2] += w2 * es;
+      acc[2] -= w2 * (ec + em);
       acc[3] += w2 * ec;
       acc[4] += w2 * em;
     }
