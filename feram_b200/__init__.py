@@ -187,6 +187,11 @@ class Context:
         self._check(lib().fg_leapfrog(self._h, C.byref(e), i_step))
         return e
 
+    def velocity_scaling(self, e: fg_energy) -> fg_energy:
+        """velocity_scaling(p, c, e) of velocity_scaling.F:9-103."""
+        self._check(lib().fg_velocity_scaling(self._h, C.byref(e)))
+        return e
+
     def kinetic_energy_dipo(self) -> float:
         v = C.c_double()
         self._check(lib().fg_kinetic_energy_dipo(self._h, C.byref(v)))

@@ -160,6 +160,7 @@ def lib() -> C.CDLL:
         "fg_nose_poincare": (C.c_int, [vp, P(fg_energy)]),
         "fg_leapfrog": (C.c_int, [vp, P(fg_energy), C.c_int]),
         "fg_kinetic_energy_dipo": (C.c_int, [vp, dp]),
+        "fg_velocity_scaling": (C.c_int, [vp, P(fg_energy)]),
         "fg_nose_poincare_hamiltonian": (C.c_int, [vp, P(fg_energy)]),
         "fg_average_accumulate": (C.c_int, [vp, P(fg_energy), P(fg_average)]),
         "fg_dipoRavg_accumulate": (C.c_int, [vp]),

@@ -138,7 +138,7 @@ struct fg_ctx {
   size_t staging_n = 0;
   double* dipoRavg = nullptr;     // FP64 accumulator [3][nsite]
   std::vector<int> h_revx, h_revy, h_revz;
-  cudaGraphExec_t g_np = nullptr, g_lf = nullptr, g_force = nullptr;
+  cudaGraphExec_t g_np = nullptr, g_lf = nullptr, g_force = nullptr, g_vs = nullptr;
   bool tables_ready = false;
   bool force_fresh = false;
   bool np_ready = false;  // DevScalars' pending half step matches the state
@@ -290,10 +290,10 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
 }
 
 template <typename T>
-int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE) {
+int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE, int zero_unmasked = 0) {
   k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (const T*)ctx->F, coef, ctx->g,
                                                                ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail,
-                                                               ctx->done, ctx->ph, ctx->sc);
+                                                               ctx->done, ctx->ph, ctx->sc, zero_unmasked);
   CKL();
   return FG_OK;
 }
@@ -350,6 +350,20 @@ int enqueue_lf(fg_ctx* ctx) {
   return FG_OK;
 }
 
+// velocity_scaling (velocity_scaling.F:9-103), acoustic mass <= 0: drift by
+// dt, force, kick by dt with p = 0 outside sum_p, rescale p to the target
+// kinetic energy.
+template <typename T>
+int enqueue_vs(fg_ctx* ctx) {
+  int rc;
+  if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
+  if ((rc = enqueue_force<T>(ctx))) return rc;
+  if ((rc = enqueue_kick<T>(ctx, &ctx->sc->lf_dt, TAIL_VS, 1))) return rc;
+  k_scale<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, &ctx->sc->vs_scale, 3 * ctx->g.nsite);
+  CKL();
+  return FG_OK;
+}
+
 // Capture fn into a CUDA graph executable (once per context).
 template <typename Fn>
 int capture(fg_ctx* ctx, cudaGraphExec_t* out, Fn fn) {
@@ -372,8 +386,10 @@ int run_graph(fg_ctx* ctx, cudaGraphExec_t* gx, int which) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_force<float>(ctx) : enqueue_force<double>(ctx); });
   } else if (which == 1) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_np<float>(ctx) : enqueue_np<double>(ctx); });
-  } else {
+  } else if (which == 2) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_lf<float>(ctx) : enqueue_lf<double>(ctx); });
+  } else {
+    rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_vs<float>(ctx) : enqueue_vs<double>(ctx); });
   }
   if (rc) return rc;
   CK(cudaGraphLaunch(*gx, ctx->stream));
@@ -434,7 +450,10 @@ int validate(const fg_params* p, std::string* why) {
   if (p->N != p->Lx * p->Ly * p->Lz || p->N <= 0) { *why = "parameters not made (call fg_make_param)"; return FG_ERR_ARG; }
   if (p->Lx % 2 != 0 || p->Lx < 4) { *why = "Lx must be even and >= 4"; return FG_ERR_UNSUPPORTED; }
   if (p->Ly < 3 || p->Lz < 3) { *why = "Ly and Lz must be >= 3"; return FG_ERR_UNSUPPORTED; }
-  if (p->method != FG_METHOD_MD && p->method != FG_METHOD_LF) { *why = "only methods 'md' and 'lf' run on the device"; return FG_ERR_UNSUPPORTED; }
+  if (p->method != FG_METHOD_MD && p->method != FG_METHOD_LF && p->method != FG_METHOD_VS && p->method != FG_METHOD_HL) {
+    *why = "unknown method";
+    return FG_ERR_UNSUPPORTED;
+  }
   if (p->mass_acou[0] > 0.0) { *why = "acoustic-displacement MD (acoustic_mass_amu) is not implemented on the device"; return FG_ERR_UNSUPPORTED; }
   if (p->delta_e != 0.0 || p->delta_e_acou != 0.0) { *why = "delta_e heat pumping is not implemented on the device"; return FG_ERR_UNSUPPORTED; }
   if (p->dt <= 0.0) { *why = "dt must be positive"; return FG_ERR_ARG; }
@@ -624,6 +643,7 @@ int create_impl(fg_ctx* ctx) {
     h.Q = P.Q_Nose;
     h.nf_kT = (double)P.n_freedom * P.temperature_eV;
     h.threeN_kT = (double)(3 * (long long)P.N) * P.temperature_eV;
+    h.target_ke = P.target_kinetic_energy;
     h.n_sum_p = ctx->n_sum_p;
     h.E_on = P.E_field_always_zero ? 0 : 1;
     h.modulation_on = 0;
@@ -867,8 +887,7 @@ int fft_r2c3_impl(fg_ctx* ctx, const double* in, double* out) {
           out[2 * f] = (double)v.x;
           out[2 * f + 1] = (double)v.y;
         }
-  ctx->force_fresh = false;
-  ctx->np_ready = false;
+  // only the spectrum scratch changed: u, p, dVddi and the scalars stand
   return FG_OK;
 }
 
@@ -892,8 +911,7 @@ int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
   if (rc) return rc;
   rc = get_field<T>(ctx, out, ctx->rwork);
   if (rc) return rc;
-  ctx->force_fresh = false;
-  ctx->np_ready = false;
+  // only the spectrum and real-space scratch changed
   return check_device_error(ctx);
 }
 
@@ -918,6 +936,15 @@ int np_prepare(fg_ctx* ctx) {
   if (rc) return rc;
   ctx->np_ready = true;
   return FG_OK;
+}
+
+// The step graph of the context's method (md, lf with i_step != 0, vs).
+cudaGraphExec_t* step_graph(fg_ctx* ctx, int* which) {
+  switch (ctx->P.method) {
+    case FG_METHOD_MD: *which = 1; return &ctx->g_np;
+    case FG_METHOD_VS: *which = 3; return &ctx->g_vs;
+    default: *which = 2; return &ctx->g_lf;
+  }
 }
 
 // Everything a Nose-Poincare graph launch needs before it starts.
@@ -1001,6 +1028,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->g_np) cudaGraphExecDestroy(ctx->g_np);
   if (ctx->g_lf) cudaGraphExecDestroy(ctx->g_lf);
+  if (ctx->g_vs) cudaGraphExecDestroy(ctx->g_vs);
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
   void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->revx,
@@ -1201,15 +1229,25 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
   return FG_OK;
 }
 
+int fg_velocity_scaling(fg_ctx* ctx, fg_energy* e) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if ((rc = run_graph(ctx, &ctx->g_vs, 3))) return rc;
+  ctx->force_fresh = true;
+  ctx->np_ready = false;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (e) energy_out(ctx->sc_host, e, false);
+  return FG_OK;
+}
+
 int fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
   if (ctx->P.method == FG_METHOD_MD && (rc = np_ready_for_step(ctx))) return rc;
-  for (int i = 0; i < n_steps; ++i) {
-    if (ctx->P.method == FG_METHOD_MD) rc = run_graph(ctx, &ctx->g_np, 1);
-    else rc = run_graph(ctx, &ctx->g_lf, 2);
-    if (rc) return rc;
-  }
+  int which = 0;
+  cudaGraphExec_t* gx = step_graph(ctx, &which);
+  for (int i = 0; i < n_steps; ++i)
+    if ((rc = run_graph(ctx, gx, which))) return rc;
   ctx->force_fresh = true;
   ctx->np_ready = ctx->P.method == FG_METHOD_MD;
   if ((rc = pull_scalars(ctx))) return rc;
@@ -1223,8 +1261,8 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
   if (!ms || n_steps < 1) return FG_ERR_ARG;
   if (ctx->P.method == FG_METHOD_MD && (rc = np_ready_for_step(ctx))) return rc;
   // make sure the graph exists before the timed region
-  cudaGraphExec_t* gx = ctx->P.method == FG_METHOD_MD ? &ctx->g_np : &ctx->g_lf;
-  const int which = ctx->P.method == FG_METHOD_MD ? 1 : 2;
+  int which = 0;
+  cudaGraphExec_t* gx = step_graph(ctx, &which);
   if (!*gx) {
     if ((rc = run_graph(ctx, gx, which))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));

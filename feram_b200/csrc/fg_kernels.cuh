@@ -51,6 +51,7 @@ struct Phys {
   int bulk_or_film;
   double Zstar;
   double dt, dt_2, Q, nf_kT, threeN_kT;
+  double target_ke;  // target_kinetic_energy (param_module.F:468), velocity scaling
   double n_sum_p;
   int E_on;
   int modulation_on;
@@ -73,6 +74,7 @@ struct DevScalars {
   // step, pi_{n+1/2}, s_{n+1}, the drift coefficient and the (35f) kick
   // coefficient dt/2 s_{n+1}.
   double pend_ke_sum, pend_ke, pend_pi, pend_s, pend_drift, pend_kick_f;
+  double vs_scale;  // velocity scaling factor of the last vs step
   int status;
   int pad;
 };
@@ -531,7 +533,7 @@ __device__ __forceinline__ void z_tile_store(const cplx<T>* buf, cplx<T>* __rest
 // ------------------------------------------------------------ scalar kernels
 // Grid-wide scalar steps; each runs either as a single-block kernel or in the
 // last block of the kernel whose partial sums it reduces (tail).
-enum { TAIL_NONE = 0, TAIL_ENERGIES = 1, TAIL_LF_FINAL = 3 };
+enum { TAIL_NONE = 0, TAIL_ENERGIES = 1, TAIL_LF_FINAL = 3, TAIL_VS = 4 };
 
 __device__ __forceinline__ double sum_potential(const double* e) {
   return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
@@ -694,6 +696,22 @@ __device__ __noinline__ void np_close_tail(const Phys* __restrict__ ph, DevScala
     S->pend_s = sn;
     S->pend_drift = P->dt_2 * (1 / sn + 1 / s);
     S->pend_kick_f = P->dt_2 * sn;
+  });
+}
+
+// Velocity scaling (velocity_scaling.F:74-83): kinetic energy of the kicked
+// momenta, the factor sqrt(target / KE) for k_scale, total.  The reported
+// dipo_kinetic is the value before rescaling, as in the reference.
+__device__ void vs_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
+  double v[1];
+  reduce_partials_all<1>(part, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    S->ke_sum = v[0];
+    S->e[E_DIPO] = ke_from(P, v[0]);
+    S->vs_scale = sqrt(P->target_ke / S->e[E_DIPO]);
+    S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
+    check_finite(S, S->e, E_COUNT);
+    if (!isfinite(S->vs_scale)) S->status = 3;
   });
 }
 
@@ -1082,7 +1100,8 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
                                               const double* __restrict__ layer_minv,
                                               const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
                                               int tail, unsigned int* done, const Phys* __restrict__ ph,
-                                              DevScalars* sc) {
+                                              DevScalars* sc, int zero_unmasked) {
+  // zero_unmasked: p = 0 outside sum_p (velocity_scaling.F:61-71)
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
@@ -1094,12 +1113,13 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
       const int z = (int)(i / g.plane_r);
       V16<T> q0 = ldv(p + i), q1 = ldv(p + ns + i), q2 = ldv(p + 2 * ns + i);
       const V16<T> f0 = ldv(F + i), f1 = ldv(F + ns + i), f2 = ldv(F + 2 * ns + i);
+      const T keep = (zero_unmasked && !layer_sump[z]) ? (T)0 : (T)1;
       double ke = 0.0;
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
-        q0.v[l] = q0.v[l] - c * f0.v[l];
-        q1.v[l] = q1.v[l] - c * f1.v[l];
-        q2.v[l] = q2.v[l] - c * f2.v[l];
+        q0.v[l] = keep * (q0.v[l] - c * f0.v[l]);
+        q1.v[l] = keep * (q1.v[l] - c * f1.v[l]);
+        q2.v[l] = keep * (q2.v[l] - c * f2.v[l]);
         ke += (double)q0.v[l] * q0.v[l] + (double)q1.v[l] * q1.v[l] + (double)q2.v[l] * q2.v[l];
       }
       stv(p + i, q0);
@@ -1110,9 +1130,10 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
   } else {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
       const int z = (int)(i / g.plane_r);
-      const T p0 = p[i] - c * F[i];
-      const T p1 = p[ns + i] - c * F[ns + i];
-      const T p2 = p[2 * ns + i] - c * F[2 * ns + i];
+      const T keep = (zero_unmasked && !layer_sump[z]) ? (T)0 : (T)1;
+      const T p0 = keep * (p[i] - c * F[i]);
+      const T p1 = keep * (p[ns + i] - c * F[ns + i]);
+      const T p2 = keep * (p[2 * ns + i] - c * F[2 * ns + i]);
       p[i] = p0;
       p[ns + i] = p1;
       p[2 * ns + i] = p2;
@@ -1123,7 +1144,18 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
     }
   }
   block_partials<1>(acc, part, blockIdx.x);
-  if (tail == TAIL_LF_FINAL && is_last_block(done)) lf_final_tail(ph, sc, part, gridDim.x);
+  if (tail != TAIL_NONE && is_last_block(done)) {
+    if (tail == TAIL_LF_FINAL) lf_final_tail(ph, sc, part, gridDim.x);
+    else if (tail == TAIL_VS) vs_tail(ph, sc, part, gridDim.x);
+  }
+}
+
+// p <- scale p on every site (velocity_scaling.F:79-83)
+template <typename T>
+__global__ void __launch_bounds__(256) k_scale(T* __restrict__ p, const double* scale, long long n) {
+  const T f = (T)(*scale);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    p[i] = f * p[i];
 }
 
 // Opening half of a Nose-Poincare step in one sweep: the kick (35a)

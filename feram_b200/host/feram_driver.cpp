@@ -229,45 +229,194 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
   if ((rc = fg_kinetic_energy_dipo(ctx, &e.dipo_kinetic))) return bail(rc);
   e.H_Nose_Poincare = 0.0;
   double s = 1.0, pi = 0.0, H0 = 0.0;
-  // molecular_dynamics
-  std::ofstream log(base + ".log");
-  e.total = e.dipo_kinetic / (s * s) + e.acou_kinetic + potential(e);
-  log << "TIME_STEP        0\n";
-  write_energy(log, p, e, s, pi);
-  np_hamiltonian(p, s, pi, H0, &e);
-  H0 = e.H_Nose_Poincare / s;
-  np_hamiltonian(p, s, pi, H0, &e);
-  if ((rc = fg_set_thermostat(ctx, s, pi, H0))) return bail(rc);
-  fg_average avg;
-  std::memset(&avg, 0, sizeof(avg));
-  const int n_steps = p.n_thermalize + p.n_average;
-  auto t0 = std::chrono::steady_clock::now();
-  for (int i_step = 1; i_step <= n_steps; ++i_step) {
-    if (p.E_wave_type != FG_WAVE_NONE) {
-      double Ea[3];
-      if ((rc = fg_wave(p.E_wave_type, i_step, p.n_thermalize, p.n_E_wave_period, p.external_E_field, Ea))) return bail(rc);
-      if ((rc = fg_set_uniform_E(ctx, Ea))) return bail(rc);
-    }
-    if (p.method == FG_METHOD_MD) rc = fg_nose_poincare(ctx, &e);
-    else rc = fg_leapfrog(ctx, &e, i_step);
-    if (rc) return bail(rc);
-    if (p.method == FG_METHOD_MD && (rc = fg_get_state(ctx, nullptr, nullptr, nullptr, nullptr, &s, &pi, nullptr)))
-      return bail(rc);
-    e.total = e.dipo_kinetic / (s * s) + e.acou_kinetic + potential(e);
-    const bool detail = p.verbose >= 2 || i_step % p.n_coord_freq == 0 || i_step == n_steps;
-    if (detail) {
-      log << "TIME_STEP " << i_step << "\n";
-      write_energy(log, p, e, s, pi);
-    }
-    if (i_step <= p.n_thermalize) continue;
-    if ((rc = fg_average_accumulate(ctx, &e, &avg))) return bail(rc);
-  }
-  auto t1 = std::chrono::steady_clock::now();
-  const double tsim = std::chrono::duration<double>(t1 - t0).count();
   int n_sum_p = p.N;
   if (p.bulk_or_film == FG_FILM || p.bulk_or_film == FG_EPIT) n_sum_p = p.Lx * p.Ly * ((p.Lz + 1) / 2);
   if (p.gap_id > 0) n_sum_p -= p.Lx * p.Ly * (p.gap_id == 2 ? 2 : 1);
-  write_avg(base + ".avg", p, avg, n_sum_p);
+  const bool coords = std::strcmp(p.coord_directory, "never") != 0;
+  // masked average of u (molecular-dynamics.F:81-84, hysteresis_loop.F:79-82)
+  auto average_u = [&](double u[3]) -> int {
+    fg_average tmp;
+    std::memset(&tmp, 0, sizeof(tmp));
+    int r = fg_average_accumulate(ctx, &e, &tmp);
+    for (int a = 0; a < 3; ++a) u[a] = tmp.u[a] / n_sum_p;
+    return r;
+  };
+  // write_system (coord_module.F:434-486)
+  auto write_system = [&](const std::string& fn) -> int {
+    if (!coords) return FG_OK;
+    std::string path = p.coord_directory[0] ? std::string(p.coord_directory) + "/" + fn : fn;
+    if (path[0] != '/') path = dir_of(base) + path;
+    std::vector<double> R(nfield), P(nfield), F(nfield), A(nfield), K(nfield);
+    double ss = 1.0;
+    int r = fg_get_state(ctx, R.data(), P.data(), F.data(), nullptr, &ss, nullptr, nullptr);
+    if (r) return r;
+    // the relaxed acoustic displacement: acouR = c2r(-i acouK) / N
+    if ((r = fg_get_acouK(ctx, K.data()))) return r;
+    for (size_t k = 0; k < K.size(); k += 2) {
+      const double re = K[k], im = K[k + 1];
+      K[k] = im;
+      K[k + 1] = -re;
+    }
+    if ((r = fg_fft_c2r3(ctx, K.data(), A.data()))) return r;
+    std::FILE* f = std::fopen(path.c_str(), "w");
+    if (!f) return FG_ERR_IO;
+    for (int iz = 0; iz < p.Lz; ++iz)
+      for (int iy = 0; iy < p.Ly; ++iy)
+        for (int ix = 0; ix < p.Lx; ++ix) {
+          const size_t o = 3 * ((size_t)ix + (size_t)NXP * ((size_t)iy + (size_t)NYP * iz));
+          std::string line;
+          char b[64];
+          std::snprintf(b, sizeof(b), "%4d%5d%5d", ix, iy, iz);
+          line += b;
+          for (int a = 0; a < 3; ++a) line += fF(R[o + a], 10, 6);
+          for (int a = 0; a < 3; ++a) line += fE(P[o + a] / ss, 14, 6);
+          for (int a = 0; a < 3; ++a) line += fE(F[o + a], 14, 6);
+          for (int a = 0; a < 3; ++a) line += fE(A[o + a] * p.Ninv, 14, 6);
+          for (int a = 0; a < 3; ++a) line += fF(0.0, 13, 6);  // acouP (acoustic mass off)
+          std::fprintf(f, "%s\n", line.c_str());
+        }
+    std::fclose(f);
+    return FG_OK;
+  };
+  char step_fn[64];
+  auto numbered = [&](int i_step) {
+    std::snprintf(step_fn, sizeof(step_fn), ".%010d.coord", i_step);
+    return std::string(p.filename) + step_fn;
+  };
+  std::ofstream log(base + ".log");
+  fg_average avg;
+  std::memset(&avg, 0, sizeof(avg));
+  const int n_steps = p.n_thermalize + p.n_average;
+  std::chrono::steady_clock::time_point t0, t1;
+  if (p.method == FG_METHOD_HL && p.continue_run) {
+    set_msg(errbuf, errlen, "'continue' keeps the state of a previous run in the same process; every fg_feram_run starts afresh");
+    fg_destroy(ctx);
+    return FG_ERR_UNSUPPORTED;
+  }
+  if (p.method == FG_METHOD_HL) {
+    // hysteresis_loop (hysteresis_loop.F:9-103): velocity scaling under a
+    // field ramped from +E to -E over the averaging steps
+    e.total = e.acou_kinetic + e.dipo_kinetic + potential(e);
+    log << "TIME_STEP        0\n";
+    write_energy(log, p, e, s, pi);
+    std::ofstream hl(base + ".hl");
+    double Eadd[3] = {0.0, 0.0, 0.0};
+    t0 = std::chrono::steady_clock::now();
+    for (int i_step = p.n_hysteresis_loop_continue; i_step <= n_steps; ++i_step) {
+      if (i_step >= p.n_thermalize) {
+        for (int a = 0; a < 3; ++a)
+          Eadd[a] = p.external_E_field[a] - 2 * p.external_E_field[a] * (i_step - p.n_thermalize) / p.n_average;
+        if ((rc = fg_set_uniform_E(ctx, Eadd))) return bail(rc);
+      }
+      if ((rc = fg_velocity_scaling(ctx, &e))) return bail(rc);
+      e.total = e.acou_kinetic + e.dipo_kinetic + potential(e);
+      if (p.verbose >= 2) {
+        log << "TIME_STEP " << i_step << "\n";
+        write_energy(log, p, e, s, pi);
+      }
+      if (i_step < p.n_thermalize) continue;
+      if ((i_step - p.n_thermalize) % p.n_hl_freq == 0) {
+        double u[3], strain[6];
+        if ((rc = average_u(u))) return bail(rc);
+        if ((rc = fg_get_state(ctx, nullptr, nullptr, nullptr, strain, nullptr, nullptr, nullptr))) return bail(rc);
+        char b[32];
+        std::snprintf(b, sizeof(b), "%010d", i_step);
+        std::string line = b + fF(p.kelvin, 6, 1);
+        for (int a = 0; a < 3; ++a) line += fF(Eadd[a], 16, 12);
+        for (int a = 0; a < 6; ++a) line += fE(strain[a], 13, 5);
+        for (int a = 0; a < 3; ++a) line += fE(u[a], 13, 5);
+        hl << line << "\n" << std::flush;
+        if ((rc = write_system(std::string(p.filename) + ".coord"))) return bail(rc);
+      }
+      if ((i_step - p.n_thermalize) % p.n_coord_freq == 0 && (rc = write_system(numbered(i_step)))) return bail(rc);
+    }
+    t1 = std::chrono::steady_clock::now();
+  } else {
+    // molecular_dynamics (molecular-dynamics.F:10-160)
+    e.total = e.dipo_kinetic / (s * s) + e.acou_kinetic + potential(e);
+    log << "TIME_STEP        0\n";
+    write_energy(log, p, e, s, pi);
+    np_hamiltonian(p, s, pi, H0, &e);
+    H0 = e.H_Nose_Poincare / s;
+    np_hamiltonian(p, s, pi, H0, &e);
+    if ((rc = fg_set_thermostat(ctx, s, pi, H0))) return bail(rc);
+    std::ofstream hl;
+    if (p.n_E_wave_period > 0) hl.open(base + ".hl");
+    const bool ramping = p.E_wave_type == FG_WAVE_RAMPING_ON || p.E_wave_type == FG_WAVE_RAMPING_OFF;
+    t0 = std::chrono::steady_clock::now();
+    for (int i_step = 1; i_step <= n_steps; ++i_step) {
+      if (p.E_wave_type != FG_WAVE_NONE) {
+        double Ea[3];
+        if ((rc = fg_wave(p.E_wave_type, i_step, p.n_thermalize, p.n_E_wave_period, p.external_E_field, Ea)))
+          return bail(rc);
+        if ((rc = fg_set_uniform_E(ctx, Ea))) return bail(rc);
+        if (hl.is_open() && (i_step >= p.n_thermalize || ramping) && (i_step - p.n_thermalize) % p.n_hl_freq == 0) {
+          double u[3], strain[6];
+          if ((rc = average_u(u))) return bail(rc);
+          if ((rc = fg_get_state(ctx, nullptr, nullptr, nullptr, strain, nullptr, nullptr, nullptr))) return bail(rc);
+          char b[32];
+          std::snprintf(b, sizeof(b), "%010d", i_step);
+          std::string line = b + fF(p.kelvin, 6, 1);
+          for (int a = 0; a < 3; ++a) line += fF(Ea[a], 16, 12);
+          for (int a = 0; a < 6; ++a) line += fE(strain[a], 13, 5);
+          for (int a = 0; a < 3; ++a) line += fE(u[a], 13, 5);
+          for (int a = 0; a < 6; ++a) line += fF(0.0, 4, 1);
+          const double ev[15] = {e.dipo_kinetic, e.short_range, e.long_range, e.dipole_E_field, e.unharmonic,
+                                 e.homo_strain, e.homo_coupling, e.inho_strain, e.inho_coupling, e.inho_modulation,
+                                 e.total, e.H_Nose_Poincare, e.total * e.total, e.dipo_kinetic / (s * s),
+                                 e.acou_kinetic};
+          for (int a = 0; a < 15; ++a) line += fE(ev[a], a == 0 ? 15 : 13, 5);
+          hl << line << "\n" << std::flush;
+          if ((rc = write_system(std::string(p.filename) + ".coord"))) return bail(rc);
+        }
+      }
+      if (p.method == FG_METHOD_MD) rc = fg_nose_poincare(ctx, &e);
+      else if (p.method == FG_METHOD_VS) rc = fg_velocity_scaling(ctx, &e);
+      else rc = fg_leapfrog(ctx, &e, i_step);
+      if (rc) return bail(rc);
+      if (p.method == FG_METHOD_MD && (rc = fg_get_state(ctx, nullptr, nullptr, nullptr, nullptr, &s, &pi, nullptr)))
+        return bail(rc);
+      if (i_step % p.n_coord_freq == 0 && (rc = write_system(numbered(i_step)))) return bail(rc);
+      e.total = e.dipo_kinetic / (s * s) + e.acou_kinetic + potential(e);
+      const bool detail = p.verbose >= 2 || i_step % p.n_coord_freq == 0 || i_step == n_steps;
+      if (detail) {
+        log << "TIME_STEP " << i_step << "\n";
+        write_energy(log, p, e, s, pi);
+      }
+      if (i_step <= p.n_thermalize) continue;
+      if ((rc = fg_average_accumulate(ctx, &e, &avg))) return bail(rc);
+      if (coords && (rc = fg_dipoRavg_accumulate(ctx))) return bail(rc);
+    }
+    t1 = std::chrono::steady_clock::now();
+    write_avg(base + ".avg", p, avg, n_sum_p);
+    // divide_and_write_dipoRavg (coord_module.F:578-608); the reference joins
+    // coord_directory and the file name without a separator
+    if (coords && p.n_average > 0) {
+      std::vector<double> Ravg(nfield);
+      if ((rc = fg_get_dipoRavg(ctx, Ravg.data()))) return bail(rc);
+      std::string fn = std::string(p.coord_directory) + p.filename + ".dipoRavg";
+      if (fn[0] != '/') fn = dir_of(base) + fn;
+      std::FILE* f = std::fopen(fn.c_str(), "w");
+      if (!f) {
+        set_msg(errbuf, errlen, "cannot write " + fn);
+        fg_destroy(ctx);
+        return FG_ERR_IO;
+      }
+      for (int iz = 0; iz < p.Lz; ++iz)
+        for (int iy = 0; iy < p.Ly; ++iy)
+          for (int ix = 0; ix < p.Lx; ++ix) {
+            const size_t o = 3 * ((size_t)ix + (size_t)NXP * ((size_t)iy + (size_t)NYP * iz));
+            std::string line;
+            char b[64];
+            std::snprintf(b, sizeof(b), "%4d%5d%5d", ix, iy, iz);
+            line += b;
+            for (int a = 0; a < 3; ++a) line += fF(Ravg[o + a] / p.n_average, 10, 6);
+            std::fprintf(f, "%s\n", line.c_str());
+          }
+      std::fclose(f);
+    }
+  }
+  const double tsim = std::chrono::duration<double>(t1 - t0).count();
   {
     char b[120];
     std::snprintf(b, sizeof(b), "%10.2f%15.2f%15.2f%5d     #TIMING_REPORT", 0.0, tsim, tsim, 1);

@@ -241,6 +241,11 @@ int  fg_mirror_force_mirror(fg_ctx* ctx, fg_energy* e);
 int  fg_nose_poincare(fg_ctx* ctx, fg_energy* e);
 /* leapfrog (leapfrog.F:9-157), acoustic mass <= 0, delta_e = 0. */
 int  fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step);
+/* velocity_scaling (velocity_scaling.F:9-103), acoustic mass <= 0: u moves by
+   dt p/m, the force is evaluated, p is kicked by dt (zero outside sum_p) and
+   rescaled to the target kinetic energy 3/2 N k T; e->dipo_kinetic is the
+   kinetic energy before the rescale, as in the reference. */
+int  fg_velocity_scaling(fg_ctx* ctx, fg_energy* e);
 /* kinetic_energy_dipo (kinetic_energy_dipo.F:14-28). */
 int  fg_kinetic_energy_dipo(fg_ctx* ctx, double* ke);
 /* Nose_Poincare_Hamiltonian (energy_module.F:128-148), e->H_Nose_Poincare. */
@@ -251,8 +256,9 @@ int  fg_average_accumulate(fg_ctx* ctx, const fg_energy* e, fg_average* avg);
 int  fg_dipoRavg_accumulate(fg_ctx* ctx);
 int  fg_get_dipoRavg(fg_ctx* ctx, double* dipoRavg);
 
-/* Run n_steps of the method of p (md or lf) on the device as one CUDA graph
-   per step; the energies of the last step are returned in e. */
+/* Run n_steps of the method of p (md, lf with i_step != 0, or vs) on the
+   device as one CUDA graph per step; the energies of the last step are
+   returned in e. */
 int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
 
 /* ---- measurement ----------------------------------------------------------

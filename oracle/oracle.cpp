@@ -1002,6 +1002,42 @@ void leapfrog(oracle_ctx* o, fg_energy* e, int i_step) {  // leapfrog.F:9-157
   if (acou) e->acou_kinetic = kinetic_energy_acou(o);
 }
 
+void velocity_scaling(oracle_ctx* o, fg_energy* e) {  // velocity_scaling.F:9-103
+  const fg_params& p = o->p;
+  const Layout& L = o->L;
+  const bool acou = p.mass_acou[0] > 0.0;
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < L.Lz; ++z)
+    for (int y = 0; y < L.Ly; ++y)
+      for (int x = 0; x < L.Lx; ++x)
+        for (int a = 0; a < 3; ++a) {
+          o->dipoR[L.r(a, 3, x, y, z)] =
+              o->dipoR[L.r(a, 3, x, y, z)] + p.dt * o->dipoP[L.r(a, 3, x, y, z)] * o->mass_dipo_inv[L.s(x, y, z)];
+          if (acou)
+            o->acouR[L.r(a, 3, x, y, z)] =
+                o->acouR[L.r(a, 3, x, y, z)] + p.dt * o->acouP[L.r(a, 3, x, y, z)] * o->mass_acou_inv[L.s(x, y, z)];
+        }
+  mirror_force_mirror(o, e);
+#pragma omp parallel for schedule(static)
+  for (int z = 0; z < L.Lz; ++z)
+    for (int y = 0; y < L.Ly; ++y)
+      for (int x = 0; x < L.Lx; ++x)
+        for (int a = 0; a < 3; ++a) {
+          double& q = o->dipoP[L.r(a, 3, x, y, z)];
+          q = o->sum_p[L.s(x, y, z)] ? q - p.dt * o->dVddi[L.r(a, 3, x, y, z)] : 0.0;
+        }
+  e->dipo_kinetic = kinetic_energy_dipo(o);
+  double scale = std::sqrt(p.target_kinetic_energy / e->dipo_kinetic);
+  for (double& q : o->dipoP) q = q * scale;
+  if (acou) {
+    const size_t plane = (size_t)3 * L.NXP * L.NYP;
+    kick_all(o->acouP, o->dVdacR, p.dt, L.Lz, plane);
+    e->acou_kinetic = kinetic_energy_acou(o);
+    scale = std::sqrt(p.target_kinetic_energy / e->acou_kinetic);
+    for (double& q : o->acouP) q = q * scale;
+  }
+}
+
 // read_defects_u (read_defects_u.F:8-80) without a .defects file
 void read_defects_u(oracle_ctx* o) {
   const fg_params& p = o->p;
@@ -1234,6 +1270,11 @@ int oracle_nose_poincare(oracle_ctx* o, fg_energy* e) {
   return 0;
 }
 
+int oracle_velocity_scaling(oracle_ctx* o, fg_energy* e) {
+  velocity_scaling(o, e);
+  return 0;
+}
+
 int oracle_leapfrog(oracle_ctx* o, fg_energy* e, int i_step) {
   leapfrog(o, e, i_step);
   return 0;
@@ -1294,6 +1335,7 @@ int oracle_md(oracle_ctx* o, int i_first, int i_last, int set_H0, fg_energy* e, 
     switch (p.method) {
       case FG_METHOD_MD: nose_poincare(o, e); break;
       case FG_METHOD_LF: leapfrog(o, e, i_step); break;
+      case FG_METHOD_VS: velocity_scaling(o, e); break;
       default: return FG_ERR_UNSUPPORTED;
     }
     e->total = e->dipo_kinetic / (o->s_Nose * o->s_Nose) + e->acou_kinetic + sum_potential(e);

@@ -41,6 +41,8 @@ int    oracle_set_uniform_E(oracle_ctx* o, const double E[3]);
 int    oracle_force(oracle_ctx* o, fg_energy* e);
 int    oracle_nose_poincare(oracle_ctx* o, fg_energy* e);
 int    oracle_leapfrog(oracle_ctx* o, fg_energy* e, int i_step);
+/* velocity_scaling (velocity_scaling.F:9-103). */
+int    oracle_velocity_scaling(oracle_ctx* o, fg_energy* e);
 double oracle_kinetic_energy_dipo(oracle_ctx* o);
 double oracle_nose_poincare_hamiltonian(oracle_ctx* o, fg_energy* e);
 /* initialize_E_field + initialize_dipoR (no .restart): uni64 Gaussian u,

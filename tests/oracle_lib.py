@@ -39,6 +39,7 @@ def load():
         "oracle_force": (C.c_int, [vp, P(A.fg_energy)]),
         "oracle_nose_poincare": (C.c_int, [vp, P(A.fg_energy)]),
         "oracle_leapfrog": (C.c_int, [vp, P(A.fg_energy), C.c_int]),
+        "oracle_velocity_scaling": (C.c_int, [vp, P(A.fg_energy)]),
         "oracle_kinetic_energy_dipo": (C.c_double, [vp]),
         "oracle_nose_poincare_hamiltonian": (C.c_double, [vp, P(A.fg_energy)]),
         "oracle_initialize": (C.c_int, [vp, P(A.fg_energy)]),
@@ -132,6 +133,10 @@ class Oracle:
 
     def leapfrog(self, e, i_step):
         self.L.oracle_leapfrog(self.h, C.byref(e), i_step)
+        return e
+
+    def velocity_scaling(self, e):
+        self.L.oracle_velocity_scaling(self.h, C.byref(e))
         return e
 
     def kinetic_energy_dipo(self):

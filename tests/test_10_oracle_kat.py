@@ -197,3 +197,16 @@ def test_oracle_nose_poincare_is_second_order(fg):
             h = max(h, abs(e.H_Nose_Poincare))
         peaks.append(h)
     assert 3.6 < peaks[0] / peaks[1] < 4.4, peaks
+
+
+def test_oracle_velocity_scaling_hits_target_kinetic_energy(fg):
+    """velocity_scaling.F:75-83: after the rescale the kinetic energy of the
+    masked momenta equals target_kinetic_energy = 3/2 N k T."""
+    p = helpers.params(L="8 8 8", method="'vs'", kelvin="250")
+    o = oracle_lib.Oracle(p)
+    o.set_state(helpers.seeded_u(p, 3, sigma=0.05), helpers.seeded_p(p, 3, sigma=0.01))
+    e = o.force()
+    for _ in range(3):
+        o.velocity_scaling(e)
+    assert abs(o.kinetic_energy_dipo() - p.target_kinetic_energy) <= 1e-12 * p.target_kinetic_energy
+    assert e.dipo_kinetic > 0.0

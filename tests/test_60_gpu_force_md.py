@@ -210,3 +210,34 @@ def test_feram_run_matches_oracle_md(fg, tmp_path, extra):
         assert abs(avg.strain[i] - ao.strain[i]) <= 1e-9 * max(abs(ao.strain[i]), 1e-6)
     avg_line = (tmp_path / "run.avg").read_text().split()
     assert len(avg_line) == 1 + 3 + 6 + 3 + 6 + 15 + 3 + 6
+
+
+@pytest.mark.parametrize("prec", [A.FG_PREC_FP64, A.FG_PREC_MIXED])
+@pytest.mark.parametrize("geom", [dict(L="16 16 16"), dict(L="12 10 8", bulk_or_film="'film'")], ids=["bulk", "film"])
+def test_velocity_scaling_steps_match_oracle(fg, prec, geom):
+    """velocity_scaling.F:9-103 on the device against the oracle: 8 steps,
+    momenta zero outside sum_p and rescaled to 3/2 N k T each step."""
+    p = helpers.params(method="'vs'", kelvin="220", **geom)
+    o = oracle_lib.Oracle(p)
+    u = helpers.seeded_u(p, 41, sigma=0.06)
+    q = helpers.seeded_p(p, 41, sigma=0.01)
+    o.set_state(u, q)
+    eo = o.force()
+    with fg.Context(p, prec) as ctx:
+        ctx.build_tables()
+        ctx.set_state(u, q)
+        eg = ctx.mirror_force_mirror()
+        for _ in range(8):
+            o.velocity_scaling(eo)
+            ctx.velocity_scaling(eg)
+        sg = ctx.get_state()
+        ke_after = ctx.kinetic_energy_dipo()
+    so = o.get_state()
+    ref_u, ref_p = A.physical(so["dipoR"], p), A.physical(so["dipoP"], p)
+    ru = np.abs(A.physical(sg["dipoR"], p) - ref_u).max() / np.abs(ref_u).max()
+    rp = np.abs(A.physical(sg["dipoP"], p) - ref_p).max() / np.abs(ref_p).max()
+    ee = helpers.energy_errors(eg, eo, A.POTENTIAL_FIELDS + ["dipo_kinetic"])
+    _record(f"vs8[{prec},{'film' if 'bulk_or_film' in geom else 'bulk'}]", dict(u=float(ru), p=float(rp), e=float(max(ee.values()))))
+    tol = 1e-10 if prec == A.FG_PREC_FP64 else 2e-5
+    assert ru <= tol and rp <= tol and max(ee.values()) <= tol, (ru, rp, ee)
+    assert abs(ke_after - p.target_kinetic_energy) <= (1e-12 if prec == A.FG_PREC_FP64 else 1e-6) * p.target_kinetic_energy
