@@ -210,6 +210,67 @@ class Context:
         return e
 
 
+class _Replica(Context):
+    """A replica of a Batch: a Context view that the batch owns."""
+
+    def __init__(self, handle, params, precision):  # noqa: super().__init__ would create a context
+        self.p = params
+        self.precision = precision
+        self._h = C.c_void_p(handle)
+
+    def close(self):
+        self._h = C.c_void_p()
+
+
+class Batch:
+    """Independent replicas (sweep points of any sizes and methods) stepped
+    together as one CUDA graph (fg_batch_create / fg_batch_step)."""
+
+    def __init__(self, params_list, precision: int = FG_PREC_FP64):
+        arr = (fg_params * len(params_list))(*params_list)
+        self._b = C.c_void_p()
+        eb = C.create_string_buffer(512)
+        rc = lib().fg_batch_create(len(params_list), arr, precision, C.byref(self._b), eb, 512)
+        if rc:
+            raise FeramError(rc, _err(eb))
+        self.replicas = [_Replica(lib().fg_batch_context(self._b, i), params_list[i], precision)
+                         for i in range(len(params_list))]
+
+    def __len__(self):
+        return len(self.replicas)
+
+    def __getitem__(self, i) -> Context:
+        return self.replicas[i]
+
+    def step(self, n_steps: int = 1):
+        """n_steps steps of every replica; returns each replica's energies."""
+        e = (fg_energy * len(self.replicas))()
+        rc = lib().fg_batch_step(self._b, n_steps, e)
+        if rc:
+            r = lib().fg_batch_last_error(self._b)
+            raise FeramError(rc, r.decode() if r else "")
+        return list(e)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            for r in self.replicas:
+                r.close()
+            lib().fg_batch_destroy(self._b)
+            self._b = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def feram_run(path: str, precision: int = FG_PREC_FP64):
     """feram_common + molecular_dynamics for one .feram file (writes .avg/.log)."""
     avg = fg_average()

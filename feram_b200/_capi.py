@@ -161,6 +161,12 @@ def lib() -> C.CDLL:
         "fg_leapfrog": (C.c_int, [vp, P(fg_energy), C.c_int]),
         "fg_kinetic_energy_dipo": (C.c_int, [vp, dp]),
         "fg_velocity_scaling": (C.c_int, [vp, P(fg_energy)]),
+        "fg_batch_create": (C.c_int, [C.c_int, P(fg_params), C.c_int, P(vp), C.c_char_p, C.c_int]),
+        "fg_batch_destroy": (None, [vp]),
+        "fg_batch_size": (C.c_int, [vp]),
+        "fg_batch_context": (vp, [vp, C.c_int]),
+        "fg_batch_last_error": (C.c_char_p, [vp]),
+        "fg_batch_step": (C.c_int, [vp, C.c_int, P(fg_energy)]),
         "fg_nose_poincare_hamiltonian": (C.c_int, [vp, P(fg_energy)]),
         "fg_average_accumulate": (C.c_int, [vp, P(fg_energy), P(fg_average)]),
         "fg_dipoRavg_accumulate": (C.c_int, [vp]),

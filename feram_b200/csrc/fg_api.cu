@@ -484,6 +484,7 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaGetDevice(&dev));
   int smem_max = 0, nsm = 0;
   CK(cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int smem_optin = smem_max;
   smem_max -= 8192;  // static shared memory: twiddles, block reductions, scalar tails
   CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
   ctx->smem_xy = (int)(sizeof(cplx<T>) * g.Ly * (g.m + 1));
@@ -513,9 +514,17 @@ int create_impl(fg_ctx* ctx) {
   ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->zt1.CW * sizeof(cplx<double>));
   ctx->grid_elem = std::max(1, std::min(div_up(g.nsite, kThreadsElem), nsm * 8));
   {
+    // The dynamic shared-memory cap is an attribute of the kernel, shared by
+    // every context in the process: raise it to what the device allows next
+    // to the kernel's static shared memory, never to this context's size
+    // (a smaller supercell would lower it under a larger one's launches).
     cudaError_t ea = cudaSuccess;
     auto setattr = [&](auto kern, int bytes) {
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+      cudaFuncAttributes fa;
+      cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+      const int cap = smem_optin - (int)fa.sharedSizeBytes;
+      if (e == cudaSuccess && bytes > cap) e = cudaErrorInvalidValue;
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
       if (e != cudaSuccess) ea = e;
     };
     with_xy_fwd<T, SRC_U9>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
@@ -523,12 +532,12 @@ int create_impl(fg_ctx* ctx) {
     with_xy_fwd<double, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy64); });
     with_xy_inv<T>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
     with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto k) { setattr(k, ctx->smem_z); });
+    setattr(k_z_pass<T, false>, ctx->smem_z3);
+    setattr(k_z_pass<T, true>, ctx->smem_z3);
+    setattr(k_z_ewald_pack<T>, ctx->smem_z6);
+    setattr(k_z_modulation_pack<T>, ctx->smem_z1);
     if (ea != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
   }
-  CK(cudaFuncSetAttribute(k_z_pass<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z3));
-  CK(cudaFuncSetAttribute(k_z_pass<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z3));
-  CK(cudaFuncSetAttribute(k_z_ewald_pack<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z6));
-  CK(cudaFuncSetAttribute(k_z_modulation_pack<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ctx->smem_z1));
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 
   // slot maps
@@ -944,6 +953,18 @@ cudaGraphExec_t* step_graph(fg_ctx* ctx, int* which) {
     case FG_METHOD_MD: *which = 1; return &ctx->g_np;
     case FG_METHOD_VS: *which = 3; return &ctx->g_vs;
     default: *which = 2; return &ctx->g_lf;
+  }
+}
+
+// One step of the context's method enqueued on its stream (md, vs, lf with
+// i_step != 0).
+int enqueue_step(fg_ctx* ctx) {
+  const bool f32 = ctx->prec == FG_PREC_MIXED;
+  switch (ctx->P.method) {
+    case FG_METHOD_MD: return f32 ? enqueue_np<float>(ctx) : enqueue_np<double>(ctx);
+    case FG_METHOD_VS:
+    case FG_METHOD_HL: return f32 ? enqueue_vs<float>(ctx) : enqueue_vs<double>(ctx);
+    default: return f32 ? enqueue_lf<float>(ctx) : enqueue_lf<double>(ctx);
   }
 }
 
@@ -1494,3 +1515,137 @@ extern "C" int fg_kinetic_energy_dipo_noalloc(const double* dipoP, int Lx, int L
   if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, cudaGetErrorString(e));
   return FG_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Replica batches: independent supercells (temperature or field points of a
+// sweep, of any sizes and methods) stepped together.  One CUDA graph holds one
+// branch per replica, forked from and joined to the batch stream, so the
+// kernels of small replicas run concurrently instead of one launch at a time.
+struct fg_batch {
+  std::vector<fg_ctx*> ctx;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraphExec_t graph = nullptr;
+  std::string err;
+};
+
+namespace {
+int batch_fail(fg_batch* b, int rc, const std::string& msg) {
+  b->err = msg;
+  return rc;
+}
+int batch_capture(fg_batch* b) {
+  if (b->graph) return FG_OK;
+  cudaGraph_t graph;
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(e));
+  int rc = FG_OK;
+  if ((e = cudaEventRecord(b->fork, b->stream)) != cudaSuccess) rc = FG_ERR_CUDA;
+  for (size_t i = 0; i < b->ctx.size() && rc == FG_OK; ++i) {
+    fg_ctx* c = b->ctx[i];
+    if ((e = cudaStreamWaitEvent(c->stream, b->fork, 0)) != cudaSuccess) { rc = FG_ERR_CUDA; break; }
+    if ((rc = enqueue_step(c))) {
+      b->err = "replica " + std::to_string(i) + ": " + c->err;
+      break;
+    }
+    if ((e = cudaEventRecord(b->join[i], c->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(b->stream, b->join[i], 0)) != cudaSuccess)
+      rc = FG_ERR_CUDA;
+  }
+  cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+  if (rc) return rc == FG_ERR_CUDA && b->err.empty() ? batch_fail(b, rc, cudaGetErrorString(e)) : rc;
+  if (ee != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ee));
+  e = cudaGraphInstantiate(&b->graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  return FG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+void fg_batch_destroy(fg_batch* b) {
+  if (!b) return;
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (cudaEvent_t ev : b->join)
+    if (ev) cudaEventDestroy(ev);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  for (fg_ctx* c : b->ctx) fg_destroy(c);
+  delete b;
+}
+
+int fg_batch_create(int n, const fg_params* params, int precision, fg_batch** out, char* errbuf, int errlen) {
+  auto msg = [&](const std::string& m) {
+    if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", m.c_str());
+  };
+  if (!out || !params || n < 1) {
+    msg("fg_batch_create: n >= 1, params and out are required");
+    return FG_ERR_ARG;
+  }
+  *out = nullptr;
+  fg_batch* b = new fg_batch();
+  for (int i = 0; i < n; ++i) {
+    fg_ctx* c = nullptr;
+    const int rc = fg_create(&params[i], precision, &c);
+    if (rc) {
+      msg("replica " + std::to_string(i) + ": " + (c ? c->err : std::string("fg_create failed")));
+      if (c) fg_destroy(c);
+      fg_batch_destroy(b);
+      return rc;
+    }
+    b->ctx.push_back(c);
+  }
+  b->join.assign((size_t)n, nullptr);
+  cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  for (int i = 0; i < n && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&b->join[(size_t)i], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    msg(std::string("fg_batch_create: ") + cudaGetErrorString(e));
+    fg_batch_destroy(b);
+    return FG_ERR_CUDA;
+  }
+  *out = b;
+  return FG_OK;
+}
+
+int fg_batch_size(const fg_batch* b) { return b ? (int)b->ctx.size() : 0; }
+
+fg_ctx* fg_batch_context(fg_batch* b, int i) {
+  return (b && i >= 0 && i < (int)b->ctx.size()) ? b->ctx[(size_t)i] : nullptr;
+}
+
+const char* fg_batch_last_error(const fg_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int fg_batch_step(fg_batch* b, int n_steps, fg_energy* e) {
+  if (!b || n_steps < 0) return FG_ERR_ARG;
+  int rc;
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    fg_ctx* c = b->ctx[i];
+    if ((rc = ensure_ready(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+    if (c->P.method == FG_METHOD_MD && (rc = np_ready_for_step(c)))
+      return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+    // set-up work on the replica's own stream must finish before the batch
+    // stream starts the graph
+    cudaError_t ce = cudaStreamSynchronize(c->stream);
+    if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  if ((rc = batch_capture(b))) return rc;
+  for (int k = 0; k < n_steps; ++k) {
+    cudaError_t ce = cudaGraphLaunch(b->graph, b->stream);
+    if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  cudaError_t ce = cudaStreamSynchronize(b->stream);
+  if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    fg_ctx* c = b->ctx[i];
+    c->force_fresh = true;
+    c->np_ready = c->P.method == FG_METHOD_MD;
+    if ((rc = pull_scalars(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+    if (e) energy_out(c->sc_host, &e[i], false);
+  }
+  return FG_OK;
+}
+
+}  // extern "C"

@@ -261,6 +261,27 @@ int  fg_get_dipoRavg(fg_ctx* ctx, double* dipoRavg);
    returned in e. */
 int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
 
+/* ---- replica batches -------------------------------------------------------
+   Independent supercells (the temperature or field points of a sweep; any
+   sizes and methods md / vs / hl / lf, one precision) stepped together: one
+   CUDA graph with a branch per replica, so the kernels of small supercells run
+   side by side.  This replaces the reference's feram_mpi task farm
+   (feram_mpi.F:33-36), which runs one .feram file per MPI rank. */
+typedef struct fg_batch fg_batch;
+/* n contexts from params[0..n-1] (each as fg_create); errbuf names the
+   failing replica. */
+int  fg_batch_create(int n, const fg_params* params, int precision, fg_batch** out,
+                     char* errbuf, int errlen);
+void fg_batch_destroy(fg_batch* b);
+int  fg_batch_size(const fg_batch* b);
+/* Replica i for set-up and read-out (fg_build_tables, fg_set_state,
+   fg_get_state, ...); owned by the batch, do not fg_destroy it. */
+fg_ctx* fg_batch_context(fg_batch* b, int i);
+const char* fg_batch_last_error(const fg_batch* b);
+/* n_steps steps of every replica's method (lf: i_step != 0); e (may be NULL)
+   receives each replica's energies of the last step, e[i] for replica i. */
+int  fg_batch_step(fg_batch* b, int n_steps, fg_energy* e);
+
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */
 #define FG_NPROF 6
