@@ -177,6 +177,40 @@ def ncu_traffic():
         return {}
 
 
+def batched_sweep(n_rep=96, steps=200):
+    """The batched cooling sweep: n_rep independent replicas of uneven sizes
+    (16^3 .. 64^3) on a 450 -> 100 K grid in 5 K steps, mixed precision,
+    stepped as one graph (fg_batch_step) and, for comparison, one replica
+    after another (fg_run_steps).  Wall-clock seconds around synchronous
+    calls; site-steps/s summed over replicas."""
+    import feram_b200 as fb
+    from feram_b200 import _capi as A
+    sizes = [16, 24, 32, 48, 64]
+    ps = [make_params(sizes[i % len(sizes)], kelvin=450.0 - 5.0 * (i % 71), Ez=0.0,
+                      seed=(123456789 + i, 987654321)) for i in range(n_rep)]
+    sites = sum(p.N for p in ps)
+    with fb.Batch(ps, A.FG_PREC_MIXED) as b:
+        for r, p in zip(b.replicas, ps):
+            u, q = initial_state(p)
+            r.build_tables()
+            prepare(r, p, u, q)
+        b.step(3)  # warm-up: graph capture and first launches
+        t0 = time.perf_counter()
+        b.step(steps)
+        t_batch = time.perf_counter() - t0
+        # the same replicas, one after another
+        for r in b.replicas:
+            r.run_steps(3)
+        t0 = time.perf_counter()
+        for r in b.replicas:
+            r.run_steps(steps)
+        t_seq = time.perf_counter() - t0
+    return {"replicas": n_rep, "sizes": sizes, "kelvin_grid": [450.0, 100.0, -5.0], "sites": sites, "steps": steps, "precision": "mixed",
+            "value": sites * steps / t_batch, "unit": UNIT,
+            "sequential_value": sites * steps / t_seq, "speedup": t_seq / t_batch,
+            "timing": "wall clock around synchronous calls"}
+
+
 def cpu_baseline(p, budget_s=20.0):
     """The oracle (FP64 C++/OpenMP restatement of the reference's CPU path)
     on this host's cores: one NP step after setup, then as many more as fit
@@ -256,6 +290,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--size", type=int, default=L_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 96-replica batched sweep measurement")
     ap.add_argument("--mixed-only", action="store_true",
                     help="skip the FP64 context, the force-error check and e2e (small device footprint, for profiling)")
     args = ap.parse_args()
@@ -393,6 +428,9 @@ def main():
                "steps": k_e2e, "includes": "fg_set_state + fg_mirror_force_mirror + K x (fg_set_uniform_E, "
                                            "fg_nose_poincare) + fg_get_state"}
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched and not args.mixed_only:
+        batched = batched_sweep()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(p)
@@ -409,7 +447,7 @@ def main():
         "mixed_over_fp64": (value / value64) if value64 else None,
         "force_err_mixed_vs_fp64": ferr,
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
-        "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "batched": batched,
         "gpu_launches": A.FG_NPROF * args.steps,  # kernels per bulk NP step graph
     }
     ctxm.close()
