@@ -187,6 +187,16 @@ class Context:
         self._check(lib().fg_leapfrog(self._h, C.byref(e), i_step))
         return e
 
+    def set_acou(self, acouR=None, acouP=None):
+        """acouR / acouP (acoustic mass > 0), padded Fortran layout."""
+        self._check(lib().fg_set_acou(self._h, dptr(acouR) if acouR is not None else None,
+                                      dptr(acouP) if acouP is not None else None))
+
+    def get_acou(self) -> dict:
+        r, q, d = real_field(self.p), real_field(self.p), real_field(self.p)
+        self._check(lib().fg_get_acou(self._h, dptr(r), dptr(q), dptr(d)))
+        return {"acouR": r, "acouP": q, "dVdacR": d}
+
     def velocity_scaling(self, e: fg_energy) -> fg_energy:
         """velocity_scaling(p, c, e) of velocity_scaling.F:9-103."""
         self._check(lib().fg_velocity_scaling(self._h, C.byref(e)))

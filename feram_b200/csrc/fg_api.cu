@@ -124,6 +124,13 @@ struct fg_ctx {
   double2* trz = nullptr;
   double* layer_minv = nullptr;
   unsigned char* layer_sump = nullptr;
+  // acoustic-displacement MD (acoustic mass > 0): u, p and F hold three more
+  // components (acouR, acouP, unused), the passes transform 12 components and
+  // rwork's components 9..11 hold dVdacR after a force evaluation
+  bool acou = false;
+  int ncx = 9;
+  double* layer_macou = nullptr;       // 1 / mass_acou per layer
+  unsigned char* layer_all = nullptr;  // all layers counted
   Phys* ph = nullptr;
   Phys ph_host{};
   DevScalars* sc = nullptr;
@@ -213,9 +220,15 @@ void with_xy_inv(int m, int Ly, F f) {
 template <typename T>
 constexpr int z_cw_cap() { return sizeof(T) == 4 ? 8 : 4; }
 template <typename T, class F>
-void with_z_kspace(int Lz, int cw, F f) {
+void with_z_kspace(int Lz, int cw, bool acou, F f) {
   constexpr int C = z_cw_cap<T>();
-  if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C>);
+  if (acou) {
+    if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C, true>);
+    else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C, true>);
+    else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C, true>);
+    else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C, true>);
+    else f(k_z_kspace<T, 0, 0, true>);
+  } else if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C>);
   else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C>);
   else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C>);
   else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C>);
@@ -252,7 +265,7 @@ int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp, bool stra
 template <typename T>
 int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
   const Geom& g = ctx->g;
-  with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto kern) {
+  with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, [&](auto kern) {
     kern<<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z, ctx->stream>>>(
         (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
         (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, nullptr);
@@ -272,11 +285,11 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
     CKL();
   }
   int rc;
-  if ((rc = launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
+  if ((rc = launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, ctx->ncx, ctx->smem_xy, (const cplx<T>*)ctx->twx,
                                      (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy)))
     return rc;
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
-  if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9, true))) return rc;
+  if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
   // np_post: the energies and (35e) are finished by the closing kick's block 0
   k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
                                                          ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
@@ -302,6 +315,40 @@ template <typename T>
 int enqueue_drift(fg_ctx* ctx, const double* coef) {
   k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->u, (const T*)ctx->p, coef, ctx->g,
                                                                 ctx->layer_minv);
+  CKL();
+  return FG_OK;
+}
+
+// Acoustic momenta and displacements (acouP, acouR: components 3..5 of p and
+// u): kick by dVdacR (rwork components 9..11), no sum_p mask, uniform mass.
+template <typename T>
+int enqueue_kick_acou(fg_ctx* ctx, const double* coef, int tail) {
+  const long long ns = ctx->g.nsite;
+  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+      (T*)ctx->p + 3 * ns, (const T*)ctx->rwork + 9 * ns, coef, ctx->g, ctx->layer_macou, ctx->layer_all,
+      ctx->part_ke, tail, ctx->done, ctx->ph, ctx->sc, 0);
+  CKL();
+  return FG_OK;
+}
+
+template <typename T>
+int enqueue_drift_acou(fg_ctx* ctx, const double* coef) {
+  const long long ns = ctx->g.nsite;
+  k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->u + 3 * ns, (const T*)ctx->p + 3 * ns, coef,
+                                                                ctx->g, ctx->layer_macou);
+  CKL();
+  return FG_OK;
+}
+
+// leapfrog.F:44-87 heat pump, when delta_e or delta_e_acou is set
+template <typename T>
+int enqueue_pump(fg_ctx* ctx) {
+  const fg_params& P = ctx->P;
+  if (P.delta_e == 0.0 && P.delta_e_acou == 0.0) return FG_OK;
+  const long long ns = ctx->g.nsite;
+  k_layer_pump<T><<<2, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, ctx->acou ? (T*)ctx->p + 3 * ns : nullptr, ctx->g,
+                                                        ctx->layer_minv, ctx->layer_macou, ctx->layer_sump, P.delta_e,
+                                                        P.delta_e_acou);
   CKL();
   return FG_OK;
 }
@@ -344,8 +391,11 @@ int enqueue_np(fg_ctx* ctx) {
 template <typename T>
 int enqueue_lf(fg_ctx* ctx) {
   int rc;
+  if ((rc = enqueue_pump<T>(ctx))) return rc;
   if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
+  if (ctx->acou && (rc = enqueue_drift_acou<T>(ctx, &ctx->sc->lf_dt))) return rc;
   if ((rc = enqueue_force<T>(ctx))) return rc;
+  if (ctx->acou && (rc = enqueue_kick_acou<T>(ctx, &ctx->sc->lf_dt, TAIL_ACOU))) return rc;
   if ((rc = enqueue_kick<T>(ctx, &ctx->sc->lf_dt, TAIL_LF_FINAL))) return rc;
   return FG_OK;
 }
@@ -357,10 +407,17 @@ template <typename T>
 int enqueue_vs(fg_ctx* ctx) {
   int rc;
   if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
+  if (ctx->acou && (rc = enqueue_drift_acou<T>(ctx, &ctx->sc->lf_dt))) return rc;
   if ((rc = enqueue_force<T>(ctx))) return rc;
   if ((rc = enqueue_kick<T>(ctx, &ctx->sc->lf_dt, TAIL_VS, 1))) return rc;
   k_scale<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, &ctx->sc->vs_scale, 3 * ctx->g.nsite);
   CKL();
+  if (ctx->acou) {
+    if ((rc = enqueue_kick_acou<T>(ctx, &ctx->sc->lf_dt, TAIL_VS_ACOU))) return rc;
+    k_scale<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p + 3 * ctx->g.nsite, &ctx->sc->vs_scale_acou,
+                                                                  3 * ctx->g.nsite);
+    CKL();
+  }
   return FG_OK;
 }
 
@@ -454,8 +511,14 @@ int validate(const fg_params* p, std::string* why) {
     *why = "unknown method";
     return FG_ERR_UNSUPPORTED;
   }
-  if (p->mass_acou[0] > 0.0) { *why = "acoustic-displacement MD (acoustic_mass_amu) is not implemented on the device"; return FG_ERR_UNSUPPORTED; }
-  if (p->delta_e != 0.0 || p->delta_e_acou != 0.0) { *why = "delta_e heat pumping is not implemented on the device"; return FG_ERR_UNSUPPORTED; }
+  if (p->mass_acou[0] > 0.0 && p->method == FG_METHOD_MD) {
+    *why = "acoustic_mass_amu with method 'md' (param_module.F:239-242)";
+    return FG_ERR_ARG;
+  }
+  if ((p->delta_e != 0.0 || p->delta_e_acou != 0.0) && (p->Lz < 4 || p->method != FG_METHOD_LF)) {
+    *why = "delta_e pumps heat in leapfrog runs with Lz >= 4 only";
+    return FG_ERR_UNSUPPORTED;
+  }
   if (p->dt <= 0.0) { *why = "dt must be positive"; return FG_ERR_ARG; }
   if (p->method == FG_METHOD_MD && p->Q_Nose <= 0.0) { *why = "Q_Nose must be positive"; return FG_ERR_ARG; }
   return FG_OK;
@@ -503,12 +566,14 @@ int create_impl(fg_ctx* ctx) {
     t.nnyq = div_up(g.Ly, cw);
     return t;
   };
-  ctx->zt = tiles(9, sizeof(cplx<T>), sizeof(T) == 4 ? 8 : 4);
+  ctx->acou = P.mass_acou[0] > 0.0;
+  ctx->ncx = ctx->acou ? 12 : 9;
+  ctx->zt = tiles(ctx->ncx, sizeof(cplx<T>), sizeof(T) == 4 ? 8 : 4);
   ctx->zt6 = tiles(6, sizeof(cplx<double>), 8);
   ctx->zt1 = tiles(1, sizeof(cplx<double>), 8);
-  if ((size_t)9 * g.Lz * ctx->zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
+  if ((size_t)ctx->ncx * g.Lz * ctx->zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
     return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
-  ctx->smem_z = (int)(9 * ((size_t)g.Lz * ctx->zt.CW + kZPad<T>) * sizeof(cplx<T>));
+  ctx->smem_z = (int)(ctx->ncx * ((size_t)g.Lz * ctx->zt.CW + kZPad<T>) * sizeof(cplx<T>));
   ctx->smem_z3 = (int)(3 * (size_t)g.Lz * ctx->zt.CW * sizeof(cplx<T>));
   ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->zt6.CW * sizeof(cplx<double>));
   ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->zt1.CW * sizeof(cplx<double>));
@@ -531,7 +596,7 @@ int create_impl(fg_ctx* ctx) {
     with_xy_fwd<T, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
     with_xy_fwd<double, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy64); });
     with_xy_inv<T>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
-    with_z_kspace<T>(g.Lz, ctx->zt.CW, [&](auto k) { setattr(k, ctx->smem_z); });
+    with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, [&](auto k) { setattr(k, ctx->smem_z); });
     setattr(k_z_pass<T, false>, ctx->smem_z3);
     setattr(k_z_pass<T, true>, ctx->smem_z3);
     setattr(k_z_ewald_pack<T>, ctx->smem_z6);
@@ -603,6 +668,11 @@ int create_impl(fg_ctx* ctx) {
     ctx->n_sum_p = n;
     if ((rc = upload(ctx, (void**)&ctx->layer_minv, minv))) return rc;
     if ((rc = upload(ctx, (void**)&ctx->layer_sump, sump))) return rc;
+    // acoustic masses are the same on every site (alloc_Coord)
+    std::vector<double> mai(g.Lz, P.mass_acou[0] > 0.0 ? 1.0 / P.mass_acou[0] : 0.0);
+    std::vector<unsigned char> all(g.Lz, 1);
+    if ((rc = upload(ctx, (void**)&ctx->layer_macou, mai))) return rc;
+    if ((rc = upload(ctx, (void**)&ctx->layer_all, all))) return rc;
   }
   // physics constants (elastic.F:26-75, dVddi-unharmonic.F:28-32)
   {
@@ -673,15 +743,16 @@ int create_impl(fg_ctx* ctx) {
   // fields
   const size_t es = sizeof(T);
   ctx->real_bytes = es * (size_t)g.nsite;
-  CK(cudaMalloc(&ctx->u, 3 * ctx->real_bytes));
-  CK(cudaMalloc(&ctx->p, 3 * ctx->real_bytes));
+  const size_t nfc = ctx->acou ? 6 : 3;
+  CK(cudaMalloc(&ctx->u, nfc * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->p, nfc * ctx->real_bytes));
   CK(cudaMalloc(&ctx->F, 3 * ctx->real_bytes));
-  CK(cudaMemset(ctx->u, 0, 3 * ctx->real_bytes));
-  CK(cudaMemset(ctx->p, 0, 3 * ctx->real_bytes));
+  CK(cudaMemset(ctx->u, 0, nfc * ctx->real_bytes));  // acouR = acouP = 0 (initialize-dipoR.F:56)
+  CK(cudaMemset(ctx->p, 0, nfc * ctx->real_bytes));
   CK(cudaMemset(ctx->F, 0, 3 * ctx->real_bytes));
-  CK(cudaMalloc(&ctx->spec, 9 * sizeof(cplx<T>) * (size_t)g.ncplx));
+  CK(cudaMalloc(&ctx->spec, (size_t)ctx->ncx * sizeof(cplx<T>) * (size_t)g.ncplx));
   CK(cudaMemset(ctx->spec, 0, 9 * sizeof(cplx<T>) * (size_t)g.ncplx));
-  CK(cudaMalloc(&ctx->rwork, 9 * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->rwork, (size_t)ctx->ncx * ctx->real_bytes));
   CK(cudaMalloc(&ctx->dtab, 6 * es * (size_t)g.nkpos));
   CK(cudaMemset(ctx->dtab, 0, 6 * es * (size_t)g.nkpos));
   CK(cudaMalloc(&ctx->ckmod, 3 * sizeof(cplx<T>) * (size_t)g.nkpos));
@@ -1055,7 +1126,7 @@ void fg_destroy(fg_ctx* ctx) {
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->revx,
                   ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
-                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done};
+                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->sc_host) cudaFreeHost(ctx->sc_host);
@@ -1183,6 +1254,38 @@ int fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi, doubl
   return FG_OK;
 }
 
+int fg_set_acou(fg_ctx* ctx, const double* acouR, const double* acouP) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  if (!ctx->acou) return fail(ctx, FG_ERR_STATE, "the acoustic field is dynamic only with acoustic_mass_amu > 0");
+  const long long ns = ctx->g.nsite;
+  const bool f32 = ctx->prec == FG_PREC_MIXED;
+  const size_t off = (size_t)3 * ns * (f32 ? sizeof(float) : sizeof(double));
+  int rc;
+  if (acouR && (rc = f32 ? set_field<float>(ctx, (char*)ctx->u + off, acouR) : set_field<double>(ctx, (char*)ctx->u + off, acouR)))
+    return rc;
+  if (acouP && (rc = f32 ? set_field<float>(ctx, (char*)ctx->p + off, acouP) : set_field<double>(ctx, (char*)ctx->p + off, acouP)))
+    return rc;
+  ctx->force_fresh = false;
+  ctx->np_ready = false;
+  return FG_OK;
+}
+
+int fg_get_acou(fg_ctx* ctx, double* acouR, double* acouP, double* dVdacR) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  if (!ctx->acou) return fail(ctx, FG_ERR_STATE, "the acoustic field is dynamic only with acoustic_mass_amu > 0");
+  const long long ns = ctx->g.nsite;
+  const bool f32 = ctx->prec == FG_PREC_MIXED;
+  const size_t es = f32 ? sizeof(float) : sizeof(double);
+  const char* u = (const char*)ctx->u + 3 * ns * es;
+  const char* q = (const char*)ctx->p + 3 * ns * es;
+  const char* d = (const char*)ctx->rwork + 9 * ns * es;
+  int rc;
+  if (acouR && (rc = f32 ? get_field<float>(ctx, acouR, u) : get_field<double>(ctx, acouR, u))) return rc;
+  if (acouP && (rc = f32 ? get_field<float>(ctx, acouP, q) : get_field<double>(ctx, acouP, q))) return rc;
+  if (dVdacR && (rc = f32 ? get_field<float>(ctx, dVdacR, d) : get_field<double>(ctx, dVdacR, d))) return rc;
+  return FG_OK;
+}
+
 int fg_get_acouK(fg_ctx* ctx, double* acouK) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
@@ -1232,8 +1335,12 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
   if (i_step == 0) {  // leapfrog.F:89-102
-    if ((rc = force_now(ctx))) return rc;
     const bool f32 = ctx->prec == FG_PREC_MIXED;
+    if ((rc = f32 ? enqueue_pump<float>(ctx) : enqueue_pump<double>(ctx))) return rc;
+    if ((rc = force_now(ctx))) return rc;
+    if (ctx->acou && (rc = f32 ? enqueue_kick_acou<float>(ctx, &ctx->sc->lf_dt_2, TAIL_ACOU)
+                               : enqueue_kick_acou<double>(ctx, &ctx->sc->lf_dt_2, TAIL_ACOU)))
+      return rc;
     if ((rc = f32 ? enqueue_kick<float>(ctx, &ctx->sc->lf_dt_2, TAIL_LF_FINAL)
                   : enqueue_kick<double>(ctx, &ctx->sc->lf_dt_2, TAIL_LF_FINAL)))
       return rc;
@@ -1245,6 +1352,7 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) {
     e->dipo_kinetic = ctx->sc_host->e[E_DIPO];
+    e->acou_kinetic = ctx->sc_host->e[E_ACOU];
     for (int i = E_SHORT; i <= E_IM; ++i) (&e->acou_kinetic)[i] = ctx->sc_host->e[i];
   }
   return FG_OK;

@@ -74,7 +74,8 @@ struct DevScalars {
   // step, pi_{n+1/2}, s_{n+1}, the drift coefficient and the (35f) kick
   // coefficient dt/2 s_{n+1}.
   double pend_ke_sum, pend_ke, pend_pi, pend_s, pend_drift, pend_kick_f;
-  double vs_scale;  // velocity scaling factor of the last vs step
+  double vs_scale;       // velocity scaling factor of the last vs step
+  double vs_scale_acou;  // the same for the acoustic momenta
   int status;
   int pad;
 };
@@ -226,7 +227,9 @@ enum { SRC_U9 = 0, SRC_FIELD = 1 };
 // Per (z-plane, component): load a real plane, DIF along x on Lx/2 complex
 // pairs, unpack to the Lx/2+1 bins of the real transform, DIF along y.
 // SRC_U9: component c of (u_x, u_y, u_z, u_x^2, u_y^2, u_z^2, u_y u_z,
-// u_z u_x, u_x u_y) from u (dipoFFT.F:19-44).  SRC_FIELD: component c of src.
+// u_z u_x, u_x u_y) from u (dipoFFT.F:19-44); components 9..11 are src
+// components 3..5 (the acoustic displacement stored after u).  SRC_FIELD:
+// component c of src.
 // MC, LYC > 0 select the compile-time transforms for m = Lx/2 = MC and
 // Ly = LYC (launched with exactly kXYThreads threads); 0 = runtime plans.
 constexpr int kXYThreads = 512;
@@ -261,8 +264,9 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
   if constexpr (MC > 0) {
     // First x stage straight from the real rows (packed (x even, x odd)
     // pairs, products formed on load), then the rest of the x pass.
-    const int ca = (MODE == SRC_FIELD || c < 3) ? c : (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
-    const int cb = (MODE == SRC_FIELD || c < 3) ? -1 : (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
+    const bool plain = MODE == SRC_FIELD || c < 3 || c >= 9;
+    const int ca = plain ? (c >= 9 && MODE == SRC_U9 ? c - 6 : c) : (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
+    const int cb = plain ? -1 : (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
     const T* pa = src + (long long)ca * g.nsite + plane_off;
     const T* pb = src + (long long)(cb < 0 ? ca : cb) * g.nsite + plane_off;
     auto st = [&](int y, int e, const cplx<T>& v) { buf[y * (MC + 1) + e] = v; };
@@ -282,9 +286,9 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
     }
     __syncthreads();
     ct_forward_range<T, MC, 1, ct_nst(MC), kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
-  } else if (MODE == SRC_FIELD || c < 3) {
+  } else if (MODE == SRC_FIELD || c < 3 || c >= 9) {
     // plain component: asynchronous copies of packed (x even, x odd) pairs
-    const T* sp = src + (long long)c * g.nsite + plane_off;
+    const T* sp = src + (long long)(c >= 9 && MODE == SRC_U9 ? c - 6 : c) * g.nsite + plane_off;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
       const int y = idx / m, jx = idx - y * m;
       cp_async<(int)sizeof(cplx<T>)>(&buf[y * RS + jx], sp + (long long)y * Lx + 2 * jx);
@@ -533,7 +537,7 @@ __device__ __forceinline__ void z_tile_store(const cplx<T>* buf, cplx<T>* __rest
 // ------------------------------------------------------------ scalar kernels
 // Grid-wide scalar steps; each runs either as a single-block kernel or in the
 // last block of the kernel whose partial sums it reduces (tail).
-enum { TAIL_NONE = 0, TAIL_ENERGIES = 1, TAIL_LF_FINAL = 3, TAIL_VS = 4 };
+enum { TAIL_NONE = 0, TAIL_ENERGIES = 1, TAIL_LF_FINAL = 3, TAIL_VS = 4, TAIL_ACOU = 5, TAIL_VS_ACOU = 6 };
 
 __device__ __forceinline__ double sum_potential(const double* e) {
   return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
@@ -715,6 +719,22 @@ __device__ void vs_tail(const Phys* __restrict__ ph, DevScalars* sc, const doubl
   });
 }
 
+// Acoustic kinetic energy sum acouP^2 / m / 2 (kinetic_energy_acou.F:15-27);
+// with vs also the rescale factor (velocity_scaling.F:86-98) and the total.
+__device__ void acou_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk,
+                          bool vs) {
+  double v[1];
+  reduce_partials_all<1>(part, nblk, v);
+  scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    S->e[E_ACOU] = v[0] / 2;
+    if (vs) {
+      S->vs_scale_acou = sqrt(P->target_ke / S->e[E_ACOU]);
+      if (!isfinite(S->vs_scale_acou)) S->status = 3;
+      S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
+    }
+  });
+}
+
 // Leapfrog closing reduction (leapfrog.F:151) and total.
 __device__ void lf_final_tail(const Phys* __restrict__ ph, DevScalars* sc, const double* __restrict__ part, int nblk) {
   double v[1];
@@ -770,7 +790,7 @@ constexpr int kZThreads = 256;
 template <typename T>
 constexpr int kZPad = 64 / (int)sizeof(cplx<T>);
 
-template <typename T, int LZC = 0, int CWC = 0>
+template <typename T, int LZC = 0, int CWC = 0, bool ACOU = false>
 __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
                                                      const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
                                                      Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
@@ -780,7 +800,10 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
-  const int buf_len = 9 * Lz * CW;
+  // ACOU: acoustic-displacement MD, three more components in and out
+  // (FFT(acouR) in, dVdacK out; acouFFT.F:9-26, dVdac.F:11-63)
+  constexpr int NC = ACOU ? 12 : 9;
+  const int buf_len = NC * Lz * CW;
   // component stride of the tile; the compile-time path pads it by 64 bytes
   // so that the 4 components a warp spans fall on different banks
   const int ZS = LZC > 0 ? LZC * CWC + kZPad<T> : Lz * CW;
@@ -790,7 +813,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   int colp = 0, ysp = 0;
   const bool okp = tile_pencil(zt, g, cwp, &colp, &ysp);
   cplx<T>* gp = spec + (okp ? (long long)ysp * g.KXP + colp : 0);
-  using BZ = BatchCT<9 * (CWC > 0 ? CWC : 1), (CWC > 0 ? CWC : 1), 1,
+  using BZ = BatchCT<NC * (CWC > 0 ? CWC : 1), (CWC > 0 ? CWC : 1), 1,
                      (LZC > 0 ? LZC : 1) * (CWC > 0 ? CWC : 1) + kZPad<T>, (CWC > 0 ? CWC : 1)>;
   if constexpr (LZC > 0) {
     for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws_z[i] = twz[i];
@@ -800,12 +823,12 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       return okp ? gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] : mk<cplx<T>>((T)0, (T)0);
     };
     auto st = [&](int t, int e, const cplx<T>& v) { buf[(t / CWC) * ZS + (t % CWC) + e * CWC] = v; };
-    ct_stage_io<T, LZC, 0, false, kZThreads, 9 * CWC, false>(ld, st, twz);
+    ct_stage_io<T, LZC, 0, false, kZThreads, NC * CWC, false>(ld, st, twz);
     __syncthreads();
     ct_forward_range<T, LZC, 1, ct_nst(LZC), kZThreads, BZ>(buf, tws_z);
   } else {
-    z_tile_load<T, LZC, CWC>(buf, spec, g, zt, 9);
-    Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
+    z_tile_load<T, LZC, CWC>(buf, spec, g, zt, NC);
+    Batch B{NC * CW, CW, 1, Lz * CW, CW, true};
     fft_forward<T>(buf, B, pz, twz, buf_len);
   }
   const double Ninv = ph->Ninv;
@@ -903,7 +926,38 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       for (int i = 0; i < 6; ++i) t = mk<cplx<T>>(t.x + C2[a][i] * d[i].x, t.y + C2[a][i] * d[i].y);
       cs[a] = t;
     }
-    if (kx == 0 && ky == 0 && kz == 0) {
+    if constexpr (ACOU) {
+      // dynamic acoustic field: acouK = i FFT(acouR) (acouFFT.F:22);
+      // dVdacK = -i (c_k + coup2 didiK + K acouK) / N (dVdac.F:30-60);
+      // energies with the K acouK of this field (energy_module.F:150-240)
+      cplx<T> KA[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const cplx<T> X = buf[(9 + a) * ZS + zs * CW + cw];
+        acou[a] = mk<cplx<T>>(-X.y, X.x);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        KA[a] = mk<cplx<T>>(K[a][0] * acou[0].x + K[a][1] * acou[1].x + K[a][2] * acou[2].x,
+                            K[a][0] * acou[0].y + K[a][1] * acou[1].y + K[a][2] * acou[2].y);
+      const double w2 = 0.5 * w1;
+      double es = 0.0, ec = 0.0, em = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        es += (double)acou[a].x * KA[a].x + (double)acou[a].y * KA[a].y;
+        ec += (double)acou[a].x * cs[a].x + (double)acou[a].y * cs[a].y;
+        em += (double)acou[a].x * ck[a].x + (double)acou[a].y * ck[a].y;
+      }
+      acc[2] += w2 * es;
+      acc[3] += w2 * ec;
+      acc[4] += w2 * em;
+      const T ni = (T)Ninv;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const cplx<T> v = mk<cplx<T>>(ck[a].x + cs[a].x + KA[a].x, ck[a].y + cs[a].y + KA[a].y);
+        buf[(9 + a) * ZS + zs * CW + cw] = mk<cplx<T>>(v.y * ni, -v.x * ni);
+      }
+    } else if (kx == 0 && ky == 0 && kz == 0) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) acou[a] = mk<cplx<T>>((T)0, (T)0);  // inhomo_K_G(:,:,0,0,0) = 0
     } else {
@@ -921,7 +975,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       acou[1] = mk<cplx<T>>(c01 * r[0].x + c11 * r[1].x + c12 * r[2].x, c01 * r[0].y + c11 * r[1].y + c12 * r[2].y);
       acou[2] = mk<cplx<T>>(c02 * r[0].x + c12 * r[1].x + c22 * r[2].x, c02 * r[0].y + c12 * r[1].y + c22 * r[2].y);
     }
-    {
+    if constexpr (!ACOU) {
       // coupling Re(acou* . coup2 didiK), modulation Re(acou* . c_k); the
       // strain energy Re(acou* K acou) = -(coupling + modulation) because
       // K acou = -(c_k + coup2 didiK)
@@ -960,11 +1014,11 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     auto st = [&](int t, int e, const cplx<T>& v) {
       if (okp) gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] = v;
     };
-    ct_stage_io<T, LZC, 0, true, kZThreads, 9 * CWC, false>(ld, st, tws_z);
+    ct_stage_io<T, LZC, 0, true, kZThreads, NC * CWC, false>(ld, st, tws_z);
   } else {
-    Batch B{9 * CW, CW, 1, Lz * CW, CW, true};
+    Batch B{NC * CW, CW, 1, Lz * CW, CW, true};
     fft_inverse<T>(buf, B, pz, twz, buf_len);
-    z_tile_store<T, LZC, CWC>(buf, spec, g, zt, 9);
+    z_tile_store<T, LZC, CWC>(buf, spec, g, zt, NC);
   }
   block_partials<NQ_K>(acc, part, blockIdx.x);
   if (done != nullptr && is_last_block(done)) homo_strain_tail(ph, sc, part, gridDim.x);
@@ -1147,6 +1201,58 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
   if (tail != TAIL_NONE && is_last_block(done)) {
     if (tail == TAIL_LF_FINAL) lf_final_tail(ph, sc, part, gridDim.x);
     else if (tail == TAIL_VS) vs_tail(ph, sc, part, gridDim.x);
+    else if (tail == TAIL_ACOU || tail == TAIL_VS_ACOU) acou_tail(ph, sc, part, gridDim.x, tail == TAIL_VS_ACOU);
+  }
+}
+
+// Sum of v over the block, returned to every thread.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  v = warp_sum(v);
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// Heat pump of leapfrog.F:44-87: block 0 scales layer Lz/4 up by delta_e
+// per site, block 1 layer 3 (Lz/4) down, the dipole momenta by
+// sqrt((e_layer +- Lx Ly delta_e) / e_layer) with e_layer the layer's kinetic
+// energy (sum p^2/m / 2 times Lx Ly / counted sites), and likewise the
+// acoustic momenta with delta_e_acou (sum acouP^2/m / 2).
+template <typename T>
+__global__ void __launch_bounds__(256) k_layer_pump(T* __restrict__ p, T* __restrict__ pa, Geom g,
+                                                    const double* __restrict__ layer_minv,
+                                                    const double* __restrict__ layer_macou,
+                                                    const unsigned char* __restrict__ layer_sump, double de,
+                                                    double dea) {
+  const int z = blockIdx.x == 0 ? g.Lz / 4 : (g.Lz / 4) * 3;
+  const double sgn = blockIdx.x == 0 ? 1.0 : -1.0;
+  const long long ns = g.nsite, pr = g.plane_r, base = (long long)z * pr;
+  const double LxLy = (double)pr;
+  if (de != 0.0) {
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) {
+      const T q = p[(i / pr) * ns + base + i % pr];
+      s += (double)q * q;
+    }
+    const double n_layer = layer_sump[z] ? LxLy : 0.0;
+    const double e = block_sum(s) * layer_minv[z] / 2 * LxLy / n_layer;
+    const T f = (T)sqrt((e + sgn * LxLy * de) / e);
+    for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) p[(i / pr) * ns + base + i % pr] *= f;
+  }
+  if (dea != 0.0 && pa != nullptr) {
+    double s = 0.0;
+    for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) {
+      const T q = pa[(i / pr) * ns + base + i % pr];
+      s += (double)q * q;
+    }
+    const double e = block_sum(s) * layer_macou[z] / 2;
+    const T f = (T)sqrt((e + sgn * LxLy * dea) / e);
+    for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) pa[(i / pr) * ns + base + i % pr] *= f;
   }
 }
 

@@ -196,7 +196,8 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
   if ((rc = fg_wave(p.E_wave_type, 0, p.n_thermalize, p.n_E_wave_period, p.external_E_field, E0))) return bail(rc);
   if ((rc = fg_set_uniform_E(ctx, E0))) return bail(rc);
   // initialize_dipoR
-  std::vector<double> dipoR(nfield, 0.0), dipoP(nfield, 0.0);
+  std::vector<double> dipoR(nfield, 0.0), dipoP(nfield, 0.0), acouR(nfield, 0.0), acouP(nfield, 0.0);
+  const bool acoustic = p.mass_acou[0] > 0.0;
   {
     std::ifstream rs(base + ".restart");
     if (rs) {
@@ -215,6 +216,8 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
             for (int a = 0; a < 3; ++a) {
               dipoR[o + a] = v[a];
               dipoP[o + a] = v[3 + a];
+              acouR[o + a] = v[9 + a];
+              acouP[o + a] = v[12 + a];
             }
           }
     } else {
@@ -222,6 +225,7 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
     }
   }
   if ((rc = fg_set_state(ctx, dipoR.data(), dipoP.data(), 1.0, 0.0, 0.0))) return bail(rc);
+  if (acoustic && (rc = fg_set_acou(ctx, acouR.data(), acouP.data()))) return bail(rc);
   fg_energy e;
   std::memset(&e, 0, sizeof(e));
   if ((rc = fg_mirror_force_mirror(ctx, &e))) return bail(rc);
@@ -250,14 +254,20 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
     double ss = 1.0;
     int r = fg_get_state(ctx, R.data(), P.data(), F.data(), nullptr, &ss, nullptr, nullptr);
     if (r) return r;
-    // the relaxed acoustic displacement: acouR = c2r(-i acouK) / N
-    if ((r = fg_get_acouK(ctx, K.data()))) return r;
-    for (size_t k = 0; k < K.size(); k += 2) {
-      const double re = K[k], im = K[k + 1];
-      K[k] = im;
-      K[k + 1] = -re;
+    std::vector<double> AP(nfield, 0.0);
+    double ascale = 1.0;
+    if (acoustic) {  // the dynamic acoustic field
+      if ((r = fg_get_acou(ctx, A.data(), AP.data(), nullptr))) return r;
+    } else {  // the relaxed acoustic displacement: acouR = c2r(-i acouK) / N
+      if ((r = fg_get_acouK(ctx, K.data()))) return r;
+      for (size_t k = 0; k < K.size(); k += 2) {
+        const double re = K[k], im = K[k + 1];
+        K[k] = im;
+        K[k + 1] = -re;
+      }
+      if ((r = fg_fft_c2r3(ctx, K.data(), A.data()))) return r;
+      ascale = p.Ninv;
     }
-    if ((r = fg_fft_c2r3(ctx, K.data(), A.data()))) return r;
     std::FILE* f = std::fopen(path.c_str(), "w");
     if (!f) return FG_ERR_IO;
     for (int iz = 0; iz < p.Lz; ++iz)
@@ -271,8 +281,8 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
           for (int a = 0; a < 3; ++a) line += fF(R[o + a], 10, 6);
           for (int a = 0; a < 3; ++a) line += fE(P[o + a] / ss, 14, 6);
           for (int a = 0; a < 3; ++a) line += fE(F[o + a], 14, 6);
-          for (int a = 0; a < 3; ++a) line += fE(A[o + a] * p.Ninv, 14, 6);
-          for (int a = 0; a < 3; ++a) line += fF(0.0, 13, 6);  // acouP (acoustic mass off)
+          for (int a = 0; a < 3; ++a) line += fE(A[o + a] * ascale, 14, 6);
+          for (int a = 0; a < 3; ++a) line += fF(AP[o + a], 13, 6);
           std::fprintf(f, "%s\n", line.c_str());
         }
     std::fclose(f);

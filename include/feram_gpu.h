@@ -223,6 +223,13 @@ int  fg_set_state(fg_ctx* ctx, const double* dipoR, const double* dipoP,
 int  fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi,
                   double strain[6], double* s_Nose, double* pi_Nose, double* H0);
 int  fg_set_thermostat(fg_ctx* ctx, double s_Nose, double pi_Nose, double H0);
+/* Acoustic displacement and momentum (Coord_type acouR, acouP,
+   coord_module.F:25-31) when acoustic_mass_amu > 0 (otherwise FG_ERR_STATE:
+   the acoustic field is then the relaxed one of each force evaluation).
+   fg_get_acou also returns dVdacR (dVdac.F:11-63) of the last force
+   evaluation; any argument may be NULL.  Both start at zero. */
+int  fg_set_acou(fg_ctx* ctx, const double* acouR, const double* acouP);
+int  fg_get_acou(fg_ctx* ctx, double* acouR, double* acouP, double* dVdacR);
 /* acouK (complex, 3 comps) of the last force evaluation, Fortran layout. */
 int  fg_get_acouK(fg_ctx* ctx, double* acouK);
 /* Uniform external field E(R) = E (initialize_E_field.F:139-146,
@@ -239,12 +246,14 @@ int  fg_mirror_force_mirror(fg_ctx* ctx, fg_energy* e);
 /* nose_poincare (nose-poincare.F:10-78): one Nose-Poincare step.  e must hold
    the energies of the previous call on entry (the reference reads them). */
 int  fg_nose_poincare(fg_ctx* ctx, fg_energy* e);
-/* leapfrog (leapfrog.F:9-157), acoustic mass <= 0, delta_e = 0. */
+/* leapfrog (leapfrog.F:9-157), with the acoustic branch when
+   acoustic_mass_amu > 0 and the delta_e / delta_e_acou heat pump. */
 int  fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step);
-/* velocity_scaling (velocity_scaling.F:9-103), acoustic mass <= 0: u moves by
-   dt p/m, the force is evaluated, p is kicked by dt (zero outside sum_p) and
-   rescaled to the target kinetic energy 3/2 N k T; e->dipo_kinetic is the
-   kinetic energy before the rescale, as in the reference. */
+/* velocity_scaling (velocity_scaling.F:9-103): u moves by dt p/m, the force
+   is evaluated, p is kicked by dt (zero outside sum_p) and rescaled to the
+   target kinetic energy 3/2 N k T, and likewise the acoustic momenta when
+   acoustic_mass_amu > 0; e->dipo_kinetic and e->acou_kinetic are the kinetic
+   energies before the rescale, as in the reference. */
 int  fg_velocity_scaling(fg_ctx* ctx, fg_energy* e);
 /* kinetic_energy_dipo (kinetic_energy_dipo.F:14-28). */
 int  fg_kinetic_energy_dipo(fg_ctx* ctx, double* ke);

@@ -1235,6 +1235,13 @@ int oracle_set_acou(oracle_ctx* o, const double* acouR, const double* acouP) {
   return 0;
 }
 
+int oracle_get_acou(oracle_ctx* o, double* acouR, double* acouP, double* dVdacR) {
+  if (acouR) copy_out(o, o->acouR, acouR, 3);
+  if (acouP) copy_out(o, o->acouP, acouP, 3);
+  if (dVdacR) copy_out(o, o->dVdacR, dVdacR, 3);
+  return 0;
+}
+
 int oracle_get_acouK(oracle_ctx* o, double* acouK) {
   copy_out_c(o, o->acouK, acouK, 3);
   return 0;

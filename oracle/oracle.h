@@ -34,6 +34,8 @@ int    oracle_set_state(oracle_ctx* o, const double* dipoR, const double* dipoP,
 int    oracle_get_state(oracle_ctx* o, double* dipoR, double* dipoP, double* dVddi,
                         double* strain6, double* s_Nose, double* pi_Nose, double* H0);
 int    oracle_set_acou(oracle_ctx* o, const double* acouR, const double* acouP);
+/* acouR, acouP and dVdacR (acoustic-displacement MD), padded layout. */
+int    oracle_get_acou(oracle_ctx* o, double* acouR, double* acouP, double* dVdacR);
 int    oracle_get_acouK(oracle_ctx* o, double* acouK);
 /* acouR as write_system computes it for .coord (coord_module.F:457-469) */
 int    oracle_acouR_for_coord(oracle_ctx* o, double* acouR);

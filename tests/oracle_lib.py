@@ -34,6 +34,8 @@ def load():
         "oracle_set_state": (C.c_int, [vp, dp, dp, C.c_double, C.c_double, C.c_double]),
         "oracle_get_state": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
         "oracle_get_acouK": (C.c_int, [vp, dp]),
+        "oracle_set_acou": (C.c_int, [vp, dp, dp]),
+        "oracle_get_acou": (C.c_int, [vp, dp, dp, dp]),
         "oracle_acouR_for_coord": (C.c_int, [vp, dp]),
         "oracle_set_uniform_E": (C.c_int, [vp, dp]),
         "oracle_force": (C.c_int, [vp, P(A.fg_energy)]),
@@ -112,6 +114,15 @@ class Oracle:
         a = A.complex_field(self.p)
         self.L.oracle_get_acouK(self.h, A.dptr(a.view(np.float64)))
         return a
+
+    def set_acou(self, acouR=None, acouP=None):
+        self.L.oracle_set_acou(self.h, A.dptr(acouR) if acouR is not None else None,
+                               A.dptr(acouP) if acouP is not None else None)
+
+    def get_acou(self):
+        r, q, d = A.real_field(self.p), A.real_field(self.p), A.real_field(self.p)
+        self.L.oracle_get_acou(self.h, A.dptr(r), A.dptr(q), A.dptr(d))
+        return {"acouR": r, "acouP": q, "dVdacR": d}
 
     def acouR_for_coord(self):
         a = A.real_field(self.p)
