@@ -187,6 +187,15 @@ class Context:
         self._check(lib().fg_leapfrog(self._h, C.byref(e), i_step))
         return e
 
+    def upload_site_arrays(self, Z_starR=None, mass_dipo_inv=None, mass_acou_inv=None, relaxor=None, sum_p=None,
+                           E_field_local=None):
+        """fg_upload_site_arrays: padded Fortran-layout per-site arrays (int32
+        for relaxor and sum_p); None keeps the default."""
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+        dp_ = lambda a: dptr(a) if a is not None else None
+        self._check(lib().fg_upload_site_arrays(self._h, dp_(Z_starR), dp_(mass_dipo_inv), dp_(mass_acou_inv),
+                                                ip(relaxor), ip(sum_p), dp_(E_field_local)))
+
     def set_acou(self, acouR=None, acouP=None):
         """acouR / acouP (acoustic mass > 0), padded Fortran layout."""
         self._check(lib().fg_set_acou(self._h, dptr(acouR) if acouR is not None else None,

@@ -156,6 +156,7 @@ def lib() -> C.CDLL:
         "fg_set_thermostat": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),
         "fg_get_acouK": (C.c_int, [vp, dp]),
         "fg_set_acou": (C.c_int, [vp, dp, dp]),
+        "fg_upload_site_arrays": (C.c_int, [vp, dp, dp, dp, P(C.c_int), P(C.c_int), dp]),
         "fg_get_acou": (C.c_int, [vp, dp, dp, dp]),
         "fg_set_uniform_E": (C.c_int, [vp, dp]),
         "fg_mirror_force_mirror": (C.c_int, [vp, P(fg_energy)]),

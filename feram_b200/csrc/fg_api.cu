@@ -131,6 +131,15 @@ struct fg_ctx {
   int ncx = 9;
   double* layer_macou = nullptr;       // 1 / mass_acou per layer
   unsigned char* layer_all = nullptr;  // all layers counted
+  // per-site tables (fg_upload_site_arrays: .relaxor, .defects, .localfield);
+  // null: the per-layer tables hold
+  void* site_minv = nullptr;             // T, 1 / mass_dipo
+  void* site_macou = nullptr;            // T, 1 / mass_acou
+  unsigned char* site_sump = nullptr;    // sum_p
+  unsigned char* site_species = nullptr; // relaxor index - 1
+  void* site_zstar = nullptr;            // T, Z*
+  void* site_E = nullptr;                // T, local field, 3 components
+  double* layer_nsum = nullptr;          // counted sites per layer
   Phys* ph = nullptr;
   Phys ph_host{};
   DevScalars* sc = nullptr;
@@ -291,9 +300,9 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
   // np_post: the energies and (35e) are finished by the closing kick's block 0
-  k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc,
-                                                         ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
-                                                         ctx->done + 2);
+  k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(
+      (const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc, ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
+      ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
@@ -304,9 +313,9 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
 
 template <typename T>
 int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE, int zero_unmasked = 0) {
-  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (const T*)ctx->F, coef, ctx->g,
-                                                               ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail,
-                                                               ctx->done, ctx->ph, ctx->sc, zero_unmasked);
+  k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+      (T*)ctx->p, (const T*)ctx->F, coef, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, tail, ctx->done,
+      ctx->ph, ctx->sc, zero_unmasked, (const T*)ctx->site_minv, ctx->site_sump);
   CKL();
   return FG_OK;
 }
@@ -314,7 +323,7 @@ int enqueue_kick(fg_ctx* ctx, const double* coef, int tail = TAIL_NONE, int zero
 template <typename T>
 int enqueue_drift(fg_ctx* ctx, const double* coef) {
   k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->u, (const T*)ctx->p, coef, ctx->g,
-                                                                ctx->layer_minv);
+                                                                ctx->layer_minv, (const T*)ctx->site_minv);
   CKL();
   return FG_OK;
 }
@@ -326,7 +335,7 @@ int enqueue_kick_acou(fg_ctx* ctx, const double* coef, int tail) {
   const long long ns = ctx->g.nsite;
   k_kick<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
       (T*)ctx->p + 3 * ns, (const T*)ctx->rwork + 9 * ns, coef, ctx->g, ctx->layer_macou, ctx->layer_all,
-      ctx->part_ke, tail, ctx->done, ctx->ph, ctx->sc, 0);
+      ctx->part_ke, tail, ctx->done, ctx->ph, ctx->sc, 0, (const T*)ctx->site_macou, nullptr);
   CKL();
   return FG_OK;
 }
@@ -335,7 +344,7 @@ template <typename T>
 int enqueue_drift_acou(fg_ctx* ctx, const double* coef) {
   const long long ns = ctx->g.nsite;
   k_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->u + 3 * ns, (const T*)ctx->p + 3 * ns, coef,
-                                                                ctx->g, ctx->layer_macou);
+                                                                ctx->g, ctx->layer_macou, (const T*)ctx->site_macou);
   CKL();
   return FG_OK;
 }
@@ -348,15 +357,16 @@ int enqueue_pump(fg_ctx* ctx) {
   const long long ns = ctx->g.nsite;
   k_layer_pump<T><<<2, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, ctx->acou ? (T*)ctx->p + 3 * ns : nullptr, ctx->g,
                                                         ctx->layer_minv, ctx->layer_macou, ctx->layer_sump, P.delta_e,
-                                                        P.delta_e_acou);
+                                                        P.delta_e_acou, (const T*)ctx->site_minv,
+                                                        (const T*)ctx->site_macou, ctx->layer_nsum);
   CKL();
   return FG_OK;
 }
 
 template <typename T>
 int enqueue_kick_drift(fg_ctx* ctx) {
-  k_kick_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
-                                                                     ctx->sc, ctx->g, ctx->layer_minv);
+  k_kick_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+      (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F, ctx->sc, ctx->g, ctx->layer_minv, (const T*)ctx->site_minv);
   CKL();
   return FG_OK;
 }
@@ -366,7 +376,7 @@ template <typename T, bool PREP>
 int enqueue_kick_close(fg_ctx* ctx) {
   k_kick_close<T, PREP><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
       (T*)ctx->p, (const T*)ctx->F, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, ctx->done, ctx->ph,
-      ctx->sc, ctx->part_r, ctx->grid_elem);
+      ctx->sc, ctx->part_r, ctx->grid_elem, (const T*)ctx->site_minv, ctx->site_sump);
   CKL();
   return FG_OK;
 }
@@ -693,6 +703,22 @@ int create_impl(fg_ctx* ctx) {
     h.sk = 6 * P.P_k1[0] + 2 * P.P_k2[0];
     h.tk2 = 2 * P.P_k2[0];
     h.fk = 4 * P.P_k2[0] - 2 * P.P_k3[0];
+    for (int sp = 0; sp < FG_RELAXOR_MAX; ++sp) {
+      Phys::Species& q = h.sp[sp];
+      q.fa2g = 4 * P.P_alpha[sp] + 2 * P.P_gamma[sp];
+      q.tg = 2 * P.P_gamma[sp];
+      q.sk = 6 * P.P_k1[sp] + 2 * P.P_k2[sp];
+      q.tk2 = 2 * P.P_k2[sp];
+      q.fk = 4 * P.P_k2[sp] - 2 * P.P_k3[sp];
+      q.k4x8 = 8 * P.P_k4[sp];
+      q.Pa = P.P_alpha[sp];
+      q.Pg = P.P_gamma[sp];
+      q.P1 = P.P_k1[sp];
+      q.P2 = P.P_k2[sp];
+      q.P3 = P.P_k3[sp];
+      q.P4 = P.P_k4[sp];
+      q.dk2 = P.P_kappa2[sp] - P.P_kappa2[0];
+    }
     h.B11 = P.B11;
     h.B12 = P.B12;
     h.B44 = P.B44;
@@ -995,6 +1021,90 @@ int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
   return check_device_error(ctx);
 }
 
+// fg_upload_site_arrays: per-site tables in the device's site order
+// i = x + Lx (y + Ly z) from the padded Fortran arrays of alloc_Coord
+// (coord_module.F:100-170) and read_relaxor / read_defects_u /
+// initialize_E_field.
+template <typename T>
+int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, const double* macou, const int* relaxor,
+                      const int* sum_p, const double* Eloc) {
+  const Geom& g = ctx->g;
+  const fg_params& P = ctx->P;
+  const size_t ns = (size_t)g.nsite, nxp = (size_t)ctx->NXP, nyp = (size_t)ctx->NYP;
+  auto fidx = [&](size_t i) {
+    const size_t x = i % (size_t)g.Lx, y = (i / (size_t)g.Lx) % (size_t)g.Ly, z = i / ((size_t)g.Lx * g.Ly);
+    return x + nxp * (y + nyp * z);
+  };
+  auto replace = [&](void** dst, auto vec) -> int {
+    if (*dst) cudaFree(*dst);
+    *dst = nullptr;
+    return upload(ctx, dst, vec);
+  };
+  int rc;
+  if (relaxor) {
+    std::vector<unsigned char> sp(ns);
+    for (size_t i = 0; i < ns; ++i) {
+      const int r = relaxor[fidx(i)];
+      if (r < 1 || r > FG_RELAXOR_MAX) return fail(ctx, FG_ERR_ARG, "relaxor index outside 1..3");
+      if (P.Z_star[r - 1] != P.Z_star[0])
+        return fail(ctx, FG_ERR_UNSUPPORTED,
+                    "species with a different Z_star: per-site Z* in the dipole-dipole term is not built on the device");
+      sp[i] = (unsigned char)(r - 1);
+    }
+    if ((rc = replace((void**)&ctx->site_species, sp))) return rc;
+  }
+  if (zstar) {
+    std::vector<T> v(ns);
+    for (size_t i = 0; i < ns; ++i) {
+      v[i] = (T)zstar[fidx(i)];
+      if (zstar[fidx(i)] != P.Z_star[0])
+        return fail(ctx, FG_ERR_UNSUPPORTED, "per-site Z* differing from Z_star(1) is not built on the device");
+    }
+    if ((rc = replace(&ctx->site_zstar, v))) return rc;
+  }
+  if (minv) {
+    std::vector<T> v(ns);
+    for (size_t i = 0; i < ns; ++i) v[i] = (T)minv[fidx(i)];
+    if ((rc = replace(&ctx->site_minv, v))) return rc;
+  }
+  if (macou) {
+    std::vector<T> v(ns);
+    for (size_t i = 0; i < ns; ++i) v[i] = (T)macou[fidx(i)];
+    if ((rc = replace(&ctx->site_macou, v))) return rc;
+  }
+  if (sum_p) {
+    std::vector<unsigned char> v(ns);
+    std::vector<double> nl(g.Lz, 0.0);
+    double n = 0.0;
+    for (size_t i = 0; i < ns; ++i) {
+      v[i] = sum_p[fidx(i)] ? 1 : 0;
+      nl[i / ((size_t)g.Lx * g.Ly)] += v[i];
+      n += v[i];
+    }
+    if ((rc = replace((void**)&ctx->site_sump, v))) return rc;
+    if ((rc = replace((void**)&ctx->layer_nsum, nl))) return rc;
+    ctx->n_sum_p = n;
+    ctx->ph_host.n_sum_p = n;
+  }
+  if (Eloc) {
+    std::vector<T> v(3 * ns);
+    for (size_t i = 0; i < ns; ++i)
+      for (int a = 0; a < 3; ++a) v[(size_t)a * ns + i] = (T)Eloc[3 * fidx(i) + (size_t)a];
+    if ((rc = replace(&ctx->site_E, v))) return rc;
+    ctx->ph_host.E_on = 1;  // a .localfield clears E_field_always_zero (initialize_E_field.F:21)
+  }
+  CK(cudaMemcpy(ctx->ph, &ctx->ph_host, sizeof(Phys), cudaMemcpyHostToDevice));
+  // the step graphs hold the old table pointers as kernel arguments
+  for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
+    if (*gx) {
+      cudaGraphExecDestroy(*gx);
+      *gx = nullptr;
+    }
+  ctx->force_fresh = false;
+  ctx->np_ready = false;
+  return FG_OK;
+}
+
 int ensure_ready(fg_ctx* ctx) {
   if (!ctx) return FG_ERR_ARG;
   if (!ctx->tables_ready) return fail(ctx, FG_ERR_STATE, "no k-space tables: call fg_build_tables or fg_upload_tables");
@@ -1126,7 +1236,9 @@ void fg_destroy(fg_ctx* ctx) {
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->revx,
                   ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
-                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all};
+                  ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all,
+                  ctx->site_minv, ctx->site_macou, ctx->site_sump, ctx->site_species, ctx->site_zstar, ctx->site_E,
+                  ctx->layer_nsum};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->sc_host) cudaFreeHost(ctx->sc_host);
@@ -1286,6 +1398,14 @@ int fg_get_acou(fg_ctx* ctx, double* acouR, double* acouP, double* dVdacR) {
   return FG_OK;
 }
 
+int fg_upload_site_arrays(fg_ctx* ctx, const double* Z_starR, const double* mass_dipo_inv, const double* mass_acou_inv,
+                          const int* relaxor, const int* sum_p, const double* E_field_local) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  return ctx->prec == FG_PREC_MIXED
+             ? upload_sites_impl<float>(ctx, Z_starR, mass_dipo_inv, mass_acou_inv, relaxor, sum_p, E_field_local)
+             : upload_sites_impl<double>(ctx, Z_starR, mass_dipo_inv, mass_acou_inv, relaxor, sum_p, E_field_local);
+}
+
 int fg_get_acouK(fg_ctx* ctx, double* acouK) {
   int rc = ensure_ready(ctx);
   if (rc) return rc;
@@ -1432,11 +1552,13 @@ int fg_profile_step(fg_ctx* ctx, int reps, double* ms) {
 int fg_kinetic_energy_dipo(fg_ctx* ctx, double* ke) {
   if (!ctx || !ctx->stream || !ke) return FG_ERR_ARG;
   if (ctx->prec == FG_PREC_MIXED)
-    k_ke_only<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const float*)ctx->p, ctx->g, ctx->layer_minv,
-                                                                       ctx->layer_sump, ctx->part_ke);
+    k_ke_only<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+        (const float*)ctx->p, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, (const float*)ctx->site_minv,
+        ctx->site_sump);
   else
-    k_ke_only<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const double*)ctx->p, ctx->g, ctx->layer_minv,
-                                                                        ctx->layer_sump, ctx->part_ke);
+    k_ke_only<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+        (const double*)ctx->p, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, (const double*)ctx->site_minv,
+        ctx->site_sump);
   CKL();
   k_ke_finish<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->ph, ctx->sc, ctx->part_ke, ctx->grid_elem);
   CKL();
@@ -1463,11 +1585,13 @@ int fg_nose_poincare_hamiltonian(fg_ctx* ctx, fg_energy* e) {
 int fg_average_accumulate(fg_ctx* ctx, const fg_energy* e, fg_average* avg) {
   if (!ctx || !ctx->stream || !e || !avg) return FG_ERR_ARG;
   if (ctx->prec == FG_PREC_MIXED)
-    k_avg_sums<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const float*)ctx->u, ctx->g, ctx->P.Z_star[0],
-                                                                        ctx->layer_sump, ctx->part_avg);
+    k_avg_sums<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+        (const float*)ctx->u, ctx->g, ctx->P.Z_star[0], ctx->layer_sump, ctx->part_avg, ctx->site_sump,
+        (const float*)ctx->site_zstar);
   else
-    k_avg_sums<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((const double*)ctx->u, ctx->g, ctx->P.Z_star[0],
-                                                                         ctx->layer_sump, ctx->part_avg);
+    k_avg_sums<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+        (const double*)ctx->u, ctx->g, ctx->P.Z_star[0], ctx->layer_sump, ctx->part_avg, ctx->site_sump,
+        (const double*)ctx->site_zstar);
   CKL();
   k_avg_finish<<<1, RED_THREADS, 0, ctx->stream>>>(ctx->avg6, ctx->part_avg, ctx->grid_elem);
   CKL();

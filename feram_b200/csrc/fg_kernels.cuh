@@ -52,6 +52,11 @@ struct Phys {
   double Zstar;
   double dt, dt_2, Q, nf_kT, threeN_kT;
   double target_ke;  // target_kinetic_energy (param_module.F:468), velocity scaling
+  // per-species on-site constants for .relaxor runs (dVddi-unharmonic.F:
+  // 28-32,40,73): force combinations, energy coefficients, kappa2(s)-kappa2(1)
+  struct Species {
+    double fa2g, tg, sk, tk2, fk, k4x8, Pa, Pg, P1, P2, P3, P4, dk2;
+  } sp[3];
   double n_sum_p;
   int E_on;
   int modulation_on;
@@ -1100,7 +1105,12 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
                                                   T* __restrict__ F, Geom g, const Phys* __restrict__ ph,
                                                   DevScalars* sc, double* __restrict__ part, int tail,
-                                                  unsigned int* done) {
+                                                  unsigned int* done,
+                                                  const unsigned char* __restrict__ site_species = nullptr,
+                                                  const T* __restrict__ site_zstar = nullptr,
+                                                  const T* __restrict__ site_E = nullptr) {
+  // site_*: per-site species (.relaxor), Z* and local field (.localfield);
+  // they take the scalar loop
   const long long ns = g.nsite;
   AsmConst<T> k;
   k.fa2g = (T)ph->fa2g; k.tg = (T)ph->tg; k.sk = (T)ph->sk; k.tk2 = (T)ph->tk2; k.fk = (T)ph->fk;
@@ -1114,7 +1124,41 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
   double acc[NQ_R] = {0.0, 0.0};
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if (g.plane_r % NV == 0) {
+  const bool sites = site_species != nullptr || site_zstar != nullptr || site_E != nullptr;
+  if (sites) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
+      AsmConst<T> ks = k;
+      double dk2 = 0.0;
+      if (site_species) {
+        const Phys::Species& q = ph->sp[site_species[i]];
+        ks.fa2g = (T)q.fa2g; ks.tg = (T)q.tg; ks.sk = (T)q.sk; ks.tk2 = (T)q.tk2; ks.fk = (T)q.fk; ks.k4x8 = (T)q.k4x8;
+        ks.Pa = q.Pa; ks.Pg = q.Pg; ks.P1 = q.P1; ks.P2 = q.P2; ks.P3 = q.P3; ks.P4 = q.P4;
+        dk2 = q.dk2;
+      }
+      if (site_zstar) ks.Zs = site_zstar[i];
+      if (site_E) {
+        ks.E0 = (T)(sc->E[0] + (double)site_E[i]);
+        ks.E1 = (T)(sc->E[1] + (double)site_E[ns + i]);
+        ks.E2 = (T)(sc->E[2] + (double)site_E[2 * ns + i]);
+      }
+      T eta[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
+      const T ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
+      T o0, o1, o2;
+      assemble_site(ks, ux, uy, uz, rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
+      if (dk2 != 0.0) {  // kappa2(s) - kappa2(1) (dVddi-unharmonic.F:40,73)
+        const T t = (T)(2 * dk2);
+        o0 = o0 + t * ux;
+        o1 = o1 + t * uy;
+        o2 = o2 + t * uz;
+        acc[0] += dk2 * ((double)ux * ux + (double)uy * uy + (double)uz * uz);
+      }
+      F[i] = o0;
+      F[ns + i] = o1;
+      F[2 * ns + i] = o2;
+    }
+  } else if (g.plane_r % NV == 0) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
       const V16<T> ux = ldv(u + i), uy = ldv(u + ns + i), uz = ldv(u + 2 * ns + i);
@@ -1154,14 +1198,17 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
                                               const double* __restrict__ layer_minv,
                                               const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
                                               int tail, unsigned int* done, const Phys* __restrict__ ph,
-                                              DevScalars* sc, int zero_unmasked) {
-  // zero_unmasked: p = 0 outside sum_p (velocity_scaling.F:61-71)
+                                              DevScalars* sc, int zero_unmasked, const T* __restrict__ site_minv = nullptr,
+                                              const unsigned char* __restrict__ site_sump = nullptr) {
+  // zero_unmasked: p = 0 outside sum_p (velocity_scaling.F:61-71).
+  // site_minv / site_sump: per-site masses and masks (.relaxor, .defects)
+  // instead of the per-layer tables; they take the scalar loop.
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if (g.plane_r % NV == 0) {
+  if (g.plane_r % NV == 0 && site_minv == nullptr && site_sump == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
       const int z = (int)(i / g.plane_r);
@@ -1184,15 +1231,16 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
   } else {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
       const int z = (int)(i / g.plane_r);
-      const T keep = (zero_unmasked && !layer_sump[z]) ? (T)0 : (T)1;
+      const bool counted = site_sump ? site_sump[i] != 0 : layer_sump[z] != 0;
+      const T keep = (zero_unmasked && !counted) ? (T)0 : (T)1;
       const T p0 = keep * (p[i] - c * F[i]);
       const T p1 = keep * (p[ns + i] - c * F[ns + i]);
       const T p2 = keep * (p[2 * ns + i] - c * F[2 * ns + i]);
       p[i] = p0;
       p[ns + i] = p1;
       p[2 * ns + i] = p2;
-      if (layer_sump[z]) {
-        const double mi = layer_minv[z];
+      if (counted) {
+        const double mi = site_minv ? (double)site_minv[i] : layer_minv[z];
         acc[0] += (double)p0 * p0 * mi + (double)p1 * p1 * mi + (double)p2 * p2 * mi;
       }
     }
@@ -1228,7 +1276,9 @@ __global__ void __launch_bounds__(256) k_layer_pump(T* __restrict__ p, T* __rest
                                                     const double* __restrict__ layer_minv,
                                                     const double* __restrict__ layer_macou,
                                                     const unsigned char* __restrict__ layer_sump, double de,
-                                                    double dea) {
+                                                    double dea, const T* __restrict__ site_minv = nullptr,
+                                                    const T* __restrict__ site_macou = nullptr,
+                                                    const double* __restrict__ layer_nsum = nullptr) {
   const int z = blockIdx.x == 0 ? g.Lz / 4 : (g.Lz / 4) * 3;
   const double sgn = blockIdx.x == 0 ? 1.0 : -1.0;
   const long long ns = g.nsite, pr = g.plane_r, base = (long long)z * pr;
@@ -1236,21 +1286,23 @@ __global__ void __launch_bounds__(256) k_layer_pump(T* __restrict__ p, T* __rest
   if (de != 0.0) {
     double s = 0.0;
     for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) {
-      const T q = p[(i / pr) * ns + base + i % pr];
-      s += (double)q * q;
+      const long long j = base + i % pr;
+      const T q = p[(i / pr) * ns + j];
+      s += (double)q * q * (site_minv ? (double)site_minv[j] : layer_minv[z]);
     }
-    const double n_layer = layer_sump[z] ? LxLy : 0.0;
-    const double e = block_sum(s) * layer_minv[z] / 2 * LxLy / n_layer;
+    const double n_layer = layer_nsum ? layer_nsum[z] : (layer_sump[z] ? LxLy : 0.0);
+    const double e = block_sum(s) / 2 * LxLy / n_layer;
     const T f = (T)sqrt((e + sgn * LxLy * de) / e);
     for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) p[(i / pr) * ns + base + i % pr] *= f;
   }
   if (dea != 0.0 && pa != nullptr) {
     double s = 0.0;
     for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) {
-      const T q = pa[(i / pr) * ns + base + i % pr];
-      s += (double)q * q;
+      const long long j = base + i % pr;
+      const T q = pa[(i / pr) * ns + j];
+      s += (double)q * q * (site_macou ? (double)site_macou[j] : layer_macou[z]);
     }
-    const double e = block_sum(s) * layer_macou[z] / 2;
+    const double e = block_sum(s) / 2;
     const T f = (T)sqrt((e + sgn * LxLy * dea) / e);
     for (long long i = threadIdx.x; i < 3 * pr; i += blockDim.x) pa[(i / pr) * ns + base + i % pr] *= f;
   }
@@ -1271,13 +1323,14 @@ __global__ void __launch_bounds__(256) k_scale(T* __restrict__ p, const double* 
 template <typename T>
 __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __restrict__ u, const T* __restrict__ F,
                                                     const DevScalars* __restrict__ sc, Geom g,
-                                                    const double* __restrict__ layer_minv) {
+                                                    const double* __restrict__ layer_minv,
+                                                    const T* __restrict__ site_minv = nullptr) {
   const long long ns = g.nsite;
   const T ck = (T)sc->kick_coef;
   const double cd = sc->pend_drift;
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if (g.plane_r % NV == 0) {
+  if (g.plane_r % NV == 0 && site_minv == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
       const T f = (T)(cd * layer_minv[(int)(i / g.plane_r)]);
@@ -1296,7 +1349,7 @@ __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __rest
     }
   } else {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-      const T f = (T)(cd * layer_minv[(int)(i / g.plane_r)]);
+      const T f = (T)(cd * (site_minv ? (double)site_minv[i] : layer_minv[(int)(i / g.plane_r)]));
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const T q = p[a * ns + i] - ck * F[a * ns + i];
@@ -1320,7 +1373,9 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
                                                     const unsigned char* __restrict__ layer_sump,
                                                     double* __restrict__ part, unsigned int* done,
                                                     const Phys* __restrict__ ph, DevScalars* sc,
-                                                    const double* __restrict__ part_r, int nblk_r) {
+                                                    const double* __restrict__ part_r, int nblk_r,
+                                                    const T* __restrict__ site_minv = nullptr,
+                                                    const unsigned char* __restrict__ site_sump = nullptr) {
   if (!PREP && blockIdx.x == 0) force_energies_tail(ph, sc, part_r, nblk_r, true);
   const long long ns = g.nsite;
   // pend_kick_f is not changed by block 0's commit
@@ -1328,7 +1383,7 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
   double acc[3] = {0.0, 0.0, 0.0};
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if (g.plane_r % NV == 0) {
+  if (g.plane_r % NV == 0 && site_minv == nullptr && site_sump == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
       const int z = (int)(i / g.plane_r);
@@ -1369,8 +1424,8 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
         pf += (double)q * y;
         ff += (double)y * y;
       }
-      if (layer_sump[z]) {
-        const double mi = layer_minv[z];
+      if (site_sump ? site_sump[i] != 0 : layer_sump[z] != 0) {
+        const double mi = site_minv ? (double)site_minv[i] : layer_minv[z];
         acc[0] += pp * mi;
         acc[1] += pf * mi;
         acc[2] += ff * mi;
@@ -1384,12 +1439,13 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
 // u <- u + coef * p * m^-1 (nose-poincare.F:41-53, leapfrog.F:104-114)
 template <typename T>
 __global__ void __launch_bounds__(256) k_drift(T* __restrict__ u, const T* __restrict__ p, const double* coef, Geom g,
-                                               const double* __restrict__ layer_minv) {
+                                               const double* __restrict__ layer_minv,
+                                               const T* __restrict__ site_minv = nullptr) {
   const long long ns = g.nsite;
   const double c = *coef;
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  if (g.plane_r % NV == 0) {
+  if (g.plane_r % NV == 0 && site_minv == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
       const T f = (T)(c * layer_minv[(int)(i / g.plane_r)]);
@@ -1405,7 +1461,7 @@ __global__ void __launch_bounds__(256) k_drift(T* __restrict__ u, const T* __res
   } else {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
       const int z = (int)(i / g.plane_r);
-      const T f = (T)(c * layer_minv[z]);
+      const T f = (T)(c * (site_minv ? (double)site_minv[i] : layer_minv[z]));
       u[i] = u[i] + f * p[i];
       u[ns + i] = u[ns + i] + f * p[ns + i];
       u[2 * ns + i] = u[2 * ns + i] + f * p[2 * ns + i];
@@ -1435,13 +1491,15 @@ __global__ void k_mirror(T* __restrict__ f, Geom g, int gap_id) {
 // KE of the current momenta without changing them.
 template <typename T>
 __global__ void __launch_bounds__(256) k_ke_only(const T* __restrict__ p, Geom g, const double* __restrict__ layer_minv,
-                                                 const unsigned char* __restrict__ layer_sump, double* __restrict__ part) {
+                                                 const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
+                                                 const T* __restrict__ site_minv = nullptr,
+                                                 const unsigned char* __restrict__ site_sump = nullptr) {
   const long long ns = g.nsite;
   double acc[1] = {0.0};
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
     const int z = (int)(i / g.plane_r);
-    if (layer_sump[z]) {
-      const double mi = layer_minv[z];
+    if (site_sump ? site_sump[i] != 0 : layer_sump[z] != 0) {
+      const double mi = site_minv ? (double)site_minv[i] : layer_minv[z];
       const double p0 = p[i], p1 = p[ns + i], p2 = p[2 * ns + i];
       acc[0] += p0 * p0 * mi + p1 * p1 * mi + p2 * p2 * mi;
     }
@@ -1461,12 +1519,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_ke_finish(const Phys* __restric
 // Z* u per component.  part[b*6 + q]: q = 0..2 sum u, 3..5 sum Z* u.
 template <typename T>
 __global__ void __launch_bounds__(256) k_avg_sums(const T* __restrict__ u, Geom g, double Zs,
-                                                  const unsigned char* __restrict__ layer_sump, double* __restrict__ part) {
+                                                  const unsigned char* __restrict__ layer_sump, double* __restrict__ part,
+                                                  const unsigned char* __restrict__ site_sump = nullptr,
+                                                  const T* __restrict__ site_zstar = nullptr) {
   const long long ns = g.nsite;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long long)gridDim.x * blockDim.x) {
     const int z = (int)(i / g.plane_r);
-    if (!layer_sump[z]) continue;
+    if (site_sump ? !site_sump[i] : !layer_sump[z]) continue;
+    if (site_zstar) Zs = site_zstar[i];
     const double a = u[i], b = u[ns + i], c = u[2 * ns + i];
     acc[0] += a;
     acc[1] += b;

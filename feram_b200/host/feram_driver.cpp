@@ -147,10 +147,6 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
   if (rc) return rc;
   if ((rc = fg_make_param(&p, errbuf, errlen))) return rc;
   const std::string base = dir_of(path) + p.filename;
-  if (file_exists(base + ".localfield") || file_exists(base + ".defects") || file_exists(base + ".relaxor")) {
-    set_msg(errbuf, errlen, "sidecar .localfield/.defects/.relaxor files are not supported by the device path");
-    return FG_ERR_UNSUPPORTED;
-  }
   fg_ctx* ctx = nullptr;
   rc = fg_create(&p, precision, &ctx);
   auto bail = [&](int code) {
@@ -222,6 +218,84 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
           }
     } else {
       fg_init_dipoR_host(&p, dipoR.data(), dipoP.data());
+    }
+  }
+  // read_relaxor (read_relaxor.F), read_defects_u (read_defects_u.F) and the
+  // .localfield of initialize_E_field (initialize_E_field.F:14-45): per-site
+  // arrays, uploaded when any of the three files is present
+  {
+    const size_t n1 = (size_t)NXP * NYP * p.Lz;
+    auto at = [&](int x, int y, int z) { return (size_t)x + (size_t)NXP * ((size_t)y + (size_t)NYP * z); };
+    std::vector<int> relaxor(n1, 1), sum_p(n1, 0);
+    std::vector<double> zs(n1, p.Z_star[0]), minv(n1, 1.0 / p.mass_dipo[0]),
+        macou(n1, p.mass_acou[0] > 0.0 ? 1.0 / p.mass_acou[0] : 0.0), eloc(3 * n1, 0.0);
+    for (int z = 0; z < p.Lz; ++z)
+      for (int y = 0; y < p.Ly; ++y)
+        for (int x = 0; x < p.Lx; ++x) sum_p[at(x, y, z)] = 1;
+    // lines "ix iy iz v1 .. vn", '#' comments; false on a malformed line
+    auto read_sites = [&](const std::string& fn, int nv, auto&& apply) -> int {
+      std::ifstream f(fn);
+      if (!f) return 0;
+      std::string line;
+      int ln = 0;
+      while (std::getline(f, line)) {
+        ++ln;
+        std::istringstream is(line);
+        std::string first;
+        if (!(is >> first) || first[0] == '#') continue;
+        std::istringstream is2(line);
+        int x, y, z;
+        double v[3] = {0.0, 0.0, 0.0};
+        bool ok = (bool)(is2 >> x >> y >> z);
+        for (int k = 0; k < nv && ok; ++k) ok = (bool)(is2 >> v[k]);
+        if (!ok || x < 0 || x >= p.Lx || y < 0 || y >= p.Ly || z < 0 || z >= p.Lz) {
+          set_msg(errbuf, errlen, "there is something wrong in line " + std::to_string(ln) + " of " + fn);
+          return -1;
+        }
+        apply(x, y, z, v);
+      }
+      return 1;
+    };
+    const int has_rel = read_sites(base + ".relaxor", 1, [&](int x, int y, int z, const double* v) {
+      const int r = (int)v[0];
+      relaxor[at(x, y, z)] = r;
+      if (r >= 1 && r <= FG_RELAXOR_MAX) {
+        zs[at(x, y, z)] = p.Z_star[r - 1];
+        minv[at(x, y, z)] = 1.0 / p.mass_dipo[r - 1];
+        macou[at(x, y, z)] = p.mass_acou[r - 1] > 0.0 ? 1.0 / p.mass_acou[r - 1] : 0.0;
+      }
+    });
+    const int has_def = read_sites(base + ".defects", 3, [&](int x, int y, int z, const double* v) {
+      for (int a = 0; a < 3; ++a) dipoR[3 * at(x, y, z) + a] = v[a];
+      minv[at(x, y, z)] = 0.0;  // 1/infinity
+      sum_p[at(x, y, z)] = 0;
+    });
+    const int has_loc = read_sites(base + ".localfield", 3, [&](int x, int y, int z, const double* v) {
+      for (int a = 0; a < 3; ++a) eloc[3 * at(x, y, z) + a] = v[a];
+    });
+    if (has_rel < 0 || has_def < 0 || has_loc < 0) {
+      fg_destroy(ctx);
+      return FG_ERR_IO;
+    }
+    if (p.bulk_or_film == FG_FILM || p.bulk_or_film == FG_EPIT)
+      for (int z = (p.Lz + 1) / 2; z < p.Lz; ++z)
+        for (int y = 0; y < p.Ly; ++y)
+          for (int x = 0; x < p.Lx; ++x) sum_p[at(x, y, z)] = 0;
+    if (p.gap_id > 0) {  // read_defects_u.F:52-66
+      const int gaps[2] = {0, p.Lz / 2};
+      for (int g = 0; g < (p.gap_id == 2 ? 2 : 1); ++g)
+        for (int y = 0; y < p.Ly; ++y)
+          for (int x = 0; x < p.Lx; ++x) {
+            for (int a = 0; a < 3; ++a) dipoR[3 * at(x, y, gaps[g]) + a] = p.gap_dipole_u[a];
+            minv[at(x, y, gaps[g])] = 0.0;
+            sum_p[at(x, y, gaps[g])] = 0;
+          }
+    }
+    if (has_rel || has_def || has_loc) {
+      rc = fg_upload_site_arrays(ctx, has_rel ? zs.data() : nullptr, minv.data(),
+                                 (has_rel && p.mass_acou[0] > 0.0) ? macou.data() : nullptr,
+                                 has_rel ? relaxor.data() : nullptr, sum_p.data(), has_loc ? eloc.data() : nullptr);
+      if (rc) return bail(rc);
     }
   }
   if ((rc = fg_set_state(ctx, dipoR.data(), dipoP.data(), 1.0, 0.0, 0.0))) return bail(rc);

@@ -223,6 +223,20 @@ int  fg_set_state(fg_ctx* ctx, const double* dipoR, const double* dipoP,
 int  fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi,
                   double strain[6], double* s_Nose, double* pi_Nose, double* H0);
 int  fg_set_thermostat(fg_ctx* ctx, double s_Nose, double pi_Nose, double H0);
+/* Per-site arrays of Coord_type (coord_module.F:100-170) as read_relaxor
+   (read_relaxor.F), read_defects_u (read_defects_u.F) and initialize_E_field
+   (initialize_E_field.F:14-45) fill them: Z_starR, mass_dipo_inv and
+   mass_acou_inv real*8 (0:2*(Lx/2+1)-1, 0:Ly+padding_y-1, 0:Lz-1), relaxor
+   integer (same shape, species 1..3), sum_p logical as int (same shape),
+   E_field_local real*8 (3, same shape).  NULL keeps the default (uniform
+   species 1, the film/gap masks, no local field).  Species select their own
+   on-site polynomial and masses; a local field switches the E-field term on.
+   Species or Z_starR values with a Z* other than Z_star(1) return
+   FG_ERR_UNSUPPORTED (per-site Z* in the dipole-dipole term is not built).
+   Call before stepping; the step graphs are rebuilt. */
+int  fg_upload_site_arrays(fg_ctx* ctx, const double* Z_starR, const double* mass_dipo_inv,
+                           const double* mass_acou_inv, const int* relaxor, const int* sum_p,
+                           const double* E_field_local);
 /* Acoustic displacement and momentum (Coord_type acouR, acouP,
    coord_module.F:25-31) when acoustic_mass_amu > 0 (otherwise FG_ERR_STATE:
    the acoustic field is then the relaxed one of each force evaluation).

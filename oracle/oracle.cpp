@@ -176,6 +176,7 @@ struct oracle_ctx {
   double H[6][6], HG[6][6], HG_inv[6], HC2[6][6];   // homogeneous, _G, _G_inv, _coupling_2
   double s_Nose = 1.0, pi_Nose = 0.0, H0 = 0.0;
   int n_sum_p = 0;
+  double E_add[3] = {0.0, 0.0, 0.0};  // last uniform field added to E_field_local
   std::vector<int> n_sum_layer;
   std::vector<double> e_layer_dipo, e_layer_acou;
   bool modulation_present = false;
@@ -1261,7 +1262,44 @@ int oracle_acouR_for_coord(oracle_ctx* o, double* acouR) {
   return 0;
 }
 
+// Per-site arrays as read_relaxor (read_relaxor.F), read_defects_u
+// (read_defects_u.F) and initialize_E_field (initialize_E_field.F:14-45) set
+// them; padded layouts; NULL keeps the current values.
+int oracle_set_sites(oracle_ctx* o, const double* Z_starR, const double* mass_dipo_inv, const double* mass_acou_inv,
+                     const int* relaxor, const int* sum_p, const double* E_field_local) {
+  const Layout& L = o->L;
+  const size_t n1 = L.nreal(1);
+  for (size_t i = 0; i < n1; ++i) {
+    if (Z_starR) o->Z_starR[i] = Z_starR[i];
+    if (mass_dipo_inv) o->mass_dipo_inv[i] = mass_dipo_inv[i];
+    if (mass_acou_inv) o->mass_acou_inv[i] = mass_acou_inv[i];
+    if (relaxor) o->relaxor[i] = relaxor[i];
+  }
+  if (sum_p) {
+    int n = 0;
+    for (int z = 0; z < L.Lz; ++z) {
+      int nl = 0;
+      for (int y = 0; y < L.Ly; ++y)
+        for (int x = 0; x < L.Lx; ++x) {
+          o->sum_p[L.s(x, y, z)] = sum_p[L.s(x, y, z)] ? 1 : 0;
+          nl += o->sum_p[L.s(x, y, z)];
+        }
+      o->n_sum_layer[z] = nl;
+      n += nl;
+    }
+    o->n_sum_p = n;
+  }
+  if (E_field_local) {
+    copy_in(o, o->E_field_local, E_field_local, 3);
+    o->p.E_field_always_zero = 0;
+    set_E_field(o, o->E_add);
+    if (o->film()) mirror(o, o->E_field);
+  }
+  return 0;
+}
+
 int oracle_set_uniform_E(oracle_ctx* o, const double E[3]) {
+  for (int a = 0; a < 3; ++a) o->E_add[a] = E[a];
   set_E_field(o, E);
   if (o->film()) mirror(o, o->E_field);
   return 0;

@@ -39,6 +39,11 @@ int    oracle_get_acou(oracle_ctx* o, double* acouR, double* acouP, double* dVda
 int    oracle_get_acouK(oracle_ctx* o, double* acouK);
 /* acouR as write_system computes it for .coord (coord_module.F:457-469) */
 int    oracle_acouR_for_coord(oracle_ctx* o, double* acouR);
+/* Per-site arrays (read_relaxor.F, read_defects_u.F, initialize_E_field.F),
+   padded layouts, NULL keeps the current values. */
+int    oracle_set_sites(oracle_ctx* o, const double* Z_starR, const double* mass_dipo_inv,
+                        const double* mass_acou_inv, const int* relaxor, const int* sum_p,
+                        const double* E_field_local);
 int    oracle_set_uniform_E(oracle_ctx* o, const double E[3]);
 int    oracle_force(oracle_ctx* o, fg_energy* e);
 int    oracle_nose_poincare(oracle_ctx* o, fg_energy* e);

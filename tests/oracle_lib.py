@@ -35,6 +35,7 @@ def load():
         "oracle_get_state": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
         "oracle_get_acouK": (C.c_int, [vp, dp]),
         "oracle_set_acou": (C.c_int, [vp, dp, dp]),
+        "oracle_set_sites": (C.c_int, [vp, dp, dp, dp, P(C.c_int), P(C.c_int), dp]),
         "oracle_get_acou": (C.c_int, [vp, dp, dp, dp]),
         "oracle_acouR_for_coord": (C.c_int, [vp, dp]),
         "oracle_set_uniform_E": (C.c_int, [vp, dp]),
@@ -114,6 +115,13 @@ class Oracle:
         a = A.complex_field(self.p)
         self.L.oracle_get_acouK(self.h, A.dptr(a.view(np.float64)))
         return a
+
+    def set_sites(self, Z_starR=None, mass_dipo_inv=None, mass_acou_inv=None, relaxor=None, sum_p=None,
+                  E_field_local=None):
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
+        dp_ = lambda a: A.dptr(a) if a is not None else None
+        self.L.oracle_set_sites(self.h, dp_(Z_starR), dp_(mass_dipo_inv), dp_(mass_acou_inv), ip(relaxor),
+                                ip(sum_p), dp_(E_field_local))
 
     def set_acou(self, acouR=None, acouP=None):
         self.L.oracle_set_acou(self.h, A.dptr(acouR) if acouR is not None else None,

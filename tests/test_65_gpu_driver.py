@@ -109,3 +109,55 @@ def test_feram_run_coord_and_dipoRavg(fg, tmp_path):
     ravg = _rows(tmp_path / "run.dipoRavg")
     assert ravg.shape == (p.N, 6)
     assert np.abs(ravg[:, 3:].reshape(p.Lz, p.Ly, p.Lx, 3) - uavg / n_av).max() <= 1e-6
+
+
+def test_feram_run_reads_relaxor_defects_localfield(fg, tmp_path):
+    """initialize_dipoR's read_relaxor and read_defects_u and
+    initialize_E_field's .localfield through the host driver, against the
+    oracle given the same per-site arrays."""
+    text = helpers.deck("zzznp.feram", L="8 8 8", n_thermalize="4", n_average="6", verbose="1", kelvin="240",
+                        P_kappa2="5.502 4.61 4.61", P_alpha="110.4 98.2 98.2", mass_amu="39.0 47.5 47.5")
+    (tmp_path / "run.feram").write_text(text)
+    p = fg.params_from_text(text, "run")
+    rng = np.random.default_rng(8)
+    rel = [(x, y, z, int(rng.integers(1, 3))) for z in range(8) for y in range(8) for x in range(8)]
+    (tmp_path / "run.relaxor").write_text("# ix iy iz species\n" + "".join(f"{x} {y} {z} {r}\n" for x, y, z, r in rel))
+    defects = [(1, 1, 1, 0.05, 0.0, -0.03), (6, 2, 5, 0.0, 0.07, 0.0)]
+    (tmp_path / "run.defects").write_text("".join(f"{x} {y} {z} {a} {b} {c}\n" for x, y, z, a, b, c in defects))
+    loc = [(x, y, 3, 0.0, 0.0, 0.004) for y in range(8) for x in range(8)]
+    (tmp_path / "run.localfield").write_text("".join(f"{x} {y} {z} {a} {b} {c}\n" for x, y, z, a, b, c in loc))
+    avg, _ = fg.feram_run(str(tmp_path / "run.feram"), A.FG_PREC_FP64)
+    # the oracle with the same arrays
+    shape = (p.Lz, p.Ly + p.padding_y, 2 * (p.Lx // 2 + 1))
+    relaxor = np.ones(shape, dtype=np.int32)
+    zs = np.full(shape, p.Z_star[0])
+    minv = np.zeros(shape)
+    sum_p = np.zeros(shape, dtype=np.int32)
+    sum_p[:, :p.Ly, :p.Lx] = 1
+    for x, y, z, r in rel:
+        relaxor[z, y, x] = r
+        minv[z, y, x] = 1.0 / p.mass_dipo[r - 1]
+    eloc = A.real_field(p)
+    for x, y, z, a, b, c in loc:
+        A.physical(eloc, p)[z, y, x] = (a, b, c)
+    o = oracle_lib.Oracle(p)
+    o.initialize()
+    st = o.get_state()
+    u = st["dipoR"].copy()
+    for x, y, z, a, b, c in defects:
+        A.physical(u, p)[z, y, x] = (a, b, c)
+        minv[z, y, x] = 0.0
+        sum_p[z, y, x] = 0
+    o.set_sites(Z_starR=zs, relaxor=relaxor, mass_dipo_inv=minv, sum_p=sum_p, E_field_local=eloc)
+    o.set_state(u, st["dipoP"], 1.0, 0.0, 0.0)
+    e = o.force()
+    e.dipo_kinetic = o.kinetic_energy_dipo()
+    ao = A.fg_average()
+    o.md(1, p.n_thermalize + p.n_average, 1, e, ao)
+    assert avg.n_steps == ao.n_steps == 6
+    for f in ("total", "unharmonic", "dipole_E_field", "dipo_kinetic"):
+        a, b = getattr(avg.energy, f), getattr(ao.energy, f)
+        assert abs(a - b) <= 1e-9 * max(abs(b), 1.0), (f, a, b)
+    assert avg.energy.dipole_E_field != 0.0
+    for i in range(3):
+        assert abs(avg.u[i] - ao.u[i]) <= 1e-9 * max(abs(ao.u[i]), 1.0)
