@@ -158,6 +158,7 @@ struct fg_ctx {
   bool tables_ready = false;
   bool force_fresh = false;
   bool np_ready = false;  // DevScalars' pending half step matches the state
+  bool pdl = false;       // launch the step kernels as programmatic dependents
   bool store_acouK = false;
   double n_sum_p = 0;
   int NXP = 0, NYP = 0;
@@ -244,13 +245,31 @@ void with_z_kspace(int Lz, int cw, bool acou, F f) {
   else f(k_z_kspace<T, 0, 0>);
 }
 
+// Kernel launch that, while ctx->pdl is set, lets the kernel be scheduled
+// before its predecessor on the stream has finished (programmatic stream
+// serialization).  Only kernels that start with pdl_enter() go through it.
+template <typename... KArgs, typename... Args>
+void launch_dep(fg_ctx* ctx, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = ctx->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = ctx->pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <typename T, int MODE>
 int launch_xy_fwd(fg_ctx* ctx, const T* src, cplx<T>* spec, int ncomp, int smem, const cplx<T>* twx,
                   const cplx<T>* twm, const cplx<T>* twy) {
   const Geom& g = ctx->g;
   with_xy_fwd<T, MODE>(g.m, g.Ly, [&](auto kern) {
-    kern<<<dim3(g.Lz, ncomp), kThreadsFFT, smem, ctx->stream>>>(src, spec, g, ctx->px, ctx->py, twx, twm, twy,
-                                                                 ctx->posm, 0);
+    launch_dep(ctx, kern, dim3(g.Lz, ncomp), kThreadsFFT, smem, src, spec, g, ctx->px, ctx->py, twx, twm, twy,
+               ctx->posm, 0);
   });
   CKL();
   return FG_OK;
@@ -262,7 +281,7 @@ template <typename T>
 int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp, bool strain_prologue = false) {
   const Geom& g = ctx->g;
   with_xy_inv<T>(g.m, g.Ly, [&](auto kern) {
-    kern<<<dim3(g.Lz, ncomp), kThreadsFFT, ctx->smem_xy, ctx->stream>>>(
+    launch_dep(ctx, kern, dim3(g.Lz, ncomp), kThreadsFFT, ctx->smem_xy,
         spec, out, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy,
         ctx->posm, 0, strain_prologue ? ctx->ph : nullptr, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
   });
@@ -275,7 +294,7 @@ template <typename T>
 int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
   const Geom& g = ctx->g;
   with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, [&](auto kern) {
-    kern<<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z, ctx->stream>>>(
+    launch_dep(ctx, kern, ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z,
         (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
         (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, nullptr);
   });
@@ -300,7 +319,7 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
   // np_post: the energies and (35e) are finished by the closing kick's block 0
-  k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(
+  launch_dep(ctx, k_assemble<T>, ctx->grid_elem, kThreadsElem, 0,
       (const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc, ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
       ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E);
   CKL();
@@ -374,7 +393,7 @@ int enqueue_kick_drift(fg_ctx* ctx) {
 // prep: sums of the current state only (np_prepare)
 template <typename T, bool PREP>
 int enqueue_kick_close(fg_ctx* ctx) {
-  k_kick_close<T, PREP><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
+  launch_dep(ctx, k_kick_close<T, PREP>, ctx->grid_elem, kThreadsElem, 0,
       (T*)ctx->p, (const T*)ctx->F, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, ctx->done, ctx->ph,
       ctx->sc, ctx->part_r, ctx->grid_elem, (const T*)ctx->site_minv, ctx->site_sump);
   CKL();
@@ -393,8 +412,12 @@ template <typename T>
 int enqueue_np(fg_ctx* ctx) {
   int rc;
   if ((rc = enqueue_kick_drift<T>(ctx))) return rc;
-  if ((rc = enqueue_force<T>(ctx, true))) return rc;
-  return enqueue_kick_close<T, false>(ctx);
+  // the five kernels after the first start while their predecessor drains
+  ctx->pdl = !ctx->bulk_or_film_mirror();
+  rc = enqueue_force<T>(ctx, true);
+  if (!rc) rc = enqueue_kick_close<T, false>(ctx);
+  ctx->pdl = false;
+  return rc;
 }
 
 // leapfrog (leapfrog.F:103-151), i_step != 0

@@ -57,6 +57,15 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Programmatic dependent launch: let the next kernel of the stream be
+// scheduled now, then wait until the previous kernel has completed and its
+// writes are visible.  Both are no-ops for launches without the
+// programmatic-serialization attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+}
+
 // Device error record (bounds checks, non-finite reductions).  The library
 // is one translation unit, so this __device__ variable has one definition.
 struct DevError {

@@ -254,6 +254,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int out_comp0) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
@@ -390,6 +391,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
                                                 const int* __restrict__ posm, int in_comp0,
                                                 const Phys* __restrict__ ph, DevScalars* sc,
                                                 const double* __restrict__ part_k, int nblk_k) {
+  pdl_enter();
   // Block (0, 0) first finishes the k-space pass that wrote spec: its
   // energies and the homogeneous strain, from k_z_kspace's block partials
   // (nothing in this kernel needs them; k_assemble does).
@@ -801,6 +803,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
                                                      Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
                                                      const Phys* __restrict__ ph, double* __restrict__ part,
                                                      DevScalars* sc, ZTiles zt, unsigned int* done) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
@@ -1109,6 +1112,7 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
                                                   const unsigned char* __restrict__ site_species = nullptr,
                                                   const T* __restrict__ site_zstar = nullptr,
                                                   const T* __restrict__ site_E = nullptr) {
+  pdl_enter();
   // site_*: per-site species (.relaxor), Z* and local field (.localfield);
   // they take the scalar loop
   const long long ns = g.nsite;
@@ -1325,6 +1329,7 @@ __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __rest
                                                     const DevScalars* __restrict__ sc, Geom g,
                                                     const double* __restrict__ layer_minv,
                                                     const T* __restrict__ site_minv = nullptr) {
+  pdl_enter();
   const long long ns = g.nsite;
   const T ck = (T)sc->kick_coef;
   const double cd = sc->pend_drift;
@@ -1376,6 +1381,7 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
                                                     const double* __restrict__ part_r, int nblk_r,
                                                     const T* __restrict__ site_minv = nullptr,
                                                     const unsigned char* __restrict__ site_sump = nullptr) {
+  pdl_enter();
   if (!PREP && blockIdx.x == 0) force_energies_tail(ph, sc, part_r, nblk_r, true);
   const long long ns = g.nsite;
   // pend_kick_f is not changed by block 0's commit
