@@ -112,6 +112,9 @@ struct fg_ctx {
   cplx<double>* twy64 = nullptr;
   cplx<double>* twz64 = nullptr;
   double* L64 = nullptr;  // long-range table (FP64, table slots)
+  void* ltab = nullptr;   // L/N in T (table slots), per-site Z* only
+  bool ltab_ready = false;
+  bool zsite = false;     // per-site Z* differs: Z* u transformed on its own
   int* revx = nullptr;
   int* revy = nullptr;
   int* revz = nullptr;
@@ -230,9 +233,12 @@ void with_xy_inv(int m, int Ly, F f) {
 template <typename T>
 constexpr int z_cw_cap() { return sizeof(T) == 4 ? 8 : 4; }
 template <typename T, class F>
-void with_z_kspace(int Lz, int cw, bool acou, F f) {
+void with_z_kspace(int Lz, int cw, bool acou, bool zsite, F f) {
   constexpr int C = z_cw_cap<T>();
-  if (acou) {
+  if (zsite) {  // per-site Z*: runtime transforms
+    if (acou) f(k_z_kspace<T, 0, 0, true, true>);
+    else f(k_z_kspace<T, 0, 0, false, true>);
+  } else if (acou) {
     if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C, true>);
     else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C, true>);
     else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C, true>);
@@ -244,6 +250,10 @@ void with_z_kspace(int Lz, int cw, bool acou, F f) {
   else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C>);
   else f(k_z_kspace<T, 0, 0>);
 }
+
+// First component of Z*(R) u in the spectrum and of the long-range dipole
+// field in rwork (per-site Z*): after u, u u and the acoustic displacement.
+inline int zu_comp(const fg_ctx* ctx) { return ctx->acou ? 12 : 9; }
 
 // Kernel launch that, while ctx->pdl is set, lets the kernel be scheduled
 // before its predecessor on the stream has finished (programmatic stream
@@ -263,13 +273,14 @@ void launch_dep(fg_ctx* ctx, void (*kern)(KArgs...), dim3 grid, dim3 block, size
   cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
+// zstar: per-site Z*, transformed times u in components zu0..zu0+2
 template <typename T, int MODE>
 int launch_xy_fwd(fg_ctx* ctx, const T* src, cplx<T>* spec, int ncomp, int smem, const cplx<T>* twx,
-                  const cplx<T>* twm, const cplx<T>* twy) {
+                  const cplx<T>* twm, const cplx<T>* twy, const T* zstar = nullptr, int zu0 = 0) {
   const Geom& g = ctx->g;
   with_xy_fwd<T, MODE>(g.m, g.Ly, [&](auto kern) {
     launch_dep(ctx, kern, dim3(g.Lz, ncomp), kThreadsFFT, smem, src, spec, g, ctx->px, ctx->py, twx, twm, twy,
-               ctx->posm, 0);
+               ctx->posm, 0, zstar, zu0);
   });
   CKL();
   return FG_OK;
@@ -293,10 +304,11 @@ int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp, bool stra
 template <typename T>
 int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
   const Geom& g = ctx->g;
-  with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, [&](auto kern) {
+  with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, ctx->zsite, [&](auto kern) {
     launch_dep(ctx, kern, ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z,
         (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
-        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, nullptr);
+        (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, nullptr,
+        (const T*)ctx->ltab);
   });
   CKL();
   return FG_OK;
@@ -314,14 +326,16 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   }
   int rc;
   if ((rc = launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, ctx->ncx, ctx->smem_xy, (const cplx<T>*)ctx->twx,
-                                     (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy)))
+                                     (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy,
+                                     ctx->zsite ? (const T*)ctx->site_zstar : nullptr, zu_comp(ctx))))
     return rc;
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
   // np_post: the energies and (35e) are finished by the closing kick's block 0
   launch_dep(ctx, k_assemble<T>, ctx->grid_elem, kThreadsElem, 0,
       (const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc, ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
-      ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E);
+      ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
+      ctx->zsite ? zu_comp(ctx) : 0);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
@@ -557,6 +571,19 @@ int validate(const fg_params* p, std::string* why) {
   return FG_OK;
 }
 
+// z tiles: CW is the largest power of two <= cwmax dividing Lx/2 whose
+// tile of nc components fits in shared memory
+ZTiles z_tiles(const Geom& g, int nc, size_t esz, int cwmax, int smem_max) {
+  ZTiles t{};
+  int cw = cwmax;
+  while (cw > 1 && (g.m % cw != 0 || (size_t)nc * g.Lz * cw * esz > (size_t)smem_max)) cw /= 2;
+  t.CW = cw;
+  t.ntx = g.m / cw;
+  t.nreg = t.ntx * g.Ly;
+  t.nnyq = div_up(g.Ly, cw);
+  return t;
+}
+
 template <typename T>
 int create_impl(fg_ctx* ctx) {
   const fg_params& P = ctx->P;
@@ -587,21 +614,10 @@ int create_impl(fg_ctx* ctx) {
   ctx->smem_xy64 = (int)(sizeof(cplx<double>) * g.Ly * (g.m + 1));
   if (ctx->smem_xy > smem_max || ctx->smem_xy64 > smem_max)
     return fail(ctx, FG_ERR_UNSUPPORTED, "an x-y plane of the supercell does not fit in shared memory");
-  // z tiles: CW is the largest power of two <= cwmax dividing Lx/2 whose
-  // tile fits in shared memory
-  auto tiles = [&](int nc, size_t esz, int cwmax) {
-    ZTiles t{};
-    int cw = cwmax;
-    while (cw > 1 && (g.m % cw != 0 || (size_t)nc * g.Lz * cw * esz > (size_t)smem_max)) cw /= 2;
-    t.CW = cw;
-    t.ntx = g.m / cw;
-    t.nreg = t.ntx * g.Ly;
-    t.nnyq = div_up(g.Ly, cw);
-    return t;
-  };
+  auto tiles = [&](int nc, size_t esz, int cwmax) { return z_tiles(g, nc, esz, cwmax, smem_max); };
   ctx->acou = P.mass_acou[0] > 0.0;
   ctx->ncx = ctx->acou ? 12 : 9;
-  ctx->zt = tiles(ctx->ncx, sizeof(cplx<T>), sizeof(T) == 4 ? 8 : 4);
+  ctx->zt = tiles(ctx->ncx, sizeof(cplx<T>), z_cw_cap<T>());
   ctx->zt6 = tiles(6, sizeof(cplx<double>), 8);
   ctx->zt1 = tiles(1, sizeof(cplx<double>), 8);
   if ((size_t)ctx->ncx * g.Lz * ctx->zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
@@ -629,7 +645,7 @@ int create_impl(fg_ctx* ctx) {
     with_xy_fwd<T, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
     with_xy_fwd<double, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy64); });
     with_xy_inv<T>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
-    with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, [&](auto k) { setattr(k, ctx->smem_z); });
+    with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, false, [&](auto k) { setattr(k, ctx->smem_z); });
     setattr(k_z_pass<T, false>, ctx->smem_z3);
     setattr(k_z_pass<T, true>, ctx->smem_z3);
     setattr(k_z_ewald_pack<T>, ctx->smem_z6);
@@ -846,6 +862,7 @@ int build_tables_impl(fg_ctx* ctx) {
   int rc = check_device_error(ctx);
   if (rc) return rc;
   ctx->tables_ready = true;
+  ctx->ltab_ready = false;
   return FG_OK;
 }
 
@@ -918,6 +935,7 @@ int upload_tables_impl(fg_ctx* ctx, const double* sr, const double* lr) {
   if (!ctx->L64) CK(cudaMalloc(&ctx->L64, sizeof(double) * 6 * (size_t)g.nkpos));
   CK(cudaMemcpy(ctx->L64, L.data(), L.size() * sizeof(double), cudaMemcpyHostToDevice));
   ctx->tables_ready = true;
+  ctx->ltab_ready = false;
   return FG_OK;
 }
 
@@ -1048,6 +1066,52 @@ int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
 // i = x + Lx (y + Ly z) from the padded Fortran arrays of alloc_Coord
 // (coord_module.F:100-170) and read_relaxor / read_defects_u /
 // initialize_E_field.
+// Per-site Z* on or off: three more components in the force transforms
+// (Z*(R) u forward, the long-range field inverse), wider spectrum and rwork,
+// new z tiles, and the L/N table in T.
+template <typename T>
+int set_zsite(fg_ctx* ctx, bool on) {
+  if (on == ctx->zsite) return FG_OK;
+  const Geom& g = ctx->g;
+  int dev = 0, smem_optin = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int smem_max = smem_optin - 8192;
+  const int ncx = (ctx->acou ? 12 : 9) + (on ? 3 : 0);
+  const ZTiles zt = z_tiles(g, ncx, sizeof(cplx<T>), z_cw_cap<T>(), smem_max);
+  if ((size_t)ncx * g.Lz * zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
+    return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
+  const int smem_z = (int)(ncx * ((size_t)g.Lz * zt.CW + kZPad<T>) * sizeof(cplx<T>));
+  cudaError_t ea = cudaSuccess;
+  with_z_kspace<T>(g.Lz, zt.CW, ctx->acou, on, [&](auto kern) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    const int cap = smem_optin - (int)fa.sharedSizeBytes;
+    if (e == cudaSuccess && smem_z > cap) e = cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+    ea = e;
+  });
+  if (ea != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (void** b : {&ctx->spec, &ctx->rwork, (void**)&ctx->part_k, &ctx->ltab})
+    if (*b) {
+      cudaFree(*b);
+      *b = nullptr;
+    }
+  ctx->ncx = ncx;
+  ctx->zt = zt;
+  ctx->smem_z = smem_z;
+  ctx->smem_z3 = (int)(3 * (size_t)g.Lz * zt.CW * sizeof(cplx<T>));
+  ctx->zsite = on;
+  ctx->ltab_ready = false;
+  CK(cudaMalloc(&ctx->spec, (size_t)ncx * sizeof(cplx<T>) * (size_t)g.ncplx));
+  CK(cudaMemset(ctx->spec, 0, (size_t)ncx * sizeof(cplx<T>) * (size_t)g.ncplx));
+  CK(cudaMalloc(&ctx->rwork, (size_t)ncx * ctx->real_bytes));
+  CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)(zt.nreg + zt.nnyq)));
+  if (on) CK(cudaMalloc(&ctx->ltab, 6 * sizeof(T) * (size_t)g.nkpos));
+  return FG_OK;
+}
+
 template <typename T>
 int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, const double* macou, const int* relaxor,
                       const int* sum_p, const double* Eloc) {
@@ -1064,26 +1128,37 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
     return upload(ctx, dst, vec);
   };
   int rc;
+  // Z*(R): the array if given, else Z_star of each site's species when the
+  // species differ in it (read_relaxor.F:35)
+  std::vector<double> zs;
+  if (zstar) {
+    zs.resize(ns);
+    for (size_t i = 0; i < ns; ++i) zs[i] = zstar[fidx(i)];
+  }
   if (relaxor) {
     std::vector<unsigned char> sp(ns);
     for (size_t i = 0; i < ns; ++i) {
       const int r = relaxor[fidx(i)];
       if (r < 1 || r > FG_RELAXOR_MAX) return fail(ctx, FG_ERR_ARG, "relaxor index outside 1..3");
-      if (P.Z_star[r - 1] != P.Z_star[0])
-        return fail(ctx, FG_ERR_UNSUPPORTED,
-                    "species with a different Z_star: per-site Z* in the dipole-dipole term is not built on the device");
       sp[i] = (unsigned char)(r - 1);
+    }
+    bool differ = false;
+    for (int r = 1; r < FG_RELAXOR_MAX; ++r) differ |= P.Z_star[r] != P.Z_star[0];
+    if (!zstar && differ) {
+      zs.resize(ns);
+      for (size_t i = 0; i < ns; ++i) zs[i] = P.Z_star[sp[i]];
     }
     if ((rc = replace((void**)&ctx->site_species, sp))) return rc;
   }
-  if (zstar) {
+  if (!zs.empty()) {
     std::vector<T> v(ns);
+    bool differ = false;
     for (size_t i = 0; i < ns; ++i) {
-      v[i] = (T)zstar[fidx(i)];
-      if (zstar[fidx(i)] != P.Z_star[0])
-        return fail(ctx, FG_ERR_UNSUPPORTED, "per-site Z* differing from Z_star(1) is not built on the device");
+      v[i] = (T)zs[i];
+      differ |= zs[i] != P.Z_star[0];
     }
     if ((rc = replace(&ctx->site_zstar, v))) return rc;
+    if ((rc = set_zsite<T>(ctx, differ))) return rc;
   }
   if (minv) {
     std::vector<T> v(ns);
@@ -1131,6 +1206,16 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
 int ensure_ready(fg_ctx* ctx) {
   if (!ctx) return FG_ERR_ARG;
   if (!ctx->tables_ready) return fail(ctx, FG_ERR_STATE, "no k-space tables: call fg_build_tables or fg_upload_tables");
+  if (ctx->zsite && !ctx->ltab_ready) {  // L/N for the per-site Z* path, from the FP64 long-range table
+    const long long n = 6 * ctx->g.nkpos;
+    const int grid = (int)std::min<long long>(div_up(n, 256), 4096);
+    if (ctx->prec == FG_PREC_MIXED)
+      k_table_scale<float><<<grid, 256, 0, ctx->stream>>>((float*)ctx->ltab, ctx->L64, ctx->P.Ninv, n);
+    else
+      k_table_scale<double><<<grid, 256, 0, ctx->stream>>>((double*)ctx->ltab, ctx->L64, ctx->P.Ninv, n);
+    CKL();
+    ctx->ltab_ready = true;
+  }
   return FG_OK;
 }
 
@@ -1196,15 +1281,17 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     CK(cudaEventRecord(ev[k], st));
     rc |= enqueue_kick_drift<T>(ctx);
     CK(cudaEventRecord(ev[++k], st));
-    rc |= launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, 9, ctx->smem_xy, (const cplx<T>*)ctx->twx,
-                                   (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy);
+    rc |= launch_xy_fwd<T, SRC_U9>(ctx, u, (cplx<T>*)ctx->spec, ctx->ncx, ctx->smem_xy, (const cplx<T>*)ctx->twx,
+                                   (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy,
+                                   ctx->zsite ? (const T*)ctx->site_zstar : nullptr, zu_comp(ctx));
     CK(cudaEventRecord(ev[++k], st));
     rc |= launch_z_kspace<T>(ctx, nullptr);
     CK(cudaEventRecord(ev[++k], st));
-    rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 9, true);
+    rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true);
     CK(cudaEventRecord(ev[++k], st));
-    k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph,
-                                                           ctx->sc, ctx->part_r, TAIL_NONE, ctx->done + 2);
+    k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(
+        (const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, TAIL_NONE, ctx->done + 2,
+        ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E, ctx->zsite ? zu_comp(ctx) : 0);
     CK(cudaEventRecord(ev[++k], st));
     rc |= enqueue_kick_close<T, false>(ctx);
     CK(cudaEventRecord(ev[++k], st));
@@ -1256,7 +1343,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (ctx->g_vs) cudaGraphExecDestroy(ctx->g_vs);
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
   void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
-                  ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->revx,
+                  ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->ltab, ctx->revx,
                   ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
                   ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all,

@@ -233,8 +233,9 @@ enum { SRC_U9 = 0, SRC_FIELD = 1 };
 // pairs, unpack to the Lx/2+1 bins of the real transform, DIF along y.
 // SRC_U9: component c of (u_x, u_y, u_z, u_x^2, u_y^2, u_z^2, u_y u_z,
 // u_z u_x, u_x u_y) from u (dipoFFT.F:19-44); components 9..11 are src
-// components 3..5 (the acoustic displacement stored after u).  SRC_FIELD:
-// component c of src.
+// components 3..5 (the acoustic displacement stored after u); with a per-site
+// Z* (zstar != null) components zu0..zu0+2 are Z*(R) u (Z_u_R, dipoFFT.F:
+// 36-44).  SRC_FIELD: component c of src.
 // MC, LYC > 0 select the compile-time transforms for m = Lx/2 = MC and
 // Ly = LYC (launched with exactly kXYThreads threads); 0 = runtime plans.
 constexpr int kXYThreads = 512;
@@ -253,7 +254,8 @@ template <typename T, int MODE, int MC = 0, int LYC = 0>
 __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T* __restrict__ src, cplx<T>* __restrict__ spec, Geom g,
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
-                                                const int* __restrict__ posm, int out_comp0) {
+                                                const int* __restrict__ posm, int out_comp0,
+                                                const T* __restrict__ zstar = nullptr, int zu0 = 0) {
   pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
@@ -267,16 +269,18 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
   const cplx<T>* twx_u = MC > 0 ? tws_x : twx;
   const long long plane_off = (long long)z * g.plane_r;
   const int total = Ly * m;
+  const bool zu = MODE == SRC_U9 && zstar != nullptr && c >= zu0;  // Z*(R) u_(c - zu0)
   if constexpr (MC > 0) {
     // First x stage straight from the real rows (packed (x even, x odd)
     // pairs, products formed on load), then the rest of the x pass.
-    const bool plain = MODE == SRC_FIELD || c < 3 || c >= 9;
-    const int ca = plain ? (c >= 9 && MODE == SRC_U9 ? c - 6 : c) : (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
-    const int cb = plain ? -1 : (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
+    const bool plain = !zu && (MODE == SRC_FIELD || c < 3 || c >= 9);
+    const int ca = zu ? c - zu0
+                      : plain ? (c >= 9 && MODE == SRC_U9 ? c - 6 : c) : (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
+    const int cb = plain || zu ? -1 : (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
     const T* pa = src + (long long)ca * g.nsite + plane_off;
-    const T* pb = src + (long long)(cb < 0 ? ca : cb) * g.nsite + plane_off;
+    const T* pb = zu ? zstar + plane_off : src + (long long)(cb < 0 ? ca : cb) * g.nsite + plane_off;
     auto st = [&](int y, int e, const cplx<T>& v) { buf[y * (MC + 1) + e] = v; };
-    if (cb < 0) {
+    if (plain) {
       auto ld = [&](int y, int e) {
         const T2 a = *reinterpret_cast<const T2*>(pa + (long long)y * (2 * MC) + 2 * e);
         return mk<cplx<T>>(a.x, a.y);
@@ -292,7 +296,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
     }
     __syncthreads();
     ct_forward_range<T, MC, 1, ct_nst(MC), kXYThreads, BatchCT<LYC, 1, 0, MC + 1, 1>>(buf, tws_m);
-  } else if (MODE == SRC_FIELD || c < 3 || c >= 9) {
+  } else if (!zu && (MODE == SRC_FIELD || c < 3 || c >= 9)) {
     // plain component: asynchronous copies of packed (x even, x odd) pairs
     const T* sp = src + (long long)(c >= 9 && MODE == SRC_U9 ? c - 6 : c) * g.nsite + plane_off;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
@@ -311,10 +315,10 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
         if (idx < total) {
           const int y = idx / m, jx = idx - y * m;
           const long long o = plane_off + (long long)y * Lx + 2 * jx;
-          const int ca = (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
+          const int ca = zu ? c - zu0 : (c == 3 || c == 8) ? 0 : (c == 4 || c == 6) ? 1 : 2;
           const int cb = (c == 3) ? 0 : (c == 4) ? 1 : (c == 5) ? 2 : (c == 6) ? 2 : (c == 7) ? 0 : 1;
           va[r] = *reinterpret_cast<const T2*>(src + (long long)ca * g.nsite + o);
-          vb[r] = *reinterpret_cast<const T2*>(src + (long long)cb * g.nsite + o);
+          vb[r] = *reinterpret_cast<const T2*>(zu ? zstar + o : src + (long long)cb * g.nsite + o);
         }
       }
 #pragma unroll
@@ -790,6 +794,9 @@ __global__ void __launch_bounds__(256) k_z_pass(cplx<T>* __restrict__ spec, Geom
 // (elastic.F:79-180), and the half-spectrum energy sums of
 // dVddi-dipole-dipole.F:226-250 (by Parseval) and energy_module.F:150-240;
 // then DIT along z.  Slots 0..2 return F(k), slots 3..8 inhoK(k).
+// ZSC (per-site Z*, dVddi-dipole-dipole.F:20-60): slots Z0..Z0+2 carry
+// FFT(Z*(R) u) in and the long-range part (L/N) FFT(Z* u) out, while slots
+// 0..2 return the short-range part (S/N) uK alone; L/N comes from ltab.
 // LZC, CWC > 0 select the compile-time z transforms (launched with exactly
 // kZThreads threads); 0 = runtime plan and tile width.
 constexpr int kZThreads = 256;
@@ -797,12 +804,13 @@ constexpr int kZThreads = 256;
 template <typename T>
 constexpr int kZPad = 64 / (int)sizeof(cplx<T>);
 
-template <typename T, int LZC = 0, int CWC = 0, bool ACOU = false>
+template <typename T, int LZC = 0, int CWC = 0, bool ACOU = false, bool ZSC = false>
 __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
                                                      const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
                                                      Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
                                                      const Phys* __restrict__ ph, double* __restrict__ part,
-                                                     DevScalars* sc, ZTiles zt, unsigned int* done) {
+                                                     DevScalars* sc, ZTiles zt, unsigned int* done,
+                                                     const T* __restrict__ ltab) {
   pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
@@ -810,7 +818,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
   // ACOU: acoustic-displacement MD, three more components in and out
   // (FFT(acouR) in, dVdacK out; acouFFT.F:9-26, dVdac.F:11-63)
-  constexpr int NC = ACOU ? 12 : 9;
+  constexpr int Z0 = ACOU ? 12 : 9;  // first Z* u slot (ZSC)
+  constexpr int NC = Z0 + (ZSC ? 3 : 0);
   const int buf_len = NC * Lz * CW;
   // component stride of the tile; the compile-time path pads it by 64 bytes
   // so that the 4 components a warp spans fall on different banks
@@ -867,8 +876,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     // ---- dipole-dipole
     const long long tpos = tpos0 + (long long)zs * g.KXP;
     using T2 = typename RT2<T>::type;
-    const T2* Dp = reinterpret_cast<const T2*>(dtab + tpos * 6);  // 6 T per k: 2 T-aligned pairs
-    T D[6];
+    const T2* Dp = reinterpret_cast<const T2*>((ZSC ? ltab : dtab) + tpos * 6);  // 6 T per k: 2 T-aligned pairs
+    T D[6];  // D = (S + Z*^2 L)/N; ZSC: L/N
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const T2 v = __ldg(&Dp[q]);
@@ -887,9 +896,36 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       const double cc[3] = {tx.x, ty.x, tz.x}, ss[3] = {tx.y, ty.y, tz.y};
       double S[6];
       short_range_k(ph->j, ph->kap2x2, cc, ss, S);
-      acc[0] += w1 * (S[0] * qv[0] + S[1] * qv[1] + S[2] * qv[2] + 2.0 * (S[3] * qv[3] + S[4] * qv[4] + S[5] * qv[5]));
-      acc[1] += w1 * ((double)D[0] * qv[0] + (double)D[1] * qv[1] + (double)D[2] * qv[2] +
-                      2.0 * ((double)D[3] * qv[3] + (double)D[4] * qv[4] + (double)D[5] * qv[5]));
+      const double es = w1 * (S[0] * qv[0] + S[1] * qv[1] + S[2] * qv[2] + 2.0 * (S[3] * qv[3] + S[4] * qv[4] + S[5] * qv[5]));
+      acc[0] += es;
+      if constexpr (ZSC) {
+        // short range on uK, long range on FFT(Z* u): Fl = (L/N) ZuK,
+        // energy (1/2N) sum w' Re(ZuK* L ZuK) by Parseval
+        cplx<T> zu[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) zu[a] = buf[(Z0 + a) * ZS + zs * CW + cw];
+        double qz[6];
+        qz[0] = (double)zu[0].x * zu[0].x + (double)zu[0].y * zu[0].y;
+        qz[1] = (double)zu[1].x * zu[1].x + (double)zu[1].y * zu[1].y;
+        qz[2] = (double)zu[2].x * zu[2].x + (double)zu[2].y * zu[2].y;
+        qz[3] = (double)zu[1].x * zu[2].x + (double)zu[1].y * zu[2].y;
+        qz[4] = (double)zu[2].x * zu[0].x + (double)zu[2].y * zu[0].y;
+        qz[5] = (double)zu[0].x * zu[1].x + (double)zu[0].y * zu[1].y;
+        acc[1] += es * Ninv + w1 * ((double)D[0] * qz[0] + (double)D[1] * qz[1] + (double)D[2] * qz[2] +
+                                    2.0 * ((double)D[3] * qz[3] + (double)D[4] * qz[4] + (double)D[5] * qz[5]));
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const int b = (a + 1) % 3, c3 = (a + 2) % 3;  // off-diagonal slots: yz 3, zx 4, xy 5
+          const T dab = D[a == 0 ? 5 : a == 1 ? 3 : 4], dac = D[a == 0 ? 4 : a == 1 ? 5 : 3];
+          buf[(Z0 + a) * ZS + zs * CW + cw] =
+              mk<cplx<T>>(D[a] * zu[a].x + dab * zu[b].x + dac * zu[c3].x, D[a] * zu[a].y + dab * zu[b].y + dac * zu[c3].y);
+        }
+#pragma unroll
+        for (int q = 0; q < 6; ++q) D[q] = (T)(S[q] * Ninv);
+      } else {
+        acc[1] += w1 * ((double)D[0] * qv[0] + (double)D[1] * qv[1] + (double)D[2] * qv[2] +
+                        2.0 * ((double)D[3] * qv[3] + (double)D[4] * qv[4] + (double)D[5] * qv[5]));
+      }
     }
     cplx<T> F[3];
     F[0] = mk<cplx<T>>(D[0] * u[0].x + D[5] * u[1].x + D[4] * u[2].x, D[0] * u[0].y + D[5] * u[1].y + D[4] * u[2].y);
@@ -1111,10 +1147,12 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
                                                   unsigned int* done,
                                                   const unsigned char* __restrict__ site_species = nullptr,
                                                   const T* __restrict__ site_zstar = nullptr,
-                                                  const T* __restrict__ site_E = nullptr) {
+                                                  const T* __restrict__ site_E = nullptr, int zl0 = 0) {
   pdl_enter();
   // site_*: per-site species (.relaxor), Z* and local field (.localfield);
-  // they take the scalar loop
+  // they take the scalar loop.  zl0 > 0: rw components zl0..zl0+2 hold the
+  // long-range dipole field of Z* u, which acts on the site times its Z*
+  // (dVddi-dipole-dipole.F:52-60); components 0..2 the short-range part.
   const long long ns = g.nsite;
   AsmConst<T> k;
   k.fa2g = (T)ph->fa2g; k.tg = (T)ph->tg; k.sk = (T)ph->sk; k.tk2 = (T)ph->tk2; k.fk = (T)ph->fk;
@@ -1149,8 +1187,14 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
 #pragma unroll
       for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
       const T ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
+      T f0 = rw[i], f1 = rw[ns + i], f2 = rw[2 * ns + i];
+      if (zl0 > 0) {
+        f0 = f0 + ks.Zs * rw[(zl0 + 0) * ns + i];
+        f1 = f1 + ks.Zs * rw[(zl0 + 1) * ns + i];
+        f2 = f2 + ks.Zs * rw[(zl0 + 2) * ns + i];
+      }
       T o0, o1, o2;
-      assemble_site(ks, ux, uy, uz, rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
+      assemble_site(ks, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
       if (dk2 != 0.0) {  // kappa2(s) - kappa2(1) (dVddi-unharmonic.F:40,73)
         const T t = (T)(2 * dk2);
         o0 = o0 + t * ux;
@@ -1690,6 +1734,14 @@ __global__ void __launch_bounds__(256) k_z_ewald_pack(const cplx<double>* __rest
       if (L64) L64[tpos * 6 + q] = Lt[q];
     }
   }
+}
+
+// dst = (T)(src * scale): the L/N table of the per-site Z* path
+template <typename T>
+__global__ void __launch_bounds__(256) k_table_scale(T* __restrict__ dst, const double* __restrict__ src, double scale,
+                                                     long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = (T)(src[i] * scale);
 }
 
 // c_k_modulation_k = modulation_constant * k * r2c(modulation_R) (elastic.F:212-225)

@@ -231,9 +231,11 @@ int  fg_set_thermostat(fg_ctx* ctx, double s_Nose, double pi_Nose, double H0);
    E_field_local real*8 (3, same shape).  NULL keeps the default (uniform
    species 1, the film/gap masks, no local field).  Species select their own
    on-site polynomial and masses; a local field switches the E-field term on.
-   Species or Z_starR values with a Z* other than Z_star(1) return
-   FG_ERR_UNSUPPORTED (per-site Z* in the dipole-dipole term is not built).
-   Call before stepping; the step graphs are rebuilt. */
+   Z*(R) is Z_starR when given, else Z_star of each site's species
+   (read_relaxor.F:35).  When it differs from Z_star(1) anywhere, Z*(R) u is
+   transformed on its own and the long-range dipole field acts on each site
+   times its Z* (dipoFFT.F:36-44, dVddi-dipole-dipole.F:38-60): three more
+   force components.  Call before stepping; the step graphs are rebuilt. */
 int  fg_upload_site_arrays(fg_ctx* ctx, const double* Z_starR, const double* mass_dipo_inv,
                            const double* mass_acou_inv, const int* relaxor, const int* sum_p,
                            const double* E_field_local);

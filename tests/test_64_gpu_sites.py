@@ -87,9 +87,85 @@ def test_site_arrays_force_and_nose_poincare_match_oracle(fg, prec):
     assert ru <= tol and abs(sg["s"] - so["s"]) <= tol, (ru, sg["s"], so["s"])
 
 
-def test_species_with_different_zstar_are_refused(fg):
-    p = helpers.params(L="8 8 8", **dict(TWO_SPECIES, Z_star="9.956 7.2 7.2"))
-    relaxor, _, _, _, _ = _sites(p, 6)
-    with fb.Context(p, A.FG_PREC_FP64) as ctx:
-        with pytest.raises(fb.FeramError, match="Z"):
-            ctx.upload_site_arrays(relaxor=relaxor)
+@pytest.mark.parametrize("prec", [A.FG_PREC_FP64, A.FG_PREC_MIXED])
+def test_species_with_different_zstar_match_oracle(fg, prec):
+    """Species with their own Z* (read_relaxor.F:35): the device derives
+    Z*(R) from the species and transforms Z* u on its own; short- and
+    long-range parts as dVddi-dipole-dipole.F:20-60, the field term with
+    Z*(R) (mirror_force_mirror.F:42-50)."""
+    p = helpers.params(L="8 8 8", kelvin="260", **dict(TWO_SPECIES, Z_star="9.956 7.2 7.2"))
+    relaxor, minv, sum_p, eloc, defects = _sites(p, 6)
+    zs = np.zeros(relaxor.shape)
+    zs[:, :p.Ly, :p.Lx] = np.array(p.Z_star[:3])[relaxor[:, :p.Ly, :p.Lx] - 1]
+    u, q = _state(p, 6, defects)
+    o = oracle_lib.Oracle(p)
+    o.set_sites(Z_starR=zs, relaxor=relaxor, mass_dipo_inv=minv, sum_p=sum_p, E_field_local=eloc)
+    o.set_uniform_E([0.0, 0.0005, 0.0])
+    o.set_state(u, q)
+    eo = o.force()
+    with fb.Context(p, prec) as ctx:
+        ctx.build_tables()
+        ctx.upload_site_arrays(relaxor=relaxor, mass_dipo_inv=minv, sum_p=sum_p, E_field_local=eloc)
+        ctx.set_uniform_E([0.0, 0.0005, 0.0])
+        ctx.set_state(u, q)
+        eg = ctx.mirror_force_mirror()
+        fmax, _ = helpers.force_error(ctx.get_state()["dVddi"], o.get_state()["dVddi"], p)
+        ee = helpers.energy_errors(eg, eo, A.POTENTIAL_FIELDS)
+        tol = 1e-11 if prec == A.FG_PREC_FP64 else 1e-5
+        assert fmax <= tol and max(ee.values()) <= tol, (fmax, ee)
+        # the long-range energy differs from the uniform-Z* value
+        o2 = oracle_lib.Oracle(p)
+        o2.set_state(u, q)
+        assert abs(o2.force().long_range - eo.long_range) > 1e-3 * abs(eo.long_range)
+        o.set_state(None, None, 1.0, 0.0, 0.0)
+        h = o.L.oracle_nose_poincare_hamiltonian(o.h, C.byref(eo))
+        o.set_state(None, None, 1.0, 0.0, h)
+        ctx.set_thermostat(1.0, 0.0, h)
+        for _ in range(5):
+            o.nose_poincare(eo)
+            ctx.nose_poincare(eg)
+        sg, so = ctx.get_state(), o.get_state()
+    ug, uo = A.physical(sg["dipoR"], p), A.physical(so["dipoR"], p)
+    ru = np.abs(ug - uo).max() / np.abs(uo).max()
+    tol = 1e-10 if prec == A.FG_PREC_FP64 else 2e-5
+    assert ru <= tol and abs(sg["s"] - so["s"]) <= tol, (ru, sg["s"], so["s"])
+
+
+@pytest.mark.parametrize("prec", [A.FG_PREC_FP64, A.FG_PREC_MIXED])
+def test_per_site_zstar_array_with_acoustic_leapfrog(fg, prec):
+    """An arbitrary Z*(R) array with acoustic-displacement leapfrog: fifteen
+    force components (u, u u, acouR, Z* u) through the transforms."""
+    p = helpers.params("zzzlf.feram", L="12 10 8", kelvin="200")
+    assert p.mass_acou[0] > 0.0
+    rng = np.random.default_rng(9)
+    shape = (p.Lz, p.Ly + p.padding_y, 2 * (p.Lx // 2 + 1))
+    zs = np.zeros(shape)
+    zs[:, :p.Ly, :p.Lx] = p.Z_star[0] * (1.0 + 0.2 * rng.standard_normal((p.Lz, p.Ly, p.Lx)))
+    u = helpers.seeded_u(p, 21, sigma=0.06, avg=0.05)
+    q = helpers.seeded_p(p, 21, sigma=0.01)
+    ar = helpers.seeded_u(p, 98, sigma=0.003)
+    ap = helpers.seeded_u(p, 99, sigma=0.004)
+    o = oracle_lib.Oracle(p)
+    o.set_sites(Z_starR=zs)
+    o.set_uniform_E([0.0004, 0.0, 0.0])
+    o.set_state(u, q)
+    o.set_acou(ar, ap)
+    eo = A.fg_energy()
+    with fb.Context(p, prec) as ctx:
+        ctx.build_tables()
+        ctx.upload_site_arrays(Z_starR=zs)
+        ctx.set_uniform_E([0.0004, 0.0, 0.0])
+        ctx.set_state(u, q)
+        ctx.set_acou(ar, ap)
+        eg = A.fg_energy()
+        for step in range(0, 6):
+            o.leapfrog(eo, step)
+            ctx.leapfrog(eg, step)
+        sg, so = ctx.get_state(), o.get_state()
+        ag, ao = ctx.get_acou(), o.get_acou()
+    tol = 1e-10 if prec == A.FG_PREC_FP64 else 2e-5
+    for a, b in ((sg["dipoR"], so["dipoR"]), (sg["dVddi"], so["dVddi"]), (ag["acouR"], ao["acouR"])):
+        a, b = A.physical(a, p), A.physical(b, p)
+        assert np.abs(a - b).max() / np.abs(b).max() <= tol
+    ee = helpers.energy_errors(eg, eo, A.POTENTIAL_FIELDS + ["dipo_kinetic", "acou_kinetic"])
+    assert max(ee.values()) <= tol, ee

@@ -111,12 +111,15 @@ def test_feram_run_coord_and_dipoRavg(fg, tmp_path):
     assert np.abs(ravg[:, 3:].reshape(p.Lz, p.Ly, p.Lx, 3) - uavg / n_av).max() <= 1e-6
 
 
-def test_feram_run_reads_relaxor_defects_localfield(fg, tmp_path):
+@pytest.mark.parametrize("zstar", ["9.956 9.956 9.956", "9.956 7.3 7.3"])
+def test_feram_run_reads_relaxor_defects_localfield(fg, tmp_path, zstar):
     """initialize_dipoR's read_relaxor and read_defects_u and
     initialize_E_field's .localfield through the host driver, against the
-    oracle given the same per-site arrays."""
+    oracle given the same per-site arrays; species with equal and with
+    different Z*."""
     text = helpers.deck("zzznp.feram", L="8 8 8", n_thermalize="4", n_average="6", verbose="1", kelvin="240",
-                        P_kappa2="5.502 4.61 4.61", P_alpha="110.4 98.2 98.2", mass_amu="39.0 47.5 47.5")
+                        P_kappa2="5.502 4.61 4.61", P_alpha="110.4 98.2 98.2", mass_amu="39.0 47.5 47.5",
+                        Z_star=zstar)
     (tmp_path / "run.feram").write_text(text)
     p = fg.params_from_text(text, "run")
     rng = np.random.default_rng(8)
@@ -136,6 +139,7 @@ def test_feram_run_reads_relaxor_defects_localfield(fg, tmp_path):
     sum_p[:, :p.Ly, :p.Lx] = 1
     for x, y, z, r in rel:
         relaxor[z, y, x] = r
+        zs[z, y, x] = p.Z_star[r - 1]
         minv[z, y, x] = 1.0 / p.mass_dipo[r - 1]
     eloc = A.real_field(p)
     for x, y, z, a, b, c in loc:
@@ -155,7 +159,7 @@ def test_feram_run_reads_relaxor_defects_localfield(fg, tmp_path):
     ao = A.fg_average()
     o.md(1, p.n_thermalize + p.n_average, 1, e, ao)
     assert avg.n_steps == ao.n_steps == 6
-    for f in ("total", "unharmonic", "dipole_E_field", "dipo_kinetic"):
+    for f in ("total", "unharmonic", "dipole_E_field", "dipo_kinetic", "long_range"):
         a, b = getattr(avg.energy, f), getattr(ao.energy, f)
         assert abs(a - b) <= 1e-9 * max(abs(b), 1.0), (f, a, b)
     assert avg.energy.dipole_E_field != 0.0
