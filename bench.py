@@ -198,9 +198,10 @@ def batched_sweep(n_rep=96, steps=200):
         t0 = time.perf_counter()
         b.step(steps)
         t_batch = time.perf_counter() - t0
-        # the same replicas, one after another
+        # the same replicas, one after another (warm-up captures both the
+        # eight-step and the one-step graph of fg_run_steps)
         for r in b.replicas:
-            r.run_steps(3)
+            r.run_steps(11)
         t0 = time.perf_counter()
         for r in b.replicas:
             r.run_steps(steps)

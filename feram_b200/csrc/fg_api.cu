@@ -158,6 +158,7 @@ struct fg_ctx {
   double* dipoRavg = nullptr;     // FP64 accumulator [3][nsite]
   std::vector<int> h_revx, h_revy, h_revz;
   cudaGraphExec_t g_np = nullptr, g_lf = nullptr, g_force = nullptr, g_vs = nullptr;
+  cudaGraphExec_t g_np_multi = nullptr;  // kNpGraphSteps Nose-Poincare steps
   bool tables_ready = false;
   bool force_fresh = false;
   bool np_ready = false;  // DevScalars' pending half step matches the state
@@ -398,8 +399,8 @@ int enqueue_pump(fg_ctx* ctx) {
 
 template <typename T>
 int enqueue_kick_drift(fg_ctx* ctx) {
-  k_kick_drift<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(
-      (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F, ctx->sc, ctx->g, ctx->layer_minv, (const T*)ctx->site_minv);
+  launch_dep(ctx, k_kick_drift<T>, ctx->grid_elem, kThreadsElem, 0, (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
+             ctx->sc, ctx->g, ctx->layer_minv, (const T*)ctx->site_minv);
   CKL();
   return FG_OK;
 }
@@ -422,17 +423,25 @@ int enqueue_kick_close(fg_ctx* ctx) {
 //   k_kick_close       block 0: energies, commit of the half step, (35e);
 //                      all: (35f) and the three kinetic sums; last block:
 //                      KE, H_NP of this step and the scalars of the next.
+//
+// Each kernel after the first starts while its predecessor drains
+// (programmatic dependent launch); follows_step: the step continues a graph
+// of several steps, and its first kernel does the same after the previous
+// step's closing kick.
 template <typename T>
-int enqueue_np(fg_ctx* ctx) {
-  int rc;
-  if ((rc = enqueue_kick_drift<T>(ctx))) return rc;
-  // the five kernels after the first start while their predecessor drains
-  ctx->pdl = !ctx->bulk_or_film_mirror();
-  rc = enqueue_force<T>(ctx, true);
+int enqueue_np(fg_ctx* ctx, bool follows_step = false) {
+  const bool pdl = !ctx->bulk_or_film_mirror();
+  ctx->pdl = pdl && follows_step;
+  int rc = enqueue_kick_drift<T>(ctx);
+  ctx->pdl = pdl;
+  if (!rc) rc = enqueue_force<T>(ctx, true);
   if (!rc) rc = enqueue_kick_close<T, false>(ctx);
   ctx->pdl = false;
   return rc;
 }
+
+// Steps per graph launch of fg_run_steps / fg_time_steps (Nose-Poincare).
+constexpr int kNpGraphSteps = 8;
 
 // leapfrog (leapfrog.F:103-151), i_step != 0
 template <typename T>
@@ -490,6 +499,13 @@ int run_graph(fg_ctx* ctx, cudaGraphExec_t* gx, int which) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_force<float>(ctx) : enqueue_force<double>(ctx); });
   } else if (which == 1) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_np<float>(ctx) : enqueue_np<double>(ctx); });
+  } else if (which == 4) {
+    rc = capture(ctx, gx, [&] {
+      int r = FG_OK;
+      for (int k = 0; k < kNpGraphSteps && r == FG_OK; ++k)
+        r = ctx->prec == FG_PREC_MIXED ? enqueue_np<float>(ctx, k > 0) : enqueue_np<double>(ctx, k > 0);
+      return r;
+    });
   } else if (which == 2) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_lf<float>(ctx) : enqueue_lf<double>(ctx); });
   } else {
@@ -1193,7 +1209,7 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
   }
   CK(cudaMemcpy(ctx->ph, &ctx->ph_host, sizeof(Phys), cudaMemcpyHostToDevice));
   // the step graphs hold the old table pointers as kernel arguments
-  for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
+  for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
     if (*gx) {
       cudaGraphExecDestroy(*gx);
       *gx = nullptr;
@@ -1339,6 +1355,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->g_np) cudaGraphExecDestroy(ctx->g_np);
+  if (ctx->g_np_multi) cudaGraphExecDestroy(ctx->g_np_multi);
   if (ctx->g_lf) cudaGraphExecDestroy(ctx->g_lf);
   if (ctx->g_vs) cudaGraphExecDestroy(ctx->g_vs);
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
@@ -1605,7 +1622,11 @@ int fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e) {
   if (ctx->P.method == FG_METHOD_MD && (rc = np_ready_for_step(ctx))) return rc;
   int which = 0;
   cudaGraphExec_t* gx = step_graph(ctx, &which);
-  for (int i = 0; i < n_steps; ++i)
+  int i = 0;
+  if (which == 1)
+    for (; i + kNpGraphSteps <= n_steps; i += kNpGraphSteps)
+      if ((rc = run_graph(ctx, &ctx->g_np_multi, 4))) return rc;
+  for (; i < n_steps; ++i)
     if ((rc = run_graph(ctx, gx, which))) return rc;
   ctx->force_fresh = true;
   ctx->np_ready = ctx->P.method == FG_METHOD_MD;
@@ -1619,11 +1640,17 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
   if (rc) return rc;
   if (!ms || n_steps < 1) return FG_ERR_ARG;
   if (ctx->P.method == FG_METHOD_MD && (rc = np_ready_for_step(ctx))) return rc;
-  // make sure the graph exists before the timed region
+  // make sure the graphs exist before the timed region
   int which = 0;
   cudaGraphExec_t* gx = step_graph(ctx, &which);
-  if (!*gx) {
+  const int nmulti = which == 1 ? n_steps / kNpGraphSteps : 0;
+  const int nsingle = n_steps - nmulti * kNpGraphSteps;
+  if (nsingle > 0 && !*gx) {
     if ((rc = run_graph(ctx, gx, which))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  if (nmulti > 0 && !ctx->g_np_multi) {
+    if ((rc = run_graph(ctx, &ctx->g_np_multi, 4))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
   }
   cudaEvent_t e0, e1;
@@ -1631,7 +1658,8 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
   CK(cudaEventCreate(&e1));
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaEventRecord(e0, ctx->stream));
-  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(*gx, ctx->stream));
+  for (int i = 0; i < nmulti; ++i) CK(cudaGraphLaunch(ctx->g_np_multi, ctx->stream));
+  for (int i = 0; i < nsingle; ++i) CK(cudaGraphLaunch(*gx, ctx->stream));
   CK(cudaEventRecord(e1, ctx->stream));
   CK(cudaEventSynchronize(e1));
   float t = 0.0f;

@@ -282,8 +282,9 @@ int  fg_dipoRavg_accumulate(fg_ctx* ctx);
 int  fg_get_dipoRavg(fg_ctx* ctx, double* dipoRavg);
 
 /* Run n_steps of the method of p (md, lf with i_step != 0, or vs) on the
-   device as one CUDA graph per step; the energies of the last step are
-   returned in e. */
+   device as CUDA graphs (md: eight steps per graph launch while eight
+   remain, then one per step); the energies of the last step are returned
+   in e. */
 int  fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e);
 
 /* ---- replica batches -------------------------------------------------------
@@ -310,7 +311,8 @@ int  fg_batch_step(fg_batch* b, int n_steps, fg_energy* e);
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */
 #define FG_NPROF 6
-/* Time n_steps graph launches of the MD step of p's method; *ms = total. */
+/* Time n_steps steps of p's method launched as fg_run_steps launches them;
+   *ms = total. */
 int  fg_time_steps(fg_ctx* ctx, int n_steps, double* ms);
 /* One bulk Nose-Poincare step launched kernel by kernel (the same kernels as
    the step's graph) with an event between kernels, averaged over reps steps;
