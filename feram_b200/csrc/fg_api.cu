@@ -801,10 +801,12 @@ int create_impl(fg_ctx* ctx) {
     h.dt = P.dt;
     h.dt_2 = P.dt_2;
     h.Q = P.Q_Nose;
+    h.Qinv = 1.0 / P.Q_Nose;
     h.nf_kT = (double)P.n_freedom * P.temperature_eV;
     h.threeN_kT = (double)(3 * (long long)P.N) * P.temperature_eV;
     h.target_ke = P.target_kinetic_energy;
     h.n_sum_p = ctx->n_sum_p;
+    h.ke_scale = (double)P.N / (2.0 * ctx->n_sum_p);
     h.E_on = P.E_field_always_zero ? 0 : 1;
     h.modulation_on = 0;
     CK(cudaMalloc(&ctx->ph, sizeof(Phys)));
@@ -1199,6 +1201,7 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
     if ((rc = replace((void**)&ctx->layer_nsum, nl))) return rc;
     ctx->n_sum_p = n;
     ctx->ph_host.n_sum_p = n;
+    ctx->ph_host.ke_scale = (double)P.N / (2.0 * n);
   }
   if (Eloc) {
     std::vector<T> v(3 * ns);

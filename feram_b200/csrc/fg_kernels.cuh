@@ -51,6 +51,8 @@ struct Phys {
   int bulk_or_film;
   double Zstar;
   double dt, dt_2, Q, nf_kT, threeN_kT;
+  double Qinv;       // 1 / Q
+  double ke_scale;   // N / (2 n_sum_p): kinetic energy per masked sum p^2/m
   double target_ke;  // target_kinetic_energy (param_module.F:468), velocity scaling
   // per-species on-site constants for .relaxor runs (dVddi-unharmonic.F:
   // 28-32,40,73): force combinations, energy coefficients, kappa2(s)-kappa2(1)
@@ -554,11 +556,15 @@ __device__ __forceinline__ double sum_potential(const double* e) {
   return e[E_SHORT] + e[E_LONG] + e[E_DIPE] + e[E_UNH] + e[E_HS] + e[E_HC] + e[E_IS] + e[E_IC] + e[E_IM];
 }
 
-__device__ __forceinline__ void np_hamiltonian(const Phys* ph, DevScalars* sc) {  // energy_module.F:128-148
+// energy_module.F:128-148 with 1/s^2 and log(s) of the current s given
+__device__ __forceinline__ void np_hamiltonian(const Phys* ph, DevScalars* sc, double inv_s2, double log_s) {
   double* e = sc->e;
-  const double s = sc->s;
-  double h = e[E_DIPO] / (s * s) + sum_potential(e) + sc->pi * sc->pi / 2 / ph->Q + ph->threeN_kT * log(s) - sc->H0;
-  e[E_HNP] = h * s;
+  double h = e[E_DIPO] * inv_s2 + sum_potential(e) + sc->pi * sc->pi * 0.5 * ph->Qinv + ph->threeN_kT * log_s - sc->H0;
+  e[E_HNP] = h * sc->s;
+}
+__device__ __forceinline__ void np_hamiltonian(const Phys* ph, DevScalars* sc) {
+  const double inv_s = 1.0 / sc->s;
+  np_hamiltonian(ph, sc, inv_s * inv_s, log(sc->s));
 }
 
 __device__ __forceinline__ void check_finite(DevScalars* sc, const double* v, int n) {
@@ -640,15 +646,15 @@ __device__ __noinline__ void homo_strain_tail(const Phys* __restrict__ ph, DevSc
 }
 
 // kinetic_energy_dipo.F:106 from the kick partials
-__device__ __forceinline__ double ke_from(const Phys* ph, double sum) { return sum / ph->n_sum_p * ph->N / 2; }
+__device__ __forceinline__ double ke_from(const Phys* ph, double sum) { return sum * ph->ke_scale; }
 
 // Nose-Poincare after the force (nose-poincare.F:60-66): H_NP, (35e).
 // Thread 0 only.
 __device__ void np_post_body(const Phys* __restrict__ ph, DevScalars* sc) {
-  np_hamiltonian(ph, sc);
-  const double s = sc->s;
-  const double delta_H = sc->e[E_HNP] / s;
-  sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] / (s * s) - ph->nf_kT) - ph->dt_2 * delta_H;
+  const double inv_s = 1.0 / sc->s, inv_s2 = inv_s * inv_s;
+  np_hamiltonian(ph, sc, inv_s2, log(sc->s));
+  const double delta_H = sc->e[E_HNP] * inv_s;
+  sc->pi = sc->pi + ph->dt_2 * (2 * sc->e[E_DIPO] * inv_s2 - ph->nf_kT) - ph->dt_2 * delta_H;
 }
 
 // After k_assemble: real-space energies.  With np_close also the commit of
@@ -688,28 +694,33 @@ __device__ __noinline__ void np_close_tail(const Phys* __restrict__ ph, DevScala
   double v[3];
   reduce_partials_all<3>(part, nblk, v);
   scalar_tail(ph, sc, [&](const Phys* P, DevScalars* S) {
+    // one thread's serial FP64 chain: one log, four divisions, one sqrt
+    const double s = S->s;
+    const double inv_s = 1.0 / s, inv_s2 = inv_s * inv_s, log_s = log(s);
+    const double epot = sum_potential(S->e);
     if (step_done) {
       S->ke_sum = v[0];
       S->e[E_DIPO] = ke_from(P, v[0]);
-      np_hamiltonian(P, S);
-      S->e[E_TOT] = S->e[E_DIPO] / (S->s * S->s) + S->e[E_ACOU] + sum_potential(S->e);
+      np_hamiltonian(P, S, inv_s2, log_s);
+      S->e[E_TOT] = S->e[E_DIPO] * inv_s2 + S->e[E_ACOU] + epot;
       check_finite(S, S->e, E_COUNT);
     }
-    const double s = S->s;
     const double ca = P->dt_2 * s;
     const double kh = v[0] - 2 * ca * v[1] + ca * ca * v[2];
     const double ke = ke_from(P, kh);
-    double CB = P->nf_kT * (1.0 + log(s)) - ke / (s * s) + sum_potential(S->e) - S->H0;
+    double CB = P->nf_kT * (1.0 + log_s) - ke * inv_s2 + epot - S->H0;
     CB = P->dt_2 * CB - S->pi;
-    if (1.0 - CB * P->dt / P->Q < 0.0) S->status = 10;  // (38) has no real root: Q_Nose too small
-    const double pih = -2 * CB / (1.0 + sqrt(1.0 - CB * P->dt / P->Q));
-    const double sn = s * (1.0 + P->dt_2 * pih / P->Q) / (1.0 - P->dt_2 * pih / P->Q);
+    const double r = CB * P->dt * P->Qinv;
+    if (1.0 - r < 0.0) S->status = 10;  // (38) has no real root: Q_Nose too small
+    const double pih = -2 * CB / (1.0 + sqrt(1.0 - r));
+    const double a = P->dt_2 * pih * P->Qinv;
+    const double sn = s * (1.0 + a) / (1.0 - a);
     S->kick_coef = ca;
     S->pend_ke_sum = kh;
     S->pend_ke = ke;
     S->pend_pi = pih;
     S->pend_s = sn;
-    S->pend_drift = P->dt_2 * (1 / sn + 1 / s);
+    S->pend_drift = P->dt_2 * (1.0 / sn + inv_s);
     S->pend_kick_f = P->dt_2 * sn;
   });
 }
