@@ -92,6 +92,9 @@ struct fg_ctx {
   ZTiles zt{}, zt6{}, zt1{};  // z tiles: MD k-space (9 comps, T), table build (6, FP64), modulation (1, FP64)
   int smem_xy = 0, smem_xy64 = 0, smem_z = 0, smem_z3 = 0, smem_z6 = 0, smem_z1 = 0;
   int grid_elem = 1;
+  // one resident wave of the step's streaming kernels (grid-stride loops):
+  // k_kick_drift, k_kick_close, k_assemble; <= grid_elem
+  int grid_kd = 1, grid_kc = 1, grid_as = 1;
   cudaStream_t stream = nullptr;
   // fields (T = float or double)
   void* u = nullptr;
@@ -333,7 +336,7 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
   // np_post: the energies and (35e) are finished by the closing kick's block 0
-  launch_dep(ctx, k_assemble<T>, ctx->grid_elem, kThreadsElem, 0,
+  launch_dep(ctx, k_assemble<T>, ctx->grid_as, kThreadsElem, 0,
       (const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc, ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
       ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
       ctx->zsite ? zu_comp(ctx) : 0);
@@ -399,7 +402,7 @@ int enqueue_pump(fg_ctx* ctx) {
 
 template <typename T>
 int enqueue_kick_drift(fg_ctx* ctx) {
-  launch_dep(ctx, k_kick_drift<T>, ctx->grid_elem, kThreadsElem, 0, (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
+  launch_dep(ctx, k_kick_drift<T>, ctx->grid_kd, kThreadsElem, 0, (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
              ctx->sc, ctx->g, ctx->layer_minv, (const T*)ctx->site_minv);
   CKL();
   return FG_OK;
@@ -408,9 +411,9 @@ int enqueue_kick_drift(fg_ctx* ctx) {
 // prep: sums of the current state only (np_prepare)
 template <typename T, bool PREP>
 int enqueue_kick_close(fg_ctx* ctx) {
-  launch_dep(ctx, k_kick_close<T, PREP>, ctx->grid_elem, kThreadsElem, 0,
+  launch_dep(ctx, k_kick_close<T, PREP>, ctx->grid_kc, kThreadsElem, 0,
       (T*)ctx->p, (const T*)ctx->F, ctx->g, ctx->layer_minv, ctx->layer_sump, ctx->part_ke, ctx->done, ctx->ph,
-      ctx->sc, ctx->part_r, ctx->grid_elem, (const T*)ctx->site_minv, ctx->site_sump);
+      ctx->sc, ctx->part_r, ctx->grid_as, (const T*)ctx->site_minv, ctx->site_sump);
   CKL();
   return FG_OK;
 }
@@ -643,6 +646,16 @@ int create_impl(fg_ctx* ctx) {
   ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->zt6.CW * sizeof(cplx<double>));
   ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->zt1.CW * sizeof(cplx<double>));
   ctx->grid_elem = std::max(1, std::min(div_up(g.nsite, kThreadsElem), nsm * 8));
+  {
+    auto wave = [&](auto kern) {
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kThreadsElem, 0) != cudaSuccess || nb < 1) nb = 8;
+      return std::max(1, std::min(ctx->grid_elem, nb * nsm));
+    };
+    ctx->grid_kd = wave(k_kick_drift<T>);
+    ctx->grid_kc = std::min(wave(k_kick_close<T, false>), wave(k_kick_close<T, true>));
+    ctx->grid_as = wave(k_assemble<T>);
+  }
   {
     // The dynamic shared-memory cap is an attribute of the kernel, shared by
     // every context in the process: raise it to what the device allows next
@@ -1308,7 +1321,7 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     CK(cudaEventRecord(ev[++k], st));
     rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true);
     CK(cudaEventRecord(ev[++k], st));
-    k_assemble<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>(
+    k_assemble<T><<<ctx->grid_as, kThreadsElem, 0, st>>>(
         (const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, TAIL_NONE, ctx->done + 2,
         ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E, ctx->zsite ? zu_comp(ctx) : 0);
     CK(cudaEventRecord(ev[++k], st));
