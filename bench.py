@@ -83,6 +83,43 @@ def initial_state(p):
     return u, q
 
 
+ENERGY_TERMS = ("short_range", "long_range", "dipole_E_field", "unharmonic", "homo_strain", "homo_coupling",
+                "inho_strain", "inho_coupling")
+
+
+def force_errors_16(ctxm, ctx64, p, sigma=0.1):
+    """Mixed against FP64 force and energies on 16 fixed configurations,
+    u ~ N(0, sigma) per component from uni64 seeds (s, 987654321), s = 1..16;
+    the FP64 path matches the oracle to 1e-11.  Force errors: rms |dF| / rms
+    |F| (the relative L2 norm), max |dF| / max |F| (relative max norm) and
+    max |dF| / rms |F| (the worst site against the typical force); energy
+    error per term over the sum of the terms' magnitudes."""
+    from feram_b200 import _capi as A
+    worst = {"max": 0.0, "rms": 0.0, "maxnorm": 0.0, "energy": 0.0}
+    for s in range(1, 17):
+        q = A.fg_params.from_buffer_copy(p)
+        q.seed[0], q.seed[1] = s, 987654321
+        for a in range(3):
+            q.init_dipo_avg[a], q.init_dipo_dev[a], q.k_stripe[a] = 0.0, sigma, 0.0
+        u = A.real_field(p)
+        assert A.lib().fg_init_dipoR_host(C.byref(q), A.dptr(u), None) == 0
+        es, fs = [], []
+        for ctx in (ctx64, ctxm):
+            ctx.set_state(u)
+            es.append(ctx.mirror_force_mirror())
+            fs.append(A.physical(ctx.get_state()["dVddi"], p))
+        d = np.sqrt(np.sum((fs[1] - fs[0]) ** 2, axis=-1))
+        rms = float(np.sqrt(np.mean(np.sum(fs[0] ** 2, axis=-1))))
+        scale = sum(abs(getattr(es[0], t)) for t in ENERGY_TERMS)
+        worst["max"] = max(worst["max"], float(d.max()) / rms)
+        worst["maxnorm"] = max(worst["maxnorm"], float(d.max()) / float(np.sqrt(np.sum(fs[0] ** 2, axis=-1)).max()))
+        worst["rms"] = max(worst["rms"], float(np.sqrt(np.mean(d ** 2))) / rms)
+        worst["energy"] = max(worst["energy"],
+                              max(abs(getattr(es[1], t) - getattr(es[0], t)) for t in ENERGY_TERMS) / scale)
+    return {"configs": 16, "sigma": sigma, "seeds": "uni64 (1..16, 987654321)", "force_rms": worst["rms"],
+            "force_maxnorm": worst["maxnorm"], "force_max_site_over_rms": worst["max"], "energy_max": worst["energy"]}
+
+
 def prepare(ctx, p, u, q):
     """initialize_dipoR's tail and molecular-dynamics.F:209-212 (H0)."""
     ctx.set_state(u, q, 1.0, 0.0, 0.0)
@@ -331,7 +368,7 @@ def main():
     ctxm = fb.Context(p, A.FG_PREC_MIXED)
     ctxm.build_tables()
     H0 = prepare(ctxm, p, u, q)
-    ctx64, ferr = None, None
+    ctx64, ferr, ferr16 = None, None, None
     if not args.mixed_only:
         # force error of the mixed path against the FP64 path on the same state
         ctx64 = fb.Context(p, A.FG_PREC_FP64)
@@ -342,7 +379,12 @@ def main():
         d = A.physical(fmx, p) - A.physical(f64, p)
         rms = float(np.sqrt(np.mean(np.sum(A.physical(f64, p) ** 2, axis=-1))))
         dn = np.sqrt(np.sum(d ** 2, axis=-1))
-        ferr = {"max": float(dn.max() / rms), "rms": float(np.sqrt(np.mean(dn ** 2)) / rms)}
+        fmaxn = float(np.sqrt(np.sum(A.physical(f64, p) ** 2, axis=-1)).max())
+        ferr = {"rms": float(np.sqrt(np.mean(dn ** 2)) / rms), "maxnorm": float(dn.max()) / fmaxn,
+                "max_site_over_rms": float(dn.max() / rms)}
+        ferr16 = force_errors_16(ctxm, ctx64, p)
+        prepare(ctxm, p, u, q)
+        prepare(ctx64, p, u, q)
 
     def timed(ctx, steps, warmup, sample_clocks):
         ms = C.c_double()
@@ -447,6 +489,7 @@ def main():
         "fp64": {"value": value64, "ms_per_step": (ms_fp64 / steps64) if ms_fp64 else None, "steps": steps64},
         "mixed_over_fp64": (value / value64) if value64 else None,
         "force_err_mixed_vs_fp64": ferr,
+        "force_err_16_configs": ferr16,
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "batched": batched,
         "gpu_launches": A.FG_NPROF * args.steps,  # kernels per bulk NP step graph
