@@ -860,6 +860,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     fft_forward<T>(buf, B, pz, twz, buf_len);
   }
   const double Ninv = ph->Ninv;
+  // Energy sums: the per-k products in T (FP32 in the mixed path, whose
+  // spectra are FP32), accumulated per thread in FP64
   double acc[NQ_K] = {0, 0, 0, 0, 0};
   // this thread's pencil (fixed cw), decoded once
   const int cw = cwp, col = colp, yslot = ysp;
@@ -870,10 +872,30 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   const double2 ty = __ldg(&km.try_[ky]);
   const double2 tx = __ldg(&km.trx[kx]);
   const double kv1 = __ldg(&km.kvx[kx]);
+  // S(k) of short_range_k along this pencil: with c = cos, s = sin of the
+  // x, y and z phases, S_aa = A_a + B_a cz, S_yz = C_3 sz, S_zx = C_4 sz,
+  // S_xy = A_5 + B_5 cz (the x-y parts fixed per pencil, FP64)
+  double sA[6], sB[6];
+  {
+    const double* j = ph->j;
+    const double kap = ph->kap2x2, c0 = tx.x, c1 = ty.x, s0 = tx.y, s1 = ty.y;
+    sA[0] = kap + 2 * j[1] * c0 + 2 * j[0] * c1 + 4 * j[2] * c0 * c1;
+    sB[0] = 2 * j[0] + 4 * j[3] * c1 + 4 * j[2] * c0 + 8 * j[5] * c0 * c1;
+    sA[1] = kap + 2 * j[1] * c1 + 2 * j[0] * c0 + 4 * j[2] * c1 * c0;
+    sB[1] = 2 * j[0] + 4 * j[3] * c0 + 4 * j[2] * c1 + 8 * j[5] * c0 * c1;
+    sA[2] = kap + 2 * j[0] * (c0 + c1) + 4 * j[3] * c0 * c1;
+    sB[2] = 2 * j[1] + 4 * j[2] * (c0 + c1) + 8 * j[5] * c0 * c1;
+    sA[3] = 0.0;
+    sB[3] = -4 * j[4] * s1 - 8 * j[6] * s1 * c0;  // times sz
+    sA[4] = 0.0;
+    sB[4] = -4 * j[4] * s0 - 8 * j[6] * s0 * c1;  // times sz
+    sA[5] = -4 * j[4] * s0 * s1;
+    sB[5] = -8 * j[6] * s0 * s1;
+  }
+  const T w1 = (kx == 0 || kx == g.m) ? (T)1 : (T)2;  // full-spectrum multiplicity
   const long long tpos0 = (long long)yslot * Lz * g.KXP + col;
   for (int zs = threadIdx.x / CW; pencil_ok && zs < Lz; zs += blockDim.x / CW) {
     const int kz = __ldg(&km.revz[zs]);
-    const double w1 = (kx == 0 || kx == g.m) ? 1.0 : 2.0;  // full-spectrum multiplicity
     cplx<T> u[3], d[6];
 #pragma unroll
     for (int a = 0; a < 3; ++a) u[a] = buf[a * ZS + zs * CW + cw];
@@ -895,19 +917,28 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       D[2 * q] = v.x;
       D[2 * q + 1] = v.y;
     }
-    double qv[6];  // Re(conj(u_a) u_b): xx, yy, zz, yz, zx, xy
-    qv[0] = (double)u[0].x * u[0].x + (double)u[0].y * u[0].y;
-    qv[1] = (double)u[1].x * u[1].x + (double)u[1].y * u[1].y;
-    qv[2] = (double)u[2].x * u[2].x + (double)u[2].y * u[2].y;
-    qv[3] = (double)u[1].x * u[2].x + (double)u[1].y * u[2].y;
-    qv[4] = (double)u[2].x * u[0].x + (double)u[2].y * u[0].y;
-    qv[5] = (double)u[0].x * u[1].x + (double)u[0].y * u[1].y;
+    T qv[6];  // Re(conj(u_a) u_b): xx, yy, zz, yz, zx, xy
+    qv[0] = u[0].x * u[0].x + u[0].y * u[0].y;
+    qv[1] = u[1].x * u[1].x + u[1].y * u[1].y;
+    qv[2] = u[2].x * u[2].x + u[2].y * u[2].y;
+    qv[3] = u[1].x * u[2].x + u[1].y * u[2].y;
+    qv[4] = u[2].x * u[0].x + u[2].y * u[0].y;
+    qv[5] = u[0].x * u[1].x + u[0].y * u[1].y;
     {
+      // short- and total dipole energies in FP64 from the same qv, so that
+      // their difference (the long-range energy) keeps its digits
       const double2 tz = __ldg(&km.trz[kz]);
-      const double cc[3] = {tx.x, ty.x, tz.x}, ss[3] = {tx.y, ty.y, tz.y};
       double S[6];
-      short_range_k(ph->j, ph->kap2x2, cc, ss, S);
-      const double es = w1 * (S[0] * qv[0] + S[1] * qv[1] + S[2] * qv[2] + 2.0 * (S[3] * qv[3] + S[4] * qv[4] + S[5] * qv[5]));
+      S[0] = sA[0] + sB[0] * tz.x;
+      S[1] = sA[1] + sB[1] * tz.x;
+      S[2] = sA[2] + sB[2] * tz.x;
+      S[3] = sB[3] * tz.y;
+      S[4] = sB[4] * tz.y;
+      S[5] = sA[5] + sB[5] * tz.x;
+      double qd[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) qd[q] = (double)qv[q];
+      const double es = (double)w1 * (S[0] * qd[0] + S[1] * qd[1] + S[2] * qd[2] + 2.0 * (S[3] * qd[3] + S[4] * qd[4] + S[5] * qd[5]));
       acc[0] += es;
       if constexpr (ZSC) {
         // short range on uK, long range on FFT(Z* u): Fl = (L/N) ZuK,
@@ -915,15 +946,15 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         cplx<T> zu[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) zu[a] = buf[(Z0 + a) * ZS + zs * CW + cw];
-        double qz[6];
-        qz[0] = (double)zu[0].x * zu[0].x + (double)zu[0].y * zu[0].y;
-        qz[1] = (double)zu[1].x * zu[1].x + (double)zu[1].y * zu[1].y;
-        qz[2] = (double)zu[2].x * zu[2].x + (double)zu[2].y * zu[2].y;
-        qz[3] = (double)zu[1].x * zu[2].x + (double)zu[1].y * zu[2].y;
-        qz[4] = (double)zu[2].x * zu[0].x + (double)zu[2].y * zu[0].y;
-        qz[5] = (double)zu[0].x * zu[1].x + (double)zu[0].y * zu[1].y;
-        acc[1] += es * Ninv + w1 * ((double)D[0] * qz[0] + (double)D[1] * qz[1] + (double)D[2] * qz[2] +
-                                    2.0 * ((double)D[3] * qz[3] + (double)D[4] * qz[4] + (double)D[5] * qz[5]));
+        T qz[6];
+        qz[0] = zu[0].x * zu[0].x + zu[0].y * zu[0].y;
+        qz[1] = zu[1].x * zu[1].x + zu[1].y * zu[1].y;
+        qz[2] = zu[2].x * zu[2].x + zu[2].y * zu[2].y;
+        qz[3] = zu[1].x * zu[2].x + zu[1].y * zu[2].y;
+        qz[4] = zu[2].x * zu[0].x + zu[2].y * zu[0].y;
+        qz[5] = zu[0].x * zu[1].x + zu[0].y * zu[1].y;
+        acc[1] += es * Ninv + (double)w1 * ((double)D[0] * qz[0] + (double)D[1] * qz[1] + (double)D[2] * qz[2] +
+                                            2.0 * ((double)D[3] * qz[3] + (double)D[4] * qz[4] + (double)D[5] * qz[5]));
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
           const int b = (a + 1) % 3, c3 = (a + 2) % 3;  // off-diagonal slots: yz 3, zx 4, xy 5
@@ -934,8 +965,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 #pragma unroll
         for (int q = 0; q < 6; ++q) D[q] = (T)(S[q] * Ninv);
       } else {
-        acc[1] += w1 * ((double)D[0] * qv[0] + (double)D[1] * qv[1] + (double)D[2] * qv[2] +
-                        2.0 * ((double)D[3] * qv[3] + (double)D[4] * qv[4] + (double)D[5] * qv[5]));
+        acc[1] += (double)w1 * ((double)D[0] * qd[0] + (double)D[1] * qd[1] + (double)D[2] * qd[2] +
+                                2.0 * ((double)D[3] * qd[3] + (double)D[4] * qd[4] + (double)D[5] * qd[5]));
       }
     }
     cplx<T> F[3];
@@ -995,17 +1026,17 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       for (int a = 0; a < 3; ++a)
         KA[a] = mk<cplx<T>>(K[a][0] * acou[0].x + K[a][1] * acou[1].x + K[a][2] * acou[2].x,
                             K[a][0] * acou[0].y + K[a][1] * acou[1].y + K[a][2] * acou[2].y);
-      const double w2 = 0.5 * w1;
-      double es = 0.0, ec = 0.0, em = 0.0;
+      const T w2 = (T)0.5 * w1;
+      T es = 0, ec = 0, em = 0;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        es += (double)acou[a].x * KA[a].x + (double)acou[a].y * KA[a].y;
-        ec += (double)acou[a].x * cs[a].x + (double)acou[a].y * cs[a].y;
-        em += (double)acou[a].x * ck[a].x + (double)acou[a].y * ck[a].y;
+        es += acou[a].x * KA[a].x + acou[a].y * KA[a].y;
+        ec += acou[a].x * cs[a].x + acou[a].y * cs[a].y;
+        em += acou[a].x * ck[a].x + acou[a].y * ck[a].y;
       }
-      acc[2] += w2 * es;
-      acc[3] += w2 * ec;
-      acc[4] += w2 * em;
+      acc[2] += (double)(w2 * es);
+      acc[3] += (double)(w2 * ec);
+      acc[4] += (double)(w2 * em);
       const T ni = (T)Ninv;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
@@ -1034,16 +1065,16 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       // coupling Re(acou* . coup2 didiK), modulation Re(acou* . c_k); the
       // strain energy Re(acou* K acou) = -(coupling + modulation) because
       // K acou = -(c_k + coup2 didiK)
-      const double w2 = 0.5 * w1;  // energy_module.F weights: 1/2 at kx = 0, Lx/2
-      double ec = 0.0, em = 0.0;
+      const T w2 = (T)0.5 * w1;  // energy_module.F weights: 1/2 at kx = 0, Lx/2
+      T ec = 0, em = 0;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        ec += (double)acou[a].x * cs[a].x + (double)acou[a].y * cs[a].y;
-        em += (double)acou[a].x * ck[a].x + (double)acou[a].y * ck[a].y;
+        ec += acou[a].x * cs[a].x + acou[a].y * cs[a].y;
+        em += acou[a].x * ck[a].x + acou[a].y * ck[a].y;
       }
-      acc[2] -= w2 * (ec + em);
-      acc[3] += w2 * ec;
-      acc[4] += w2 * em;
+      acc[2] -= (double)(w2 * (ec + em));
+      acc[3] += (double)(w2 * ec);
+      acc[4] += (double)(w2 * em);
     }
     if (acouK_out) {
 #pragma unroll
@@ -1105,11 +1136,12 @@ struct AsmConst {
   T hx, hy, h4;                   // homogeneous_coupling_2: B1xx/2, B1yy/2, B4yz
   T wh[6];                        // strain . B2
   T Zs, E0, E1, E2;
-  double Pa, Pg, P1, P2, P3, P4;
+  T Pa, Pg, P1, P2, P3, P4;       // energy coefficients (dVddi-unharmonic.F:67-99)
   int E_on;
 };
 
-// Force on one site from F_dd, u and eta (see k_assemble); acc += energies.
+// Force on one site from F_dd, u and eta (see k_assemble); acc += energies
+// (the site's terms in T, FP32 in the mixed path, summed in FP64).
 template <typename T>
 __device__ __forceinline__ void assemble_site(const AsmConst<T>& k, T ux, T uy, T uz, T f0, T f1, T f2,
                                               const T* eta, T& o0, T& o1, T& o2, double* acc) {
@@ -1124,17 +1156,14 @@ __device__ __forceinline__ void assemble_site(const AsmConst<T>& k, T ux, T uy, 
   f0 = f0 + ux * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d0 * d0) - k.fk * d1 * d2);
   f1 = f1 + uy * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d1 * d1) - k.fk * d2 * d0);
   f2 = f2 + uz * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d2 * d2) - k.fk * d0 * d1);
-  {
-    const double D0 = d0, D1 = d1, D2 = d2, U = uu;
-    acc[0] += k.Pa * (U * U) + k.Pg * (D0 * D1 + D1 * D2 + D2 * D0) + k.P1 * (U * U * U) +
-              k.P2 * ((D0 * D0) * (D1 + D2) + (D1 * D1) * (D2 + D0) + (D2 * D2) * (D0 + D1)) + k.P3 * D0 * D1 * D2 +
-              k.P4 * (U * U * U * U);
-  }
+  acc[0] += (double)(k.Pa * uu2 + k.Pg * (d0 * d1 + d1 * d2 + d2 * d0) + k.P1 * uu3 +
+                     k.P2 * ((d0 * d0) * (d1 + d2) + (d1 * d1) * (d2 + d0) + (d2 * d2) * (d0 + d1)) +
+                     k.P3 * d0 * d1 * d2 + k.P4 * (uu2 * uu2));
   if (k.E_on) {
     f0 = f0 - k.Zs * k.E0;
     f1 = f1 - k.Zs * k.E1;
     f2 = f2 - k.Zs * k.E2;
-    acc[1] += (double)k.Zs * ((double)ux * k.E0 + (double)uy * k.E1 + (double)uz * k.E2);
+    acc[1] += (double)(k.Zs * (ux * k.E0 + uy * k.E1 + uz * k.E2));
   }
   // homogeneous strain coupling
   f0 = f0 + 2 * k.wh[0] * ux + k.wh[4] * uz + k.wh[5] * uy;
@@ -1152,7 +1181,7 @@ __device__ __forceinline__ void assemble_site(const AsmConst<T>& k, T ux, T uy, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
                                                   T* __restrict__ F, Geom g, const Phys* __restrict__ ph,
                                                   DevScalars* sc, double* __restrict__ part, int tail,
                                                   unsigned int* done,
@@ -1172,7 +1201,8 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
 #pragma unroll
   for (int i = 0; i < 6; ++i) k.wh[i] = (T)sc->w_hom[i];
   k.Zs = (T)ph->Zstar; k.E0 = (T)sc->E[0]; k.E1 = (T)sc->E[1]; k.E2 = (T)sc->E[2];
-  k.Pa = ph->P_alpha; k.Pg = ph->P_gamma; k.P1 = ph->P_k1; k.P2 = ph->P_k2; k.P3 = ph->P_k3; k.P4 = ph->P_k4;
+  k.Pa = (T)ph->P_alpha; k.Pg = (T)ph->P_gamma; k.P1 = (T)ph->P_k1; k.P2 = (T)ph->P_k2; k.P3 = (T)ph->P_k3;
+  k.P4 = (T)ph->P_k4;
   k.E_on = ph->E_on;
   double acc[NQ_R] = {0.0, 0.0};
   constexpr int NV = V16<T>::n;
@@ -1185,7 +1215,7 @@ __global__ void __launch_bounds__(256) k_assemble(const T* __restrict__ rw, cons
       if (site_species) {
         const Phys::Species& q = ph->sp[site_species[i]];
         ks.fa2g = (T)q.fa2g; ks.tg = (T)q.tg; ks.sk = (T)q.sk; ks.tk2 = (T)q.tk2; ks.fk = (T)q.fk; ks.k4x8 = (T)q.k4x8;
-        ks.Pa = q.Pa; ks.Pg = q.Pg; ks.P1 = q.P1; ks.P2 = q.P2; ks.P3 = q.P3; ks.P4 = q.P4;
+        ks.Pa = (T)q.Pa; ks.Pg = (T)q.Pg; ks.P1 = (T)q.P1; ks.P2 = (T)q.P2; ks.P3 = (T)q.P3; ks.P4 = (T)q.P4;
         dk2 = q.dk2;
       }
       if (site_zstar) ks.Zs = site_zstar[i];
@@ -1448,7 +1478,8 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
       const int z = (int)(i / g.plane_r);
-      double pp = 0.0, pf = 0.0, ff = 0.0;
+      // the vector's 3 NV products summed in T, then accumulated in FP64
+      T pp = 0, pf = 0, ff = 0;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         V16<T> q = ldv(p + a * ns + i);
@@ -1456,17 +1487,17 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
           if (!PREP) q.v[l] = q.v[l] - c * y.v[l];
-          pp += (double)q.v[l] * q.v[l];
-          pf += (double)q.v[l] * y.v[l];
-          ff += (double)y.v[l] * y.v[l];
+          pp += q.v[l] * q.v[l];
+          pf += q.v[l] * y.v[l];
+          ff += y.v[l] * y.v[l];
         }
         if (!PREP) stv(p + a * ns + i, q);
       }
       if (layer_sump[z]) {
         const double mi = layer_minv[z];
-        acc[0] += pp * mi;
-        acc[1] += pf * mi;
-        acc[2] += ff * mi;
+        acc[0] += (double)pp * mi;
+        acc[1] += (double)pf * mi;
+        acc[2] += (double)ff * mi;
       }
     }
   } else {
