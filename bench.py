@@ -191,11 +191,11 @@ def kernel_bytes(p, esz):
     nk = (p.Lx // 2 + 1) * p.Ly * p.Lz  # half-spectrum points per component
     c = 2 * esz
     return {
-        "k_kick_drift(35a,35c)": 15 * N * esz, "k_kick_close(35e,35f)+np_tail": 9 * N * esz,
+        "k_kick_drift(35a,35c)": 15 * N * esz,
         "k_xy_fwd": 3 * N * esz + 9 * nk * c,
         "k_z_kspace": 18 * nk * c + 6 * nk * esz,
         "k_xy_inv+homo_strain": 9 * nk * c + 9 * N * esz,
-        "k_assemble": 15 * N * esz,
+        "k_assemble+kick(35e,35f)+np_tail": 21 * N * esz,  # R rw9 u3 p3, W F3 p3
     }
 
 

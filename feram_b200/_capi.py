@@ -17,7 +17,7 @@ FILENAME_LEN = 300
 
 FG_OK, FG_ERR_ARG, FG_ERR_CUDA, FG_ERR_NAN, FG_ERR_TIMEOUT, FG_ERR_UNSUPPORTED, FG_ERR_IO, FG_ERR_STATE = range(8)
 FG_BULK, FG_FILM, FG_EPIT, FG_E110 = range(4)
-FG_NPROF = 6  # kernels of one Nose-Poincare step in fg_profile_step
+FG_NPROF = 5  # kernels of one Nose-Poincare step in fg_profile_step
 FG_METHOD_MD, FG_METHOD_VS, FG_METHOD_LF, FG_METHOD_HL = range(4)
 (FG_WAVE_NONE, FG_WAVE_TRIANGULAR_COS, FG_WAVE_TRIANGULAR_SIN,
  FG_WAVE_RAMPING_ON, FG_WAVE_RAMPING_OFF, FG_WAVE_OTHER) = range(6)

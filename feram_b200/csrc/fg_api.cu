@@ -94,7 +94,7 @@ struct fg_ctx {
   int grid_elem = 1;
   // one resident wave of the step's streaming kernels (grid-stride loops):
   // k_kick_drift, k_kick_close, k_assemble; <= grid_elem
-  int grid_kd = 1, grid_kc = 1, grid_as = 1;
+  int grid_kd = 1, grid_kc = 1, grid_as = 1, grid_asc = 1;  // grid_asc: k_assemble<T, true>
   cudaStream_t stream = nullptr;
   // fields (T = float or double)
   void* u = nullptr;
@@ -319,8 +319,24 @@ int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
 }
 
 // ----------------------------------------------------------- force pipeline
+// k_assemble on the context's arrays; CLOSE: with the closing kick of a
+// Nose-Poincare step and the step's tails
+template <typename T, bool CLOSE>
+void launch_assemble(fg_ctx* ctx, int tail) {
+  launch_dep(ctx, k_assemble<T, CLOSE>, CLOSE ? ctx->grid_asc : ctx->grid_as, kThreadsElem, 0,
+             (const T*)ctx->rwork, (const T*)ctx->u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, tail,
+             ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
+             ctx->zsite ? zu_comp(ctx) : 0, (T*)ctx->p, ctx->layer_minv, ctx->layer_sump, (const T*)ctx->site_minv,
+             ctx->site_sump, ctx->part_ke);
+}
+
+// Force modes: FORCE_PLAIN finishes the energies in k_assemble's tail;
+// FORCE_NP_POST leaves them to a following closing kick (k_kick_close);
+// FORCE_NP_CLOSE runs the closing kick and the step's tails in k_assemble.
+enum { FORCE_PLAIN = 0, FORCE_NP_POST = 1, FORCE_NP_CLOSE = 2 };
+
 template <typename T>
-int enqueue_force(fg_ctx* ctx, bool np_post = false) {
+int enqueue_force(fg_ctx* ctx, int mode = FORCE_PLAIN) {
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   T* u = (T*)ctx->u;
@@ -335,11 +351,8 @@ int enqueue_force(fg_ctx* ctx, bool np_post = false) {
     return rc;
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
-  // np_post: the energies and (35e) are finished by the closing kick's block 0
-  launch_dep(ctx, k_assemble<T>, ctx->grid_as, kThreadsElem, 0,
-      (const T*)ctx->rwork, u, (T*)ctx->F, g, ctx->ph, ctx->sc, ctx->part_r, np_post ? TAIL_NONE : TAIL_ENERGIES,
-      ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
-      ctx->zsite ? zu_comp(ctx) : 0);
+  if (mode == FORCE_NP_CLOSE) launch_assemble<T, true>(ctx, TAIL_NONE);
+  else launch_assemble<T, false>(ctx, mode == FORCE_NP_POST ? TAIL_NONE : TAIL_ENERGIES);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
@@ -437,8 +450,11 @@ int enqueue_np(fg_ctx* ctx, bool follows_step = false) {
   ctx->pdl = pdl && follows_step;
   int rc = enqueue_kick_drift<T>(ctx);
   ctx->pdl = pdl;
-  if (!rc) rc = enqueue_force<T>(ctx, true);
-  if (!rc) rc = enqueue_kick_close<T, false>(ctx);
+  // bulk: the closing kick runs inside k_assemble; films mirror the force
+  // first, so the kick is a kernel of its own
+  const bool fused = !ctx->bulk_or_film_mirror();
+  if (!rc) rc = enqueue_force<T>(ctx, fused ? FORCE_NP_CLOSE : FORCE_NP_POST);
+  if (!rc && !fused) rc = enqueue_kick_close<T, false>(ctx);
   ctx->pdl = false;
   return rc;
 }
@@ -654,7 +670,8 @@ int create_impl(fg_ctx* ctx) {
     };
     ctx->grid_kd = wave(k_kick_drift<T>);
     ctx->grid_kc = std::min(wave(k_kick_close<T, false>), wave(k_kick_close<T, true>));
-    ctx->grid_as = wave(k_assemble<T>);
+    ctx->grid_as = wave(k_assemble<T, false>);
+    ctx->grid_asc = wave(k_assemble<T, true>);
   }
   {
     // The dynamic shared-memory cap is an attribute of the kernel, shared by
@@ -1298,7 +1315,7 @@ int np_ready_for_step(fg_ctx* ctx) {
 }
 
 const char* kProfNames[FG_NPROF] = {"k_kick_drift(35a,35c)", "k_xy_fwd", "k_z_kspace", "k_xy_inv+homo_strain",
-                                    "k_assemble", "k_kick_close(35e,35f)+np_tail"};
+                                    "k_assemble+kick(35e,35f)+np_tail"};
 
 template <typename T>
 int profile_impl(fg_ctx* ctx, int reps, double* ms) {
@@ -1321,11 +1338,7 @@ int profile_impl(fg_ctx* ctx, int reps, double* ms) {
     CK(cudaEventRecord(ev[++k], st));
     rc |= launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true);
     CK(cudaEventRecord(ev[++k], st));
-    k_assemble<T><<<ctx->grid_as, kThreadsElem, 0, st>>>(
-        (const T*)ctx->rwork, u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, TAIL_NONE, ctx->done + 2,
-        ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E, ctx->zsite ? zu_comp(ctx) : 0);
-    CK(cudaEventRecord(ev[++k], st));
-    rc |= enqueue_kick_close<T, false>(ctx);
+    launch_assemble<T, true>(ctx, TAIL_NONE);
     CK(cudaEventRecord(ev[++k], st));
     CKL();
     CK(cudaEventSynchronize(ev[FG_NPROF]));

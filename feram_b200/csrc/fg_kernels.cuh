@@ -1180,20 +1180,45 @@ __device__ __forceinline__ void assemble_site(const AsmConst<T>& k, T ux, T uy, 
   o2 = f2 + 2 * w2 * uz + w3 * uy + w4 * ux;
 }
 
+// Masked kinetic sums of the closing kick (35f) of one site: p <- p - c F
+// and p^2/m, p.F/m, F^2/m in T, added to ke (FP64) when the site counts.
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_assemble(const T* __restrict__ rw, const T* __restrict__ u,
-                                                  T* __restrict__ F, Geom g, const Phys* __restrict__ ph,
-                                                  DevScalars* sc, double* __restrict__ part, int tail,
-                                                  unsigned int* done,
-                                                  const unsigned char* __restrict__ site_species = nullptr,
-                                                  const T* __restrict__ site_zstar = nullptr,
-                                                  const T* __restrict__ site_E = nullptr, int zl0 = 0) {
+__device__ __forceinline__ void close_site(T* __restrict__ p, long long ns, long long i, T c, T o0, T o1, T o2,
+                                           bool counted, double mi, double* ke) {
+  const T q0 = p[i] - c * o0, q1 = p[ns + i] - c * o1, q2 = p[2 * ns + i] - c * o2;
+  p[i] = q0;
+  p[ns + i] = q1;
+  p[2 * ns + i] = q2;
+  if (counted) {
+    ke[0] += (double)(q0 * q0 + q1 * q1 + q2 * q2) * mi;
+    ke[1] += (double)(q0 * o0 + q1 * o1 + q2 * o2) * mi;
+    ke[2] += (double)(o0 * o0 + o1 * o1 + o2 * o2) * mi;
+  }
+}
+
+// CLOSE (the force of a Nose-Poincare step, nose-poincare.F:55-71): after the
+// force, the closing kick (35f) p <- p - dt/2 s_{n+1} F with the masked sums
+// p^2/m, p.F/m, F^2/m of the new p in part_ke; the last block finishes the
+// force (energies, commit of the prepared half step, (35e)) and the step
+// (np_close_tail: KE, H_NP and (38) of the next step).
+template <typename T, bool CLOSE = false>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && !CLOSE) ? 3 : 2)
+    k_assemble(const T* __restrict__ rw, const T* __restrict__ u, T* __restrict__ F, Geom g,
+               const Phys* __restrict__ ph, DevScalars* sc, double* __restrict__ part, int tail, unsigned int* done,
+               const unsigned char* __restrict__ site_species, const T* __restrict__ site_zstar,
+               const T* __restrict__ site_E, int zl0, T* __restrict__ p, const double* __restrict__ layer_minv,
+               const unsigned char* __restrict__ layer_sump, const T* __restrict__ site_minv,
+               const unsigned char* __restrict__ site_sump, double* __restrict__ part_ke) {
   pdl_enter();
   // site_*: per-site species (.relaxor), Z* and local field (.localfield);
   // they take the scalar loop.  zl0 > 0: rw components zl0..zl0+2 hold the
   // long-range dipole field of Z* u, which acts on the site times its Z*
   // (dVddi-dipole-dipole.F:52-60); components 0..2 the short-range part.
   const long long ns = g.nsite;
+  // pend_kick_f: prepared by the previous step's tail, not changed by this
+  // step's commit
+  const T cf = CLOSE ? (T)__ldcg(&sc->pend_kick_f) : (T)0;
+  double ke[3] = {0.0, 0.0, 0.0};
   AsmConst<T> k;
   k.fa2g = (T)ph->fa2g; k.tg = (T)ph->tg; k.sk = (T)ph->sk; k.tk2 = (T)ph->tk2; k.fk = (T)ph->fk;
   k.k4x8 = (T)(8 * ph->P_k4);
@@ -1207,7 +1232,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_assemble(const 
   double acc[NQ_R] = {0.0, 0.0};
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  const bool sites = site_species != nullptr || site_zstar != nullptr || site_E != nullptr;
+  const bool sites = site_species != nullptr || site_zstar != nullptr || site_E != nullptr ||
+                     (CLOSE && (site_minv != nullptr || site_sump != nullptr));
   if (sites) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
       AsmConst<T> ks = k;
@@ -1246,6 +1272,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_assemble(const 
       F[i] = o0;
       F[ns + i] = o1;
       F[2 * ns + i] = o2;
+      if constexpr (CLOSE) {
+        const int z = (int)(i / g.plane_r);
+        close_site(p, ns, i, cf, o0, o1, o2, site_sump ? site_sump[i] != 0 : layer_sump[z] != 0,
+                   site_minv ? (double)site_minv[i] : layer_minv[z], ke);
+      }
     }
   } else if (g.plane_r % NV == 0) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1264,18 +1295,57 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_assemble(const 
       stv(F + i, o0);
       stv(F + ns + i, o1);
       stv(F + 2 * ns + i, o2);
+      if constexpr (CLOSE) {
+        const int z = (int)(i / g.plane_r);
+        V16<T> q[3] = {ldv(p + i), ldv(p + ns + i), ldv(p + 2 * ns + i)};
+        T pp = 0, pf = 0, ff = 0;
+#pragma unroll
+        for (int l = 0; l < NV; ++l) {
+          const T f3[3] = {o0.v[l], o1.v[l], o2.v[l]};
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            q[a].v[l] = q[a].v[l] - cf * f3[a];
+            pp += q[a].v[l] * q[a].v[l];
+            pf += q[a].v[l] * f3[a];
+            ff += f3[a] * f3[a];
+          }
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) stv(p + a * ns + i, q[a]);
+        if (layer_sump[z]) {
+          const double mi = layer_minv[z];
+          ke[0] += (double)pp * mi;
+          ke[1] += (double)pf * mi;
+          ke[2] += (double)ff * mi;
+        }
+      }
     }
   } else {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
       T eta[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
-      assemble_site(k, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, F[i], F[ns + i],
-                    F[2 * ns + i], acc);
+      T o0, o1, o2;
+      assemble_site(k, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
+      F[i] = o0;
+      F[ns + i] = o1;
+      F[2 * ns + i] = o2;
+      if constexpr (CLOSE) {
+        const int z = (int)(i / g.plane_r);
+        close_site(p, ns, i, cf, o0, o1, o2, layer_sump[z] != 0, layer_minv[z], ke);
+      }
     }
   }
   block_partials<NQ_R>(acc, part, blockIdx.x);
-  if (tail == TAIL_ENERGIES && is_last_block(done)) force_energies_tail(ph, sc, part, gridDim.x, false);
+  if constexpr (CLOSE) {
+    block_partials<3>(ke, part_ke, blockIdx.x);
+    if (is_last_block(done)) {
+      force_energies_tail(ph, sc, part, gridDim.x, true);
+      np_close_tail(ph, sc, part_ke, gridDim.x, true);
+    }
+  } else if (tail == TAIL_ENERGIES && is_last_block(done)) {
+    force_energies_tail(ph, sc, part, gridDim.x, false);
+  }
 }
 
 // --------------------------------------------------------------- integrators

@@ -310,7 +310,7 @@ int  fg_batch_step(fg_batch* b, int n_steps, fg_energy* e);
 
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */
-#define FG_NPROF 6
+#define FG_NPROF 5
 /* Time n_steps steps of p's method launched as fg_run_steps launches them;
    *ms = total. */
 int  fg_time_steps(fg_ctx* ctx, int n_steps, double* ms);
