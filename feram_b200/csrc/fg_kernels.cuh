@@ -851,9 +851,41 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       return okp ? gp[(long long)(t / CWC) * g.ncplx + (long long)e * g.plane_c] : mk<cplx<T>>((T)0, (T)0);
     };
     auto st = [&](int t, int e, const cplx<T>& v) { buf[(t / CWC) * ZS + (t % CWC) + e * CWC] = v; };
-    ct_stage_io<T, LZC, 0, false, kZThreads, NC * CWC, false>(ld, st, twz);
-    __syncthreads();
-    ct_forward_range<T, LZC, 1, ct_nst(LZC), kZThreads, BZ>(buf, tws_z);
+    if constexpr (sizeof(T) == 4) {
+      // FP32: the whole tile by cp.async first (every copy in flight at
+      // once; regular tiles in 16-byte pencil pairs), then all stages
+      if (blockIdx.x >= zt.nnyq) {
+        int col0 = 0, ys0 = 0;
+        tile_pencil(zt, g, 0, &col0, &ys0);
+        const cplx<T>* base = spec + (long long)ys0 * g.KXP + col0;
+        constexpr int PP = 16 / (int)sizeof(cplx<T>);
+        for (int r = threadIdx.x; r < NC * LZC * (CWC / PP); r += kZThreads) {
+          const int pp = r % (CWC / PP), rz = r / (CWC / PP);
+          const int c = rz / LZC, z = rz - c * LZC;
+          cp_async<16>(&buf[c * ZS + z * CWC + pp * PP],
+                       base + (long long)c * g.ncplx + (long long)z * g.plane_c + pp * PP);
+        }
+      } else {
+        for (int r = threadIdx.x; r < NC * LZC * CWC; r += kZThreads) {
+          const int cw = r % CWC, rz = r / CWC;
+          const int c = rz / LZC, z = rz - c * LZC;
+          int col = 0, ys = 0;
+          cplx<T>* d = &buf[c * ZS + z * CWC + cw];
+          if (tile_pencil(zt, g, cw, &col, &ys))
+            cp_async<(int)sizeof(cplx<T>)>(
+                d, spec + (long long)ys * g.KXP + col + (long long)c * g.ncplx + (long long)z * g.plane_c);
+          else
+            *d = mk<cplx<T>>((T)0, (T)0);
+        }
+      }
+      cp_async_wait();
+      __syncthreads();
+      ct_forward_range<T, LZC, 0, ct_nst(LZC), kZThreads, BZ>(buf, tws_z);
+    } else {
+      ct_stage_io<T, LZC, 0, false, kZThreads, NC * CWC, false>(ld, st, twz);
+      __syncthreads();
+      ct_forward_range<T, LZC, 1, ct_nst(LZC), kZThreads, BZ>(buf, tws_z);
+    }
   } else {
     z_tile_load<T, LZC, CWC>(buf, spec, g, zt, NC);
     Batch B{NC * CW, CW, 1, Lz * CW, CW, true};
