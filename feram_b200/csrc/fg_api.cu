@@ -150,6 +150,7 @@ struct fg_ctx {
   Phys ph_host{};
   DevScalars* sc = nullptr;
   DevScalars* sc_host = nullptr;  // pinned
+  double* E_host = nullptr;       // pinned staging of fg_set_uniform_E
   double* part_k = nullptr;
   double* part_r = nullptr;
   double* part_ke = nullptr;
@@ -845,6 +846,7 @@ int create_impl(fg_ctx* ctx) {
   // scalars
   CK(cudaMalloc(&ctx->sc, sizeof(DevScalars)));
   CK(cudaMallocHost(&ctx->sc_host, sizeof(DevScalars)));
+  CK(cudaMallocHost(&ctx->E_host, 3 * sizeof(double)));
   std::memset(ctx->sc_host, 0, sizeof(DevScalars));
   ctx->sc_host->s = 1.0;
   ctx->sc_host->pi = 0.0;
@@ -1398,6 +1400,7 @@ void fg_destroy(fg_ctx* ctx) {
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->sc_host) cudaFreeHost(ctx->sc_host);
+  if (ctx->E_host) cudaFreeHost(ctx->E_host);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -1578,9 +1581,12 @@ int fg_get_acouK(fg_ctx* ctx, double* acouK) {
 }
 
 int fg_set_uniform_E(fg_ctx* ctx, const double E[3]) {
-  if (!ctx || !ctx->stream || !E) return FG_ERR_ARG;
-  CK(cudaMemcpyAsync(ctx->sc->E, E, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  if (!ctx || !ctx->stream || !ctx->E_host || !E) return FG_ERR_ARG;
+  // Staged in pinned memory and copied in stream order, without waiting:
+  // every call that reads results synchronises the stream, and a second
+  // fg_set_uniform_E before the copy ran only makes the later field win.
+  for (int a = 0; a < 3; ++a) ctx->E_host[a] = ctx->sc_host->E[a] = E[a];  // sc_host: for push_scalars
+  CK(cudaMemcpyAsync(ctx->sc->E, ctx->E_host, 3 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   // The stored dVddi and energies stay those of the last evaluation, as
   // c%dVddi does when molecular-dynamics.F:66-76 changes c%E_field between
   // steps: the next force evaluation sees the new field.
