@@ -167,6 +167,7 @@ struct fg_ctx {
   bool force_fresh = false;
   bool np_ready = false;  // DevScalars' pending half step matches the state
   bool pdl = false;       // launch the step kernels as programmatic dependents
+  unsigned gen = 0;       // bumped when buffers that graphs hold are replaced
   bool store_acouK = false;
   double n_sum_p = 0;
   int NXP = 0, NYP = 0;
@@ -1244,6 +1245,7 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
   }
   CK(cudaMemcpy(ctx->ph, &ctx->ph_host, sizeof(Phys), cudaMemcpyHostToDevice));
   // the step graphs hold the old table pointers as kernel arguments
+  ++ctx->gen;
   for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
     if (*gx) {
       cudaGraphExecDestroy(*gx);
@@ -1931,7 +1933,8 @@ struct fg_batch {
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;   // one step of every replica
+  std::vector<unsigned> gen;         // the replicas' gen when the graphs were captured
   std::string err;
 };
 
@@ -1940,8 +1943,11 @@ int batch_fail(fg_batch* b, int rc, const std::string& msg) {
   b->err = msg;
   return rc;
 }
-int batch_capture(fg_batch* b) {
-  if (b->graph) return FG_OK;
+// The batch graph of one step: a branch per replica, forked from and joined
+// into the batch stream.  (Eight steps per branch, as fg_run_steps uses,
+// measured no faster here: the branches already overlap.)
+int batch_capture(fg_batch* b, cudaGraphExec_t* out) {
+  if (*out) return FG_OK;
   cudaGraph_t graph;
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(e));
@@ -1961,7 +1967,7 @@ int batch_capture(fg_batch* b) {
   cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
   if (rc) return rc == FG_ERR_CUDA && b->err.empty() ? batch_fail(b, rc, cudaGetErrorString(e)) : rc;
   if (ee != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ee));
-  e = cudaGraphInstantiate(&b->graph, graph, 0);
+  e = cudaGraphInstantiate(out, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   return FG_OK;
@@ -2036,7 +2042,18 @@ int fg_batch_step(fg_batch* b, int n_steps, fg_energy* e) {
     cudaError_t ce = cudaStreamSynchronize(c->stream);
     if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
   }
-  if ((rc = batch_capture(b))) return rc;
+  // a replica whose buffers were replaced (site arrays) invalidates the graphs
+  bool stale = b->gen.size() != b->ctx.size();
+  for (size_t i = 0; !stale && i < b->ctx.size(); ++i) stale = b->gen[i] != b->ctx[i]->gen;
+  if (stale) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    b->gen.resize(b->ctx.size());
+    for (size_t i = 0; i < b->ctx.size(); ++i) b->gen[i] = b->ctx[i]->gen;
+  }
+  if ((rc = batch_capture(b, &b->graph))) return rc;
   for (int k = 0; k < n_steps; ++k) {
     cudaError_t ce = cudaGraphLaunch(b->graph, b->stream);
     if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));

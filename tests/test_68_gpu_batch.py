@@ -26,21 +26,56 @@ def test_batch_equals_replicas_stepped_alone(fg, prec):
             ctx.set_state(u, q)
             e = ctx.mirror_force_mirror()
             e = ctx.run_steps(6, e)
-            alone.append((ctx.get_state(), e))
+            st6 = ctx.get_state()
+            e10 = ctx.run_steps(10)  # one eight-step graph and two single steps
+            alone.append((st6, e, ctx.get_state(), e10))
     with fb.Batch(ps, prec) as b:
         for r, (u, q) in zip(b.replicas, states):
             r.build_tables()
             r.set_state(u, q)
             r.mirror_force_mirror()
         es = b.step(6)
+        states6 = [r.get_state() for r in b.replicas]
+        es10 = b.step(10)
         for i, (r, p) in enumerate(zip(b.replicas, ps)):
-            st = r.get_state()
-            sa, ea = alone[i]
-            for k in ("dipoR", "dipoP", "dVddi"):
-                assert np.array_equal(A.physical(st[k], p), A.physical(sa[k], p)), (i, k)
-            assert st["s"] == sa["s"] and st["pi"] == sa["pi"]
-            for f in A.POTENTIAL_FIELDS + ["dipo_kinetic", "total"]:
-                assert getattr(es[i], f) == getattr(ea, f), (i, f)
+            sa, ea, sa10, ea10 = alone[i]
+            for st, s_ref, e_b, e_ref in ((states6[i], sa, es[i], ea), (r.get_state(), sa10, es10[i], ea10)):
+                for k in ("dipoR", "dipoP", "dVddi"):
+                    assert np.array_equal(A.physical(st[k], p), A.physical(s_ref[k], p)), (i, k)
+                assert st["s"] == s_ref["s"] and st["pi"] == s_ref["pi"]
+                for f in A.POTENTIAL_FIELDS + ["dipo_kinetic", "total"]:
+                    assert getattr(e_b, f) == getattr(e_ref, f), (i, f)
+
+
+def test_batch_after_replica_site_arrays_change(fg):
+    """Uploading site arrays to a replica replaces device buffers that the
+    batch's graphs hold: the next fg_batch_step captures them again."""
+    ps = [helpers.params(L="16 16 16", kelvin="250"), helpers.params(L="8 8 8", kelvin="300")]
+    p0 = ps[0]
+    minv = np.zeros((p0.Lz, p0.Ly + p0.padding_y, 2 * (p0.Lx // 2 + 1)))
+    minv[:, :p0.Ly, :p0.Lx] = 1.0 / p0.mass_dipo[0]
+    minv[3, 4, 5] = 0.0  # one fixed dipole
+    states = [(helpers.seeded_u(p, 80 + i, sigma=0.05), helpers.seeded_p(p, 80 + i, sigma=0.01))
+              for i, p in enumerate(ps)]
+    with fb.Context(p0, A.FG_PREC_MIXED) as ctx:
+        ctx.build_tables()
+        ctx.set_state(*states[0])
+        ctx.mirror_force_mirror()
+        ctx.run_steps(3)
+        ctx.upload_site_arrays(mass_dipo_inv=minv)
+        e_ref = ctx.run_steps(9)
+        ref = ctx.get_state()
+    with fb.Batch(ps, A.FG_PREC_MIXED) as b:
+        for r, st in zip(b.replicas, states):
+            r.build_tables()
+            r.set_state(*st)
+            r.mirror_force_mirror()
+        b.step(3)
+        b.replicas[0].upload_site_arrays(mass_dipo_inv=minv)
+        es = b.step(9)
+        got = b.replicas[0].get_state()
+    assert np.array_equal(A.physical(got["dipoR"], p0), A.physical(ref["dipoR"], p0))
+    assert es[0].total == e_ref.total
 
 
 def test_batch_rejects_bad_replica(fg):
