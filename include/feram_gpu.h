@@ -251,7 +251,9 @@ int  fg_get_acouK(fg_ctx* ctx, double* acouK);
 /* Uniform external field E(R) = E (initialize_E_field.F:139-146,
    molecular-dynamics.F:66-76 with no .localfield).  dVddi and the energies
    of the last force evaluation are kept; the next evaluation (inside the
-   next nose_poincare / leapfrog step) uses E, as in the reference. */
+   next nose_poincare / leapfrog step) uses E, as in the reference.  The
+   copy to the device is queued on the context's stream without waiting;
+   E may be reused by the caller as soon as the call returns. */
 int  fg_set_uniform_E(fg_ctx* ctx, const double E[3]);
 
 /* ---- the hot path -------------------------------------------------------- */
