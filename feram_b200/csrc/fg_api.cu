@@ -168,6 +168,7 @@ struct fg_ctx {
   bool np_ready = false;  // DevScalars' pending half step matches the state
   bool pdl = false;       // launch the step kernels as programmatic dependents
   unsigned gen = 0;       // bumped when buffers that graphs hold are replaced
+  bool broken = false;    // a reallocation failed half way: refuse further work
   bool store_acouK = false;
   double n_sum_p = 0;
   int NXP = 0, NYP = 0;
@@ -1144,6 +1145,7 @@ int set_zsite(fg_ctx* ctx, bool on) {
   });
   if (ea != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
   CK(cudaStreamSynchronize(ctx->stream));
+  ctx->broken = true;  // until every buffer below is allocated again
   for (void** b : {&ctx->spec, &ctx->rwork, (void**)&ctx->part_k, &ctx->ltab})
     if (*b) {
       cudaFree(*b);
@@ -1160,6 +1162,7 @@ int set_zsite(fg_ctx* ctx, bool on) {
   CK(cudaMalloc(&ctx->rwork, (size_t)ncx * ctx->real_bytes));
   CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)(zt.nreg + zt.nnyq)));
   if (on) CK(cudaMalloc(&ctx->ltab, 6 * sizeof(T) * (size_t)g.nkpos));
+  ctx->broken = false;
   return FG_OK;
 }
 
@@ -1258,6 +1261,7 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
 
 int ensure_ready(fg_ctx* ctx) {
   if (!ctx) return FG_ERR_ARG;
+  if (ctx->broken) return fail(ctx, FG_ERR_CUDA, "a device buffer could not be reallocated: destroy this context");
   if (!ctx->tables_ready) return fail(ctx, FG_ERR_STATE, "no k-space tables: call fg_build_tables or fg_upload_tables");
   if (ctx->zsite && !ctx->ltab_ready) {  // L/N for the per-site Z* path, from the FP64 long-range table
     const long long n = 6 * ctx->g.nkpos;
@@ -1468,11 +1472,13 @@ int fg_get_long_range(fg_ctx* ctx, double* lr) {
 
 int fg_fft_r2c3(fg_ctx* ctx, const double* in, double* out) {
   if (!ctx || !ctx->stream || !in || !out) return FG_ERR_ARG;
+  if (ctx->broken) return fail(ctx, FG_ERR_CUDA, "a device buffer could not be reallocated: destroy this context");
   return ctx->prec == FG_PREC_MIXED ? fft_r2c3_impl<float>(ctx, in, out) : fft_r2c3_impl<double>(ctx, in, out);
 }
 
 int fg_fft_c2r3(fg_ctx* ctx, const double* in, double* out) {
   if (!ctx || !ctx->stream || !in || !out) return FG_ERR_ARG;
+  if (ctx->broken) return fail(ctx, FG_ERR_CUDA, "a device buffer could not be reallocated: destroy this context");
   return ctx->prec == FG_PREC_MIXED ? fft_c2r3_impl<float>(ctx, in, out) : fft_c2r3_impl<double>(ctx, in, out);
 }
 
