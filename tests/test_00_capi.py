@@ -40,3 +40,16 @@ def test_host_functions_need_no_device(fg):
 def test_oracle_loads(oracle):
     for n in ("oracle_create", "oracle_force", "oracle_nose_poincare", "oracle_leapfrog", "oracle_uni64"):
         assert hasattr(oracle, n)
+
+
+def test_profile_names_match_header_count(fg):
+    """fg_profile_name names FG_NPROF kernels (the bulk step graph) and
+    returns "" past them; the Python constant mirrors the header's."""
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "feram_gpu.h")).read()
+    n = int(hdr.split("#define FG_NPROF")[1].split()[0])
+    assert n == A.FG_NPROF
+    L = A.lib()
+    names = [L.fg_profile_name(i).decode() for i in range(n + 1)]
+    assert all(names[:n]) and names[n] == ""
+    assert names[0].startswith("k_kick_drift") and names[-2].startswith("k_assemble")
