@@ -36,6 +36,8 @@ sys.path.insert(0, ROOT)
 METRIC = "MD site-steps/s at 128^3: mixed vs FP64 GPU (force err<=1e-6); % HBM peak"
 UNIT = "site-steps/s"
 L_DEFAULT = 128
+# fg_nose_poincare calls in the end-to-end measurement, independent of --steps
+E2E_STEPS = 400
 
 # BaTiO3, Zhong-Vanderbilt-Rabe effective-Hamiltonian parameters as used by
 # the reference's BaTiO3 cooling sweep and 64^3 benchmark input decks (eV,
@@ -49,9 +51,32 @@ ZVR = dict(GPa=-5.0, mass_amu=39.0, Q_Nose_64=1.0, a0=3.94, dt=0.002,
            Z_star=9.956, epsilon_inf=5.24)
 
 
-def make_params(L, kelvin=300.0, Ez=0.001, seed=(123456789, 987654321)):
-    import feram_b200 as fb
-    p = fb.default_params()
+def _param_lib(impl):
+    """(defaults, make) of the arm: the product's host code for ours, the
+    oracle's own restatement of read_Param/make_Param for the reference arm,
+    so that the reference process never loads the product library."""
+    from feram_b200 import _capi as A
+    if impl == "ours":
+        import feram_b200 as fb
+        return fb.default_params, fb.make_param
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    L = oracle_lib.load()
+
+    def defaults():
+        p = A.fg_params()
+        L.oracle_default_param(C.byref(p))
+        return p
+
+    def make(p):
+        assert L.oracle_make_param(C.byref(p)) == 0
+        return p
+    return defaults, make
+
+
+def make_params(L, kelvin=300.0, Ez=0.001, seed=(123456789, 987654321), impl="ours"):
+    defaults, make = _param_lib(impl)
+    p = defaults()
     z = ZVR
     p.method = 0
     p.GPa[0] = p.GPa[1] = p.GPa[2] = z["GPa"]
@@ -72,15 +97,40 @@ def make_params(L, kelvin=300.0, Ez=0.001, seed=(123456789, 987654321)):
     p.external_E_field[2] = Ez
     p.E_field_always_zero = 0 if Ez != 0.0 else 1
     p.seed[0], p.seed[1] = seed
-    return fb.make_param(p)
+    return make(p)
 
 
-def initial_state(p):
+def initial_state(p, impl="ours"):
+    """initialize_dipoR's seeded u and p = 0 (product host code, or the
+    oracle's restatement for the reference arm)."""
     from feram_b200 import _capi as A
     u = A.real_field(p)
     q = A.real_field(p)
-    assert A.lib().fg_init_dipoR_host(C.byref(p), A.dptr(u), A.dptr(q)) == 0
+    if impl == "ours":
+        assert A.lib().fg_init_dipoR_host(C.byref(p), A.dptr(u), A.dptr(q)) == 0
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        assert oracle_lib.load().oracle_init_dipoR(C.byref(p), A.dptr(u), A.dptr(q)) == 0
     return u, q
+
+
+def loaded_repo_libs():
+    """Shared objects of this repository mapped into the process."""
+    libs = set()
+    try:
+        for line in open("/proc/self/maps"):
+            path = line.split()[-1] if len(line.split()) >= 6 else ""
+            if path.endswith(".so") and os.path.abspath(path).startswith(ROOT):
+                libs.add(os.path.relpath(path, ROOT))
+    except OSError:
+        return None
+    return sorted(libs)
+
+
+def fp32_config(u):
+    """u rounded to FP32: the configuration the mixed path holds."""
+    return u.astype(np.float32).astype(np.float64)
 
 
 ENERGY_TERMS = ("short_range", "long_range", "dipole_E_field", "unharmonic", "homo_strain", "homo_coupling",
@@ -89,25 +139,34 @@ ENERGY_TERMS = ("short_range", "long_range", "dipole_E_field", "unharmonic", "ho
 
 def force_errors_16(ctxm, ctx64, p, sigma=0.1):
     """Mixed against FP64 force and energies on 16 fixed configurations,
-    u ~ N(0, sigma) per component from uni64 seeds (s, 987654321), s = 1..16;
-    the FP64 path matches the oracle to 1e-11.  Force errors: rms |dF| / rms
-    |F| (the relative L2 norm), max |dF| / max |F| (relative max norm) and
-    max |dF| / rms |F| (the worst site against the typical force); energy
-    error per term over the sum of the terms' magnitudes."""
+    u ~ N(0, sigma) per component from uni64 seeds (s, 987654321), s = 1..16,
+    rounded to FP32 (the state the mixed path holds) and given identically to
+    both paths; the FP64 path matches the oracle to 1e-12.  Force errors:
+    max |dF| / rms |F| over sites (worst site against the typical force), rms
+    |dF| / rms |F| (relative L2 norm) and max |dF| / max |F| (relative max
+    norm); energy error per term over the sum of the terms' magnitudes.
+    state_rounding: the same worst-site measure between the FP64 forces of
+    the unrounded and the FP32-rounded configuration, i.e. what holding u in
+    FP32 at all moves the force by (a property of FP32 state, not of the
+    mixed arithmetic)."""
     from feram_b200 import _capi as A
-    worst = {"max": 0.0, "rms": 0.0, "maxnorm": 0.0, "energy": 0.0}
+    worst = {"max": 0.0, "rms": 0.0, "maxnorm": 0.0, "energy": 0.0, "state": 0.0}
     for s in range(1, 17):
         q = A.fg_params.from_buffer_copy(p)
         q.seed[0], q.seed[1] = s, 987654321
         for a in range(3):
             q.init_dipo_avg[a], q.init_dipo_dev[a], q.k_stripe[a] = 0.0, sigma, 0.0
-        u = A.real_field(p)
-        assert A.lib().fg_init_dipoR_host(C.byref(q), A.dptr(u), None) == 0
+        u64 = A.real_field(p)
+        assert A.lib().fg_init_dipoR_host(C.byref(q), A.dptr(u64), None) == 0
+        u = fp32_config(u64)
         es, fs = [], []
         for ctx in (ctx64, ctxm):
             ctx.set_state(u)
             es.append(ctx.mirror_force_mirror())
-            fs.append(A.physical(ctx.get_state()["dVddi"], p))
+            fs.append(A.physical(ctx.get_state()["dVddi"], p).copy())
+        ctx64.set_state(u64)
+        ctx64.mirror_force_mirror()
+        f64u = A.physical(ctx64.get_state()["dVddi"], p)
         d = np.sqrt(np.sum((fs[1] - fs[0]) ** 2, axis=-1))
         rms = float(np.sqrt(np.mean(np.sum(fs[0] ** 2, axis=-1))))
         scale = sum(abs(getattr(es[0], t)) for t in ENERGY_TERMS)
@@ -116,8 +175,10 @@ def force_errors_16(ctxm, ctx64, p, sigma=0.1):
         worst["rms"] = max(worst["rms"], float(np.sqrt(np.mean(d ** 2))) / rms)
         worst["energy"] = max(worst["energy"],
                               max(abs(getattr(es[1], t) - getattr(es[0], t)) for t in ENERGY_TERMS) / scale)
-    return {"configs": 16, "sigma": sigma, "seeds": "uni64 (1..16, 987654321)", "force_rms": worst["rms"],
-            "force_maxnorm": worst["maxnorm"], "force_max_site_over_rms": worst["max"], "energy_max": worst["energy"]}
+        worst["state"] = max(worst["state"], float(np.sqrt(np.sum((f64u - fs[0]) ** 2, axis=-1)).max()) / rms)
+    return {"configs": 16, "sigma": sigma, "seeds": "uni64 (1..16, 987654321), rounded to FP32",
+            "force_rms": worst["rms"], "force_maxnorm": worst["maxnorm"], "force_max_site_over_rms": worst["max"],
+            "energy_max": worst["energy"], "state_rounding_max_site_over_rms": worst["state"]}
 
 
 def prepare(ctx, p, u, q):
@@ -279,18 +340,20 @@ def cpu_baseline(p, budget_s=20.0):
 
 def run_reference(args):
     """--impl reference: the reference's CPU path (its C++ restatement, since
-    the Fortran/FFTW binary cannot be built here) on all host cores."""
+    the Fortran/FFTW binary cannot be built here) on all host cores.  Inputs
+    come from the oracle's own read_Param/make_Param/initialize_dipoR, so
+    nothing of the product is loaded in this process."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     L = args.size
-    p = make_params(L)
+    p = make_params(L, impl="reference")
     budget = 120.0
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
     threads = os.cpu_count() or 1
     oracle_lib.load().oracle_set_threads(threads)
-    u, q = initial_state(p)
+    u, q = initial_state(p, impl="reference")
     o = oracle_lib.Oracle(p)
     o.set_state(u, q)
     o.set_uniform_E([0.0, 0.0, p.external_E_field[2]])
@@ -316,6 +379,7 @@ def run_reference(args):
         "config": {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "repo_libs_loaded": loaded_repo_libs(),
     }), flush=True)
     return 0
 
@@ -373,7 +437,7 @@ def main():
         # force error of the mixed path against the FP64 path on the same state
         ctx64 = fb.Context(p, A.FG_PREC_FP64)
         ctx64.build_tables()
-        prepare(ctx64, p, u, q)
+        prepare(ctx64, p, fp32_config(u), q)
         f64 = ctx64.get_state()["dVddi"]
         fmx = ctxm.get_state()["dVddi"]
         d = A.physical(fmx, p) - A.physical(f64, p)
@@ -449,7 +513,7 @@ def main():
         out_u, out_q, out_f = pin(A.real_field(p)), pin(A.real_field(p)), pin(A.real_field(p))
         E = np.array([0.0, 0.0, p.external_E_field[2]])
         e = fb.fg_energy()
-        k_e2e = max(args.steps // 4, 10)
+        k_e2e = E2E_STEPS
         barrier()
         t0 = time.perf_counter()
         ctxm.set_state(hu, hq, 1.0, 0.0, H0)

@@ -149,6 +149,31 @@ class Context:
         self._check(lib().fg_fft_c2r3(self._h, dptr(s.view(np.float64)), dptr(out)))
         return out
 
+    def time_fft(self, reps: int = 20):
+        """fg_time_fft: device milliseconds of the 3-component r2c and c2r."""
+        ms = (C.c_double * 2)()
+        self._check(lib().fg_time_fft(self._h, reps, ms))
+        return ms[0], ms[1]
+
+    def chain_point(self, kelvin: float, E=None) -> fg_energy:
+        """fg_chain_point: the next sweep point from the state on the device
+        (p / s, new kelvin and field, force, s = 1, pi = 0, H0)."""
+        e = fg_energy()
+        Ea = None if E is None else np.ascontiguousarray(E, dtype=np.float64)
+        self._check(lib().fg_chain_point(self._h, kelvin, dptr(Ea), C.byref(e)))
+        p = fg_params()
+        self._check(lib().fg_get_params(self._h, C.byref(p)))
+        self.p = p
+        return e
+
+    def set_wave(self, on: bool = True, i_step: int = 0):
+        """fg_set_wave: the per-step field wave() evaluated on the device."""
+        self._check(lib().fg_set_wave(self._h, 1 if on else 0, i_step))
+
+    def write_coord(self, path: str, full_precision: bool = True):
+        """fg_write_coord: write_system's .coord of the current state."""
+        self._check(lib().fg_write_coord(self._h, os.fsencode(path), 1 if full_precision else 0))
+
     # -- state
     def set_state(self, dipoR=None, dipoP=None, s=1.0, pi=0.0, H0=0.0):
         self._check(lib().fg_set_state(self._h, dptr(dipoR), dptr(dipoP), s, pi, H0))

@@ -151,6 +151,11 @@ def lib() -> C.CDLL:
         "fg_get_long_range": (C.c_int, [vp, dp]),
         "fg_fft_r2c3": (C.c_int, [vp, dp, dp]),
         "fg_fft_c2r3": (C.c_int, [vp, dp, dp]),
+        "fg_time_fft": (C.c_int, [vp, C.c_int, dp]),
+        "fg_get_params": (C.c_int, [vp, C.POINTER(fg_params)]),
+        "fg_chain_point": (C.c_int, [vp, C.c_double, dp, C.POINTER(fg_energy)]),
+        "fg_write_coord": (C.c_int, [vp, C.c_char_p, C.c_int]),
+        "fg_set_wave": (C.c_int, [vp, C.c_int, C.c_int]),
         "fg_set_state": (C.c_int, [vp, dp, dp, C.c_double, C.c_double, C.c_double]),
         "fg_get_state": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
         "fg_set_thermostat": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),

@@ -100,6 +100,11 @@ struct fg_ctx {
   void* u = nullptr;
   void* p = nullptr;
   void* F = nullptr;
+  // mixed path: FP32 residual of F (F + Flo = the FP64 site sum), written by
+  // the force-only evaluation (fg_mirror_force_mirror); flo_valid while F
+  // has not been rewritten by a step since
+  void* Flo = nullptr;
+  bool flo_valid = false;
   void* spec = nullptr;   // 9 complex spectra
   void* rwork = nullptr;  // 9 real fields
   void* dtab = nullptr;   // 6 per table slot
@@ -170,6 +175,7 @@ struct fg_ctx {
   unsigned gen = 0;       // bumped when buffers that graphs hold are replaced
   bool broken = false;    // a reallocation failed half way: refuse further work
   bool store_acouK = false;
+  bool wave_dev = false;  // the step graphs start with k_wave_step (fg_set_wave)
   double n_sum_p = 0;
   int NXP = 0, NYP = 0;
   bool bulk_or_film_mirror() const { return P.bulk_or_film == FG_FILM || P.bulk_or_film == FG_EPIT; }
@@ -258,6 +264,19 @@ void with_z_kspace(int Lz, int cw, bool acou, bool zsite, F f) {
   else f(k_z_kspace<T, 0, 0>);
 }
 
+// The standalone z pass of the 3-component FFT entry points (fg_fft_r2c3,
+// fg_fft_c2r3, fg_time_fft): compile-time transforms where the step's own
+// z tiles have them, else runtime plans.
+template <typename T, bool INV, class F>
+void with_z_pass(int Lz, int cw, F f) {
+  constexpr int C = z_cw_cap<T>();
+  if (cw == C && Lz == 128) f(k_z_pass<T, INV, 128, C, 3>);
+  else if (cw == C && Lz == 64) f(k_z_pass<T, INV, 64, C, 3>);
+  else if (cw == C && Lz == 32) f(k_z_pass<T, INV, 32, C, 3>);
+  else if (cw == C && Lz == 16) f(k_z_pass<T, INV, 16, C, 3>);
+  else f(k_z_pass<T, INV>);
+}
+
 // First component of Z*(R) u in the spectrum and of the long-range dipole
 // field in rwork (per-site Z*): after u, u u and the acoustic displacement.
 inline int zu_comp(const fg_ctx* ctx) { return ctx->acou ? 12 : 9; }
@@ -324,13 +343,28 @@ int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
 // ----------------------------------------------------------- force pipeline
 // k_assemble on the context's arrays; CLOSE: with the closing kick of a
 // Nose-Poincare step and the step's tails
+// Static constants of the site force (dVddi-unharmonic.F:28-32,67-99,
+// elastic.F:60-75) from the context's Phys, passed to k_assemble by value.
+AsmConst asm_const(const fg_ctx* ctx) {
+  const Phys& h = ctx->ph_host;
+  AsmConst k{};
+  k.fa2g = h.fa2g; k.tg = h.tg; k.sk = h.sk; k.tk2 = h.tk2; k.fk = h.fk;
+  k.k4x8 = 8 * h.P_k4;
+  k.hx = h.HC2[0][0]; k.hy = h.HC2[0][1]; k.h4 = h.HC2[3][3];
+  k.Zs = h.Zstar;
+  k.Pa = h.P_alpha; k.Pg = h.P_gamma; k.P1 = h.P_k1; k.P2 = h.P_k2; k.P3 = h.P_k3; k.P4 = h.P_k4;
+  k.E_on = h.E_on;
+  return k;
+}
+
+// flo: also store the FP32 residual of the force (mixed path)
 template <typename T, bool CLOSE>
-void launch_assemble(fg_ctx* ctx, int tail) {
+void launch_assemble(fg_ctx* ctx, int tail, bool flo = false) {
   launch_dep(ctx, k_assemble<T, CLOSE>, CLOSE ? ctx->grid_asc : ctx->grid_as, kThreadsElem, 0,
              (const T*)ctx->rwork, (const T*)ctx->u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, tail,
              ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
              ctx->zsite ? zu_comp(ctx) : 0, (T*)ctx->p, ctx->layer_minv, ctx->layer_sump, (const T*)ctx->site_minv,
-             ctx->site_sump, ctx->part_ke);
+             ctx->site_sump, ctx->part_ke, (flo && sizeof(T) == 4) ? (T*)ctx->Flo : (T*)nullptr, asm_const(ctx));
 }
 
 // Force modes: FORCE_PLAIN finishes the energies in k_assemble's tail;
@@ -338,8 +372,10 @@ void launch_assemble(fg_ctx* ctx, int tail) {
 // FORCE_NP_CLOSE runs the closing kick and the step's tails in k_assemble.
 enum { FORCE_PLAIN = 0, FORCE_NP_POST = 1, FORCE_NP_CLOSE = 2 };
 
+// flo: the force-only evaluation of fg_mirror_force_mirror, which keeps the
+// FP32 residual of the mixed path's force for fg_get_state
 template <typename T>
-int enqueue_force(fg_ctx* ctx, int mode = FORCE_PLAIN) {
+int enqueue_force(fg_ctx* ctx, int mode = FORCE_PLAIN, bool flo = false) {
   const Geom& g = ctx->g;
   cudaStream_t st = ctx->stream;
   T* u = (T*)ctx->u;
@@ -355,11 +391,15 @@ int enqueue_force(fg_ctx* ctx, int mode = FORCE_PLAIN) {
   if ((rc = launch_z_kspace<T>(ctx, ctx->store_acouK ? (cplx<T>*)ctx->acouK : nullptr))) return rc;
   if ((rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, ctx->ncx, true))) return rc;
   if (mode == FORCE_NP_CLOSE) launch_assemble<T, true>(ctx, TAIL_NONE);
-  else launch_assemble<T, false>(ctx, mode == FORCE_NP_POST ? TAIL_NONE : TAIL_ENERGIES);
+  else launch_assemble<T, false>(ctx, mode == FORCE_NP_POST ? TAIL_NONE : TAIL_ENERGIES, flo);
   CKL();
   if (ctx->P.bulk_or_film == FG_FILM || ctx->P.bulk_or_film == FG_EPIT) {
     k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->F, g, ctx->P.gap_id);
     CKL();
+    if (flo && sizeof(T) == 4) {
+      k_mirror<T><<<ctx->grid_elem, kThreadsElem, 0, st>>>((T*)ctx->Flo, g, ctx->P.gap_id);
+      CKL();
+    }
   }
   return FG_OK;
 }
@@ -416,6 +456,14 @@ int enqueue_pump(fg_ctx* ctx) {
   return FG_OK;
 }
 
+// The device-side field schedule at the start of a step (fg_set_wave).
+int enqueue_wave(fg_ctx* ctx) {
+  if (!ctx->wave_dev) return FG_OK;
+  k_wave_step<<<1, 32, 0, ctx->stream>>>(ctx->ph, ctx->sc);
+  CKL();
+  return FG_OK;
+}
+
 template <typename T>
 int enqueue_kick_drift(fg_ctx* ctx) {
   launch_dep(ctx, k_kick_drift<T>, ctx->grid_kd, kThreadsElem, 0, (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
@@ -450,8 +498,10 @@ int enqueue_kick_close(fg_ctx* ctx) {
 template <typename T>
 int enqueue_np(fg_ctx* ctx, bool follows_step = false) {
   const bool pdl = !ctx->bulk_or_film_mirror();
-  ctx->pdl = pdl && follows_step;
-  int rc = enqueue_kick_drift<T>(ctx);
+  int rc = enqueue_wave(ctx);
+  if (rc) return rc;
+  ctx->pdl = pdl && follows_step && !ctx->wave_dev;
+  rc = enqueue_kick_drift<T>(ctx);
   ctx->pdl = pdl;
   // bulk: the closing kick runs inside k_assemble; films mirror the force
   // first, so the kick is a kernel of its own
@@ -469,6 +519,7 @@ constexpr int kNpGraphSteps = 8;
 template <typename T>
 int enqueue_lf(fg_ctx* ctx) {
   int rc;
+  if ((rc = enqueue_wave(ctx))) return rc;
   if ((rc = enqueue_pump<T>(ctx))) return rc;
   if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
   if (ctx->acou && (rc = enqueue_drift_acou<T>(ctx, &ctx->sc->lf_dt))) return rc;
@@ -484,6 +535,7 @@ int enqueue_lf(fg_ctx* ctx) {
 template <typename T>
 int enqueue_vs(fg_ctx* ctx) {
   int rc;
+  if ((rc = enqueue_wave(ctx))) return rc;
   if ((rc = enqueue_drift<T>(ctx, &ctx->sc->lf_dt))) return rc;
   if (ctx->acou && (rc = enqueue_drift_acou<T>(ctx, &ctx->sc->lf_dt))) return rc;
   if ((rc = enqueue_force<T>(ctx))) return rc;
@@ -518,7 +570,9 @@ int capture(fg_ctx* ctx, cudaGraphExec_t* out, Fn fn) {
 int run_graph(fg_ctx* ctx, cudaGraphExec_t* gx, int which) {
   int rc = FG_OK;
   if (which == 0) {
-    rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_force<float>(ctx) : enqueue_force<double>(ctx); });
+    rc = capture(ctx, gx, [&] {
+      return ctx->prec == FG_PREC_MIXED ? enqueue_force<float>(ctx, FORCE_PLAIN, true) : enqueue_force<double>(ctx);
+    });
   } else if (which == 1) {
     rc = capture(ctx, gx, [&] { return ctx->prec == FG_PREC_MIXED ? enqueue_np<float>(ctx) : enqueue_np<double>(ctx); });
   } else if (which == 4) {
@@ -695,8 +749,8 @@ int create_impl(fg_ctx* ctx) {
     with_xy_fwd<double, SRC_FIELD>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy64); });
     with_xy_inv<T>(g.m, g.Ly, [&](auto k) { setattr(k, ctx->smem_xy); });
     with_z_kspace<T>(g.Lz, ctx->zt.CW, ctx->acou, false, [&](auto k) { setattr(k, ctx->smem_z); });
-    setattr(k_z_pass<T, false>, ctx->smem_z3);
-    setattr(k_z_pass<T, true>, ctx->smem_z3);
+    with_z_pass<T, false>(g.Lz, ctx->zt.CW, [&](auto k) { setattr(k, ctx->smem_z3); });
+    with_z_pass<T, true>(g.Lz, ctx->zt.CW, [&](auto k) { setattr(k, ctx->smem_z3); });
     setattr(k_z_ewald_pack<T>, ctx->smem_z6);
     setattr(k_z_modulation_pack<T>, ctx->smem_z1);
     if (ea != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
@@ -704,14 +758,20 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 
   // slot maps
+  // posm: [0, m) the slot of each packed-x frequency; then the y maps of
+  // the xy kernels, [m, m + Ly) slot -> ky and [m + Ly, m + 2 Ly) ky -> slot
   std::vector<int> revm = digit_reversal(ctx->px);
-  std::vector<int> posm(g.m);
-  for (int s = 0; s < g.m; ++s) posm[revm[s]] = s;
   ctx->h_revx.resize(g.NKX);
   for (int s = 0; s < g.m; ++s) ctx->h_revx[s] = revm[s];
   ctx->h_revx[g.m] = g.m;
   ctx->h_revy = digit_reversal(ctx->py);
   ctx->h_revz = digit_reversal(ctx->pz);
+  std::vector<int> posm(g.m + 2 * (size_t)g.Ly);
+  for (int s = 0; s < g.m; ++s) posm[revm[s]] = s;
+  for (int s = 0; s < g.Ly; ++s) {
+    posm[g.m + s] = ctx->h_revy[s];
+    posm[g.m + g.Ly + ctx->h_revy[s]] = s;
+  }
   int rc;
   if ((rc = upload(ctx, (void**)&ctx->revx, ctx->h_revx))) return rc;
   if ((rc = upload(ctx, (void**)&ctx->revy, ctx->h_revy))) return rc;
@@ -842,6 +902,10 @@ int create_impl(fg_ctx* ctx) {
     h.ke_scale = (double)P.N / (2.0 * ctx->n_sum_p);
     h.E_on = P.E_field_always_zero ? 0 : 1;
     h.modulation_on = 0;
+    h.wave_type = P.E_wave_type;
+    h.wave_n_thermalize = P.n_thermalize;
+    h.wave_period = P.n_E_wave_period;
+    for (int a = 0; a < 3; ++a) h.wave_amp[a] = P.external_E_field[a];
     CK(cudaMalloc(&ctx->ph, sizeof(Phys)));
     CK(cudaMemcpy(ctx->ph, &h, sizeof(Phys), cudaMemcpyHostToDevice));
   }
@@ -867,6 +931,10 @@ int create_impl(fg_ctx* ctx) {
   CK(cudaMemset(ctx->u, 0, nfc * ctx->real_bytes));  // acouR = acouP = 0 (initialize-dipoR.F:56)
   CK(cudaMemset(ctx->p, 0, nfc * ctx->real_bytes));
   CK(cudaMemset(ctx->F, 0, 3 * ctx->real_bytes));
+  if (sizeof(T) == 4) {
+    CK(cudaMalloc(&ctx->Flo, 3 * ctx->real_bytes));
+    CK(cudaMemset(ctx->Flo, 0, 3 * ctx->real_bytes));
+  }
   CK(cudaMalloc(&ctx->spec, (size_t)ctx->ncx * sizeof(cplx<T>) * (size_t)g.ncplx));
   CK(cudaMemset(ctx->spec, 0, 9 * sizeof(cplx<T>) * (size_t)g.ncplx));
   CK(cudaMalloc(&ctx->rwork, (size_t)ctx->ncx * ctx->real_bytes));
@@ -1039,6 +1107,18 @@ int get_field(fg_ctx* ctx, double* dst, const void* src) {
   return FG_OK;
 }
 
+// A field held as hi + lo (the mixed path's force after fg_mirror_force_mirror)
+template <typename T>
+int get_field2(fg_ctx* ctx, double* dst, const void* hi, const void* lo) {
+  const size_t nin = (size_t)3 * ctx->NXP * ctx->NYP * ctx->P.Lz;
+  k_soa2_to_fortran<T><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>(ctx->staging, (const T*)hi, (const T*)lo,
+                                                                          ctx->g, 3, ctx->NXP, ctx->NYP);
+  CKL();
+  CK(cudaMemcpyAsync(dst, ctx->staging, sizeof(double) * nin, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FG_OK;
+}
+
 template <typename T>
 int get_acouK_impl(fg_ctx* ctx, double* out) {
   const Geom& g = ctx->g;
@@ -1060,6 +1140,63 @@ int get_acouK_impl(fg_ctx* ctx, double* out) {
 
 // 3-component r2c / c2r of the reference's plan_r2c_3_out / plan_c2r_3_out
 // (coord_module.F:155-157,310-312) on the device FFT.
+// z pass of the 3-component spectrum in ctx->spec
+template <typename T, bool INV>
+int launch_z_pass(fg_ctx* ctx) {
+  with_z_pass<T, INV>(ctx->g.Lz, ctx->zt.CW, [&](auto kern) {
+    kern<<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z3, ctx->stream>>>(
+        (cplx<T>*)ctx->spec, ctx->g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->zt);
+  });
+  CKL();
+  return FG_OK;
+}
+
+// The batched 3-component r2c (rwork -> spec) and c2r (spec -> rwork) of
+// the FFT entry points, on the device buffers only.
+template <typename T>
+int enqueue_fft_r2c3(fg_ctx* ctx) {
+  int rc = launch_xy_fwd<T, SRC_FIELD>(ctx, (const T*)ctx->rwork, (cplx<T>*)ctx->spec, 3, ctx->smem_xy,
+                                       (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy);
+  if (rc) return rc;
+  return launch_z_pass<T, false>(ctx);
+}
+template <typename T>
+int enqueue_fft_c2r3(fg_ctx* ctx) {
+  int rc = launch_z_pass<T, true>(ctx);
+  if (rc) return rc;
+  return launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 3);
+}
+
+template <typename T>
+int time_fft_impl(fg_ctx* ctx, int reps, double* ms) {
+  cudaEvent_t ev[3];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  int rc = FG_OK;
+  double t_f = 0.0, t_i = 0.0;
+  for (int r = 0; r < reps + 1 && rc == FG_OK; ++r) {  // r = 0: warm-up
+    if (cudaEventRecord(ev[0], ctx->stream) != cudaSuccess) rc = FG_ERR_CUDA;
+    if (!rc) rc = enqueue_fft_r2c3<T>(ctx);
+    if (!rc && cudaEventRecord(ev[1], ctx->stream) != cudaSuccess) rc = FG_ERR_CUDA;
+    if (!rc) rc = enqueue_fft_c2r3<T>(ctx);
+    if (!rc && cudaEventRecord(ev[2], ctx->stream) != cudaSuccess) rc = FG_ERR_CUDA;
+    if (!rc && cudaEventSynchronize(ev[2]) != cudaSuccess) rc = FG_ERR_CUDA;
+    float a = 0.0f, b = 0.0f;
+    if (!rc && (cudaEventElapsedTime(&a, ev[0], ev[1]) != cudaSuccess ||
+                cudaEventElapsedTime(&b, ev[1], ev[2]) != cudaSuccess))
+      rc = FG_ERR_CUDA;
+    if (!rc && r > 0) {
+      t_f += a;
+      t_i += b;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (rc == FG_ERR_CUDA && ctx->err.empty()) ctx->err = "fg_time_fft: CUDA event or launch error";
+  if (rc) return rc;
+  ms[0] = t_f / reps;
+  ms[1] = t_i / reps;
+  return check_device_error(ctx);
+}
+
 template <typename T>
 int fft_r2c3_impl(fg_ctx* ctx, const double* in, double* out) {
   const Geom& g = ctx->g;
@@ -1069,9 +1206,7 @@ int fft_r2c3_impl(fg_ctx* ctx, const double* in, double* out) {
                                         (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm,
                                         (const cplx<T>*)ctx->twy)))
     return rc;
-  k_z_pass<T, false><<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z3, ctx->stream>>>(
-      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->zt);
-  CKL();
+  if ((rc = launch_z_pass<T, false>(ctx))) return rc;
   std::vector<cplx<T>> S(3 * (size_t)g.ncplx);
   CK(cudaMemcpyAsync(S.data(), ctx->spec, S.size() * sizeof(cplx<T>), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1103,10 +1238,9 @@ int fft_c2r3_impl(fg_ctx* ctx, const double* in, double* out) {
           S[(size_t)c * g.ncplx + (size_t)zs * g.plane_c + (size_t)ys * g.KXP + col] = mk<cplx<T>>((T)in[2 * f], (T)in[2 * f + 1]);
         }
   CK(cudaMemcpyAsync(ctx->spec, S.data(), S.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice, ctx->stream));
-  k_z_pass<T, true><<<ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z3, ctx->stream>>>(
-      (cplx<T>*)ctx->spec, g, ctx->pz, (const cplx<T>*)ctx->twz, 3, ctx->zt);
-  CKL();
-  int rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 3);
+  int rc = launch_z_pass<T, true>(ctx);
+  if (rc) return rc;
+  rc = launch_xy_inv<T>(ctx, (const cplx<T>*)ctx->spec, (T*)ctx->rwork, 3);
   if (rc) return rc;
   rc = get_field<T>(ctx, out, ctx->rwork);
   if (rc) return rc;
@@ -1176,7 +1310,25 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
     const size_t x = i % (size_t)g.Lx, y = (i / (size_t)g.Lx) % (size_t)g.Ly, z = i / ((size_t)g.Lx * g.Ly);
     return x + nxp * (y + nyp * z);
   };
+  // The step graphs (and any batch graph, through gen) hold the current
+  // table pointers as kernel arguments: drop them before the first buffer is
+  // freed, so that no early return below leaves a graph pointing at freed
+  // memory.  From the first replacement until the call succeeds the context
+  // refuses work (ensure_ready), since its tables may be half replaced.
+  CK(cudaStreamSynchronize(ctx->stream));
+  ++ctx->gen;
+  for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
+    if (*gx) {
+      cudaGraphExecDestroy(*gx);
+      *gx = nullptr;
+    }
+  ctx->force_fresh = false;
+  ctx->np_ready = false;
+  ctx->flo_valid = false;
+  bool replaced = false;
   auto replace = [&](void** dst, auto vec) -> int {
+    replaced = true;
+    ctx->broken = true;
     if (*dst) cudaFree(*dst);
     *dst = nullptr;
     return upload(ctx, dst, vec);
@@ -1247,15 +1399,7 @@ int upload_sites_impl(fg_ctx* ctx, const double* zstar, const double* minv, cons
     ctx->ph_host.E_on = 1;  // a .localfield clears E_field_always_zero (initialize_E_field.F:21)
   }
   CK(cudaMemcpy(ctx->ph, &ctx->ph_host, sizeof(Phys), cudaMemcpyHostToDevice));
-  // the step graphs hold the old table pointers as kernel arguments
-  ++ctx->gen;
-  for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
-    if (*gx) {
-      cudaGraphExecDestroy(*gx);
-      *gx = nullptr;
-    }
-  ctx->force_fresh = false;
-  ctx->np_ready = false;
+  if (replaced) ctx->broken = false;
   return FG_OK;
 }
 
@@ -1280,6 +1424,7 @@ int force_now(fg_ctx* ctx) {
   int rc = run_graph(ctx, &ctx->g_force, 0);
   if (rc) return rc;
   ctx->force_fresh = true;
+  ctx->flo_valid = ctx->prec == FG_PREC_MIXED;
   ctx->np_ready = false;
   return FG_OK;
 }
@@ -1396,7 +1541,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (ctx->g_lf) cudaGraphExecDestroy(ctx->g_lf);
   if (ctx->g_vs) cudaGraphExecDestroy(ctx->g_vs);
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
-  void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
+  void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->Flo, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->ltab, ctx->revx,
                   ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
@@ -1482,6 +1627,15 @@ int fg_fft_c2r3(fg_ctx* ctx, const double* in, double* out) {
   return ctx->prec == FG_PREC_MIXED ? fft_c2r3_impl<float>(ctx, in, out) : fft_c2r3_impl<double>(ctx, in, out);
 }
 
+int fg_time_fft(fg_ctx* ctx, int reps, double* ms) {
+  if (!ctx || !ctx->stream || !ms || reps < 1) return FG_ERR_ARG;
+  if (ctx->broken) return fail(ctx, FG_ERR_CUDA, "a device buffer could not be reallocated: destroy this context");
+  ctx->err.clear();
+  // only the spectrum and real-space scratch (components 0..2) change, as in
+  // fg_fft_r2c3 / fg_fft_c2r3: u, p, dVddi and the scalars stand
+  return ctx->prec == FG_PREC_MIXED ? time_fft_impl<float>(ctx, reps, ms) : time_fft_impl<double>(ctx, reps, ms);
+}
+
 int fg_set_state(fg_ctx* ctx, const double* dipoR, const double* dipoP, double s, double pi, double H0) {
   if (!ctx || !ctx->stream) return FG_ERR_ARG;
   int rc;
@@ -1516,6 +1670,72 @@ int fg_set_thermostat(fg_ctx* ctx, double s, double pi, double H0) {
   return push_scalars(ctx);
 }
 
+int fg_get_params(const fg_ctx* ctx, fg_params* p) {
+  if (!ctx || !p) return FG_ERR_ARG;
+  *p = ctx->P;
+  return FG_OK;
+}
+
+// The next point of a temperature (or field) sweep, started from the state
+// on the device as the reference's sweep scripts start each point from the
+// previous point's final .coord read back as .restart (cooling.sh:64-69):
+// the .coord holds dipoP / s_Nose (coord_module.F:476), initialize_dipoR
+// reads it (initialize-dipoR.F:22-38), evaluates the force and sets s = 1,
+// pi = 0 (:62-68), and molecular_dynamics sets H0 from that state
+// (molecular-dynamics.F:52-55).  Here nothing leaves the device and nothing
+// is rounded to the .coord's fixed-point columns.
+int fg_chain_point(fg_ctx* ctx, double kelvin, const double E[3], fg_energy* e) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (ctx->P.method != FG_METHOD_MD)
+    return fail(ctx, FG_ERR_UNSUPPORTED, "fg_chain_point continues Nose-Poincare ('md') runs only");
+  if (!(kelvin > 0.0)) return fail(ctx, FG_ERR_ARG, "kelvin must be positive");
+  // the new point's temperature (read_Param's kelvin tag, param_module.F:226,
+  // and make_Param, :468)
+  fg_params q = ctx->P;
+  q.kelvin = kelvin;
+  char eb[128];
+  if ((rc = fg_make_param(&q, eb, sizeof(eb)))) return fail(ctx, rc, eb);
+  if ((rc = pull_scalars(ctx))) return rc;
+  const double s_old = ctx->sc_host->s;
+  ctx->P = q;
+  Phys& h = ctx->ph_host;
+  h.nf_kT = (double)q.n_freedom * q.temperature_eV;
+  h.threeN_kT = (double)(3 * (long long)q.N) * q.temperature_eV;
+  h.target_ke = q.target_kinetic_energy;
+  CK(cudaMemcpyAsync(ctx->ph, &h, sizeof(Phys), cudaMemcpyHostToDevice, ctx->stream));
+  // p <- p / s (the dipole momenta only; write_system writes acouP as is)
+  ctx->sc_host->vs_scale = 1.0 / s_old;
+  ctx->sc_host->s = 1.0;
+  ctx->sc_host->pi = 0.0;
+  ctx->sc_host->H0 = 0.0;
+  ctx->sc_host->kick_coef = ctx->P.dt_2;
+  if (E)
+    for (int a = 0; a < 3; ++a) ctx->sc_host->E[a] = E[a];
+  if ((rc = push_scalars(ctx))) return rc;
+  const long long n3 = 3 * ctx->g.nsite;
+  if (ctx->prec == FG_PREC_MIXED)
+    k_scale<float><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((float*)ctx->p, &ctx->sc->vs_scale, n3);
+  else
+    k_scale<double><<<ctx->grid_elem, kThreadsElem, 0, ctx->stream>>>((double*)ctx->p, &ctx->sc->vs_scale, n3);
+  CKL();
+  // initialize_dipoR's tail: the force of the state, s = 1, pi = 0, KE
+  fg_energy en{};
+  if ((rc = fg_mirror_force_mirror(ctx, &en))) return rc;
+  double ke = 0.0;
+  if ((rc = fg_kinetic_energy_dipo(ctx, &ke))) return rc;
+  en.dipo_kinetic = ke;
+  en.acou_kinetic = 0.0;
+  // molecular-dynamics.F:52-55 with s = 1: H0 is the total energy
+  const double V = en.short_range + en.long_range + en.dipole_E_field + en.unharmonic + en.homo_strain +
+                   en.homo_coupling + en.inho_strain + en.inho_coupling + en.inho_modulation;
+  en.total = ke + V;
+  if ((rc = fg_set_thermostat(ctx, 1.0, 0.0, en.total))) return rc;
+  en.H_Nose_Poincare = 0.0;
+  if (e) *e = en;
+  return FG_OK;
+}
+
 int fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi, double strain[6], double* s, double* pi,
                  double* H0) {
   if (!ctx || !ctx->stream) return FG_ERR_ARG;
@@ -1523,7 +1743,11 @@ int fg_get_state(fg_ctx* ctx, double* dipoR, double* dipoP, double* dVddi, doubl
   const bool f32 = ctx->prec == FG_PREC_MIXED;
   if (dipoR && (rc = f32 ? get_field<float>(ctx, dipoR, ctx->u) : get_field<double>(ctx, dipoR, ctx->u))) return rc;
   if (dipoP && (rc = f32 ? get_field<float>(ctx, dipoP, ctx->p) : get_field<double>(ctx, dipoP, ctx->p))) return rc;
-  if (dVddi && (rc = f32 ? get_field<float>(ctx, dVddi, ctx->F) : get_field<double>(ctx, dVddi, ctx->F))) return rc;
+  if (dVddi) {
+    if (f32 && ctx->flo_valid) rc = get_field2<float>(ctx, dVddi, ctx->F, ctx->Flo);
+    else rc = f32 ? get_field<float>(ctx, dVddi, ctx->F) : get_field<double>(ctx, dVddi, ctx->F);
+    if (rc) return rc;
+  }
   if ((rc = pull_scalars(ctx))) return rc;
   if (strain)
     for (int i = 0; i < 6; ++i) strain[i] = ctx->sc_host->strain[i];
@@ -1584,6 +1808,7 @@ int fg_get_acouK(fg_ctx* ctx, double* acouK) {
   if (rc) return rc;
   if ((rc = pull_scalars(ctx))) return rc;
   ctx->force_fresh = true;
+  ctx->flo_valid = false;
   ctx->np_ready = false;
   return ctx->prec == FG_PREC_MIXED ? get_acouK_impl<float>(ctx, acouK) : get_acouK_impl<double>(ctx, acouK);
 }
@@ -1598,6 +1823,38 @@ int fg_set_uniform_E(fg_ctx* ctx, const double E[3]) {
   // The stored dVddi and energies stay those of the last evaluation, as
   // c%dVddi does when molecular-dynamics.F:66-76 changes c%E_field between
   // steps: the next force evaluation sees the new field.
+  return FG_OK;
+}
+
+int fg_set_wave(fg_ctx* ctx, int on, int i_step) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  const fg_params& P = ctx->P;
+  if (on) {
+    const int t = P.E_wave_type;
+    if (t == FG_WAVE_TRIANGULAR_COS || t == FG_WAVE_TRIANGULAR_SIN) {
+      if (P.n_E_wave_period <= 0) return fail(ctx, FG_ERR_ARG, "n_E_wave_period must be positive");
+    } else if (t == FG_WAVE_RAMPING_ON || t == FG_WAVE_RAMPING_OFF) {
+      if (P.n_E_wave_period <= 0 || P.n_E_wave_period > P.n_thermalize)
+        return fail(ctx, FG_ERR_ARG, "period must be smaller than n_thermalize (wave_module.F:42-45)");
+    } else {
+      return fail(ctx, FG_ERR_ARG, "fg_set_wave needs an E_wave_type");
+    }
+    if (P.E_field_always_zero) return fail(ctx, FG_ERR_ARG, "E_field_always_zero is set: the field term is off");
+  }
+  int rc;
+  if ((rc = pull_scalars(ctx))) return rc;
+  ctx->sc_host->i_step = i_step;
+  if ((rc = push_scalars(ctx))) return rc;
+  if ((on != 0) != ctx->wave_dev) {
+    ctx->wave_dev = on != 0;
+    // the step graphs gain or lose their first kernel
+    ++ctx->gen;
+    for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
+      if (*gx) {
+        cudaGraphExecDestroy(*gx);
+        *gx = nullptr;
+      }
+  }
   return FG_OK;
 }
 
@@ -1616,6 +1873,7 @@ int fg_nose_poincare(fg_ctx* ctx, fg_energy* e) {
   if ((rc = np_ready_for_step(ctx))) return rc;
   if ((rc = run_graph(ctx, &ctx->g_np, 1))) return rc;
   ctx->np_ready = true;
+  ctx->flo_valid = false;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) energy_out(ctx->sc_host, e, false);
   return FG_OK;
@@ -1638,6 +1896,7 @@ int fg_leapfrog(fg_ctx* ctx, fg_energy* e, int i_step) {
     if ((rc = run_graph(ctx, &ctx->g_lf, 2))) return rc;
   }
   ctx->force_fresh = true;
+  ctx->flo_valid = false;
   ctx->np_ready = false;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) {
@@ -1653,6 +1912,7 @@ int fg_velocity_scaling(fg_ctx* ctx, fg_energy* e) {
   if (rc) return rc;
   if ((rc = run_graph(ctx, &ctx->g_vs, 3))) return rc;
   ctx->force_fresh = true;
+  ctx->flo_valid = false;
   ctx->np_ready = false;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) energy_out(ctx->sc_host, e, false);
@@ -1672,6 +1932,7 @@ int fg_run_steps(fg_ctx* ctx, int n_steps, fg_energy* e) {
   for (; i < n_steps; ++i)
     if ((rc = run_graph(ctx, gx, which))) return rc;
   ctx->force_fresh = true;
+  ctx->flo_valid = false;
   ctx->np_ready = ctx->P.method == FG_METHOD_MD;
   if ((rc = pull_scalars(ctx))) return rc;
   if (e) energy_out(ctx->sc_host, e, false);
@@ -1711,6 +1972,7 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
   cudaEventDestroy(e1);
   *ms = t;
   ctx->force_fresh = true;
+  ctx->flo_valid = false;
   ctx->np_ready = ctx->P.method == FG_METHOD_MD;
   return pull_scalars(ctx);
 }
@@ -1726,6 +1988,7 @@ int fg_profile_step(fg_ctx* ctx, int reps, double* ms) {
   rc = ctx->prec == FG_PREC_MIXED ? profile_impl<float>(ctx, reps, ms) : profile_impl<double>(ctx, reps, ms);
   if (rc) return rc;
   ctx->force_fresh = true;
+  ctx->flo_valid = false;
   ctx->np_ready = true;
   return pull_scalars(ctx);
 }
@@ -1850,8 +2113,8 @@ static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocDevice {
-  std::once_flag once;
-  cudaError_t status = cudaSuccess;
+  std::mutex mu;
+  bool ready = false;         // set-up done on this device (a failed one is retried)
   double* scratch = nullptr;  // device address of g_noalloc_scratch on this device
   int nsm = 0;
 };
@@ -1893,23 +2156,34 @@ extern "C" int fg_kinetic_energy_dipo_noalloc(const double* dipoP, int Lx, int L
   if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= kNoAllocMaxDevices)
     return noalloc_fail(errbuf, errlen, FG_ERR_UNSUPPORTED, "fg_kinetic_energy_dipo_noalloc: device index >= 64");
-  // one-time set-up on this device (it is current): the array's device address
+  // one-time set-up on this device (it is current): the array's device
+  // address.  Only a successful set-up is kept; after a failure (a transient
+  // error, or a call made while the device was not usable) the next call
+  // tries again.
   NoAllocDevice& d = g_noalloc_dev[dev];
-  std::call_once(d.once, [&d, dev]() {
-    void* ptr = nullptr;
-    d.status = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (d.status == cudaSuccess) d.status = cudaDeviceGetAttribute(&d.nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (d.status == cudaSuccess) d.scratch = static_cast<double*>(ptr);
-  });
-  if (d.status != cudaSuccess || !d.scratch) {
-    std::snprintf(msg, sizeof(msg), "fg_kinetic_energy_dipo_noalloc: set-up failed: %s",
-                  cudaGetErrorString(d.status));
-    return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, msg);
+  double* scratch = nullptr;
+  int nsm = 0;
+  {
+    std::lock_guard<std::mutex> lock(d.mu);
+    if (!d.ready) {
+      void* ptr = nullptr;
+      cudaError_t se = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (se == cudaSuccess) se = cudaDeviceGetAttribute(&d.nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (se != cudaSuccess || ptr == nullptr) {
+        std::snprintf(msg, sizeof(msg), "fg_kinetic_energy_dipo_noalloc: set-up failed: %s",
+                      cudaGetErrorString(se));
+        return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, msg);
+      }
+      d.scratch = static_cast<double*>(ptr);
+      d.ready = true;
+    }
+    scratch = d.scratch;
+    nsm = d.nsm;
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  double* part = d.scratch;
-  double* minv = d.scratch + kNoAllocMinv;
-  unsigned char* mask = reinterpret_cast<unsigned char*>(d.scratch + kNoAllocMask);
+  double* part = scratch;
+  double* minv = scratch + kNoAllocMinv;
+  unsigned char* mask = reinterpret_cast<unsigned char*>(scratch + kNoAllocMask);
   e = cudaMemcpyAsync(minv, layer_mass_inv, sizeof(double) * (size_t)Lz, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(mask, layer_sum_p, (size_t)Lz, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return noalloc_fail(errbuf, errlen, FG_ERR_CUDA, cudaGetErrorString(e));
@@ -1921,7 +2195,7 @@ extern "C" int fg_kinetic_energy_dipo_noalloc(const double* dipoP, int Lx, int L
   g.plane_r = plane;
   g.nsite = plane * Lz;
   const long long want = (g.nsite + kThreadsElem - 1) / kThreadsElem;
-  const int grid = (int)std::max(1LL, std::min({want, (long long)std::max(d.nsm, 1) * 8, (long long)kNoAllocPartials}));
+  const int grid = (int)std::max(1LL, std::min({want, (long long)std::max(nsm, 1) * 8, (long long)kNoAllocPartials}));
   k_ke_only<double><<<grid, kThreadsElem, 0, st>>>(dipoP, g, minv, mask, part);
   k_ke_finish_out<<<1, RED_THREADS, 0, st>>>(part, grid, (double)(counted * plane), (double)g.nsite, ke);
   e = cudaGetLastError();
@@ -2069,6 +2343,7 @@ int fg_batch_step(fg_batch* b, int n_steps, fg_energy* e) {
   for (size_t i = 0; i < b->ctx.size(); ++i) {
     fg_ctx* c = b->ctx[i];
     c->force_fresh = true;
+    c->flo_valid = false;
     c->np_ready = c->P.method == FG_METHOD_MD;
     if ((rc = pull_scalars(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
     if (e) energy_out(c->sc_host, &e[i], false);

@@ -62,6 +62,11 @@ struct Phys {
   double n_sum_p;
   int E_on;
   int modulation_on;
+  // per-step field of molecular-dynamics.F:66-76 evaluated on the device
+  // (fg_set_wave): wave(E_wave_type, i_step, n_thermalize, n_E_wave_period,
+  // external_E_field) of wave_module.F:8-67
+  int wave_type, wave_n_thermalize, wave_period, wave_pad;
+  double wave_amp[3];
 };
 
 struct DevScalars {
@@ -83,6 +88,7 @@ struct DevScalars {
   double pend_ke_sum, pend_ke, pend_pi, pend_s, pend_drift, pend_kick_f;
   double vs_scale;       // velocity scaling factor of the last vs step
   double vs_scale_acou;  // the same for the acoustic momenta
+  long long i_step;      // step counter of the device-side field schedule
   int status;
   int pad;
 };
@@ -240,7 +246,34 @@ enum { SRC_U9 = 0, SRC_FIELD = 1 };
 // 36-44).  SRC_FIELD: component c of src.
 // MC, LYC > 0 select the compile-time transforms for m = Lx/2 = MC and
 // Ly = LYC (launched with exactly kXYThreads threads); 0 = runtime plans.
+// The compile-time kernels run the y transforms on MC columns, not MC + 1:
+// the kx = 0 and kx = Lx/2 columns are real before the y pass (transforms of
+// real rows), so X(0) + i X(Lx/2) travels as one complex column and is split
+// by Hermitian symmetry after the pass (y_split); the inverse joins them the
+// same way before its y pass (y_join).  posm + m and posm + m + Ly hold the
+// y slot maps (slot -> ky, ky -> slot) that pair ky with -ky.
 constexpr int kXYThreads = 512;
+
+// Column kx = 0 after the forward y pass holds C = Y0 + i Ym, Y0 and Ym the
+// y spectra of the real kx = 0 and kx = Lx/2 columns: Y0(k) = (C(k) +
+// conj C(-k)) / 2, Ym(k) = (C(k) - conj C(-k)) / 2i.  a = C(k), b = C(-k).
+template <typename C>
+__device__ __forceinline__ void y_split(C a, C b, C& y0, C& ym) {
+  using R = decltype(a.x);
+  y0 = mk<C>((R)0.5 * (a.x + b.x), (R)0.5 * (a.y - b.y));
+  ym = mk<C>((R)0.5 * (a.y + b.y), (R)0.5 * (b.x - a.x));
+}
+// Inverse: C(k) = H0(k) + i Hm(k) with H(k) = (Y(k) + conj Y(-k)) / 2, the
+// Hermitian part, whose inverse transform is the real part of Y's (the
+// imaginary parts of the kx = 0 and kx = Lx/2 bins are dropped, as FFTW's
+// c2r does).  a0 = Y0(k), b0 = Y0(-k), am = Ym(k), bm = Ym(-k).
+template <typename C>
+__device__ __forceinline__ C y_join(C a0, C b0, C am, C bm) {
+  using R = decltype(a0.x);
+  const R h0x = (R)0.5 * (a0.x + b0.x), h0y = (R)0.5 * (a0.y - b0.y);
+  const R hmx = (R)0.5 * (am.x + bm.x), hmy = (R)0.5 * (am.y - bm.y);
+  return mk<C>(h0x - hmy, h0y + hmx);
+}
 
 template <typename T, int MC, int LYC>
 __device__ __forceinline__ void xy_twiddles_to_smem(cplx<T>* tm, cplx<T>* ty, cplx<T>* tx, const cplx<T>* twm,
@@ -347,8 +380,12 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
     cplx<T>* row = buf + y * RS;
     if (k == 0) {
       const cplx<T> z0 = row[0];
-      row[0] = mk<cplx<T>>(z0.x + z0.y, (T)0);
-      row[m] = mk<cplx<T>>(z0.x - z0.y, (T)0);
+      if constexpr (MC > 0) {
+        row[0] = mk<cplx<T>>(z0.x + z0.y, z0.x - z0.y);  // X(0) + i X(m)
+      } else {
+        row[0] = mk<cplx<T>>(z0.x + z0.y, (T)0);
+        row[m] = mk<cplx<T>>(z0.x - z0.y, (T)0);
+      }
     } else {
       const int k2 = m - k;
       const int s1 = __ldg(&posm[k]), s2 = __ldg(&posm[k2]);
@@ -368,13 +405,29 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
   __syncthreads();
   cplx<T>* dst = spec + (long long)(out_comp0 + c) * g.ncplx + (long long)z * g.plane_c;
   if constexpr (MC > 0) {
-    // y pass; its last stage writes the spectrum rows directly
+    // y pass over the MC columns (kx = Lx/2 rides in column 0); its last
+    // stage writes the spectrum rows directly, except column 0, which stays
+    // in shared memory for the Hermitian split
     constexpr int NSY = ct_nst(LYC);
-    ct_forward_range<T, LYC, 0, NSY - 1, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+    ct_forward_range<T, LYC, 0, NSY - 1, kXYThreads, BatchCT<MC, MC, 1, 0, MC + 1>>(buf, tws_y);
     const long long kxp = g.KXP;
     auto ld = [&](int col, int e) { return buf[col + e * (MC + 1)]; };
-    auto st = [&](int col, int e, const cplx<T>& v) { dst[(long long)e * kxp + col] = v; };
-    ct_stage_io<T, LYC, NSY - 1, false, kXYThreads, MC + 1, false>(ld, st, tws_y);
+    auto st = [&](int col, int e, const cplx<T>& v) {
+      if (col == 0) buf[e * (MC + 1)] = v;
+      else dst[(long long)e * kxp + col] = v;
+    };
+    ct_stage_io<T, LYC, NSY - 1, false, kXYThreads, MC, false>(ld, st, tws_y);
+    __syncthreads();
+    const int* revy = posm + MC;
+    const int* posy = posm + MC + LYC;
+    for (int sl = threadIdx.x; sl < LYC; sl += kXYThreads) {
+      const int ky = __ldg(&revy[sl]);
+      const int sp = __ldg(&posy[(LYC - ky) % LYC]);
+      cplx<T> y0, ym;
+      y_split(buf[sl * (MC + 1)], buf[sp * (MC + 1)], y0, ym);
+      dst[(long long)sl * kxp] = y0;
+      dst[(long long)sl * kxp + MC] = ym;
+    }
   } else {
     Batch B{RS, RS, 1, 0, RS, true};
     fft_forward<T>(buf, B, py, twy, buf_len);
@@ -432,10 +485,18 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
         return *a;
       }
     };
+    // column 0 carries the kx = 0 and kx = Lx/2 columns joined (y_join)
+    const int* revy = posm + MC;
+    const int* posy = posm + MC + LYC;
+    auto ldj = [&](int col, int e) {
+      if (col != 0) return ld(col, e);
+      const int sp = __ldg(&posy[(LYC - __ldg(&revy[e])) % LYC]);
+      return y_join(ld(0, e), ld(0, sp), ld(MC, e), ld(MC, sp));
+    };
     auto st = [&](int col, int e, const cplx<T>& v) { buf[col + e * (MC + 1)] = v; };
-    ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, MC + 1, false>(ld, st, tws_y);
+    ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, MC, false>(ldj, st, tws_y);
     __syncthreads();
-    ct_inverse_range<T, LYC, NSY - 2, -1, kXYThreads, BatchCT<MC + 1, MC + 1, 1, 0, MC + 1>>(buf, tws_y);
+    ct_inverse_range<T, LYC, NSY - 2, -1, kXYThreads, BatchCT<MC, MC, 1, 0, MC + 1>>(buf, tws_y);
   } else {
     for (int idx = threadIdx.x; idx < Ly * RS; idx += blockDim.x) {
       const int y = idx / RS, col = idx - y * RS;
@@ -452,7 +513,8 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
     const int k = idx / Ly, y = idx - k * Ly;
     cplx<T>* row = buf + y * RS;
     if (k == 0) {
-      const T X0 = row[0].x, Xm = row[m].x;
+      // compile-time kernels: x(kx = Lx/2) came back as the imaginary part
+      const T X0 = row[0].x, Xm = MC > 0 ? row[0].y : row[m].x;
       row[0] = mk<cplx<T>>(X0 + Xm, X0 - Xm);
     } else {
       const int k2 = m - k;
@@ -796,17 +858,29 @@ struct KMaps {
 };
 
 // Plain z pass of nc spectra in place: DIF (INV = false) or DIT (INV = true).
-template <typename T, bool INV>
+// LZC, CWC, NCC > 0: compile-time transforms for Lz = LZC, tile width CWC
+// and NCC components (launched with exactly kZThreads threads); 0 = runtime.
+template <typename T, bool INV, int LZC = 0, int CWC = 0, int NCC = 0>
 __global__ void __launch_bounds__(256) k_z_pass(cplx<T>* __restrict__ spec, Geom g, FftPlan pz,
                                                 const cplx<T>* __restrict__ twz, int nc, ZTiles zt) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
-  const int CW = zt.CW;
-  z_tile_load<T>(buf, spec, g, zt, nc);
-  Batch B{nc * CW, CW, 1, g.Lz * CW, CW, true};
-  if (INV) fft_inverse<T>(buf, B, pz, twz, nc * g.Lz * CW);
-  else fft_forward<T>(buf, B, pz, twz, nc * g.Lz * CW);
-  z_tile_store<T>(buf, spec, g, zt, nc);
+  if constexpr (LZC > 0) {
+    __shared__ cplx<T> tws[LZC];
+    for (int i = threadIdx.x; i < LZC; i += blockDim.x) tws[i] = twz[i];
+    z_tile_load<T, LZC, CWC>(buf, spec, g, zt, NCC);
+    using B = BatchCT<NCC * CWC, CWC, 1, LZC * CWC, CWC>;
+    if (INV) ct_inverse<T, LZC, 256, B>(buf, tws);
+    else ct_forward<T, LZC, 256, B>(buf, tws);
+    z_tile_store<T, LZC, CWC>(buf, spec, g, zt, NCC);
+  } else {
+    const int CW = zt.CW;
+    z_tile_load<T>(buf, spec, g, zt, nc);
+    Batch B{nc * CW, CW, 1, g.Lz * CW, CW, true};
+    if (INV) fft_inverse<T>(buf, B, pz, twz, nc * g.Lz * CW);
+    else fft_forward<T>(buf, B, pz, twz, nc * g.Lz * CW);
+    z_tile_store<T>(buf, spec, g, zt, nc);
+  }
 }
 
 // ------------------------------------------------------------------ k_z_kspace
@@ -1192,55 +1266,74 @@ __device__ __forceinline__ V16<T> ldv_first(const T* p, unsigned long long pol) 
 template <typename T>
 __device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V16<T>*>(p) = a; }
 
-template <typename T>
+// Constants of the site force, in FP64 for both precisions: the mixed path
+// reads FP32 u, the FP32 dipole-dipole force and the FP32 eta, and sums the
+// on-site polynomial, the field and both strain couplings in FP64.  Those
+// local terms carry the largest forces (|F| up to ~30x the rms force on the
+// tail sites of a sigma = 0.1 A configuration), so evaluating them in FP32
+// would put their rounding (~1e-6 of the rms force) on exactly those sites.
 struct AsmConst {
-  T fa2g, tg, sk, tk2, fk, k4x8;  // anharmonic force constants
-  T hx, hy, h4;                   // homogeneous_coupling_2: B1xx/2, B1yy/2, B4yz
-  T wh[6];                        // strain . B2
-  T Zs, E0, E1, E2;
-  T Pa, Pg, P1, P2, P3, P4;       // energy coefficients (dVddi-unharmonic.F:67-99)
+  double fa2g, tg, sk, tk2, fk, k4x8;  // anharmonic force constants
+  double hx, hy, h4;                   // homogeneous_coupling_2: B1xx/2, B1yy/2, B4yz
+  double Zs;
+  double Pa, Pg, P1, P2, P3, P4;       // energy coefficients (dVddi-unharmonic.F:67-99)
   int E_on;
+  int pad;
+};
+// Per-step values of the site force, read from DevScalars: strain . B2 and
+// the uniform field.
+struct AsmDyn {
+  double wh[6];
+  double E0, E1, E2;
 };
 
-// Force on one site from F_dd, u and eta (see k_assemble); acc += energies
-// (the site's terms in T, FP32 in the mixed path, summed in FP64).
-template <typename T>
-__device__ __forceinline__ void assemble_site(const AsmConst<T>& k, T ux, T uy, T uz, T f0, T f1, T f2,
-                                              const T* eta, T& o0, T& o1, T& o2, double* acc) {
-  const T d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
-  const T uu = d0 + d1 + d2;
+// Force on one site from F_dd, u and eta (see k_assemble); acc += energies.
+__device__ __forceinline__ void assemble_site(const AsmConst& k, const AsmDyn& dy, double ux, double uy, double uz,
+                                              double f0, double f1, double f2, const double* eta, double& o0,
+                                              double& o1, double& o2, double* acc) {
+  const double d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
+  const double uu = d0 + d1 + d2;
   // 4th order
   f0 = f0 + ux * (k.fa2g * uu - k.tg * d0);
   f1 = f1 + uy * (k.fa2g * uu - k.tg * d1);
   f2 = f2 + uz * (k.fa2g * uu - k.tg * d2);
   // 6th and 8th order
-  const T uu2 = uu * uu, uu3 = uu2 * uu;
+  const double uu2 = uu * uu, uu3 = uu2 * uu;
   f0 = f0 + ux * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d0 * d0) - k.fk * d1 * d2);
   f1 = f1 + uy * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d1 * d1) - k.fk * d2 * d0);
   f2 = f2 + uz * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d2 * d2) - k.fk * d0 * d1);
-  acc[0] += (double)(k.Pa * uu2 + k.Pg * (d0 * d1 + d1 * d2 + d2 * d0) + k.P1 * uu3 +
-                     k.P2 * ((d0 * d0) * (d1 + d2) + (d1 * d1) * (d2 + d0) + (d2 * d2) * (d0 + d1)) +
-                     k.P3 * d0 * d1 * d2 + k.P4 * (uu2 * uu2));
+  acc[0] += k.Pa * uu2 + k.Pg * (d0 * d1 + d1 * d2 + d2 * d0) + k.P1 * uu3 +
+            k.P2 * ((d0 * d0) * (d1 + d2) + (d1 * d1) * (d2 + d0) + (d2 * d2) * (d0 + d1)) + k.P3 * d0 * d1 * d2 +
+            k.P4 * (uu2 * uu2);
   if (k.E_on) {
-    f0 = f0 - k.Zs * k.E0;
-    f1 = f1 - k.Zs * k.E1;
-    f2 = f2 - k.Zs * k.E2;
-    acc[1] += (double)(k.Zs * (ux * k.E0 + uy * k.E1 + uz * k.E2));
+    f0 = f0 - k.Zs * dy.E0;
+    f1 = f1 - k.Zs * dy.E1;
+    f2 = f2 - k.Zs * dy.E2;
+    acc[1] += k.Zs * (ux * dy.E0 + uy * dy.E1 + uz * dy.E2);
   }
   // homogeneous strain coupling
-  f0 = f0 + 2 * k.wh[0] * ux + k.wh[4] * uz + k.wh[5] * uy;
-  f1 = f1 + 2 * k.wh[1] * uy + k.wh[3] * uz + k.wh[5] * ux;
-  f2 = f2 + 2 * k.wh[2] * uz + k.wh[3] * uy + k.wh[4] * ux;
+  f0 = f0 + 2 * dy.wh[0] * ux + dy.wh[4] * uz + dy.wh[5] * uy;
+  f1 = f1 + 2 * dy.wh[1] * uy + dy.wh[3] * uz + dy.wh[5] * ux;
+  f2 = f2 + 2 * dy.wh[2] * uz + dy.wh[3] * uy + dy.wh[4] * ux;
   // inhomogeneous strain coupling, w_q = sum_j eta_j B2(j, q) with the
   // sparsity of homogeneous_coupling_2 (eta already carries 1/N)
-  const T w0 = k.hx * eta[0] + k.hy * (eta[1] + eta[2]);
-  const T w1 = k.hx * eta[1] + k.hy * (eta[0] + eta[2]);
-  const T w2 = k.hx * eta[2] + k.hy * (eta[0] + eta[1]);
-  const T w3 = k.h4 * eta[3], w4 = k.h4 * eta[4], w5 = k.h4 * eta[5];
+  const double w0 = k.hx * eta[0] + k.hy * (eta[1] + eta[2]);
+  const double w1 = k.hx * eta[1] + k.hy * (eta[0] + eta[2]);
+  const double w2 = k.hx * eta[2] + k.hy * (eta[0] + eta[1]);
+  const double w3 = k.h4 * eta[3], w4 = k.h4 * eta[4], w5 = k.h4 * eta[5];
   o0 = f0 + 2 * w0 * ux + w4 * uz + w5 * uy;
   o1 = f1 + 2 * w1 * uy + w3 * uz + w5 * ux;
   o2 = f2 + 2 * w2 * uz + w3 * uy + w4 * ux;
 }
+
+// The force of one site in the field type T.  The mixed path (T = float)
+// rounds the FP64 sum once; with lo != null it also stores the rounding
+// residual, so that hi + lo carries the FP64 force to ~2^-48 for a caller
+// that reads dVddi, while the integrators consume hi.
+template <typename T>
+__device__ __forceinline__ T force_hi(double o) { return (T)o; }
+template <typename T>
+__device__ __forceinline__ T force_lo(double o, T hi) { return sizeof(T) == 4 ? (T)(o - (double)hi) : (T)0; }
 
 // Masked kinetic sums of the closing kick (35f) of one site: p <- p - c F
 // and p^2/m, p.F/m, F^2/m in T, added to ke (FP64) when the site counts.
@@ -1263,14 +1356,17 @@ __device__ __forceinline__ void close_site(T* __restrict__ p, long long ns, long
 // p^2/m, p.F/m, F^2/m of the new p in part_ke; the last block finishes the
 // force (energies, commit of the prepared half step, (35e)) and the step
 // (np_close_tail: KE, H_NP and (38) of the next step).
+// Flo (mixed path, may be null): the FP32 residual of each force component,
+// F + Flo = the FP64 site sum.
 template <typename T, bool CLOSE = false>
-__global__ void __launch_bounds__(256, (sizeof(T) == 4 && !CLOSE) ? 3 : 2)
+__global__ void __launch_bounds__(256, 2)
     k_assemble(const T* __restrict__ rw, const T* __restrict__ u, T* __restrict__ F, Geom g,
                const Phys* __restrict__ ph, DevScalars* sc, double* __restrict__ part, int tail, unsigned int* done,
                const unsigned char* __restrict__ site_species, const T* __restrict__ site_zstar,
                const T* __restrict__ site_E, int zl0, T* __restrict__ p, const double* __restrict__ layer_minv,
                const unsigned char* __restrict__ layer_sump, const T* __restrict__ site_minv,
-               const unsigned char* __restrict__ site_sump, double* __restrict__ part_ke) {
+               const unsigned char* __restrict__ site_sump, double* __restrict__ part_ke, T* __restrict__ Flo,
+               const AsmConst k) {
   pdl_enter();
   // site_*: per-site species (.relaxor), Z* and local field (.localfield);
   // they take the scalar loop.  zl0 > 0: rw components zl0..zl0+2 hold the
@@ -1282,16 +1378,12 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && !CLOSE) ? 3 : 2)
   const T cf = CLOSE ? (T)__ldcg(&sc->pend_kick_f) : (T)0;
   double ke[3] = {0.0, 0.0, 0.0};
   const unsigned long long pol_rw = l2_evict_first();
-  AsmConst<T> k;
-  k.fa2g = (T)ph->fa2g; k.tg = (T)ph->tg; k.sk = (T)ph->sk; k.tk2 = (T)ph->tk2; k.fk = (T)ph->fk;
-  k.k4x8 = (T)(8 * ph->P_k4);
-  k.hx = (T)ph->HC2[0][0]; k.hy = (T)ph->HC2[0][1]; k.h4 = (T)ph->HC2[3][3];
+  // k: the static constants (kernel parameter, built by asm_const on the
+  // host); dy: this step's strain coupling and field
+  AsmDyn dy;
 #pragma unroll
-  for (int i = 0; i < 6; ++i) k.wh[i] = (T)sc->w_hom[i];
-  k.Zs = (T)ph->Zstar; k.E0 = (T)sc->E[0]; k.E1 = (T)sc->E[1]; k.E2 = (T)sc->E[2];
-  k.Pa = (T)ph->P_alpha; k.Pg = (T)ph->P_gamma; k.P1 = (T)ph->P_k1; k.P2 = (T)ph->P_k2; k.P3 = (T)ph->P_k3;
-  k.P4 = (T)ph->P_k4;
-  k.E_on = ph->E_on;
+  for (int i = 0; i < 6; ++i) dy.wh[i] = sc->w_hom[i];
+  dy.E0 = sc->E[0]; dy.E1 = sc->E[1]; dy.E2 = sc->E[2];
   double acc[NQ_R] = {0.0, 0.0};
   constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -1299,45 +1391,52 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && !CLOSE) ? 3 : 2)
                      (CLOSE && (site_minv != nullptr || site_sump != nullptr));
   if (sites) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-      AsmConst<T> ks = k;
+      AsmConst ks = k;
+      AsmDyn dys = dy;
       double dk2 = 0.0;
       if (site_species) {
         const Phys::Species& q = ph->sp[site_species[i]];
-        ks.fa2g = (T)q.fa2g; ks.tg = (T)q.tg; ks.sk = (T)q.sk; ks.tk2 = (T)q.tk2; ks.fk = (T)q.fk; ks.k4x8 = (T)q.k4x8;
-        ks.Pa = (T)q.Pa; ks.Pg = (T)q.Pg; ks.P1 = (T)q.P1; ks.P2 = (T)q.P2; ks.P3 = (T)q.P3; ks.P4 = (T)q.P4;
+        ks.fa2g = q.fa2g; ks.tg = q.tg; ks.sk = q.sk; ks.tk2 = q.tk2; ks.fk = q.fk; ks.k4x8 = q.k4x8;
+        ks.Pa = q.Pa; ks.Pg = q.Pg; ks.P1 = q.P1; ks.P2 = q.P2; ks.P3 = q.P3; ks.P4 = q.P4;
         dk2 = q.dk2;
       }
-      if (site_zstar) ks.Zs = site_zstar[i];
+      if (site_zstar) ks.Zs = (double)site_zstar[i];
       if (site_E) {
-        ks.E0 = (T)(sc->E[0] + (double)site_E[i]);
-        ks.E1 = (T)(sc->E[1] + (double)site_E[ns + i]);
-        ks.E2 = (T)(sc->E[2] + (double)site_E[2 * ns + i]);
+        dys.E0 = dy.E0 + (double)site_E[i];
+        dys.E1 = dy.E1 + (double)site_E[ns + i];
+        dys.E2 = dy.E2 + (double)site_E[2 * ns + i];
       }
-      T eta[6];
+      double eta[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
-      const T ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
-      T f0 = rw[i], f1 = rw[ns + i], f2 = rw[2 * ns + i];
+      for (int q = 0; q < 6; ++q) eta[q] = (double)rw[(3 + q) * ns + i];
+      const double ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
+      double f0 = rw[i], f1 = rw[ns + i], f2 = rw[2 * ns + i];
       if (zl0 > 0) {
-        f0 = f0 + ks.Zs * rw[(zl0 + 0) * ns + i];
-        f1 = f1 + ks.Zs * rw[(zl0 + 1) * ns + i];
-        f2 = f2 + ks.Zs * rw[(zl0 + 2) * ns + i];
+        f0 = f0 + ks.Zs * (double)rw[(zl0 + 0) * ns + i];
+        f1 = f1 + ks.Zs * (double)rw[(zl0 + 1) * ns + i];
+        f2 = f2 + ks.Zs * (double)rw[(zl0 + 2) * ns + i];
       }
-      T o0, o1, o2;
-      assemble_site(ks, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
+      double o0, o1, o2;
+      assemble_site(ks, dys, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
       if (dk2 != 0.0) {  // kappa2(s) - kappa2(1) (dVddi-unharmonic.F:40,73)
-        const T t = (T)(2 * dk2);
+        const double t = 2 * dk2;
         o0 = o0 + t * ux;
         o1 = o1 + t * uy;
         o2 = o2 + t * uz;
-        acc[0] += dk2 * ((double)ux * ux + (double)uy * uy + (double)uz * uz);
+        acc[0] += dk2 * (ux * ux + uy * uy + uz * uz);
       }
-      F[i] = o0;
-      F[ns + i] = o1;
-      F[2 * ns + i] = o2;
+      const T h0 = force_hi<T>(o0), h1 = force_hi<T>(o1), h2 = force_hi<T>(o2);
+      F[i] = h0;
+      F[ns + i] = h1;
+      F[2 * ns + i] = h2;
+      if (Flo) {
+        Flo[i] = force_lo<T>(o0, h0);
+        Flo[ns + i] = force_lo<T>(o1, h1);
+        Flo[2 * ns + i] = force_lo<T>(o2, h2);
+      }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
-        close_site(p, ns, i, cf, o0, o1, o2, site_sump ? site_sump[i] != 0 : layer_sump[z] != 0,
+        close_site(p, ns, i, cf, h0, h1, h2, site_sump ? site_sump[i] != 0 : layer_sump[z] != 0,
                    site_minv ? (double)site_minv[i] : layer_minv[z], ke);
       }
     }
@@ -1351,15 +1450,27 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && !CLOSE) ? 3 : 2)
       V16<T> e[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) e[q] = ldv_first(rw + (3 + q) * ns + i, pol_rw);
-      V16<T> o0, o1, o2;
+      V16<T> o0, o1, o2, l0, l1, l2;
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
-        const T eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
-        assemble_site(k, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, o0.v[l], o1.v[l], o2.v[l], acc);
+        const double eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
+        double d0, d1, d2;
+        assemble_site(k, dy, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, d0, d1, d2, acc);
+        o0.v[l] = force_hi<T>(d0);
+        o1.v[l] = force_hi<T>(d1);
+        o2.v[l] = force_hi<T>(d2);
+        l0.v[l] = force_lo<T>(d0, o0.v[l]);
+        l1.v[l] = force_lo<T>(d1, o1.v[l]);
+        l2.v[l] = force_lo<T>(d2, o2.v[l]);
       }
       stv(F + i, o0);
       stv(F + ns + i, o1);
       stv(F + 2 * ns + i, o2);
+      if (Flo) {
+        stv(Flo + i, l0);
+        stv(Flo + ns + i, l1);
+        stv(Flo + 2 * ns + i, l2);
+      }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
         V16<T> q[3] = {ldv(p + i), ldv(p + ns + i), ldv(p + 2 * ns + i)};
@@ -1387,17 +1498,23 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && !CLOSE) ? 3 : 2)
     }
   } else {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-      T eta[6];
+      double eta[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) eta[q] = rw[(3 + q) * ns + i];
-      T o0, o1, o2;
-      assemble_site(k, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
-      F[i] = o0;
-      F[ns + i] = o1;
-      F[2 * ns + i] = o2;
+      for (int q = 0; q < 6; ++q) eta[q] = (double)rw[(3 + q) * ns + i];
+      double o0, o1, o2;
+      assemble_site(k, dy, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
+      const T h0 = force_hi<T>(o0), h1 = force_hi<T>(o1), h2 = force_hi<T>(o2);
+      F[i] = h0;
+      F[ns + i] = h1;
+      F[2 * ns + i] = h2;
+      if (Flo) {
+        Flo[i] = force_lo<T>(o0, h0);
+        Flo[ns + i] = force_lo<T>(o1, h1);
+        Flo[2 * ns + i] = force_lo<T>(o2, h2);
+      }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
-        close_site(p, ns, i, cf, o0, o1, o2, layer_sump[z] != 0, layer_minv[z], ke);
+        close_site(p, ns, i, cf, h0, h1, h2, layer_sump[z] != 0, layer_minv[z], ke);
       }
     }
   }
@@ -1544,6 +1661,45 @@ __global__ void __launch_bounds__(256) k_scale(T* __restrict__ p, const double* 
 // p <- p - kick_coef F and the drift (35c) u <- u + drift p m^-1
 // (nose-poincare.F:24-53).  Both coefficients come from the previous closing
 // tail, which already solved (38) with the kinetic energy of the kicked p.
+// wave (wave_module.F:8-67): the field added at step i_step.  The
+// triangular waves divide by period/4.0, a default-kind (single precision)
+// real in the reference, so the quarter period is rounded to float.
+__host__ __device__ inline void wave_field(int type, long long i_step, int n_thermalize, int period,
+                                           const double a[3], double out[3]) {
+  if (a[0] == 0.0 && a[1] == 0.0 && a[2] == 0.0) {
+    for (int k = 0; k < 3; ++k) out[k] = a[k];
+    return;
+  }
+  if (type == 1 || type == 2) {  // triangular_cos, triangular_sin
+    long long i = i_step - n_thermalize;
+    if (i < 0) i = 0;
+    const long long P = period;
+    const long long it = (type == 1) ? llabs(i % P - P / 2) - P / 4 : llabs((i + 3 * P / 4) % P - P / 2) - P / 4;
+    const double tmp = (double)it;
+    const float quarter = (float)period / 4.0f;
+    for (int k = 0; k < 3; ++k) out[k] = a[k] * tmp / (double)quarter;
+  } else if (type == 3 || type == 4) {  // ramping_on, ramping_off
+    for (int k = 0; k < 3; ++k) {
+      if (type == 3) out[k] = (i_step < period) ? a[k] * (double)i_step / period : a[k];
+      else out[k] = (i_step < period) ? a[k] * (double)(period - i_step) / period : 0.0;
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) out[k] = a[k];
+  }
+}
+
+// Start of a step under the device-side field schedule: the step counter
+// advances and the uniform field becomes that step's wave value
+// (molecular-dynamics.F:66-76, before the step's force evaluation).
+__global__ void k_wave_step(const Phys* __restrict__ ph, DevScalars* sc) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const long long i = sc->i_step + 1;
+  sc->i_step = i;
+  double E[3];
+  wave_field(ph->wave_type, i, ph->wave_n_thermalize, ph->wave_period, ph->wave_amp, E);
+  for (int k = 0; k < 3; ++k) sc->E[k] = E[k];
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __restrict__ u, const T* __restrict__ F,
                                                     const DevScalars* __restrict__ sc, Geom g,
@@ -1800,6 +1956,20 @@ __global__ void k_soa_to_fortran(double* __restrict__ dst, const T* __restrict__
     const int y = (int)(r % g.Ly), z = (int)(r / g.Ly);
     const long long s = (long long)nc * ((long long)x + (long long)NXP * ((long long)y + (long long)NYP * z));
     for (int c = 0; c < nc; ++c) dst[s + c] = (double)src[(long long)c * g.nsite + i];
+  }
+}
+
+// The same for a field held as a hi/lo pair (the mixed path's force after a
+// force evaluation that kept its FP32 residual): dst = hi + lo in FP64.
+template <typename T>
+__global__ void k_soa2_to_fortran(double* __restrict__ dst, const T* __restrict__ hi, const T* __restrict__ lo, Geom g,
+                                  int nc, int NXP, int NYP) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.nsite; i += (long long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % g.Lx);
+    const long long r = i / g.Lx;
+    const int y = (int)(r % g.Ly), z = (int)(r / g.Ly);
+    const long long s = (long long)nc * ((long long)x + (long long)NXP * ((long long)y + (long long)NYP * z));
+    for (int c = 0; c < nc; ++c) dst[s + c] = (double)hi[(long long)c * g.nsite + i] + (double)lo[(long long)c * g.nsite + i];
   }
 }
 

@@ -140,6 +140,63 @@ void write_avg(const std::string& fn, fg_params p, const fg_average& a_in, int n
 
 }  // namespace
 
+// write_system (coord_module.F:434-486): one line per site, ix iy iz,
+// dipoR, dipoP / s_Nose, dVddi, acouR, acouP.  full_precision = 0 writes the
+// reference's edit descriptors (i4,2i5,3f10.6,9e14.6,3f13.6); otherwise every
+// value gets 17 significant digits, which the .restart reader of
+// initialize_dipoR (initialize-dipoR.F:22-38, list-directed) and this
+// library's driver read back exactly.
+extern "C" int fg_write_coord(fg_ctx* ctx, const char* path, int full_precision) {
+  if (!ctx || !path) return FG_ERR_ARG;
+  fg_params p;
+  int r = fg_get_params(ctx, &p);
+  if (r) return r;
+  const int NXP = 2 * (p.Lx / 2 + 1), NYP = p.Ly + p.padding_y;
+  const size_t nfield = (size_t)3 * NXP * NYP * p.Lz;
+  const bool acoustic = p.mass_acou[0] > 0.0;
+  std::vector<double> R(nfield), P(nfield), F(nfield), A(nfield), K(nfield), AP(nfield, 0.0);
+  double ss = 1.0;
+  if ((r = fg_get_state(ctx, R.data(), P.data(), F.data(), nullptr, &ss, nullptr, nullptr))) return r;
+  double ascale = 1.0;
+  if (acoustic) {  // the dynamic acoustic field
+    if ((r = fg_get_acou(ctx, A.data(), AP.data(), nullptr))) return r;
+  } else {  // the relaxed acoustic displacement: acouR = c2r(-i acouK) / N
+    if ((r = fg_get_acouK(ctx, K.data()))) return r;
+    for (size_t k = 0; k < K.size(); k += 2) {
+      const double re = K[k], im = K[k + 1];
+      K[k] = im;
+      K[k + 1] = -re;
+    }
+    if ((r = fg_fft_c2r3(ctx, K.data(), A.data()))) return r;
+    ascale = p.Ninv;
+  }
+  std::FILE* f = std::fopen(path, "w");
+  if (!f) return FG_ERR_IO;
+  auto g = [](double v) {
+    char b[32];
+    std::snprintf(b, sizeof(b), " %.16e", v);
+    return std::string(b);
+  };
+  for (int iz = 0; iz < p.Lz; ++iz)
+    for (int iy = 0; iy < p.Ly; ++iy)
+      for (int ix = 0; ix < p.Lx; ++ix) {
+        const size_t o = 3 * ((size_t)ix + (size_t)NXP * ((size_t)iy + (size_t)NYP * iz));
+        std::string line;
+        char b[64];
+        std::snprintf(b, sizeof(b), "%4d%5d%5d", ix, iy, iz);
+        line += b;
+        for (int a = 0; a < 3; ++a) line += full_precision ? g(R[o + a]) : fF(R[o + a], 10, 6);
+        for (int a = 0; a < 3; ++a) line += full_precision ? g(P[o + a] / ss) : fE(P[o + a] / ss, 14, 6);
+        for (int a = 0; a < 3; ++a) line += full_precision ? g(F[o + a]) : fE(F[o + a], 14, 6);
+        for (int a = 0; a < 3; ++a) line += full_precision ? g(A[o + a] * ascale) : fE(A[o + a] * ascale, 14, 6);
+        for (int a = 0; a < 3; ++a) line += full_precision ? g(AP[o + a]) : fF(AP[o + a], 13, 6);
+        std::fprintf(f, "%s\n", line.c_str());
+      }
+  const bool ok = std::ferror(f) == 0;
+  std::fclose(f);
+  return ok ? FG_OK : FG_ERR_IO;
+}
+
 extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out, double* t_sim, char* errbuf,
                             int errlen) {
   fg_params p;
@@ -324,43 +381,7 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
     if (!coords) return FG_OK;
     std::string path = p.coord_directory[0] ? std::string(p.coord_directory) + "/" + fn : fn;
     if (path[0] != '/') path = dir_of(base) + path;
-    std::vector<double> R(nfield), P(nfield), F(nfield), A(nfield), K(nfield);
-    double ss = 1.0;
-    int r = fg_get_state(ctx, R.data(), P.data(), F.data(), nullptr, &ss, nullptr, nullptr);
-    if (r) return r;
-    std::vector<double> AP(nfield, 0.0);
-    double ascale = 1.0;
-    if (acoustic) {  // the dynamic acoustic field
-      if ((r = fg_get_acou(ctx, A.data(), AP.data(), nullptr))) return r;
-    } else {  // the relaxed acoustic displacement: acouR = c2r(-i acouK) / N
-      if ((r = fg_get_acouK(ctx, K.data()))) return r;
-      for (size_t k = 0; k < K.size(); k += 2) {
-        const double re = K[k], im = K[k + 1];
-        K[k] = im;
-        K[k + 1] = -re;
-      }
-      if ((r = fg_fft_c2r3(ctx, K.data(), A.data()))) return r;
-      ascale = p.Ninv;
-    }
-    std::FILE* f = std::fopen(path.c_str(), "w");
-    if (!f) return FG_ERR_IO;
-    for (int iz = 0; iz < p.Lz; ++iz)
-      for (int iy = 0; iy < p.Ly; ++iy)
-        for (int ix = 0; ix < p.Lx; ++ix) {
-          const size_t o = 3 * ((size_t)ix + (size_t)NXP * ((size_t)iy + (size_t)NYP * iz));
-          std::string line;
-          char b[64];
-          std::snprintf(b, sizeof(b), "%4d%5d%5d", ix, iy, iz);
-          line += b;
-          for (int a = 0; a < 3; ++a) line += fF(R[o + a], 10, 6);
-          for (int a = 0; a < 3; ++a) line += fE(P[o + a] / ss, 14, 6);
-          for (int a = 0; a < 3; ++a) line += fE(F[o + a], 14, 6);
-          for (int a = 0; a < 3; ++a) line += fE(A[o + a] * ascale, 14, 6);
-          for (int a = 0; a < 3; ++a) line += fF(AP[o + a], 13, 6);
-          std::fprintf(f, "%s\n", line.c_str());
-        }
-    std::fclose(f);
-    return FG_OK;
+    return fg_write_coord(ctx, path.c_str(), 0);
   };
   char step_fn[64];
   auto numbered = [&](int i_step) {

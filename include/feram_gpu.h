@@ -214,6 +214,14 @@ int  fg_fft_r2c3(fg_ctx* ctx, const double* in, double* out);
    bins are ignored as by FFTW's half-complex convention.  in is not modified. */
 int  fg_fft_c2r3(fg_ctx* ctx, const double* in, double* out);
 
+/* The same two transforms timed on the device alone (CUDA events on the
+   context's stream around each, after one untimed round): ms[0] the r2c,
+   ms[1] the c2r, averaged over reps round trips of whatever the context's
+   scratch holds.  Only that scratch changes (u, p, dVddi and the scalars
+   stand).  No counterpart in the reference (its cufft_check.F times cuFFT
+   round trips the same way, cufft_check.F:188-207). */
+int  fg_time_fft(fg_ctx* ctx, int reps, double* ms);
+
 /* ---- state --------------------------------------------------------------- */
 
 /* Coord_type members (coord_module.F:18,25,26,48,53).  dipoR/dipoP/dVddi are
@@ -239,6 +247,27 @@ int  fg_set_thermostat(fg_ctx* ctx, double s_Nose, double pi_Nose, double H0);
 int  fg_upload_site_arrays(fg_ctx* ctx, const double* Z_starR, const double* mass_dipo_inv,
                            const double* mass_acou_inv, const int* relaxor, const int* sum_p,
                            const double* E_field_local);
+/* The fg_params the context runs with (after any fg_chain_point). */
+int  fg_get_params(const fg_ctx* ctx, fg_params* p);
+/* The next point of a Nose-Poincare temperature or field sweep, started from
+   the state on the device.  The reference's sweep scripts start each point
+   from the previous point's final .coord read back as .restart
+   (03example-BaTiO3-bulk-phase-transition/16x16x16-40000-10000/cooling.sh:
+   64-69): that file holds dipoP / s_Nose (coord_module.F:476);
+   initialize_dipoR reads it (initialize-dipoR.F:22-38), evaluates the force
+   and sets s = 1, pi = 0 (:62-68); molecular_dynamics sets H0 from that
+   state (molecular-dynamics.F:52-55).  This call does the same on the
+   device at full precision: p <- p / s, kelvin (and the derived constants
+   of make_Param) of the new point, the uniform field E (NULL keeps it),
+   the force, s = 1, pi = 0, H0.  e receives the energies of the new start
+   (H_Nose_Poincare = 0).  Method 'md' only. */
+int  fg_chain_point(fg_ctx* ctx, double kelvin, const double E[3], fg_energy* e);
+/* write_system (coord_module.F:434-486): the .coord file of the current
+   state (ix iy iz, dipoR, dipoP / s_Nose, dVddi, acouR, acouP per line).
+   full_precision = 0: the reference's columns (i4,2i5,3f10.6,9e14.6,
+   3f13.6); otherwise 17 significant digits per value, which the .restart
+   readers (initialize-dipoR.F:22-38 and fg_feram_run) read back exactly. */
+int  fg_write_coord(fg_ctx* ctx, const char* path, int full_precision);
 /* Acoustic displacement and momentum (Coord_type acouR, acouP,
    coord_module.F:25-31) when acoustic_mass_amu > 0 (otherwise FG_ERR_STATE:
    the acoustic field is then the relaxed one of each force evaluation).
@@ -255,6 +284,17 @@ int  fg_get_acouK(fg_ctx* ctx, double* acouK);
    copy to the device is queued on the context's stream without waiting;
    E may be reused by the caller as soon as the call returns. */
 int  fg_set_uniform_E(fg_ctx* ctx, const double E[3]);
+
+/* The per-step field of molecular-dynamics.F:66-76 on the device: with on,
+   every step of this context (fg_nose_poincare, fg_leapfrog with
+   i_step != 0, fg_velocity_scaling, fg_run_steps, fg_batch_step) first
+   advances a device step counter and sets the uniform field to
+   wave(E_wave_type, i_step, n_thermalize, n_E_wave_period,
+   external_E_field) (wave_module.F:8-67), so replicas of a batch follow
+   their own field waveforms inside one graph.  i_step: the counter's value
+   now (the next step is i_step + 1).  on = 0 stops the schedule; the field
+   keeps its last value. */
+int  fg_set_wave(fg_ctx* ctx, int on, int i_step);
 
 /* ---- the hot path -------------------------------------------------------- */
 
@@ -350,9 +390,12 @@ int  fg_feram_run(const char* path, int precision, fg_average* avg_out,
    Lz > FG_NOALLOC_MAX_LZ, a null pointer or a mask that counts no layer give
    FG_ERR_ARG and a message in errbuf (may be NULL).  The first call on each
    device does a one-time set-up (it looks up the array's device address) and
-   should come before any stream capture.  All calls on one device share the
-   array: calls that overlap in time (different streams or host threads) race,
-   and the caller must order them. */
+   should come before any stream capture; a set-up that fails is not kept,
+   and the next call tries it again.  The two host tables are copied from
+   ordinary (pageable) host memory, so the call may wait until the stream
+   has taken them.  All calls on one device share the array: calls that
+   overlap in time (different streams or host threads) race, and the caller
+   must order them. */
 #define FG_NOALLOC_MAX_LZ 1024
 int  fg_kinetic_energy_dipo_noalloc(const double* dipoP, int Lx, int Ly, int Lz,
                                     const double* layer_mass_inv, const unsigned char* layer_sum_p,

@@ -1425,6 +1425,78 @@ int oracle_c2r(int Lx, int Ly, int Lz, int pad, int nc, double* in, double* out)
   return 0;
 }
 
+// Defaults of read_Param (param_module.F:129-194), for inputs built without
+// a .feram file.  Strings are empty ("" = current directory).
+void oracle_default_param(fg_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  p->method = FG_METHOD_MD;
+  for (int i = 0; i < FG_RELAXOR_MAX; ++i) {
+    p->mass_dipo[i] = 100.0 / 9648.53377163899;
+    p->mass_acou[i] = -100.0;
+  }
+  p->Q_Nose = 0.1;
+  p->bulk_or_film = FG_BULK;
+  p->Lx = p->Ly = p->Lz = 32;
+  p->padding_y = 1;
+  p->a0 = 4.0;
+  p->n_thermalize = 10000;
+  p->n_average = 100000;
+  p->n_coord_freq = 2147483647;  // huge(1)
+  p->n_hl_freq = 10000;
+  p->n_hysteresis_loop_continue = 1;
+  p->E_wave_type = FG_WAVE_NONE;
+  p->seed[0] = 123456789;
+  p->seed[1] = 987654321;
+  for (int a = 0; a < 3; ++a) p->init_dipo_dev[a] = 0.05;
+  p->verbose = 1;
+  p->E_field_always_zero = 1;
+}
+
+// make_Param (param_module.F:452-480), plus temperature_eV = kelvin /
+// KELVIN_EV, which read_Param sets with the kelvin tag (param_module.F:226).
+// Constants of define.h:21,34,35.
+int oracle_make_param(fg_params* p) {
+  const double kPiRef = 3.14159265358979323846, kKelvinEV = 11604.45, kElem = 1.60217653;
+  if (p->Lx < 1 || p->Ly < 1 || p->Lz < 1) return FG_ERR_ARG;
+  p->N = p->Lx * p->Ly * p->Lz;
+  p->Ninv = 1.0 / p->N;
+  p->dt_2 = p->dt / 2;
+  p->n_freedom = 3 * p->N;
+  if (p->kappa <= 0.0) p->kappa = std::sqrt(kPiRef) / p->a0 / std::pow((double)p->N, 1.0 / 6);
+  p->unit_cell_volume = p->a0 * p->a0 * p->a0;
+  for (int i = 0; i < 3; ++i) p->pNa03[i] = p->GPa[i] * 0.01 / kElem * p->N * p->unit_cell_volume;
+  p->target_kinetic_energy = p->kelvin * 1.5 * p->N / kKelvinEV;
+  p->temperature_eV = p->kelvin / kKelvinEV;
+  if (p->bulk_or_film == FG_BULK) {
+    if (p->gap_id != 0) return FG_ERR_ARG;
+  } else if (p->Lz % 2 != p->gap_id % 2) {
+    return FG_ERR_ARG;
+  }
+  return 0;
+}
+
+// initialize_dipoR without a .restart file (initialize-dipoR.F:41-56): the
+// seeded Gaussian u in the reference's draw order, stripe sign flips, p = 0.
+// Padded layout; dipoP may be NULL.
+int oracle_init_dipoR(const fg_params* p, double* dipoR, double* dipoP) {
+  if (!p || !dipoR) return FG_ERR_ARG;
+  Layout L;
+  L.set(p->Lx, p->Ly, p->Lz, p->padding_y);
+  std::fill(dipoR, dipoR + L.nreal(3), 0.0);
+  if (dipoP) std::fill(dipoP, dipoP + L.nreal(3), 0.0);
+  g_normal.sw = true;
+  g_uni64.seed(p->seed[0], p->seed[1]);
+  for (int a = 0; a < 3; ++a)
+    for (int iz = 0; iz < L.Lz; ++iz)
+      for (int iy = 0; iy < L.Ly; ++iy)
+        for (int ix = 0; ix < L.Lx; ++ix) {
+          double v = normal_dist(p->init_dipo_avg[a], p->init_dipo_dev[a]);
+          if (std::cos(k2Pi * (p->k_stripe[0] * ix + p->k_stripe[1] * iy + p->k_stripe[2] * iz + 1.0e-4)) < 0.0) v = -v;
+          dipoR[L.r(a, 3, ix, iy, iz)] = v;
+        }
+  return 0;
+}
+
 void oracle_set_threads(int n) { omp_set_num_threads(n); }
 
 }  // extern "C"

@@ -76,6 +76,12 @@ void   oracle_wave(int wave_type, int i_step, int n_thermalize, int period,
 int    oracle_r2c(int Lx, int Ly, int Lz, int padding_y, int nc, const double* in, double* out_complex);
 int    oracle_c2r(int Lx, int Ly, int Lz, int padding_y, int nc, double* in_complex, double* out);
 void   oracle_set_threads(int n);
+/* read_Param defaults (param_module.F:129-194), make_Param (:452-480) and the
+   no-.restart branch of initialize_dipoR (initialize-dipoR.F:41-56): inputs
+   built by the oracle alone, for a CPU run that loads nothing else. */
+void   oracle_default_param(fg_params* p);
+int    oracle_make_param(fg_params* p);
+int    oracle_init_dipoR(const fg_params* p, double* dipoR, double* dipoP);
 
 #ifdef __cplusplus
 }

@@ -1,8 +1,8 @@
 """Regenerate the committed golden fixtures of tests/golden from the reference tree.
 
-Run in the build container (where the reference is mounted):
+Run where a checkout of the reference is available, giving its root:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the reference checkout>
 
 Every fixture is data the reference's own tests or examples hold:
   uni64_kat.json         marsaglia_tsang_uni64_check.F:11-16,22-40,42-46
@@ -101,4 +101,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to the reference checkout>")
+    main(sys.argv[1])

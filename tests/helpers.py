@@ -54,6 +54,14 @@ def seeded_u(p, seed, sigma=0.1, avg=0.0):
     return u
 
 
+def fp32_config(u):
+    """The configuration rounded to FP32: the state the mixed path holds
+    (its fields are FP32).  Parity of the mixed path is measured on such
+    configurations, given identically to the FP64 oracle; the effect of the
+    rounding itself is a property of FP32 state, reported apart."""
+    return u.astype(np.float32).astype(np.float64)
+
+
 def seeded_p(p, seed, sigma=0.02):
     return seeded_u(p, seed + 5000, sigma=sigma)
 

@@ -56,6 +56,9 @@ def load():
         "oracle_r2c": (C.c_int, [C.c_int] * 5 + [dp, dp]),
         "oracle_c2r": (C.c_int, [C.c_int] * 5 + [dp, dp]),
         "oracle_set_threads": (None, [C.c_int]),
+        "oracle_default_param": (None, [P(A.fg_params)]),
+        "oracle_make_param": (C.c_int, [P(A.fg_params)]),
+        "oracle_init_dipoR": (C.c_int, [P(A.fg_params), dp, dp]),
     }
     for n, (r, a) in sig.items():
         f = getattr(L, n)

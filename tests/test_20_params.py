@@ -1,6 +1,8 @@
 """The host-side .feram parser (read_Param / make_Param mirror)."""
 import math
 
+import numpy as np
+
 import pytest
 
 import helpers
@@ -58,3 +60,60 @@ def test_make_param_gap_check(fg):
         fg.params_from_text("gap_id = 1\n", "bad")
     p = fg.params_from_text("bulk_or_film = 'epit'\nL = 8 8 7\ngap_id = 1\n", "ok")
     assert p.gap_id == 1
+
+
+def _struct_bytes(p):
+    import ctypes as C
+    return bytes(C.string_at(C.addressof(p), C.sizeof(p)))
+
+
+def test_oracle_defaults_match_product(fg, oracle):
+    """read_Param's defaults restated twice (product host code and oracle)."""
+    import ctypes as C
+    a, b = A.fg_params(), A.fg_params()
+    fg.lib().fg_default_param(C.byref(a))
+    oracle.oracle_default_param(C.byref(b))
+    assert _struct_bytes(a) == _struct_bytes(b)
+
+
+@pytest.mark.parametrize("deck,tags", [
+    ("zzznp.feram", {}),
+    ("zzz16.feram", {}),
+    ("zzznp.feram", dict(L="20 12 18", kelvin="450", GPa="-3 -4 -5")),
+    ("zzznp.feram", dict(L="12 12 8", bulk_or_film="'epit'", epi_strain="0.01")),
+])
+def test_oracle_make_param_and_init_match_product(fg, oracle, deck, tags):
+    """make_Param's derived constants and initialize_dipoR's uni64 draw:
+    the oracle's own restatements give the product's values bit for bit, so
+    a CPU run built from the oracle alone (the timed reference arm) has the
+    inputs of the device run."""
+    import ctypes as C
+    p = helpers.params(deck, **tags)
+    q = A.fg_params.from_buffer_copy(p)
+    q.N = 0
+    q.kappa = 0.0  # none of these decks sets kappa: make_Param derives it
+    assert oracle.oracle_make_param(C.byref(q)) == 0
+    assert _struct_bytes(p) == _struct_bytes(q)
+    u1, q1 = A.real_field(p), A.real_field(p)
+    u2, q2 = A.real_field(p), A.real_field(p)
+    assert fg.lib().fg_init_dipoR_host(C.byref(p), A.dptr(u1), A.dptr(q1)) == 0
+    assert oracle.oracle_init_dipoR(C.byref(p), A.dptr(u2), A.dptr(q2)) == 0
+    assert np.array_equal(u1, u2) and np.array_equal(q1, q2)
+
+
+def test_reference_arm_inputs_load_no_product_library():
+    """bench.py --impl reference builds its parameters and initial state from
+    the oracle alone: a fresh process doing so maps no product library."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path.insert(0, %r); import bench, json; "
+            "p = bench.make_params(16, impl='reference'); u, q = bench.initial_state(p, impl='reference'); "
+            "print(json.dumps({'libs': bench.loaded_repo_libs(), 'N': p.N, 'u': float(abs(u).sum())}))" % root)
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    assert out["libs"] == ["oracle/liboracle.so"], out
+    assert out["N"] == 4096 and out["u"] > 0

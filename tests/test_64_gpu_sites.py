@@ -169,3 +169,30 @@ def test_per_site_zstar_array_with_acoustic_leapfrog(fg, prec):
         assert np.abs(a - b).max() / np.abs(b).max() <= tol
     ee = helpers.energy_errors(eg, eo, A.POTENTIAL_FIELDS + ["dipo_kinetic", "acou_kinetic"])
     assert max(ee.values()) <= tol, ee
+
+
+def test_failed_site_upload_leaves_no_stale_graph(fg):
+    """A site upload that replaces buffers and then fails (here: a per-site
+    Z* whose 12-component z tiles do not fit in shared memory at Lz = 1280,
+    FP64, while the plain 9-component tiles do) must not leave a step graph
+    that holds the freed buffers: the next step is refused with an error
+    instead of replaying the graph."""
+    p = helpers.params(L="4 4 1280", Q_Nose="1.0", Z_star="9.956 7.0 7.0", **{
+        k: v for k, v in TWO_SPECIES.items() if k != "Z_star"})
+    u = helpers.seeded_u(p, 3, sigma=0.05)
+    shape = (p.Lz, p.Ly + p.padding_y, 2 * (p.Lx // 2 + 1))
+    relaxor = np.ones(shape, dtype=np.int32)
+    relaxor[:, :p.Ly, :p.Lx] = 1
+    relaxor[::2, :p.Ly, :p.Lx] = 2  # species 2 has its own Z*: per-site Z* path
+    with fb.Context(p, A.FG_PREC_FP64) as ctx:
+        ctx.build_tables()
+        ctx.set_state(u)
+        e = ctx.mirror_force_mirror()
+        e.dipo_kinetic = ctx.kinetic_energy_dipo()
+        ctx.nose_poincare(e)  # captures the step graph with the current tables
+        with pytest.raises(fb.FeramError) as ei:
+            ctx.upload_site_arrays(relaxor=relaxor)
+        assert ei.value.code == A.FG_ERR_UNSUPPORTED, ei.value
+        with pytest.raises(fb.FeramError) as ei:
+            ctx.nose_poincare(e)
+        assert "destroy this context" in str(ei.value)

@@ -84,3 +84,57 @@ def test_batch_rejects_bad_replica(fg):
     bad.Lx = 7  # odd Lx with a made N: fg_create refuses it
     with pytest.raises(fb.FeramError, match="replica 1"):
         fb.Batch([good, bad])
+
+
+def test_batch_epit_field_waves_match_oracle(fg):
+    """Config-4-style batch: epitaxial films with their own misfit strain and
+    a triangular E_z wave each, the per-step field evaluated on the device
+    (fg_set_wave) inside one batch graph; every replica against the oracle's
+    molecular_dynamics (molecular-dynamics.F:66-76 with wave_module.F), FP64."""
+    import ctypes as C
+    import oracle_lib
+    strains = (-0.01, 0.0, 0.015)
+    periods = (8, 12, 16)
+    ps = [helpers.params(L="8 8 8", bulk_or_film="'epit'", epi_strain=str(es), kelvin="280",
+                         E_wave_type="'triangular_cos'", external_E_field="0.0 0.0 0.002",
+                         n_E_wave_period=str(T), n_thermalize="4", n_average="8")
+          for es, T in zip(strains, periods)]
+    n = 12
+    states = [(helpers.seeded_u(p, 90 + i, sigma=0.05), helpers.seeded_p(p, 90 + i, sigma=0.01))
+              for i, p in enumerate(ps)]
+
+    def wave0(p):
+        out = (C.c_double * 3)()
+        amp = (C.c_double * 3)(*p.external_E_field)
+        assert A.lib().fg_wave(p.E_wave_type, 0, p.n_thermalize, p.n_E_wave_period, amp, out) == 0
+        return list(out)
+
+    refs = []
+    for p, (u, q) in zip(ps, states):
+        o = oracle_lib.Oracle(p)
+        o.set_state(u, q)
+        o.set_uniform_E(wave0(p))
+        e = o.force()
+        e.dipo_kinetic = o.kinetic_energy_dipo()
+        o.md(1, n, 1, e)
+        refs.append((o.get_state(), e))
+    with fb.Batch(ps, A.FG_PREC_FP64) as b:
+        for r, p, (u, q) in zip(b.replicas, ps, states):
+            r.build_tables()
+            r.set_state(u, q)
+            r.set_uniform_E(wave0(p))
+            e = r.mirror_force_mirror()
+            e.dipo_kinetic = r.kinetic_energy_dipo()
+            r.nose_poincare_hamiltonian(e)
+            r.set_thermostat(1.0, 0.0, e.H_Nose_Poincare)
+            r.set_wave(True, 0)
+        es = b.step(n)
+        got = [r.get_state() for r in b.replicas]
+    for i, (p, (so, eo)) in enumerate(zip(ps, refs)):
+        du = np.abs(A.physical(got[i]["dipoR"], p) - A.physical(so["dipoR"], p)).max()
+        assert du <= 1e-10, (i, du)
+        assert abs(got[i]["s"] - so["s"]) <= 1e-12
+        assert np.allclose(got[i]["strain"], so["strain"], rtol=1e-9, atol=1e-14), (i, got[i]["strain"], so["strain"])
+        for f in ("total", "dipole_E_field", "unharmonic", "dipo_kinetic"):
+            a, c = getattr(es[i], f), getattr(eo, f)
+            assert abs(a - c) <= 1e-9 * max(abs(c), 1e-3), (i, f, a, c)

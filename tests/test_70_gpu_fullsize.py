@@ -1,5 +1,13 @@
 """Full-size checks: the compile-time FFT instances (32^3 .. 128^3) against
-numpy and the oracle, and size-independent properties at 128^3."""
+numpy and the oracle, and size-independent properties at 128^3.
+
+Force parity at full size: FP64 worst site and RMS of |dF| <= 1e-12 of
+RMS |F| and every energy term <= 1e-12; mixed worst site and RMS <= 1e-6
+(on the FP32-rounded configuration both paths hold), energies <= 1e-5.
+Measured errors go to FERAM_PARITY_LOG when it is set."""
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -29,27 +37,44 @@ def test_fft_roundtrip_fullsize(fg, L, prec):
         assert err2 <= TOL[prec] * 5, err2
 
 
+LOG = os.environ.get("FERAM_PARITY_LOG")
+
+
+def _record(name, data):
+    if not LOG:
+        return
+    os.makedirs(os.path.dirname(os.path.abspath(LOG)), exist_ok=True)
+    with open(LOG, "a") as f:
+        f.write(json.dumps({"test": name, **data}) + "\n")
+
+
 @pytest.mark.parametrize("prec", [A.FG_PREC_FP64, A.FG_PREC_MIXED])
+@pytest.mark.parametrize("Ez", [0.0, 0.001])
 @pytest.mark.parametrize("L", [32, 64, 128])
-def test_force_matches_oracle_fullsize(fg, L, prec):
-    p = helpers.params(L=f"{L} {L} {L}", external_E_field="0.0 0.0 0.001")
+def test_force_matches_oracle_fullsize(fg, L, Ez, prec):
+    """The 128^3 workload at E_z = 0 and 100 kV/cm (0.001 V/A)."""
+    p = helpers.params(L=f"{L} {L} {L}", external_E_field=f"0.0 0.0 {Ez}")
     u = helpers.seeded_u(p, 100 + L, sigma=0.1)
+    if prec == A.FG_PREC_MIXED:
+        u = helpers.fp32_config(u)
     o = oracle_lib.Oracle(p)
     o.set_state(u)
-    o.set_uniform_E([0.0, 0.0, 0.001])
+    o.set_uniform_E([0.0, 0.0, Ez])
     eo = o.force()
     with fg.Context(p, prec) as ctx:
         ctx.build_tables()
         ctx.set_state(u)
-        ctx.set_uniform_E([0.0, 0.0, 0.001])
+        ctx.set_uniform_E([0.0, 0.0, Ez])
         eg = ctx.mirror_force_mirror()
         fgd = ctx.get_state()["dVddi"]
     fmax, frms = helpers.force_error(fgd, o.get_state()["dVddi"], p)
     ee = helpers.energy_errors(eg, eo)
+    _record(f"force_fullsize[{L},{Ez},{prec}]", dict(fmax=fmax, frms=frms, emax=max(ee.values()),
+                                                      energies={k: float(v) for k, v in ee.items()}))
     if prec == A.FG_PREC_FP64:
-        assert fmax <= 1e-11 and max(ee.values()) <= 1e-11, (fmax, ee)
+        assert fmax <= 1e-12 and frms <= 1e-12 and max(ee.values()) <= 1e-12, (fmax, ee)
     else:
-        assert frms <= 1e-6 and fmax <= 1e-5 and max(ee.values()) <= 1e-5, (fmax, frms, ee)
+        assert frms <= 1e-6 and fmax <= 1e-6 and max(ee.values()) <= 1e-5, (fmax, frms, ee)
 
 
 def test_nose_poincare_128_matches_oracle(fg):
