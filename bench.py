@@ -310,6 +310,110 @@ def batched_sweep(n_rep=96, steps=200):
             "timing": "wall clock around synchronous calls"}
 
 
+def fft_vs_cufft(L=128, reps=20):
+    """The device FFT stage (3-component r2c and c2r: k_xy_fwd + z pass, z
+    pass + k_xy_inv; fg_time_fft) against cuFFT on the same GPU, planned as
+    the reference's cufft_check.F:180-207 plans it (D2Z / Z2D, howmany 3,
+    interleaved components, padded embeds) and, as cuFFT's own best case,
+    three contiguous unpadded fields.  CUDA events; ms per transform."""
+    import torch
+    import feram_b200 as fb
+    from feram_b200 import _capi as A
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import cufft_lib
+    p = make_params(L, Ez=0.0)
+    out = {"L": L, "components": 3, "reps": reps}
+    for prec, name, fp64 in ((A.FG_PREC_MIXED, "fp32", False), (A.FG_PREC_FP64, "fp64", True)):
+        with fb.Context(p, prec) as ctx:
+            ms = ctx.time_fft(reps)
+        dt, ct = (torch.float64, torch.complex128) if fp64 else (torch.float32, torch.complex64)
+        res = {"ours_r2c_ms": ms[0], "ours_c2r_ms": ms[1]}
+        for layout in ("reference", "contiguous"):
+            if layout == "reference":
+                x = torch.zeros(A.real_field(p).shape, dtype=dt, device="cuda")
+                X = torch.zeros(A.complex_field(p).shape, dtype=ct, device="cuda")
+            else:
+                x = torch.zeros((3, L, L, L), dtype=dt, device="cuda")
+                X = torch.zeros((3, L, L, L // 2 + 1), dtype=ct, device="cuda")
+            x.normal_()
+            plan = cufft_lib.PlanMany(L, L, L, 1, 3, fp64, layout)
+            try:
+                ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+                tf = tb = 0.0
+                for r in range(reps + 1):
+                    ev[0].record()
+                    plan.forward(x.data_ptr(), X.data_ptr())
+                    ev[1].record()
+                    plan.backward(X.data_ptr(), x.data_ptr())
+                    ev[2].record()
+                    torch.cuda.synchronize()
+                    if r > 0:
+                        tf += ev[0].elapsed_time(ev[1])
+                        tb += ev[1].elapsed_time(ev[2])
+            finally:
+                plan.close()
+            res[f"cufft_{layout}_r2c_ms"] = tf / reps
+            res[f"cufft_{layout}_c2r_ms"] = tb / reps
+        res["cufft_reference_over_ours"] = (res["cufft_reference_r2c_ms"] + res["cufft_reference_c2r_ms"]) / (ms[0] + ms[1])
+        res["cufft_contiguous_over_ours"] = (res["cufft_contiguous_r2c_ms"] + res["cufft_contiguous_c2r_ms"]) / (ms[0] + ms[1])
+        out[name] = res
+    return out
+
+
+def epit_hysteresis(n_rep=16, L=64, steps=400, period=20000):
+    """The batched thin-film hysteresis workload: n_rep epitaxial films of
+    L x L x L sites (L/2 layers and their mirror image in z), misfit strain
+    on a grid from -2% to +2%, a triangular_cos E_z wave of amplitude
+    0.002 V/A (200 kV/cm) and period `period` steps evaluated on the device
+    every step (fg_set_wave), 300 K, Nose-Poincare, mixed precision, all
+    replicas as one batch graph.  `steps` timed steps (of the 2e4 a full loop
+    takes); wall clock around the synchronous fg_batch_step."""
+    import feram_b200 as fb
+    from feram_b200 import _capi as A
+    ps = []
+    for i in range(n_rep):
+        p = make_params(L, kelvin=300.0, Ez=0.002)
+        p.bulk_or_film = A.FG_EPIT
+        p.epi_strain = -0.02 + 0.04 * i / max(n_rep - 1, 1)
+        p.E_wave_type = A.FG_WAVE_TRIANGULAR_COS
+        p.n_E_wave_period = period
+        p.n_thermalize = 0
+        p.seed[0] = 123456789 + i
+        ps.append(fb.make_param(p))
+    sites = sum(p.N for p in ps)
+    with fb.Batch(ps, A.FG_PREC_MIXED) as b:
+        for r, p in zip(b.replicas, ps):
+            u, q = initial_state(p)
+            r.build_tables()
+            prepare(r, p, u, q)
+            r.set_wave(True, 0)
+        b.step(5)
+        t0 = time.perf_counter()
+        es = b.step(steps)
+        t = time.perf_counter() - t0
+    return {"replicas": n_rep, "L": [L, L, L], "layers": L // 2, "epi_strain": [-0.02, 0.02],
+            "E_wave": "triangular_cos, 0.002 V/A, period %d steps, on the device" % period, "kelvin": 300.0,
+            "sites": sites, "steps": steps, "value": sites * steps / t, "unit": UNIT,
+            "ms_per_batch_step": 1000.0 * t / steps, "timing": "wall clock around synchronous fg_batch_step",
+            "finite": bool(all(np.isfinite(e.total) for e in es))}
+
+
+def warm_start_leg(L=32, log=None):
+    """The learned warm start (32^3): MD-generated training set, training on
+    the tensor cores, 40 held-out (T, E) points against the chained
+    fallback (feram_b200.warm_start.experiment)."""
+    from feram_b200 import warm_start as W
+
+    def mp(Lw, T, ez, gpa):
+        import feram_b200 as fb
+        p = make_params(Lw, kelvin=T, Ez=ez)
+        p.GPa[0] = p.GPa[1] = p.GPa[2] = gpa
+        p.E_field_always_zero = 0
+        p.N = 0
+        return fb.make_param(p)
+    return W.experiment(mp, L=L, log=log)
+
+
 def cpu_baseline(p, budget_s=20.0):
     """The oracle (FP64 C++/OpenMP restatement of the reference's CPU path)
     on this host's cores: one NP step after setup, then as many more as fit
@@ -393,6 +497,8 @@ def main():
     ap.add_argument("--size", type=int, default=L_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-replica batched sweep measurement")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the FFT-vs-cuFFT, thin-film hysteresis and warm-start legs")
     ap.add_argument("--mixed-only", action="store_true",
                     help="skip the FP64 context, the force-error check and e2e (small device footprint, for profiling)")
     args = ap.parse_args()
@@ -538,6 +644,11 @@ def main():
     batched = None
     if rank == 0 and world == 1 and not args.no_batched and not args.mixed_only:
         batched = batched_sweep()
+    fftc = epit = wstart = None
+    if rank == 0 and world == 1 and not args.no_extras and not args.mixed_only:
+        fftc = fft_vs_cufft(L)
+        epit = epit_hysteresis()
+        wstart = warm_start_leg(log=lambda m: print(m, file=sys.stderr, flush=True))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(p)
@@ -556,6 +667,7 @@ def main():
         "force_err_16_configs": ferr16,
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "batched": batched,
+        "fft_vs_cufft": fftc, "epit_hysteresis": epit, "warm_start": wstart,
         "gpu_launches": A.FG_NPROF * args.steps,  # kernels per bulk NP step graph
     }
     ctxm.close()

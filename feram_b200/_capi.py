@@ -129,6 +129,7 @@ def lib() -> C.CDLL:
     L = C.CDLL(LIB_PATH)
     P = C.POINTER
     dp = P(C.c_double)
+    fp = P(C.c_float)
     vp = C.c_void_p
     sig = {
         "fg_default_param": (None, [P(fg_params)]),
@@ -156,6 +157,17 @@ def lib() -> C.CDLL:
         "fg_chain_point": (C.c_int, [vp, C.c_double, dp, C.POINTER(fg_energy)]),
         "fg_write_coord": (C.c_int, [vp, C.c_char_p, C.c_int]),
         "fg_set_wave": (C.c_int, [vp, C.c_int, C.c_int]),
+        "fg_ws_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(vp)]),
+        "fg_ws_destroy": (None, [vp]),
+        "fg_ws_last_error": (C.c_char_p, [vp]),
+        "fg_ws_forward": (C.c_int, [vp, fp, C.POINTER(C.c_ulonglong), fp]),
+        "fg_ws_backward": (C.c_int, [vp, fp, C.POINTER(C.c_ulonglong), fp, fp, fp]),
+        "fg_ws_adam": (C.c_int, [vp, C.c_float]),
+        "fg_ws_layer_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "fg_ws_get_layer": (C.c_int, [vp, C.c_int, fp, fp, fp, fp]),
+        "fg_ws_set_layer": (C.c_int, [vp, C.c_int, fp, fp]),
+        "fg_ws_get_io": (C.c_int, [vp, fp, fp]),
+        "fg_ws_field": (C.c_int, [vp, C.c_int, C.c_int, dp]),
         "fg_set_state": (C.c_int, [vp, dp, dp, C.c_double, C.c_double, C.c_double]),
         "fg_get_state": (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
         "fg_set_thermostat": (C.c_int, [vp, C.c_double, C.c_double, C.c_double]),

@@ -5,7 +5,9 @@
 
 nvcc compiles the CUDA translation unit for ``compute_100a``/``sm_100a``
 (no other architectures), g++ compiles the host-side C++ (parser, driver),
-and nvcc links the shared library.  It cross-compiles without a GPU.
+and nvcc links the shared library.  Two CUDA translation units: the MD
+step (csrc/fg_api.cu) and the warm-start network (csrc/ws_net.cu).  It
+cross-compiles without a GPU.
 """
 from __future__ import annotations
 
@@ -44,13 +46,16 @@ def build(checked: bool = False, verbose: bool = False, ptxas_v: bool = False) -
     out_dir = os.path.join(HERE, "_build", "checked" if checked else "release")
     os.makedirs(out_dir, exist_ok=True)
     defs = ["-DFG_BOUNDS_CHECK=1"] if checked else []
-    cu_obj = os.path.join(out_dir, "fg_api.o")
-    cu_flags = [nvcc, "-c", os.path.join(HERE, "csrc", "fg_api.cu"), "-o", cu_obj, *ARCH, "-O3", "-lineinfo",
-                "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", *defs]
-    if ptxas_v:
-        cu_flags += ["-Xptxas", "-v"]
-    _run(cu_flags, verbose or ptxas_v)
-    objs = [cu_obj]
+    objs = []
+    # fg_api.cu: the MD step; ws_net.cu: the warm-start network (tcgen05)
+    for src in ("fg_api.cu", "ws_net.cu"):
+        cu_obj = os.path.join(out_dir, src.replace(".cu", ".o"))
+        cu_flags = [nvcc, "-c", os.path.join(HERE, "csrc", src), "-o", cu_obj, *ARCH, "-O3", "-lineinfo",
+                    "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", *defs]
+        if ptxas_v:
+            cu_flags += ["-Xptxas", "-v"]
+        _run(cu_flags, verbose or ptxas_v)
+        objs.append(cu_obj)
     cxx = shutil.which("g++") or "g++"
     for src in ("feram_host.cpp", "feram_driver.cpp"):
         obj = os.path.join(out_dir, src.replace(".cpp", ".o"))

@@ -1698,6 +1698,18 @@ int fg_chain_point(fg_ctx* ctx, double kelvin, const double E[3], fg_energy* e) 
   if ((rc = fg_make_param(&q, eb, sizeof(eb)))) return fail(ctx, rc, eb);
   if ((rc = pull_scalars(ctx))) return rc;
   const double s_old = ctx->sc_host->s;
+  // a point with a field clears E_field_always_zero (param_module.F:294-298);
+  // the field term's switch is a kernel argument of the step graphs
+  if (E && (E[0] != 0.0 || E[1] != 0.0 || E[2] != 0.0) && q.E_field_always_zero) {
+    q.E_field_always_zero = 0;
+    ctx->ph_host.E_on = 1;
+    ++ctx->gen;
+    for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
+      if (*gx) {
+        cudaGraphExecDestroy(*gx);
+        *gx = nullptr;
+      }
+  }
   ctx->P = q;
   Phys& h = ctx->ph_host;
   h.nf_kT = (double)q.n_freedom * q.temperature_eV;

@@ -1,0 +1,350 @@
+"""Learned warm start for sweep points (no counterpart in the reference).
+
+The reference starts every point of a temperature or field sweep from the
+previous point's final state (its sweep scripts link the last .coord as the
+next .restart, e.g. 03example-BaTiO3-bulk-phase-transition/16x16x16-40000-
+10000/cooling.sh:64-69; here fg_chain_point does that on the device).  This
+module trains a small periodic 3D convolutional network on configurations
+the MD generates, so that it proposes a field u(R) for a new (T, E, p) point
+that starts closer to equilibrium; the MD then judges the proposal: a warm
+start whose averages fall outside the statistical error of a plain run is
+rejected and the point falls back to the chained start.
+
+Everything here is orchestration of the C-ABI (fg_ws_* for the network, whose
+convolutions and their gradients run on the tensor cores; the MD calls for
+the data); no arithmetic of the model runs in Python except the site
+statistics of the training targets, which restate those of the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import _capi as A
+from ._capi import FG_PREC_MIXED
+
+NSTAT = 7
+STAT_NAMES = ("m.e", "|m|^2", "sum m_a^4", "<|u|^2>", "<sum u_a^4>", "C_long", "C_trans")
+E_SCALE = 0.001  # V/A: 100 kV/cm
+
+
+def site_stats(u: np.ndarray, E) -> np.ndarray:
+    """The seven statistics of a configuration u (Lz, Ly, Lx, 3) at field E:
+    m.e, |m|^2, sum_a m_a^4 (m = <u>, e = E / 0.001 V/A), <|u|^2>,
+    <sum_a u_a^4>, <sum_a u_a(R) u_a(R + a)>, <sum_a sum_b!=a u_a(R) u_a(R + b)>."""
+    u = np.asarray(u, dtype=np.float64)
+    m = u.reshape(-1, 3).mean(axis=0)
+    e = np.asarray(E, dtype=np.float64) / E_SCALE
+    ax = {0: 2, 1: 1, 2: 0}  # component a -> array axis of direction a (z, y, x order)
+    c_long = sum((u[..., a] * np.roll(u[..., a], -1, axis=ax[a])).mean() for a in range(3))
+    c_tr = sum((u[..., a] * np.roll(u[..., a], -1, axis=ax[b])).mean() for a in range(3) for b in range(3) if b != a)
+    return np.array([m @ e, m @ m, (m ** 4).sum(), (u ** 2).sum(-1).mean(), (u ** 4).sum(-1).mean(), c_long, c_tr])
+
+
+class WarmStartNet:
+    """fg_ws: the network of `batch` samples of an Lx x Ly x Lz supercell."""
+
+    def __init__(self, L, batch: int = 8, seed: int = 1):
+        self.L = tuple(L)
+        self.batch = batch
+        self._h = C.c_void_p()
+        rc = A.lib().fg_ws_create(L[0], L[1], L[2], batch, seed, C.byref(self._h))
+        if rc:
+            msg = A.lib().fg_ws_last_error(self._h).decode()
+            self.close()
+            raise RuntimeError(f"fg_ws_create [{rc}]: {msg}")
+
+    def _check(self, rc):
+        if rc:
+            raise RuntimeError(f"fg_ws [{rc}]: {A.lib().fg_ws_last_error(self._h).decode()}")
+
+    @staticmethod
+    def _f32(a):
+        a = np.ascontiguousarray(a, dtype=np.float32)
+        return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+    def _inputs(self, cond, seeds):
+        cond, cp = self._f32(np.asarray(cond).reshape(self.batch, 5))
+        sd = (C.c_ulonglong * self.batch)(*[int(x) for x in seeds])
+        return cond, cp, sd
+
+    def forward(self, cond, seeds) -> np.ndarray:
+        """Statistics [batch][7] of the generated fields."""
+        keep, cp, sd = self._inputs(cond, seeds)
+        S = np.zeros((self.batch, NSTAT), dtype=np.float32)
+        self._check(A.lib().fg_ws_forward(self._h, cp, sd, S.ctypes.data_as(C.POINTER(C.c_float))))
+        return S
+
+    def backward(self, cond, seeds, target, weights) -> float:
+        keep, cp, sd = self._inputs(cond, seeds)
+        t, tp = self._f32(np.asarray(target).reshape(self.batch, NSTAT))
+        w, wp = self._f32(weights)
+        loss = C.c_float()
+        self._check(A.lib().fg_ws_backward(self._h, cp, sd, tp, wp, C.byref(loss)))
+        return float(loss.value)
+
+    def adam(self, lr: float):
+        self._check(A.lib().fg_ws_adam(self._h, lr))
+
+    def layer(self, l: int):
+        co, ci = C.c_int(), C.c_int()
+        self._check(A.lib().fg_ws_layer_shape(self._h, l, C.byref(co), C.byref(ci)))
+        w = np.zeros((co.value, 27, ci.value), dtype=np.float32)
+        b = np.zeros(co.value, dtype=np.float32)
+        dw, db = np.zeros_like(w), np.zeros_like(b)
+        f = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(A.lib().fg_ws_get_layer(self._h, l, f(w), f(b), f(dw), f(db)))
+        return w, b, dw, db
+
+    def set_layer(self, l: int, w, b):
+        w, wp = self._f32(w)
+        b, bp = self._f32(b)
+        self._check(A.lib().fg_ws_set_layer(self._h, l, wp, bp))
+
+    def io(self):
+        """(layer-1 input [B*N][16], generated u [B*N][3]) of the last forward."""
+        n = self.batch * self.L[0] * self.L[1] * self.L[2]
+        x = np.zeros((n, 16), dtype=np.float32)
+        u = np.zeros((n, 3), dtype=np.float32)
+        f = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(A.lib().fg_ws_get_io(self._h, f(x), f(u)))
+        return x, u
+
+    def field(self, b: int, p) -> np.ndarray:
+        """Sample b of the last forward as a padded dipoR array for p."""
+        u = A.real_field(p)
+        self._check(A.lib().fg_ws_field(self._h, b, p.padding_y, A.dptr(u)))
+        return u
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            A.lib().fg_ws_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def maxwell_momenta(p, seed: int) -> np.ndarray:
+    """Momenta drawn from the Maxwell-Boltzmann distribution at p.kelvin
+    (p_a ~ N(0, sqrt(m k T)) per site and component), padded layout."""
+    rng = np.random.default_rng(seed)
+    q = A.real_field(p)
+    sd = np.sqrt(p.mass_dipo[0] * p.temperature_eV)
+    A.physical(q, p)[...] = rng.standard_normal((p.Lz, p.Ly, p.Lx, 3)) * sd
+    return q
+
+
+def start_point(ctx, p, u, q) -> "A.fg_energy":
+    """initialize_dipoR's tail and molecular-dynamics.F:52-55 for a given
+    (u, p): force, s = 1, pi = 0, H0 from the state."""
+    ctx.set_state(u, q, 1.0, 0.0, 0.0)
+    ctx.set_uniform_E([p.external_E_field[0], p.external_E_field[1], p.external_E_field[2]])
+    e = ctx.mirror_force_mirror()
+    e.dipo_kinetic = ctx.kinetic_energy_dipo()
+    ctx.nose_poincare_hamiltonian(e)
+    ctx.set_thermostat(1.0, 0.0, e.H_Nose_Poincare)
+    return e
+
+
+def potential(e) -> float:
+    return sum(getattr(e, f) for f in A.POTENTIAL_FIELDS)
+
+
+def generate_training_set(make_params, chains, temps, n_therm=3000, n_snap=14, snap_every=100,
+                          precision=FG_PREC_MIXED):
+    """Configurations generated by the MD: one cooling chain per (E_z, GPa)
+    in `chains`, each through `temps` (descending), every point started from
+    the previous one on the device (fg_chain_point), thermalised n_therm
+    steps, then n_snap snapshots snap_every steps apart.  All chains step
+    together as one replica batch.  Returns (cond [n][5], stats [n][7])."""
+    import feram_b200 as fb
+    ps = [make_params(temps[0], Ez, gpa) for Ez, gpa in chains]
+    conds, stats = [], []
+    with fb.Batch(ps, precision) as b:
+        for i, (r, p) in enumerate(zip(b.replicas, ps)):
+            r.build_tables()
+            u = A.real_field(p)
+            q = A.real_field(p)
+            assert A.lib().fg_init_dipoR_host(C.byref(p), A.dptr(u), A.dptr(q)) == 0
+            start_point(r, p, u, q)
+        for k, T in enumerate(temps):
+            if k > 0:
+                for r, (Ez, gpa) in zip(b.replicas, chains):
+                    r.chain_point(T, [0.0, 0.0, Ez])
+            b.step(n_therm)
+            for _ in range(n_snap):
+                b.step(snap_every)
+                for r, (Ez, gpa) in zip(b.replicas, chains):
+                    u = A.physical(r.get_state()["dipoR"], r.p)
+                    conds.append([T, 0.0, 0.0, Ez, gpa])
+                    stats.append(site_stats(u, [0.0, 0.0, Ez]))
+    return np.array(conds, dtype=np.float64), np.array(stats, dtype=np.float64)
+
+
+def train(net: WarmStartNet, cond, stats, steps=1500, lr=2e-3, seed=0, log_every=0):
+    """Adam on the moment-matching loss, minibatches of net.batch training
+    samples (random order, fresh noise seeds).  Weights: 1 / variance of
+    each statistic over the training set.  Returns the loss history."""
+    rng = np.random.default_rng(seed)
+    w = 1.0 / np.maximum(stats.var(axis=0), 1e-30)
+    hist = []
+    for it in range(steps):
+        idx = rng.integers(0, len(cond), size=net.batch)
+        seeds = rng.integers(1, 2 ** 62, size=net.batch)
+        lr_t = lr * (0.1 ** (it / max(steps, 1)))  # exponential decay to lr / 10
+        loss = net.backward(cond[idx], seeds, stats[idx], w)
+        net.adam(lr_t)
+        hist.append(loss)
+        if log_every and it % log_every == 0:
+            print(f"train step {it}: loss {loss:.4g}", flush=True)
+    return np.array(hist)
+
+
+def equilibration_trace(ctx, n_steps: int, every: int):
+    """(|<u>|^2, potential energy) every `every` steps over n_steps, from
+    the device reductions of add_to_Average (fg_average_accumulate)."""
+    P2, V = [], []
+    N = ctx.p.Lx * ctx.p.Ly * ctx.p.Lz
+    for _ in range(n_steps // every):
+        e = ctx.run_steps(every)
+        avg = A.fg_average()
+        ctx.average_accumulate(e, avg)
+        m = np.array(avg.u[:]) / N
+        P2.append(float(m @ m))
+        V.append(potential(e))
+    return np.array(P2), np.array(V)
+
+
+def time_to_equilibrium(P2, V, eq, every: int, block: int = 5, k: float = 3.0):
+    """Steps until three consecutive blocks (block samples each) of the trace
+    lie within k standard deviations (of block means) of the equilibrium
+    values eq = (P2 mean, P2 block sd, V mean, V block sd); None if never."""
+    nb = len(P2) // block
+    bp = P2[:nb * block].reshape(nb, block).mean(axis=1)
+    bv = V[:nb * block].reshape(nb, block).mean(axis=1)
+    ok = (np.abs(bp - eq[0]) <= k * eq[1] + 1e-12) & (np.abs(bv - eq[2]) <= k * eq[3] + 1e-12)
+    for i in range(nb - 2):
+        if ok[i] and ok[i + 1] and ok[i + 2]:
+            return i * block * every
+    return None
+
+
+def block_stats(P2, V, block: int = 5):
+    nb = len(P2) // block
+    bp = P2[:nb * block].reshape(nb, block).mean(axis=1)
+    bv = V[:nb * block].reshape(nb, block).mean(axis=1)
+    return (float(bp.mean()), float(bp.std(ddof=1)), float(bv.mean()), float(bv.std(ddof=1)))
+
+
+def timed(fn, *a, **k):
+    t0 = time.perf_counter()
+    r = fn(*a, **k)
+    return r, time.perf_counter() - t0
+
+
+def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40, seed=2024, n_therm=3000,
+               n_snap=14, train_steps=1500, probe=3000, every=20, accept_after=1000, log=None):
+    """The learned-warm-start protocol on one GPU.
+
+    1. Data: MD cooling chains (train_chains of (E_z, GPa), train_temps
+       descending) at L^3, snapshots -> (condition, statistics).
+    2. Training: Adam on the moment-matching loss.
+    3. Held-out points: n_held (T in 100-450 K, E_z in +-0.001 V/A), visited
+       as a cooling sweep (T descending).  Each point runs twice for `probe`
+       steps: from the previous point's final state (fg_chain_point, the
+       reference's .restart chaining: the fallback) and from the network's
+       proposal with Maxwell-Boltzmann momenta.  The fallback run continues
+       another `probe` steps; those give the point's equilibrium (block means
+       and their spread).  Time to equilibrium: three consecutive blocks of
+       the trace within 3 sigma of it.  Acceptance, the MD as the judge: the
+       warm run's averages over [accept_after, probe) against the equilibrium
+       ones, within 4 sigma of the difference; rejected points keep the
+       fallback.
+    Returns a dict of the measurements."""
+    import feram_b200 as fb
+    say = log or (lambda *a: None)
+    rng = np.random.default_rng(seed)
+    if train_chains is None:
+        train_chains = [(ez, gpa) for ez in (-0.001, -0.0005, 0.0, 0.0005, 0.001) for gpa in (-5.0, -3.0)]
+    if train_temps is None:
+        train_temps = [450.0 - 25.0 * i for i in range(15)]
+    out = {"L": L, "train_chains": len(train_chains), "train_temps": [train_temps[0], train_temps[-1], len(train_temps)]}
+    (cond, stats), t_data = timed(generate_training_set, lambda T, ez, gpa: make_params(L, T, ez, gpa),
+                                  train_chains, train_temps, n_therm=n_therm, n_snap=n_snap)
+    out["train_configs"] = len(cond)
+    out["data_seconds"] = t_data
+    say(f"warm start: {len(cond)} training configurations in {t_data:.1f} s")
+    net = WarmStartNet((L, L, L), batch=8, seed=seed)
+    try:
+        hist, t_train = timed(train, net, cond, stats, steps=train_steps, seed=seed)
+        out.update({"train_steps": train_steps, "train_seconds": t_train,
+                    "loss_first": float(np.mean(hist[:20])), "loss_last": float(np.mean(hist[-50:]))})
+        say(f"warm start: trained {train_steps} steps in {t_train:.1f} s, loss {out['loss_first']:.3g} -> "
+            f"{out['loss_last']:.3g}")
+        held = sorted(((float(rng.uniform(100.0, 450.0)), float(rng.uniform(-0.001, 0.001))) for _ in range(n_held)),
+                      reverse=True)
+        p0 = make_params(L, held[0][0], held[0][1], -5.0)
+        taus_w, taus_f, accepted, rows = [], [], 0, []
+        t_infer = 0.0
+        with fb.Context(p0, FG_PREC_MIXED) as cf, fb.Context(p0, FG_PREC_MIXED) as cw:
+            cf.build_tables()
+            cw.build_tables()
+            u = A.real_field(p0)
+            q = A.real_field(p0)
+            assert A.lib().fg_init_dipoR_host(C.byref(p0), A.dptr(u), A.dptr(q)) == 0
+            start_point(cf, p0, u, q)
+            cf.run_steps(probe)  # the sweep's first point, thermalised before the held-out ones
+            for i, (T, ez) in enumerate(held):
+                E = [0.0, 0.0, ez]
+                cf.chain_point(T, E)
+                Pf, Vf = equilibration_trace(cf, probe, every)
+                Pe, Ve = equilibration_trace(cf, probe, every)
+                eq = block_stats(Pe, Ve)
+                # warm start from the network
+                t0 = time.perf_counter()
+                net.forward(np.array([[T, 0.0, 0.0, ez, -5.0]] * net.batch), [seed * 1000 + i] * net.batch)
+                pw = make_params(L, T, ez, -5.0)
+                uw = net.field(0, pw)
+                t_infer += time.perf_counter() - t0
+                cw.chain_point(T, E)  # the context's temperature and field (its state is replaced below)
+                start_point(cw, cw.p, uw, maxwell_momenta(cw.p, seed + i))
+                Pw, Vw = equilibration_trace(cw, probe, every)
+                tf = time_to_equilibrium(Pf, Vf, eq, every)
+                tw = time_to_equilibrium(Pw, Vw, eq, every)
+                k0 = accept_after // every
+                a_w = block_stats(Pw[k0:], Vw[k0:])
+                nb_w, nb_e = (len(Pw) - k0) // 5, len(Pe) // 5
+                ok = (abs(a_w[0] - eq[0]) <= 4 * np.hypot(a_w[1] / np.sqrt(nb_w), eq[1] / np.sqrt(nb_e)) + 1e-12 and
+                      abs(a_w[2] - eq[2]) <= 4 * np.hypot(a_w[3] / np.sqrt(nb_w), eq[3] / np.sqrt(nb_e)) + 1e-12)
+                accepted += int(ok)
+                taus_f.append(probe if tf is None else tf)
+                taus_w.append(probe if tw is None else tw)
+                rows.append([T, ez, taus_f[-1], taus_w[-1], int(ok)])
+                say(f"  point {i}: T {T:.1f} K, E_z {ez:+.5f}: tau fallback {taus_f[-1]}, warm {taus_w[-1]}, "
+                    f"{'accepted' if ok else 'rejected'}")
+        taus_w, taus_f = np.array(taus_w), np.array(taus_f)
+        # the sweep with each point thermalised for its measured time, rejected
+        # warm starts paying both tries
+        eff_w = np.where(np.array([r[4] for r in rows]) == 1, taus_w, taus_w + taus_f)
+        out.update({"held_out": n_held, "probe_steps": probe, "accepted": accepted,
+                    "tau_fallback_median": float(np.median(taus_f)), "tau_warm_median": float(np.median(taus_w)),
+                    "tau_fallback_mean": float(taus_f.mean()), "tau_warm_mean": float(taus_w.mean()),
+                    "warm_faster_points": int(np.sum(taus_w < taus_f)),
+                    "thermalisation_steps_fallback": int(taus_f.sum()),
+                    "thermalisation_steps_warm": int(eff_w.sum()),
+                    "inference_seconds": t_infer, "points": rows})
+    finally:
+        net.close()
+    return out

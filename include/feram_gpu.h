@@ -373,6 +373,46 @@ const char* fg_profile_name(int i);
 int  fg_feram_run(const char* path, int precision, fg_average* avg_out,
                   double* t_sim, char* errbuf, int errlen);
 
+/* ---- learned warm start (no counterpart in the reference) ---------------
+   A periodic 3D convolutional network (3x3x3 kernels, 16 -> 32 -> 32 -> 32
+   -> 16 channels, SiLU, BF16 weights, FP32 accumulation on the tensor cores)
+   that maps a sweep point's condition and a seeded noise field to a proposed
+   local-mode field u(R), to start that point's MD closer to equilibrium than
+   the previous point's state (fg_chain_point, the reference's .restart
+   chaining of cooling.sh:64-69) would.  It is trained on the site statistics
+   of configurations generated by the MD: the mean dipole along the field,
+   |<u>|^2, sum_a <u_a>^4, <|u|^2>, <sum_a u_a^4> and the longitudinal and
+   transverse nearest-neighbour correlations (FG_WS_NSTAT values per sample).
+     cond[b*5 .. +5] = (kelvin, E_x, E_y, E_z [V/A], GPa) of sample b
+     seeds[b]        = the noise seed of sample b
+   A net holds `batch` samples of Lx*Ly*Lz sites (a multiple of 128 sites in
+   all).  Every call runs on the net's own stream and returns when done. */
+#define FG_WS_NSTAT 7
+typedef struct fg_ws fg_ws;
+int  fg_ws_create(int Lx, int Ly, int Lz, int batch, unsigned long long seed, fg_ws** out);
+void fg_ws_destroy(fg_ws* n);
+const char* fg_ws_last_error(const fg_ws* n);
+/* Forward pass of every sample; S (may be NULL) receives [batch][FG_WS_NSTAT]. */
+int  fg_ws_forward(fg_ws* n, const float* cond, const unsigned long long* seeds, float* S);
+/* Forward, the moment-matching loss sum_k w_k (S_k - target_k)^2 averaged
+   over the samples (target [batch][FG_WS_NSTAT], weights [FG_WS_NSTAT]),
+   and its gradients into each layer's dW, db (fg_ws_get_layer). */
+int  fg_ws_backward(fg_ws* n, const float* cond, const unsigned long long* seeds, const float* target,
+                    const float* weights, float* loss);
+/* One Adam step (Kingma & Ba) with the gradients of the last fg_ws_backward. */
+int  fg_ws_adam(fg_ws* n, float lr);
+/* Layer l (0..3): [cout][27][cin] weights (tap t = 9 (dz+1) + 3 (dy+1) +
+   (dx+1)), bias [cout], and their gradients; channel counts padded. */
+int  fg_ws_layer_shape(const fg_ws* n, int l, int* cout, int* cin);
+int  fg_ws_get_layer(fg_ws* n, int l, float* w, float* b, float* dw, float* db);
+int  fg_ws_set_layer(fg_ws* n, int l, const float* w, const float* b);
+/* Of the last forward: the layer-1 input [batch*nsite][16] and the generated
+   u [batch*nsite][3] (sites x + Lx (y + Ly z) per sample); either may be NULL. */
+int  fg_ws_get_io(fg_ws* n, float* input, float* u);
+/* Sample b's generated u in the reference's padded dipoR layout, for
+   fg_set_state. */
+int  fg_ws_field(fg_ws* n, int b, int padding_y, double* dipoR);
+
 /* ---- allocation-free entry point (no counterpart in the reference) -------
    kinetic_energy_dipo (kinetic_energy_dipo.F:14-28) of a momentum field the
    caller already holds in device memory, for callers that cannot allocate at
