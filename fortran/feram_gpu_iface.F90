@@ -122,6 +122,29 @@ module feram_gpu_c
        import :: c_ptr
        type(c_ptr), value :: ctx
      end function fg_last_error
+     ! next sweep point from the device state (replaces the .restart chaining
+     ! of the sweep scripts, e.g. cooling.sh:64-69)
+     integer(c_int) function fg_chain_point(ctx, kelvin, E, e) bind(C, name='fg_chain_point')
+       import :: c_int, c_ptr, c_double, fg_energy
+       type(c_ptr), value :: ctx
+       real(c_double), value :: kelvin
+       real(c_double), intent(in) :: E(3)
+       type(fg_energy), intent(out) :: e
+     end function fg_chain_point
+     ! write_system's .coord (coord_module.F:434-486); full_precision /= 0
+     ! writes 17 significant digits per value
+     integer(c_int) function fg_write_coord(ctx, path, full_precision) bind(C, name='fg_write_coord')
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: ctx
+       character(kind=c_char), intent(in) :: path(*)
+       integer(c_int), value :: full_precision
+     end function fg_write_coord
+     ! the per-step field of molecular-dynamics.F:66-76 evaluated on the device
+     integer(c_int) function fg_set_wave(ctx, on, i_step) bind(C, name='fg_set_wave')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: on, i_step
+     end function fg_set_wave
   end interface
 end module feram_gpu_c
 
@@ -278,4 +301,17 @@ contains
     real(c_double), intent(in) :: E_field_add(3)
     call check(fg_set_uniform_E(gctx, E_field_add), 'fg_set_uniform_E')
   end subroutine gpu_set_field
+
+  ! The next point of a temperature sweep started from the device state, in
+  ! place of reading the previous point's .coord as .restart
+  ! (initialize-dipoR.F:22-38): p / s, the new kelvin and field, the force,
+  ! s = 1, pi = 0 and H0 (molecular-dynamics.F:52-55)
+  subroutine gpu_chain_point(p, e)
+    type(Param_type), intent(in) :: p
+    type(Energy_type), intent(inout) :: e
+    type(fg_energy) :: q
+    call check(fg_chain_point(gctx, real(p%kelvin, c_double), real(p%external_E_field, c_double), q), &
+         & 'fg_chain_point')
+    call from_c_energy(q, e)
+  end subroutine gpu_chain_point
 end module feram_gpu_dropin
