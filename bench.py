@@ -292,10 +292,19 @@ def batched_sweep(n_rep=96, steps=200):
             u, q = initial_state(p)
             r.build_tables()
             prepare(r, p, u, q)
+        # one graph branch per replica, then replicas of one size grouped
+        # into one launch per kernel (fg_batch_step's default)
+        b.set_grouping(False)
         b.step(3)  # warm-up: graph capture and first launches
         t0 = time.perf_counter()
         b.step(steps)
+        t_branch = time.perf_counter() - t0
+        b.set_grouping(True)
+        b.step(3)
+        t0 = time.perf_counter()
+        b.step(steps)
         t_batch = time.perf_counter() - t0
+        groups = b.groups
         # the same replicas, one after another (warm-up captures both the
         # eight-step and the one-step graph of fg_run_steps)
         for r in b.replicas:
@@ -305,7 +314,8 @@ def batched_sweep(n_rep=96, steps=200):
             r.run_steps(steps)
         t_seq = time.perf_counter() - t0
     return {"replicas": n_rep, "sizes": sizes, "kelvin_grid": [450.0, 100.0, -5.0], "sites": sites, "steps": steps, "precision": "mixed",
-            "value": sites * steps / t_batch, "unit": UNIT,
+            "value": sites * steps / t_batch, "unit": UNIT, "graph_branches": groups,
+            "branch_per_replica_value": sites * steps / t_branch,
             "sequential_value": sites * steps / t_seq, "speedup": t_seq / t_batch,
             "timing": "wall clock around synchronous calls"}
 

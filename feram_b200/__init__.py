@@ -295,6 +295,15 @@ class Batch:
             raise FeramError(rc, r.decode() if r else "")
         return list(e)
 
+    def set_grouping(self, on: bool = True):
+        """Replicas of one size step as one launch per kernel (default)."""
+        lib().fg_batch_set_grouping(self._b, 1 if on else 0)
+
+    @property
+    def groups(self) -> int:
+        """Branches of the last captured batch graph."""
+        return lib().fg_batch_groups(self._b)
+
     def close(self):
         if getattr(self, "_b", None):
             for r in self.replicas:

@@ -157,6 +157,8 @@ def lib() -> C.CDLL:
         "fg_chain_point": (C.c_int, [vp, C.c_double, dp, C.POINTER(fg_energy)]),
         "fg_write_coord": (C.c_int, [vp, C.c_char_p, C.c_int]),
         "fg_set_wave": (C.c_int, [vp, C.c_int, C.c_int]),
+        "fg_batch_set_grouping": (C.c_int, [vp, C.c_int]),
+        "fg_batch_groups": (C.c_int, [vp]),
         "fg_ws_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(vp)]),
         "fg_ws_destroy": (None, [vp]),
         "fg_ws_last_error": (C.c_char_p, [vp]),

@@ -306,7 +306,7 @@ int launch_xy_fwd(fg_ctx* ctx, const T* src, cplx<T>* spec, int ncomp, int smem,
   const Geom& g = ctx->g;
   with_xy_fwd<T, MODE>(g.m, g.Ly, [&](auto kern) {
     launch_dep(ctx, kern, dim3(g.Lz, ncomp), kThreadsFFT, smem, src, spec, g, ctx->px, ctx->py, twx, twm, twy,
-               ctx->posm, 0, zstar, zu0);
+               ctx->posm, 0, zstar, zu0, (const RepArgs*)nullptr);
   });
   CKL();
   return FG_OK;
@@ -320,7 +320,8 @@ int launch_xy_inv(fg_ctx* ctx, const cplx<T>* spec, T* out, int ncomp, bool stra
   with_xy_inv<T>(g.m, g.Ly, [&](auto kern) {
     launch_dep(ctx, kern, dim3(g.Lz, ncomp), kThreadsFFT, ctx->smem_xy,
         spec, out, g, ctx->px, ctx->py, (const cplx<T>*)ctx->twx, (const cplx<T>*)ctx->twm, (const cplx<T>*)ctx->twy,
-        ctx->posm, 0, strain_prologue ? ctx->ph : nullptr, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq);
+        ctx->posm, 0, strain_prologue ? ctx->ph : nullptr, ctx->sc, ctx->part_k, ctx->zt.nreg + ctx->zt.nnyq,
+        (const RepArgs*)nullptr);
   });
   CKL();
   return FG_OK;
@@ -334,7 +335,7 @@ int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
     launch_dep(ctx, kern, ctx->zt.nreg + ctx->zt.nnyq, kThreadsZ, ctx->smem_z,
         (cplx<T>*)ctx->spec, (const T*)ctx->dtab, (const cplx<T>*)ctx->ckmod, acouK_out, g, ctx->pz,
         (const cplx<T>*)ctx->twz, kmaps<T>(ctx), ctx->ph, ctx->part_k, ctx->sc, ctx->zt, nullptr,
-        (const T*)ctx->ltab);
+        (const T*)ctx->ltab, (const RepArgs*)nullptr);
   });
   CKL();
   return FG_OK;
@@ -364,7 +365,8 @@ void launch_assemble(fg_ctx* ctx, int tail, bool flo = false) {
              (const T*)ctx->rwork, (const T*)ctx->u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, tail,
              ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
              ctx->zsite ? zu_comp(ctx) : 0, (T*)ctx->p, ctx->layer_minv, ctx->layer_sump, (const T*)ctx->site_minv,
-             ctx->site_sump, ctx->part_ke, (flo && sizeof(T) == 4) ? (T*)ctx->Flo : (T*)nullptr, asm_const(ctx));
+             ctx->site_sump, ctx->part_ke, (flo && sizeof(T) == 4) ? (T*)ctx->Flo : (T*)nullptr, asm_const(ctx),
+             (const RepArgs*)nullptr);
 }
 
 // Force modes: FORCE_PLAIN finishes the energies in k_assemble's tail;
@@ -467,7 +469,7 @@ int enqueue_wave(fg_ctx* ctx) {
 template <typename T>
 int enqueue_kick_drift(fg_ctx* ctx) {
   launch_dep(ctx, k_kick_drift<T>, ctx->grid_kd, kThreadsElem, 0, (T*)ctx->p, (T*)ctx->u, (const T*)ctx->F,
-             ctx->sc, ctx->g, ctx->layer_minv, (const T*)ctx->site_minv);
+             ctx->sc, ctx->g, ctx->layer_minv, (const T*)ctx->site_minv, (const RepArgs*)nullptr);
   CKL();
   return FG_OK;
 }
@@ -549,6 +551,80 @@ int enqueue_vs(fg_ctx* ctx) {
     CKL();
   }
   return FG_OK;
+}
+
+// ---------------------------------------------------------- grouped steps
+// A bulk Nose-Poincare step of nrep replicas of c0's size, precision and
+// material as one launch per kernel (the fused five-kernel step of
+// enqueue_np), each replica's buffers taken from the device table grp.
+template <typename T>
+int enqueue_np_group(fg_ctx* c0, const RepArgs* grp, int nrep) {
+  fg_ctx* ctx = c0;  // for CKL
+  const Geom& g = c0->g;
+  c0->pdl = false;
+  launch_dep(c0, k_kick_drift<T>, dim3(c0->grid_kd, nrep), kThreadsElem, 0, (T*)nullptr, (T*)nullptr,
+             (const T*)nullptr, (const DevScalars*)nullptr, g, (const double*)nullptr, (const T*)nullptr, grp);
+  CKL();
+  c0->pdl = true;
+  with_xy_fwd<T, SRC_U9>(g.m, g.Ly, [&](auto kern) {
+    launch_dep(c0, kern, dim3(g.Lz, c0->ncx, nrep), kThreadsFFT, c0->smem_xy, (const T*)nullptr, (cplx<T>*)nullptr,
+               g, c0->px, c0->py, (const cplx<T>*)c0->twx, (const cplx<T>*)c0->twm, (const cplx<T>*)c0->twy,
+               c0->posm, 0, (const T*)nullptr, 0, grp);
+  });
+  CKL();
+  with_z_kspace<T>(g.Lz, c0->zt.CW, false, false, [&](auto kern) {
+    launch_dep(c0, kern, dim3(c0->zt.nreg + c0->zt.nnyq, nrep), kThreadsZ, c0->smem_z, (cplx<T>*)nullptr,
+               (const T*)nullptr, (const cplx<T>*)c0->ckmod, (cplx<T>*)nullptr, g, c0->pz, (const cplx<T>*)c0->twz,
+               kmaps<T>(c0), (const Phys*)nullptr, (double*)nullptr, (DevScalars*)nullptr, c0->zt,
+               (unsigned int*)nullptr, (const T*)nullptr, grp);
+  });
+  CKL();
+  with_xy_inv<T>(g.m, g.Ly, [&](auto kern) {
+    launch_dep(c0, kern, dim3(g.Lz, c0->ncx, nrep), kThreadsFFT, c0->smem_xy, (const cplx<T>*)nullptr, (T*)nullptr, g,
+               c0->px, c0->py, (const cplx<T>*)c0->twx, (const cplx<T>*)c0->twm, (const cplx<T>*)c0->twy, c0->posm,
+               0, (const Phys*)c0->ph, (DevScalars*)nullptr, (const double*)nullptr, c0->zt.nreg + c0->zt.nnyq, grp);
+  });
+  CKL();
+  launch_dep(c0, k_assemble<T, true>, dim3(c0->grid_asc, nrep), kThreadsElem, 0, (const T*)nullptr,
+             (const T*)nullptr, (T*)nullptr, g, (const Phys*)nullptr, (DevScalars*)nullptr, (double*)nullptr,
+             (int)TAIL_NONE, (unsigned int*)nullptr, (const unsigned char*)nullptr, (const T*)nullptr,
+             (const T*)nullptr, 0, (T*)nullptr, (const double*)nullptr, (const unsigned char*)nullptr,
+             (const T*)nullptr, (const unsigned char*)nullptr, (double*)nullptr, (T*)nullptr, asm_const(c0), grp);
+  CKL();
+  c0->pdl = false;
+  return FG_OK;
+}
+
+// A replica that a grouped launch can step: bulk Nose-Poincare without the
+// acoustic field, per-site arrays, modulation or a device field schedule.
+bool groupable(const fg_ctx* c) {
+  return c->P.method == FG_METHOD_MD && !c->bulk_or_film_mirror() && !c->acou && !c->zsite && !c->site_species &&
+         !c->site_zstar && !c->site_E && !c->site_minv && !c->site_sump && !c->wave_dev &&
+         c->ph_host.modulation_on == 0 && !c->broken;
+}
+// Replicas a and b step together: same size, precision and site constants.
+bool same_group(const fg_ctx* a, const fg_ctx* b) {
+  if (a->prec != b->prec || a->g.Lx != b->g.Lx || a->g.Ly != b->g.Ly || a->g.Lz != b->g.Lz) return false;
+  const AsmConst ka = asm_const(a), kb = asm_const(b);
+  return std::memcmp(&ka, &kb, sizeof(AsmConst)) == 0;
+}
+RepArgs rep_args(const fg_ctx* c) {
+  RepArgs a{};
+  a.u = c->u;
+  a.p = c->p;
+  a.F = c->F;
+  a.spec = c->spec;
+  a.rwork = c->rwork;
+  a.dtab = c->dtab;
+  a.ph = c->ph;
+  a.sc = c->sc;
+  a.part_k = c->part_k;
+  a.part_r = c->part_r;
+  a.part_ke = c->part_ke;
+  a.done_as = c->done + 2;
+  a.layer_minv = c->layer_minv;
+  a.layer_sump = c->layer_sump;
+  return a;
 }
 
 // Capture fn into a CUDA graph executable (once per context).
@@ -2227,6 +2303,9 @@ struct fg_batch {
   std::vector<cudaEvent_t> join;
   cudaGraphExec_t graph = nullptr;   // one step of every replica
   std::vector<unsigned> gen;         // the replicas' gen when the graphs were captured
+  bool grouping = true;              // replicas of one size step as one launch per kernel
+  std::vector<std::vector<int>> groups;  // of the captured graph: replica indices per branch
+  std::vector<RepArgs*> grp_dev;     // device tables of the grouped branches
   std::string err;
 };
 
@@ -2238,22 +2317,69 @@ int batch_fail(fg_batch* b, int rc, const std::string& msg) {
 // The batch graph of one step: a branch per replica, forked from and joined
 // into the batch stream.  (Eight steps per branch, as fg_run_steps uses,
 // measured no faster here: the branches already overlap.)
+void free_groups(fg_batch* b) {
+  for (RepArgs* p : b->grp_dev)
+    if (p) cudaFree(p);
+  b->grp_dev.clear();
+  b->groups.clear();
+}
+
+// Branches of the batch graph: groups of replicas that one launch per kernel
+// steps (enqueue_np_group), and single replicas (enqueue_step).  The device
+// tables of the groups are written before the capture.
+int plan_groups(fg_batch* b) {
+  free_groups(b);
+  std::vector<bool> used(b->ctx.size(), false);
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    if (used[i]) continue;
+    std::vector<int> grp{(int)i};
+    used[i] = true;
+    if (b->grouping && groupable(b->ctx[i]))
+      for (size_t j = i + 1; j < b->ctx.size(); ++j)
+        if (!used[j] && groupable(b->ctx[j]) && same_group(b->ctx[i], b->ctx[j])) {
+          grp.push_back((int)j);
+          used[j] = true;
+        }
+    RepArgs* dev = nullptr;
+    if (grp.size() > 1) {
+      std::vector<RepArgs> h;
+      for (int k : grp) h.push_back(rep_args(b->ctx[(size_t)k]));
+      cudaError_t e = cudaMalloc(&dev, h.size() * sizeof(RepArgs));
+      if (e == cudaSuccess) e = cudaMemcpy(dev, h.data(), h.size() * sizeof(RepArgs), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        if (dev) cudaFree(dev);
+        return batch_fail(b, FG_ERR_CUDA, std::string("batch groups: ") + cudaGetErrorString(e));
+      }
+    }
+    b->groups.push_back(grp);
+    b->grp_dev.push_back(dev);
+  }
+  return FG_OK;
+}
+
 int batch_capture(fg_batch* b, cudaGraphExec_t* out) {
   if (*out) return FG_OK;
+  int rc = plan_groups(b);
+  if (rc) return rc;
   cudaGraph_t graph;
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(e));
-  int rc = FG_OK;
   if ((e = cudaEventRecord(b->fork, b->stream)) != cudaSuccess) rc = FG_ERR_CUDA;
-  for (size_t i = 0; i < b->ctx.size() && rc == FG_OK; ++i) {
-    fg_ctx* c = b->ctx[i];
+  for (size_t gi = 0; gi < b->groups.size() && rc == FG_OK; ++gi) {
+    const std::vector<int>& grp = b->groups[gi];
+    fg_ctx* c = b->ctx[(size_t)grp[0]];
     if ((e = cudaStreamWaitEvent(c->stream, b->fork, 0)) != cudaSuccess) { rc = FG_ERR_CUDA; break; }
-    if ((rc = enqueue_step(c))) {
-      b->err = "replica " + std::to_string(i) + ": " + c->err;
+    if (grp.size() > 1)
+      rc = c->prec == FG_PREC_MIXED ? enqueue_np_group<float>(c, b->grp_dev[gi], (int)grp.size())
+                                    : enqueue_np_group<double>(c, b->grp_dev[gi], (int)grp.size());
+    else
+      rc = enqueue_step(c);
+    if (rc) {
+      b->err = "replica " + std::to_string(grp[0]) + ": " + c->err;
       break;
     }
-    if ((e = cudaEventRecord(b->join[i], c->stream)) != cudaSuccess ||
-        (e = cudaStreamWaitEvent(b->stream, b->join[i], 0)) != cudaSuccess)
+    if ((e = cudaEventRecord(b->join[gi], c->stream)) != cudaSuccess ||
+        (e = cudaStreamWaitEvent(b->stream, b->join[gi], 0)) != cudaSuccess)
       rc = FG_ERR_CUDA;
   }
   cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
@@ -2270,7 +2396,9 @@ extern "C" {
 
 void fg_batch_destroy(fg_batch* b) {
   if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  free_groups(b);
   for (cudaEvent_t ev : b->join)
     if (ev) cudaEventDestroy(ev);
   if (b->fork) cudaEventDestroy(b->fork);
@@ -2314,6 +2442,21 @@ int fg_batch_create(int n, const fg_params* params, int precision, fg_batch** ou
 }
 
 int fg_batch_size(const fg_batch* b) { return b ? (int)b->ctx.size() : 0; }
+
+int fg_batch_set_grouping(fg_batch* b, int on) {
+  if (!b) return FG_ERR_ARG;
+  if ((on != 0) != b->grouping) {
+    b->grouping = on != 0;
+    if (b->graph) {
+      cudaStreamSynchronize(b->stream);
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+  }
+  return FG_OK;
+}
+
+int fg_batch_groups(const fg_batch* b) { return b ? (int)b->groups.size() : 0; }
 
 fg_ctx* fg_batch_context(fg_batch* b, int i) {
   return (b && i >= 0 && i < (int)b->ctx.size()) ? b->ctx[(size_t)i] : nullptr;

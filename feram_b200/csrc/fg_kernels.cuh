@@ -93,6 +93,28 @@ struct DevScalars {
   int pad;
 };
 
+// Per-replica buffers of a grouped launch: replicas of one supercell size,
+// precision and material (the points of a sweep) stepped by one launch per
+// kernel, the replica index being the grid's last dimension.  Each kernel
+// that takes a RepArgs table replaces its per-replica pointer arguments by
+// its replica's entry; null = a launch for one context.
+struct RepArgs {
+  void* u;
+  void* p;
+  void* F;
+  void* spec;
+  void* rwork;
+  const void* dtab;
+  const Phys* ph;
+  DevScalars* sc;
+  double* part_k;
+  double* part_r;
+  double* part_ke;
+  unsigned int* done_as;  // k_assemble's last-block ticket
+  const double* layer_minv;
+  const unsigned char* layer_sump;
+};
+
 // ---------------------------------------------------------------- reductions
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -290,8 +312,13 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
                                                 FftPlan px, FftPlan py, const cplx<T>* __restrict__ twx,
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int out_comp0,
-                                                const T* __restrict__ zstar = nullptr, int zu0 = 0) {
+                                                const T* __restrict__ zstar = nullptr, int zu0 = 0,
+                                                const RepArgs* __restrict__ grp = nullptr) {
   pdl_enter();
+  if (grp) {
+    src = (const T*)grp[blockIdx.z].u;
+    spec = (cplx<T>*)grp[blockIdx.z].spec;
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
@@ -449,8 +476,17 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
                                                 const cplx<T>* __restrict__ twm, const cplx<T>* __restrict__ twy,
                                                 const int* __restrict__ posm, int in_comp0,
                                                 const Phys* __restrict__ ph, DevScalars* sc,
-                                                const double* __restrict__ part_k, int nblk_k) {
+                                                const double* __restrict__ part_k, int nblk_k,
+                                                const RepArgs* __restrict__ grp = nullptr) {
   pdl_enter();
+  if (grp) {
+    const RepArgs& a = grp[blockIdx.z];
+    spec = (const cplx<T>*)a.spec;
+    out = (T*)a.rwork;
+    if (ph != nullptr) ph = a.ph;
+    sc = a.sc;
+    part_k = a.part_k;
+  }
   // Block (0, 0) first finishes the k-space pass that wrote spec: its
   // energies and the homogeneous strain, from k_z_kspace's block partials
   // (nothing in this kernel needs them; k_assemble does).
@@ -485,14 +521,17 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
         return *a;
       }
     };
-    // column 0 carries the kx = 0 and kx = Lx/2 columns joined (y_join)
+    // column 0 carries the kx = 0 and kx = Lx/2 columns joined (y_join),
+    // formed by one pass of LYC threads into shared memory first (the stage
+    // below reads it from there and writes its outputs in place)
     const int* revy = posm + MC;
     const int* posy = posm + MC + LYC;
-    auto ldj = [&](int col, int e) {
-      if (col != 0) return ld(col, e);
-      const int sp = __ldg(&posy[(LYC - __ldg(&revy[e])) % LYC]);
-      return y_join(ld(0, e), ld(0, sp), ld(MC, e), ld(MC, sp));
-    };
+    for (int sl = threadIdx.x; sl < LYC; sl += kXYThreads) {
+      const int sp = __ldg(&posy[(LYC - __ldg(&revy[sl])) % LYC]);
+      buf[sl * (MC + 1)] = y_join(ld(0, sl), ld(0, sp), ld(MC, sl), ld(MC, sp));
+    }
+    __syncthreads();
+    auto ldj = [&](int col, int e) { return col == 0 ? buf[e * (MC + 1)] : ld(col, e); };
     auto st = [&](int col, int e, const cplx<T>& v) { buf[col + e * (MC + 1)] = v; };
     ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, MC, false>(ldj, st, tws_y);
     __syncthreads();
@@ -908,8 +947,16 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
                                                      Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
                                                      const Phys* __restrict__ ph, double* __restrict__ part,
                                                      DevScalars* sc, ZTiles zt, unsigned int* done,
-                                                     const T* __restrict__ ltab) {
+                                                     const T* __restrict__ ltab, const RepArgs* __restrict__ grp = nullptr) {
   pdl_enter();
+  if (grp) {
+    const RepArgs& a = grp[blockIdx.y];
+    spec = (cplx<T>*)a.spec;
+    dtab = (const T*)a.dtab;
+    ph = a.ph;
+    part = a.part_k;
+    sc = a.sc;
+  }
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
@@ -1366,8 +1413,22 @@ __global__ void __launch_bounds__(256, 2)
                const T* __restrict__ site_E, int zl0, T* __restrict__ p, const double* __restrict__ layer_minv,
                const unsigned char* __restrict__ layer_sump, const T* __restrict__ site_minv,
                const unsigned char* __restrict__ site_sump, double* __restrict__ part_ke, T* __restrict__ Flo,
-               const AsmConst k) {
+               const AsmConst k, const RepArgs* __restrict__ grp = nullptr) {
   pdl_enter();
+  if (grp) {
+    const RepArgs& a = grp[blockIdx.y];
+    rw = (const T*)a.rwork;
+    u = (const T*)a.u;
+    F = (T*)a.F;
+    ph = a.ph;
+    sc = a.sc;
+    part = a.part_r;
+    done = a.done_as;
+    p = (T*)a.p;
+    layer_minv = a.layer_minv;
+    layer_sump = a.layer_sump;
+    part_ke = a.part_ke;
+  }
   // site_*: per-site species (.relaxor), Z* and local field (.localfield);
   // they take the scalar loop.  zl0 > 0: rw components zl0..zl0+2 hold the
   // long-range dipole field of Z* u, which acts on the site times its Z*
@@ -1704,8 +1765,17 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __restrict__ u, const T* __restrict__ F,
                                                     const DevScalars* __restrict__ sc, Geom g,
                                                     const double* __restrict__ layer_minv,
-                                                    const T* __restrict__ site_minv = nullptr) {
+                                                    const T* __restrict__ site_minv = nullptr,
+                                                    const RepArgs* __restrict__ grp = nullptr) {
   pdl_enter();
+  if (grp) {
+    const RepArgs& a = grp[blockIdx.y];
+    p = (T*)a.p;
+    u = (T*)a.u;
+    F = (const T*)a.F;
+    sc = a.sc;
+    layer_minv = a.layer_minv;
+  }
   const long long ns = g.nsite;
   const T ck = (T)sc->kick_coef;
   const double cd = sc->pend_drift;

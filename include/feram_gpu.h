@@ -347,8 +347,18 @@ int  fg_batch_size(const fg_batch* b);
 fg_ctx* fg_batch_context(fg_batch* b, int i);
 const char* fg_batch_last_error(const fg_batch* b);
 /* n_steps steps of every replica's method (lf: i_step != 0); e (may be NULL)
-   receives each replica's energies of the last step, e[i] for replica i. */
+   receives each replica's energies of the last step, e[i] for replica i.
+   Replicas of one supercell size, precision and set of on-site constants
+   that run bulk Nose-Poincare without per-site arrays, modulation or a
+   device field schedule (typically the temperature points of a sweep) are
+   stepped as one group: one launch per kernel of the step for all of them,
+   the replica index in the grid; the others get a graph branch each. */
 int  fg_batch_step(fg_batch* b, int n_steps, fg_energy* e);
+/* Grouped launches on (default) or off (a graph branch per replica); the
+   results are the same bit for bit. */
+int  fg_batch_set_grouping(fg_batch* b, int on);
+/* Branches of the batch graph last captured (groups and single replicas). */
+int  fg_batch_groups(const fg_batch* b);
 
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */

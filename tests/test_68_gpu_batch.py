@@ -138,3 +138,32 @@ def test_batch_epit_field_waves_match_oracle(fg):
         for f in ("total", "dipole_E_field", "unharmonic", "dipo_kinetic"):
             a, c = getattr(es[i], f), getattr(eo, f)
             assert abs(a - c) <= 1e-9 * max(abs(c), 1e-3), (i, f, a, c)
+
+
+@pytest.mark.parametrize("prec", [A.FG_PREC_FP64, A.FG_PREC_MIXED])
+def test_grouped_replicas_equal_branches(fg, prec):
+    """Replicas of one size (a temperature sweep's points) stepped as one
+    launch per kernel give bit for bit what a graph branch per replica
+    gives; a replica of another size and a 'vs' replica keep their branches."""
+    ps = [helpers.params(L="16 16 16", kelvin=str(400 - 50 * i)) for i in range(4)]
+    ps += [helpers.params(L="8 8 8", kelvin="250"), helpers.params(L="16 16 16", kelvin="300", method="'vs'")]
+    states = [(helpers.seeded_u(p, 70 + i, sigma=0.05), helpers.seeded_p(p, 70 + i, sigma=0.01))
+              for i, p in enumerate(ps)]
+    out = {}
+    for grouping in (False, True):
+        with fb.Batch(ps, prec) as b:
+            b.set_grouping(grouping)
+            for r, (u, q) in zip(b.replicas, states):
+                r.build_tables()
+                r.set_state(u, q)
+                r.mirror_force_mirror()
+            es = b.step(7)
+            out[grouping] = ([r.get_state() for r in b.replicas], es, b.groups)
+    assert out[False][2] == len(ps) and out[True][2] == 3
+    for i, p in enumerate(ps):
+        a, c = out[False][0][i], out[True][0][i]
+        for k in ("dipoR", "dipoP", "dVddi"):
+            assert np.array_equal(A.physical(a[k], p), A.physical(c[k], p)), (i, k)
+        assert a["s"] == c["s"] and a["pi"] == c["pi"]
+        for f in A.POTENTIAL_FIELDS + ["dipo_kinetic", "total", "H_Nose_Poincare"]:
+            assert getattr(out[False][1][i], f) == getattr(out[True][1][i], f), (i, f)

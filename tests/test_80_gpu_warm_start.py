@@ -42,13 +42,12 @@ def _torch_stats(u, e):
                         (u ** 4).sum(1).mean(dim=(1, 2, 3)), cl, ct], dim=1)
 
 
-def _reference(net, x, cond, target, wts):
-    B = net.batch
-    Lx, Ly, Lz = net.L
+def _reference(layers, B, L, x, cond, target, wts):
+    Lx, Ly, Lz = L
     h = torch.tensor(x).reshape(B, Lz, Ly, Lx, 16).permute(0, 4, 1, 2, 3).contiguous()
     params = []
     for l in range(4):
-        w, b, _, _ = net.layer(l)
+        w, b = layers[l]
         wt = torch.tensor(w).reshape(w.shape[0], 3, 3, 3, w.shape[2]).permute(0, 4, 1, 2, 3).contiguous()
         wt = _bf(wt).requires_grad_(True)
         bt = torch.tensor(b).requires_grad_(True)
@@ -79,8 +78,9 @@ def test_network_forward_and_gradients_match_torch(fg, L, batch):
         loss_dev = net.backward(cond, seeds, target, wts)
         x, u_dev = net.io()
         S_dev = net.forward(cond, seeds)
-        grads = [net.layer(l)[2:] for l in range(4)]
-    u_ref, S_ref, loss_ref, params = _reference(net, x, cond, target, wts)
+        lay = [net.layer(l) for l in range(4)]
+    grads = [(dw, db) for _, _, dw, db in lay]
+    u_ref, S_ref, loss_ref, params = _reference([(w, b) for w, b, _, _ in lay], batch, L, x, cond, target, wts)
     Lx, Ly, Lz = L
     u_ref = u_ref.detach().permute(0, 2, 3, 4, 1).reshape(-1, 3).numpy()
     assert np.abs(u_dev - u_ref).max() <= 1e-3 * np.abs(u_ref).max(), np.abs(u_dev - u_ref).max()
