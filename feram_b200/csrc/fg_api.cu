@@ -133,6 +133,8 @@ struct fg_ctx {
   double2* trx = nullptr;
   double2* try_ = nullptr;
   double2* trz = nullptr;
+  double2* trz_s = nullptr;  // trz and kvz in kz-slot order
+  double* kvz_s = nullptr;
   double* layer_minv = nullptr;
   unsigned char* layer_sump = nullptr;
   // acoustic-displacement MD (acoustic mass > 0): u, p and F hold three more
@@ -205,7 +207,7 @@ int fail(fg_ctx* c, int code, const std::string& msg) {
 
 template <typename T>
 KMaps kmaps(const fg_ctx* c) {
-  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz};
+  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz, c->trz_s, c->kvz_s};
 }
 
 int check_device_error(fg_ctx* ctx) {
@@ -349,11 +351,9 @@ int launch_z_kspace(fg_ctx* ctx, cplx<T>* acouK_out) {
 AsmConst asm_const(const fg_ctx* ctx) {
   const Phys& h = ctx->ph_host;
   AsmConst k{};
-  k.fa2g = h.fa2g; k.tg = h.tg; k.sk = h.sk; k.tk2 = h.tk2; k.fk = h.fk;
-  k.k4x8 = 8 * h.P_k4;
+  k.pl = Poly{h.fa2g, h.tg, h.sk, h.tk2, h.fk, 8 * h.P_k4, h.P_alpha, h.P_gamma, h.P_k1, h.P_k2, h.P_k3, h.P_k4};
   k.hx = h.HC2[0][0]; k.hy = h.HC2[0][1]; k.h4 = h.HC2[3][3];
   k.Zs = h.Zstar;
-  k.Pa = h.P_alpha; k.Pg = h.P_gamma; k.P1 = h.P_k1; k.P2 = h.P_k2; k.P3 = h.P_k3; k.P4 = h.P_k4;
   k.E_on = h.E_on;
   return k;
 }
@@ -882,6 +882,17 @@ int create_impl(fg_ctx* ctx) {
     if ((rc = upload(ctx, (void**)&ctx->trx, trig(g.NKX, P.Lx)))) return rc;
     if ((rc = upload(ctx, (void**)&ctx->try_, trig(g.Ly, P.Ly)))) return rc;
     if ((rc = upload(ctx, (void**)&ctx->trz, trig(g.Lz, P.Lz)))) return rc;
+    {
+      const std::vector<double2> tz = trig(g.Lz, P.Lz);
+      std::vector<double2> tzs(g.Lz);
+      std::vector<double> kzs(g.Lz);
+      for (int sl = 0; sl < g.Lz; ++sl) {
+        tzs[sl] = tz[ctx->h_revz[sl]];
+        kzs[sl] = kz[ctx->h_revz[sl]];
+      }
+      if ((rc = upload(ctx, (void**)&ctx->trz_s, tzs))) return rc;
+      if ((rc = upload(ctx, (void**)&ctx->kvz_s, kzs))) return rc;
+    }
   }
   // per-layer masses and masks (alloc_Coord, read_defects_u.F:52-69)
   {
@@ -1619,7 +1630,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
   void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->Flo, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->ltab, ctx->revx,
-                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz,
+                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz, ctx->trz_s, ctx->kvz_s,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
                   ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all,
                   ctx->site_minv, ctx->site_macou, ctx->site_sump, ctx->site_species, ctx->site_zstar, ctx->site_E,

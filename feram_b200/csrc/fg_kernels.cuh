@@ -894,6 +894,8 @@ struct KMaps {
   const double2* trx;  // (cos, sin)(2 pi kx / Lx)
   const double2* try_;
   const double2* trz;
+  const double2* trz_s;  // trz and kvz in kz-slot order (no revz lookup first)
+  const double* kvz_s;
 };
 
 // Plain z pass of nc spectra in place: DIF (INV = false) or DIT (INV = true).
@@ -1063,13 +1065,13 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   const T w1 = (kx == 0 || kx == g.m) ? (T)1 : (T)2;  // full-spectrum multiplicity
   const long long tpos0 = (long long)yslot * Lz * g.KXP + col;
   for (int zs = threadIdx.x / CW; pencil_ok && zs < Lz; zs += blockDim.x / CW) {
-    const int kz = __ldg(&km.revz[zs]);
     cplx<T> u[3], d[6];
 #pragma unroll
     for (int a = 0; a < 3; ++a) u[a] = buf[a * ZS + zs * CW + cw];
 #pragma unroll
     for (int i = 0; i < 6; ++i) d[i] = buf[(3 + i) * ZS + zs * CW + cw];
-    if (kx == 0 && ky == 0 && kz == 0) {
+    const bool k0 = kx == 0 && ky == 0 && zs == 0;  // slot 0 holds kz = 0
+    if (k0) {
 #pragma unroll
       for (int i = 0; i < 6; ++i) sc->didiK0[i] = (double)d[i].x;
       __threadfence();  // read by homo_strain_tail in another block
@@ -1095,7 +1097,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     {
       // short- and total dipole energies in FP64 from the same qv, so that
       // their difference (the long-range energy) keeps its digits
-      const double2 tz = __ldg(&km.trz[kz]);
+      const double2 tz = __ldg(&km.trz_s[zs]);
       double S[6];
       S[0] = sA[0] + sB[0] * tz.x;
       S[1] = sA[1] + sB[1] * tz.x;
@@ -1142,7 +1144,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     F[1] = mk<cplx<T>>(D[5] * u[0].x + D[1] * u[1].x + D[3] * u[2].x, D[5] * u[0].y + D[1] * u[1].y + D[3] * u[2].y);
     F[2] = mk<cplx<T>>(D[4] * u[0].x + D[3] * u[1].x + D[2] * u[2].x, D[4] * u[0].y + D[3] * u[1].y + D[2] * u[2].y);
     // ---- inhomogeneous strain
-    const T k1 = (T)kv1, k2 = (T)kv2, k3 = (T)__ldg(&km.kvz[kz]);
+    const T k1 = (T)kv1, k2 = (T)kv2, k3 = (T)__ldg(&km.kvz_s[zs]);
     const T kk[4] = {(T)0, k1, k2, k3};
     const T B11 = (T)ph->B11, B12 = (T)ph->B12, B44 = (T)ph->B44;
     T K[3][3];
@@ -1155,17 +1157,10 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         else K[a - 1][b - 1] = B12 * kk[a] * kk[b] + B44 * kk[a] * kk[b];
       }
     }
-    // coup2(a, i) (elastic.F:156-180)
+    // coup2 . didiK with coup2(a, i) of elastic.F:156-180: k_a B1xx/2 on
+    // i = a, k_a B1yy/2 on the other two diagonal entries, k_c B4yz on the
+    // shear entries (yz: b = y, c = z ...) that involve a, zero on the third
     const T hx = (T)(ph->HC2[0][0]), hy = (T)(ph->HC2[0][1]), h4 = (T)(ph->HC2[3][3]);
-    T C2[3][6];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-      for (int i = 0; i < 3; ++i) C2[a][i] = (a == i) ? kk[a + 1] * hx : kk[a + 1] * hy;
-    }
-    C2[0][3] = (T)0 * h4; C2[1][3] = k3 * h4; C2[2][3] = k2 * h4;
-    C2[0][4] = k3 * h4;   C2[1][4] = (T)0 * h4; C2[2][4] = k1 * h4;
-    C2[0][5] = k2 * h4;   C2[1][5] = k1 * h4; C2[2][5] = (T)0 * h4;
     cplx<T> ck[3] = {mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0)};
     if (ph->modulation_on) {
 #pragma unroll
@@ -1173,12 +1168,15 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     }
     // rhs = -(c_k_mod + coup2 . didiK)  (optimize-inho-strain.F:28-45)
     cplx<T> cs[3], acou[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      cplx<T> t = mk<cplx<T>>((T)0, (T)0);
-#pragma unroll
-      for (int i = 0; i < 6; ++i) t = mk<cplx<T>>(t.x + C2[a][i] * d[i].x, t.y + C2[a][i] * d[i].y);
-      cs[a] = t;
+    {
+      auto comb = [&](T ka, int ia, int ib, int ic, T kb, int sb, T kc, int sc_) {
+        // ka (hx d_ia + hy (d_ib + d_ic)) + h4 (kb d_sb + kc d_sc)
+        return mk<cplx<T>>(ka * (hx * d[ia].x + hy * (d[ib].x + d[ic].x)) + h4 * (kb * d[sb].x + kc * d[sc_].x),
+                           ka * (hx * d[ia].y + hy * (d[ib].y + d[ic].y)) + h4 * (kb * d[sb].y + kc * d[sc_].y));
+      };
+      cs[0] = comb(k1, 0, 1, 2, k3, 4, k2, 5);
+      cs[1] = comb(k2, 1, 0, 2, k3, 3, k1, 5);
+      cs[2] = comb(k3, 2, 0, 1, k2, 3, k1, 4);
     }
     if constexpr (ACOU) {
       // dynamic acoustic field: acouK = i FFT(acouR) (acouFFT.F:22);
@@ -1211,7 +1209,7 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         const cplx<T> v = mk<cplx<T>>(ck[a].x + cs[a].x + KA[a].x, ck[a].y + cs[a].y + KA[a].y);
         buf[(9 + a) * ZS + zs * CW + cw] = mk<cplx<T>>(v.y * ni, -v.x * ni);
       }
-    } else if (kx == 0 && ky == 0 && kz == 0) {
+    } else if (k0) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) acou[a] = mk<cplx<T>>((T)0, (T)0);  // inhomo_K_G(:,:,0,0,0) = 0
     } else {
@@ -1319,11 +1317,16 @@ __device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V
 // local terms carry the largest forces (|F| up to ~30x the rms force on the
 // tail sites of a sigma = 0.1 A configuration), so evaluating them in FP32
 // would put their rounding (~1e-6 of the rms force) on exactly those sites.
+// On-site polynomial of one species: force combinations and energy
+// coefficients (dVddi-unharmonic.F:28-32,67-99)
+struct Poly {
+  double fa2g, tg, sk, tk2, fk, k4x8;
+  double Pa, Pg, P1, P2, P3, P4;
+};
 struct AsmConst {
-  double fa2g, tg, sk, tk2, fk, k4x8;  // anharmonic force constants
+  Poly pl;                             // species 1 (the bulk sweeps)
   double hx, hy, h4;                   // homogeneous_coupling_2: B1xx/2, B1yy/2, B4yz
   double Zs;
-  double Pa, Pg, P1, P2, P3, P4;       // energy coefficients (dVddi-unharmonic.F:67-99)
   int E_on;
   int pad;
 };
@@ -1335,23 +1338,23 @@ struct AsmDyn {
 };
 
 // Force on one site from F_dd, u and eta (see k_assemble); acc += energies.
-__device__ __forceinline__ void assemble_site(const AsmConst& k, const AsmDyn& dy, double ux, double uy, double uz,
-                                              double f0, double f1, double f2, const double* eta, double& o0,
-                                              double& o1, double& o2, double* acc) {
+__device__ __forceinline__ void assemble_site(const Poly& pl, const AsmConst& k, const AsmDyn& dy, double ux,
+                                              double uy, double uz, double f0, double f1, double f2,
+                                              const double* eta, double& o0, double& o1, double& o2, double* acc) {
   const double d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
   const double uu = d0 + d1 + d2;
   // 4th order
-  f0 = f0 + ux * (k.fa2g * uu - k.tg * d0);
-  f1 = f1 + uy * (k.fa2g * uu - k.tg * d1);
-  f2 = f2 + uz * (k.fa2g * uu - k.tg * d2);
+  f0 = f0 + ux * (pl.fa2g * uu - pl.tg * d0);
+  f1 = f1 + uy * (pl.fa2g * uu - pl.tg * d1);
+  f2 = f2 + uz * (pl.fa2g * uu - pl.tg * d2);
   // 6th and 8th order
   const double uu2 = uu * uu, uu3 = uu2 * uu;
-  f0 = f0 + ux * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d0 * d0) - k.fk * d1 * d2);
-  f1 = f1 + uy * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d1 * d1) - k.fk * d2 * d0);
-  f2 = f2 + uz * (k.sk * uu2 + k.k4x8 * uu3 - k.tk2 * (d2 * d2) - k.fk * d0 * d1);
-  acc[0] += k.Pa * uu2 + k.Pg * (d0 * d1 + d1 * d2 + d2 * d0) + k.P1 * uu3 +
-            k.P2 * ((d0 * d0) * (d1 + d2) + (d1 * d1) * (d2 + d0) + (d2 * d2) * (d0 + d1)) + k.P3 * d0 * d1 * d2 +
-            k.P4 * (uu2 * uu2);
+  f0 = f0 + ux * (pl.sk * uu2 + pl.k4x8 * uu3 - pl.tk2 * (d0 * d0) - pl.fk * d1 * d2);
+  f1 = f1 + uy * (pl.sk * uu2 + pl.k4x8 * uu3 - pl.tk2 * (d1 * d1) - pl.fk * d2 * d0);
+  f2 = f2 + uz * (pl.sk * uu2 + pl.k4x8 * uu3 - pl.tk2 * (d2 * d2) - pl.fk * d0 * d1);
+  acc[0] += pl.Pa * uu2 + pl.Pg * (d0 * d1 + d1 * d2 + d2 * d0) + pl.P1 * uu3 +
+            pl.P2 * ((d0 * d0) * (d1 + d2) + (d1 * d1) * (d2 + d0) + (d2 * d2) * (d0 + d1)) + pl.P3 * d0 * d1 * d2 +
+            pl.P4 * (uu2 * uu2);
   if (k.E_on) {
     f0 = f0 - k.Zs * dy.E0;
     f1 = f1 - k.Zs * dy.E1;
@@ -1455,11 +1458,13 @@ __global__ void __launch_bounds__(256, 2)
       AsmConst ks = k;
       AsmDyn dys = dy;
       double dk2 = 0.0;
+      Poly pl;  // this site's species (read_relaxor.F)
       if (site_species) {
-        const Phys::Species& q = ph->sp[site_species[i]];
-        ks.fa2g = q.fa2g; ks.tg = q.tg; ks.sk = q.sk; ks.tk2 = q.tk2; ks.fk = q.fk; ks.k4x8 = q.k4x8;
-        ks.Pa = q.Pa; ks.Pg = q.Pg; ks.P1 = q.P1; ks.P2 = q.P2; ks.P3 = q.P3; ks.P4 = q.P4;
-        dk2 = q.dk2;
+        const Phys::Species* q = &ph->sp[site_species[i]];
+        pl = Poly{q->fa2g, q->tg, q->sk, q->tk2, q->fk, q->k4x8, q->Pa, q->Pg, q->P1, q->P2, q->P3, q->P4};
+        dk2 = q->dk2;
+      } else {
+        pl = k.pl;
       }
       if (site_zstar) ks.Zs = (double)site_zstar[i];
       if (site_E) {
@@ -1478,7 +1483,7 @@ __global__ void __launch_bounds__(256, 2)
         f2 = f2 + ks.Zs * (double)rw[(zl0 + 2) * ns + i];
       }
       double o0, o1, o2;
-      assemble_site(ks, dys, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
+      assemble_site(pl, ks, dys, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
       if (dk2 != 0.0) {  // kappa2(s) - kappa2(1) (dVddi-unharmonic.F:40,73)
         const double t = 2 * dk2;
         o0 = o0 + t * ux;
@@ -1516,7 +1521,7 @@ __global__ void __launch_bounds__(256, 2)
       for (int l = 0; l < NV; ++l) {
         const double eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
         double d0, d1, d2;
-        assemble_site(k, dy, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, d0, d1, d2, acc);
+        assemble_site(k.pl, k, dy, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, d0, d1, d2, acc);
         o0.v[l] = force_hi<T>(d0);
         o1.v[l] = force_hi<T>(d1);
         o2.v[l] = force_hi<T>(d2);
@@ -1563,7 +1568,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
       for (int q = 0; q < 6; ++q) eta[q] = (double)rw[(3 + q) * ns + i];
       double o0, o1, o2;
-      assemble_site(k, dy, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
+      assemble_site(k.pl, k, dy, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
       const T h0 = force_hi<T>(o0), h1 = force_hi<T>(o1), h2 = force_hi<T>(o2);
       F[i] = h0;
       F[ns + i] = h1;

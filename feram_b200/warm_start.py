@@ -272,7 +272,9 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
        warm run's averages over [accept_after, probe) against the equilibrium
        ones, within 4 sigma of the difference; rejected points keep the
        fallback.
-    Returns a dict of the measurements."""
+    Returns a dict of the measurements; "points" rows are (T, E_z, tau
+    fallback, tau warm, accepted, V/N of the first fallback and warm samples,
+    equilibrium V/N, the same three for |<u>|^2)."""
     import feram_b200 as fb
     say = log or (lambda *a: None)
     rng = np.random.default_rng(seed)
@@ -331,7 +333,11 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
                 accepted += int(ok)
                 taus_f.append(probe if tf is None else tf)
                 taus_w.append(probe if tw is None else tw)
-                rows.append([T, ez, taus_f[-1], taus_w[-1], int(ok)])
+                # per site: the first traced potential energy of each start and
+                # the equilibrium one, and |<u>|^2 likewise
+                Nn = cw.p.N
+                rows.append([T, ez, taus_f[-1], taus_w[-1], int(ok), Vf[0] / Nn, Vw[0] / Nn, eq[2] / Nn,
+                             float(Pf[0]), float(Pw[0]), eq[0]])
                 say(f"  point {i}: T {T:.1f} K, E_z {ez:+.5f}: tau fallback {taus_f[-1]}, warm {taus_w[-1]}, "
                     f"{'accepted' if ok else 'rejected'}")
         taus_w, taus_f = np.array(taus_w), np.array(taus_f)
