@@ -135,6 +135,7 @@ struct fg_ctx {
   double2* trz = nullptr;
   double2* trz_s = nullptr;  // trz and kvz in kz-slot order
   double* kvz_s = nullptr;
+  float* kvz_sf = nullptr;
   double* layer_minv = nullptr;
   unsigned char* layer_sump = nullptr;
   // acoustic-displacement MD (acoustic mass > 0): u, p and F hold three more
@@ -207,7 +208,7 @@ int fail(fg_ctx* c, int code, const std::string& msg) {
 
 template <typename T>
 KMaps kmaps(const fg_ctx* c) {
-  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz, c->trz_s, c->kvz_s};
+  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz, c->trz_s, c->kvz_s, c->kvz_sf};
 }
 
 int check_device_error(fg_ctx* ctx) {
@@ -892,6 +893,8 @@ int create_impl(fg_ctx* ctx) {
       }
       if ((rc = upload(ctx, (void**)&ctx->trz_s, tzs))) return rc;
       if ((rc = upload(ctx, (void**)&ctx->kvz_s, kzs))) return rc;
+      std::vector<float> kzf(kzs.begin(), kzs.end());
+      if ((rc = upload(ctx, (void**)&ctx->kvz_sf, kzf))) return rc;
     }
   }
   // per-layer masses and masks (alloc_Coord, read_defects_u.F:52-69)
@@ -1630,7 +1633,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
   void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->Flo, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->ltab, ctx->revx,
-                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz, ctx->trz_s, ctx->kvz_s,
+                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz, ctx->trz_s, ctx->kvz_s, ctx->kvz_sf,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
                   ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all,
                   ctx->site_minv, ctx->site_macou, ctx->site_sump, ctx->site_species, ctx->site_zstar, ctx->site_E,

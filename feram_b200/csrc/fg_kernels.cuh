@@ -896,6 +896,7 @@ struct KMaps {
   const double2* trz;
   const double2* trz_s;  // trz and kvz in kz-slot order (no revz lookup first)
   const double* kvz_s;
+  const float* kvz_sf;   // kvz_s rounded to FP32 (the mixed path's k)
 };
 
 // Plain z pass of nc spectra in place: DIF (INV = false) or DIT (INV = true).
@@ -962,6 +963,13 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
+  __shared__ T kcon[8];  // B11, B12, B44, HC2 xx, xy, yz-yz, 1/N in T
+  if (threadIdx.x < 7) {
+    const int i = threadIdx.x;
+    const double v = i == 0 ? ph->B11 : i == 1 ? ph->B12 : i == 2 ? ph->B44 : i == 3 ? ph->HC2[0][0]
+                   : i == 4 ? ph->HC2[0][1] : i == 5 ? ph->HC2[3][3] : ph->Ninv;
+    kcon[i] = (T)v;
+  }
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
   // ACOU: acoustic-displacement MD, three more components in and out
   // (FFT(acouR) in, dVdacK out; acouFFT.F:9-26, dVdac.F:11-63)
@@ -1031,8 +1039,23 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   }
   const double Ninv = ph->Ninv;
   // Energy sums: the per-k products in T (FP32 in the mixed path, whose
-  // spectra are FP32), accumulated per thread in FP64
+  // spectra are FP32), accumulated per thread in FP64 (the dipole terms) or
+  // over this thread's few k in T first (the strain terms, acc_t)
   double acc[NQ_K] = {0, 0, 0, 0, 0};
+  T acc_t[3] = {(T)0, (T)0, (T)0};
+  // constants of the loop, converted to T once per block (kcon, filled
+  // before the z stages) and read from shared memory: reading them through
+  // ph in the loop repeats the loads and FP64 -> FP32 conversions at every k
+  // (the loop's store to sc->didiK0 keeps the compiler from hoisting them)
+  const T& B11 = kcon[0];
+  const T& B12 = kcon[1];
+  const T& B44 = kcon[2];
+  const T& hx = kcon[3];
+  const T& hy = kcon[4];
+  const T& h4 = kcon[5];
+  const T& ni = kcon[6];
+  const bool mod_on = ph->modulation_on != 0;
+  const T* __restrict__ kvz_t = reinterpret_cast<const T*>(sizeof(T) == 4 ? km.kvz_sf : (const void*)km.kvz_s);
   // this thread's pencil (fixed cw), decoded once
   const int cw = cwp, col = colp, yslot = ysp;
   const bool pencil_ok = okp;
@@ -1107,8 +1130,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       S[5] = sA[5] + sB[5] * tz.x;
       double qd[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) qd[q] = (double)qv[q];
-      const double es = (double)w1 * (S[0] * qd[0] + S[1] * qd[1] + S[2] * qd[2] + 2.0 * (S[3] * qd[3] + S[4] * qd[4] + S[5] * qd[5]));
+      for (int q = 0; q < 6; ++q) qd[q] = widen(qv[q]);
+      const double w1d = widen(w1);
+      const double es = w1d * (S[0] * qd[0] + S[1] * qd[1] + S[2] * qd[2] + 2.0 * (S[3] * qd[3] + S[4] * qd[4] + S[5] * qd[5]));
       acc[0] += es;
       if constexpr (ZSC) {
         // short range on uK, long range on FFT(Z* u): Fl = (L/N) ZuK,
@@ -1135,8 +1159,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 #pragma unroll
         for (int q = 0; q < 6; ++q) D[q] = (T)(S[q] * Ninv);
       } else {
-        acc[1] += (double)w1 * ((double)D[0] * qd[0] + (double)D[1] * qd[1] + (double)D[2] * qd[2] +
-                                2.0 * ((double)D[3] * qd[3] + (double)D[4] * qd[4] + (double)D[5] * qd[5]));
+        acc[1] += w1d * (widen(D[0]) * qd[0] + widen(D[1]) * qd[1] + widen(D[2]) * qd[2] +
+                         2.0 * (widen(D[3]) * qd[3] + widen(D[4]) * qd[4] + widen(D[5]) * qd[5]));
       }
     }
     cplx<T> F[3];
@@ -1144,9 +1168,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     F[1] = mk<cplx<T>>(D[5] * u[0].x + D[1] * u[1].x + D[3] * u[2].x, D[5] * u[0].y + D[1] * u[1].y + D[3] * u[2].y);
     F[2] = mk<cplx<T>>(D[4] * u[0].x + D[3] * u[1].x + D[2] * u[2].x, D[4] * u[0].y + D[3] * u[1].y + D[2] * u[2].y);
     // ---- inhomogeneous strain
-    const T k1 = (T)kv1, k2 = (T)kv2, k3 = (T)__ldg(&km.kvz_s[zs]);
+    const T k1 = (T)kv1, k2 = (T)kv2, k3 = __ldg(&kvz_t[zs]);
     const T kk[4] = {(T)0, k1, k2, k3};
-    const T B11 = (T)ph->B11, B12 = (T)ph->B12, B44 = (T)ph->B44;
     T K[3][3];
 #pragma unroll
     for (int b = 1; b <= 3; ++b) {
@@ -1160,9 +1183,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
     // coup2 . didiK with coup2(a, i) of elastic.F:156-180: k_a B1xx/2 on
     // i = a, k_a B1yy/2 on the other two diagonal entries, k_c B4yz on the
     // shear entries (yz: b = y, c = z ...) that involve a, zero on the third
-    const T hx = (T)(ph->HC2[0][0]), hy = (T)(ph->HC2[0][1]), h4 = (T)(ph->HC2[3][3]);
     cplx<T> ck[3] = {mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0)};
-    if (ph->modulation_on) {
+    if (mod_on) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) ck[a] = ckmod[tpos * 3 + a];
     }
@@ -1200,10 +1222,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         ec += acou[a].x * cs[a].x + acou[a].y * cs[a].y;
         em += acou[a].x * ck[a].x + acou[a].y * ck[a].y;
       }
-      acc[2] += (double)(w2 * es);
-      acc[3] += (double)(w2 * ec);
-      acc[4] += (double)(w2 * em);
-      const T ni = (T)Ninv;
+      acc_t[0] += w2 * es;
+      acc_t[1] += w2 * ec;
+      acc_t[2] += w2 * em;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const cplx<T> v = mk<cplx<T>>(ck[a].x + cs[a].x + KA[a].x, ck[a].y + cs[a].y + KA[a].y);
@@ -1238,15 +1259,14 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         ec += acou[a].x * cs[a].x + acou[a].y * cs[a].y;
         em += acou[a].x * ck[a].x + acou[a].y * ck[a].y;
       }
-      acc[2] -= (double)(w2 * (ec + em));
-      acc[3] += (double)(w2 * ec);
-      acc[4] += (double)(w2 * em);
+      acc_t[0] -= w2 * (ec + em);
+      acc_t[1] += w2 * ec;
+      acc_t[2] += w2 * em;
     }
     if (acouK_out) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) acouK_out[tpos * 3 + a] = acou[a];
     }
-    const T ni = (T)Ninv;
     d[0] = mk<cplx<T>>(k1 * acou[0].x * ni, k1 * acou[0].y * ni);
     d[1] = mk<cplx<T>>(k2 * acou[1].x * ni, k2 * acou[1].y * ni);
     d[2] = mk<cplx<T>>(k3 * acou[2].x * ni, k3 * acou[2].y * ni);
@@ -1258,6 +1278,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 #pragma unroll
     for (int i = 0; i < 6; ++i) buf[(3 + i) * ZS + zs * CW + cw] = d[i];
   }
+  acc[2] += (double)acc_t[0];
+  acc[3] += (double)acc_t[1];
+  acc[4] += (double)acc_t[2];
   __syncthreads();
   if constexpr (LZC > 0) {
     ct_inverse_range<T, LZC, ct_nst(LZC) - 1, 0, kZThreads, BZ>(buf, tws_z);
@@ -1311,6 +1334,32 @@ __device__ __forceinline__ V16<T> ldv_first(const T* p, unsigned long long pol) 
 template <typename T>
 __device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V16<T>*>(p) = a; }
 
+// Two consecutive sites of one component (8 bytes FP32, 16 bytes FP64): the
+// assembly's vector width, so that its FP64 site sums stay in registers.
+template <typename T>
+struct alignas(2 * sizeof(T)) V2 {
+  static constexpr int n = 2;
+  T v[2];
+};
+template <typename T>
+__device__ __forceinline__ V2<T> ldv2(const T* p) { return *reinterpret_cast<const V2<T>*>(p); }
+template <typename T>
+__device__ __forceinline__ V2<T> ldv2_first(const T* p, unsigned long long pol) {
+  V2<T> r;
+  if constexpr (sizeof(T) == 4) {
+    const float2 v = ld_first(reinterpret_cast<const float2*>(p), pol);
+    r.v[0] = v.x; r.v[1] = v.y;
+  } else if constexpr (FG_L2_HINT_FP64) {
+    const double2 v = ld_first(reinterpret_cast<const double2*>(p), pol);
+    r.v[0] = v.x; r.v[1] = v.y;
+  } else {
+    r = ldv2(p);
+  }
+  return r;
+}
+template <typename T>
+__device__ __forceinline__ void stv2(T* p, const V2<T>& a) { *reinterpret_cast<V2<T>*>(p) = a; }
+
 // Constants of the site force, in FP64 for both precisions: the mixed path
 // reads FP32 u, the FP32 dipole-dipole force and the FP32 eta, and sums the
 // on-site polynomial, the field and both strain couplings in FP64.  Those
@@ -1338,8 +1387,8 @@ struct AsmDyn {
 };
 
 // Force on one site from F_dd, u and eta (see k_assemble); acc += energies.
-__device__ __forceinline__ void assemble_site(const Poly& pl, const AsmConst& k, const AsmDyn& dy, double ux,
-                                              double uy, double uz, double f0, double f1, double f2,
+__device__ __forceinline__ void assemble_site(const Poly& pl, const AsmConst& k, double Zs, const AsmDyn& dy,
+                                              double ux, double uy, double uz, double f0, double f1, double f2,
                                               const double* eta, double& o0, double& o1, double& o2, double* acc) {
   const double d0 = ux * ux, d1 = uy * uy, d2 = uz * uz;
   const double uu = d0 + d1 + d2;
@@ -1356,10 +1405,10 @@ __device__ __forceinline__ void assemble_site(const Poly& pl, const AsmConst& k,
             pl.P2 * ((d0 * d0) * (d1 + d2) + (d1 * d1) * (d2 + d0) + (d2 * d2) * (d0 + d1)) + pl.P3 * d0 * d1 * d2 +
             pl.P4 * (uu2 * uu2);
   if (k.E_on) {
-    f0 = f0 - k.Zs * dy.E0;
-    f1 = f1 - k.Zs * dy.E1;
-    f2 = f2 - k.Zs * dy.E2;
-    acc[1] += k.Zs * (ux * dy.E0 + uy * dy.E1 + uz * dy.E2);
+    f0 = f0 - Zs * dy.E0;
+    f1 = f1 - Zs * dy.E1;
+    f2 = f2 - Zs * dy.E2;
+    acc[1] += Zs * (ux * dy.E0 + uy * dy.E1 + uz * dy.E2);
   }
   // homogeneous strain coupling
   f0 = f0 + 2 * dy.wh[0] * ux + dy.wh[4] * uz + dy.wh[5] * uy;
@@ -1449,13 +1498,12 @@ __global__ void __launch_bounds__(256, 2)
   for (int i = 0; i < 6; ++i) dy.wh[i] = sc->w_hom[i];
   dy.E0 = sc->E[0]; dy.E1 = sc->E[1]; dy.E2 = sc->E[2];
   double acc[NQ_R] = {0.0, 0.0};
-  constexpr int NV = V16<T>::n;
+  constexpr int NV = V2<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const bool sites = site_species != nullptr || site_zstar != nullptr || site_E != nullptr ||
                      (CLOSE && (site_minv != nullptr || site_sump != nullptr));
   if (sites) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
-      AsmConst ks = k;
       AsmDyn dys = dy;
       double dk2 = 0.0;
       Poly pl;  // this site's species (read_relaxor.F)
@@ -1466,7 +1514,7 @@ __global__ void __launch_bounds__(256, 2)
       } else {
         pl = k.pl;
       }
-      if (site_zstar) ks.Zs = (double)site_zstar[i];
+      const double Zs = site_zstar ? (double)site_zstar[i] : k.Zs;
       if (site_E) {
         dys.E0 = dy.E0 + (double)site_E[i];
         dys.E1 = dy.E1 + (double)site_E[ns + i];
@@ -1478,12 +1526,12 @@ __global__ void __launch_bounds__(256, 2)
       const double ux = u[i], uy = u[ns + i], uz = u[2 * ns + i];
       double f0 = rw[i], f1 = rw[ns + i], f2 = rw[2 * ns + i];
       if (zl0 > 0) {
-        f0 = f0 + ks.Zs * (double)rw[(zl0 + 0) * ns + i];
-        f1 = f1 + ks.Zs * (double)rw[(zl0 + 1) * ns + i];
-        f2 = f2 + ks.Zs * (double)rw[(zl0 + 2) * ns + i];
+        f0 = f0 + Zs * (double)rw[(zl0 + 0) * ns + i];
+        f1 = f1 + Zs * (double)rw[(zl0 + 1) * ns + i];
+        f2 = f2 + Zs * (double)rw[(zl0 + 2) * ns + i];
       }
       double o0, o1, o2;
-      assemble_site(pl, ks, dys, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
+      assemble_site(pl, k, Zs, dys, ux, uy, uz, f0, f1, f2, eta, o0, o1, o2, acc);
       if (dk2 != 0.0) {  // kappa2(s) - kappa2(1) (dVddi-unharmonic.F:40,73)
         const double t = 2 * dk2;
         o0 = o0 + t * ux;
@@ -1509,19 +1557,21 @@ __global__ void __launch_bounds__(256, 2)
   } else if (g.plane_r % NV == 0) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
-      const V16<T> ux = ldv(u + i), uy = ldv(u + ns + i), uz = ldv(u + 2 * ns + i);
+      const V2<T> ux = ldv2(u + i), uy = ldv2(u + ns + i), uz = ldv2(u + 2 * ns + i);
       // rw is consumed here: evict_first keeps u, p and F in L2
-      const V16<T> a0 = ldv_first(rw + i, pol_rw), a1 = ldv_first(rw + ns + i, pol_rw),
-                   a2 = ldv_first(rw + 2 * ns + i, pol_rw);
-      V16<T> e[6];
+      const V2<T> a0 = ldv2_first(rw + i, pol_rw), a1 = ldv2_first(rw + ns + i, pol_rw),
+                  a2 = ldv2_first(rw + 2 * ns + i, pol_rw);
+      V2<T> e[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) e[q] = ldv_first(rw + (3 + q) * ns + i, pol_rw);
-      V16<T> o0, o1, o2, l0, l1, l2;
+      for (int q = 0; q < 6; ++q) e[q] = ldv2_first(rw + (3 + q) * ns + i, pol_rw);
+      V2<T> o0, o1, o2, l0, l1, l2;
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
-        const double eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
+        const double eta[6] = {widen(e[0].v[l]), widen(e[1].v[l]), widen(e[2].v[l]),
+                               widen(e[3].v[l]), widen(e[4].v[l]), widen(e[5].v[l])};
         double d0, d1, d2;
-        assemble_site(k.pl, k, dy, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, d0, d1, d2, acc);
+        assemble_site(k.pl, k, k.Zs, dy, widen(ux.v[l]), widen(uy.v[l]), widen(uz.v[l]), widen(a0.v[l]), widen(a1.v[l]),
+                      widen(a2.v[l]), eta, d0, d1, d2, acc);
         o0.v[l] = force_hi<T>(d0);
         o1.v[l] = force_hi<T>(d1);
         o2.v[l] = force_hi<T>(d2);
@@ -1529,17 +1579,17 @@ __global__ void __launch_bounds__(256, 2)
         l1.v[l] = force_lo<T>(d1, o1.v[l]);
         l2.v[l] = force_lo<T>(d2, o2.v[l]);
       }
-      stv(F + i, o0);
-      stv(F + ns + i, o1);
-      stv(F + 2 * ns + i, o2);
+      stv2(F + i, o0);
+      stv2(F + ns + i, o1);
+      stv2(F + 2 * ns + i, o2);
       if (Flo) {
-        stv(Flo + i, l0);
-        stv(Flo + ns + i, l1);
-        stv(Flo + 2 * ns + i, l2);
+        stv2(Flo + i, l0);
+        stv2(Flo + ns + i, l1);
+        stv2(Flo + 2 * ns + i, l2);
       }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
-        V16<T> q[3] = {ldv(p + i), ldv(p + ns + i), ldv(p + 2 * ns + i)};
+        V2<T> q[3] = {ldv2(p + i), ldv2(p + ns + i), ldv2(p + 2 * ns + i)};
         T pp = 0, pf = 0, ff = 0;
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
@@ -1553,7 +1603,7 @@ __global__ void __launch_bounds__(256, 2)
           }
         }
 #pragma unroll
-        for (int a = 0; a < 3; ++a) stv(p + a * ns + i, q[a]);
+        for (int a = 0; a < 3; ++a) stv2(p + a * ns + i, q[a]);
         if (layer_sump[z]) {
           const double mi = layer_minv[z];
           ke[0] += (double)pp * mi;
@@ -1568,7 +1618,7 @@ __global__ void __launch_bounds__(256, 2)
 #pragma unroll
       for (int q = 0; q < 6; ++q) eta[q] = (double)rw[(3 + q) * ns + i];
       double o0, o1, o2;
-      assemble_site(k.pl, k, dy, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
+      assemble_site(k.pl, k, k.Zs, dy, u[i], u[ns + i], u[2 * ns + i], rw[i], rw[ns + i], rw[2 * ns + i], eta, o0, o1, o2, acc);
       const T h0 = force_hi<T>(o0), h1 = force_hi<T>(o1), h2 = force_hi<T>(o2);
       F[i] = h0;
       F[ns + i] = h1;

@@ -16,7 +16,7 @@
 //
 // Training target (moment matching): for every training configuration u_j
 // generated by the MD itself at condition c_j, the statistics
-//   S = (m.e, |m|^2, sum_a m_a^4, <|u|^2>, <sum_a u_a^4>,
+//   S = (m.e, |m|, (sum_a m_a^4)^(1/4), <|u|^2>, <sum_a u_a^4>,
 //        <sum_a u_a(R) u_a(R + a)>, <sum_a sum_b!=a u_a(R) u_a(R + b)>)
 // (m = <u> the mean dipole, e = E / 0.001 V/A, <> site averages) are the
 // regression targets of the generated field at c_j; their conditional means
@@ -49,6 +49,7 @@ constexpr int kThreads = 128;     // 4 warps: one TMEM lane quarter each
 constexpr int kTaps = 27;
 constexpr int kNS = 7;            // statistics per sample
 constexpr long long kWaitIter = 1LL << 22;  // bounded mbarrier waits (~0.3 s)
+constexpr double kEps2 = 1e-8, kEps4 = 1e-16;  // floors of |m|^2 and sum m_a^4
 
 struct Geo {
   int Lx, Ly, Lz, nsite;  // one sample
@@ -362,20 +363,27 @@ __global__ void k_ws_stats_finish(const double* __restrict__ part, int nblk, Geo
   const double m[3] = {v[0] / N, v[1] / N, v[2] / N};
   const float* c = cond + 5 * b;
   const double e[3] = {c[1] / 0.001, c[2] / 0.001, c[3] / 0.001};
-  double st[kNS];
+  // |m| and (sum m_a^4)^(1/4) rather than their powers: both scale with the
+  // polarisation, so the paraelectric and the ordered points weigh alike
+  const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+  const double m4 = m[0] * m[0] * m[0] * m[0] + m[1] * m[1] * m[1] * m[1] + m[2] * m[2] * m[2] * m[2];
+  double st[kNS], dsd[kNS];  // statistic, and its derivative by the raw moment it comes from
   st[0] = m[0] * e[0] + m[1] * e[1] + m[2] * e[2];
-  st[1] = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
-  st[2] = m[0] * m[0] * m[0] * m[0] + m[1] * m[1] * m[1] * m[1] + m[2] * m[2] * m[2] * m[2];
+  st[1] = sqrt(m2 + kEps2);
+  st[2] = sqrt(sqrt(m4 + kEps4));
   st[3] = v[3] / N;
   st[4] = v[4] / N;
   st[5] = v[5] / N;
   st[6] = v[6] / N;
+  for (int k = 0; k < kNS; ++k) dsd[k] = 1.0;
+  dsd[1] = 0.5 / st[1];
+  dsd[2] = 0.25 / (st[2] * st[2] * st[2]);
   double L = 0.0;
   for (int k = 0; k < kNS; ++k) {
     S[b * kNS + k] = (float)st[k];
     if (target) {
       const double d = st[k] - (double)target[b * kNS + k];
-      coef[b * kNS + k] = (float)(2.0 * wts[k] * d);
+      coef[b * kNS + k] = (float)(2.0 * wts[k] * d * dsd[k]);  // dL / d(raw moment)
       L += wts[k] * d * d;
     }
   }

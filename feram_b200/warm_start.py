@@ -26,21 +26,23 @@ from . import _capi as A
 from ._capi import FG_PREC_MIXED
 
 NSTAT = 7
-STAT_NAMES = ("m.e", "|m|^2", "sum m_a^4", "<|u|^2>", "<sum u_a^4>", "C_long", "C_trans")
+STAT_NAMES = ("m.e", "|m|", "(sum m_a^4)^1/4", "<|u|^2>", "<sum u_a^4>", "C_long", "C_trans")
 E_SCALE = 0.001  # V/A: 100 kV/cm
 
 
 def site_stats(u: np.ndarray, E) -> np.ndarray:
     """The seven statistics of a configuration u (Lz, Ly, Lx, 3) at field E:
-    m.e, |m|^2, sum_a m_a^4 (m = <u>, e = E / 0.001 V/A), <|u|^2>,
-    <sum_a u_a^4>, <sum_a u_a(R) u_a(R + a)>, <sum_a sum_b!=a u_a(R) u_a(R + b)>."""
+    m.e, |m|, (sum_a m_a^4)^(1/4) (m = <u>, e = E / 0.001 V/A; floors 1e-8
+    and 1e-16 under the roots), <|u|^2>, <sum_a u_a^4>,
+    <sum_a u_a(R) u_a(R + a)>, <sum_a sum_b!=a u_a(R) u_a(R + b)>."""
     u = np.asarray(u, dtype=np.float64)
     m = u.reshape(-1, 3).mean(axis=0)
     e = np.asarray(E, dtype=np.float64) / E_SCALE
     ax = {0: 2, 1: 1, 2: 0}  # component a -> array axis of direction a (z, y, x order)
     c_long = sum((u[..., a] * np.roll(u[..., a], -1, axis=ax[a])).mean() for a in range(3))
     c_tr = sum((u[..., a] * np.roll(u[..., a], -1, axis=ax[b])).mean() for a in range(3) for b in range(3) if b != a)
-    return np.array([m @ e, m @ m, (m ** 4).sum(), (u ** 2).sum(-1).mean(), (u ** 4).sum(-1).mean(), c_long, c_tr])
+    return np.array([m @ e, np.sqrt(m @ m + 1e-8), np.sqrt(np.sqrt((m ** 4).sum() + 1e-16)), (u ** 2).sum(-1).mean(),
+                     (u ** 4).sum(-1).mean(), c_long, c_tr])
 
 
 class WarmStartNet:
@@ -254,28 +256,92 @@ def timed(fn, *a, **k):
     return r, time.perf_counter() - t0
 
 
-def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40, seed=2024, n_therm=3000,
-               n_snap=14, train_steps=1500, probe=3000, every=20, accept_after=1000, log=None):
+def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, tag):
+    """One pass over held-out points in the given order: for each, the
+    fallback (chained from the previous point), the network's warm start and
+    a cold start (initialize_dipoR's uni64 field, p = 0), `probe` steps
+    each; the fallback continues `probe` more steps for the equilibrium."""
+    import feram_b200 as fb
+    p0 = make_params(L, points[0][0], points[0][1], -5.0)
+    rows, t_infer = [], 0.0
+    with fb.Context(p0, FG_PREC_MIXED) as cf, fb.Context(p0, FG_PREC_MIXED) as cw, \
+            fb.Context(p0, FG_PREC_MIXED) as cc:
+        for c in (cf, cw, cc):
+            c.build_tables()
+        u = A.real_field(p0)
+        q = A.real_field(p0)
+        assert A.lib().fg_init_dipoR_host(C.byref(p0), A.dptr(u), A.dptr(q)) == 0
+        start_point(cf, p0, u, q)
+        cf.run_steps(probe)  # the sweep's first point, thermalised before the held-out ones
+        for i, (T, ez) in enumerate(points):
+            E = [0.0, 0.0, ez]
+            cf.chain_point(T, E)
+            Pf, Vf = equilibration_trace(cf, probe, every)
+            Pe, Ve = equilibration_trace(cf, probe, every)
+            eq = block_stats(Pe, Ve)
+            t0 = time.perf_counter()
+            net.forward(np.array([[T, 0.0, 0.0, ez, -5.0]] * net.batch), [seed * 1000 + i] * net.batch)
+            pw = make_params(L, T, ez, -5.0)
+            uw = net.field(0, pw)
+            t_infer += time.perf_counter() - t0
+            cw.chain_point(T, E)  # the context's temperature and field; its state is replaced
+            start_point(cw, cw.p, uw, maxwell_momenta(cw.p, seed + i))
+            Pw, Vw = equilibration_trace(cw, probe, every)
+            cc.chain_point(T, E)
+            pc = A.fg_params.from_buffer_copy(cc.p)
+            pc.seed[0] = 123456789 + i
+            uc = A.real_field(pc)
+            assert A.lib().fg_init_dipoR_host(C.byref(pc), A.dptr(uc), None) == 0
+            start_point(cc, cc.p, uc, A.real_field(pc))
+            Pc, Vc = equilibration_trace(cc, probe, every)
+            tf = time_to_equilibrium(Pf, Vf, eq, every)
+            tw = time_to_equilibrium(Pw, Vw, eq, every)
+            tc = time_to_equilibrium(Pc, Vc, eq, every)
+            k0 = accept_after // every
+            a_w = block_stats(Pw[k0:], Vw[k0:])
+            nb_w, nb_e = (len(Pw) - k0) // 5, len(Pe) // 5
+            ok = (abs(a_w[0] - eq[0]) <= 4 * np.hypot(a_w[1] / np.sqrt(nb_w), eq[1] / np.sqrt(nb_e)) + 1e-12 and
+                  abs(a_w[2] - eq[2]) <= 4 * np.hypot(a_w[3] / np.sqrt(nb_w), eq[3] / np.sqrt(nb_e)) + 1e-12)
+            val = lambda t: probe if t is None else t
+            Nn = cw.p.N
+            rows.append([T, ez, val(tf), val(tw), val(tc), int(ok), Vf[0] / Nn, Vw[0] / Nn, eq[2] / Nn,
+                         float(Pf[0]), float(Pw[0]), eq[0]])
+            say(f"  {tag} point {i}: T {T:.1f} K, E_z {ez:+.5f}: tau fallback {val(tf)}, warm {val(tw)}, "
+                f"cold {val(tc)}, {'accepted' if ok else 'rejected'}")
+    r = np.array(rows)
+    tf, tw, tc, acc = r[:, 2], r[:, 3], r[:, 4], r[:, 5]
+    eff = np.where(acc == 1, tw, tw + tf)  # a rejected warm start pays both tries
+    return {"points": len(rows), "accepted": int(acc.sum()),
+            "tau_fallback_median": float(np.median(tf)), "tau_warm_median": float(np.median(tw)),
+            "tau_cold_median": float(np.median(tc)), "tau_fallback_mean": float(tf.mean()),
+            "tau_warm_mean": float(tw.mean()), "tau_cold_mean": float(tc.mean()),
+            "warm_faster_than_fallback": int(np.sum(tw < tf)), "warm_faster_than_cold": int(np.sum(tw < tc)),
+            "thermalisation_steps_fallback": int(tf.sum()), "thermalisation_steps_warm_with_fallback": int(eff.sum()),
+            "thermalisation_steps_cold": int(tc.sum()), "inference_seconds": t_infer,
+            "rows": [[round(x, 6) for x in row] for row in rows]}
+
+
+def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40, n_shuffled=20, seed=2024,
+               n_therm=3000, n_snap=14, train_steps=4000, probe=3000, every=20, accept_after=1000, log=None):
     """The learned-warm-start protocol on one GPU.
 
     1. Data: MD cooling chains (train_chains of (E_z, GPa), train_temps
        descending) at L^3, snapshots -> (condition, statistics).
     2. Training: Adam on the moment-matching loss.
-    3. Held-out points: n_held (T in 100-450 K, E_z in +-0.001 V/A), visited
-       as a cooling sweep (T descending).  Each point runs twice for `probe`
-       steps: from the previous point's final state (fg_chain_point, the
-       reference's .restart chaining: the fallback) and from the network's
-       proposal with Maxwell-Boltzmann momenta.  The fallback run continues
-       another `probe` steps; those give the point's equilibrium (block means
-       and their spread).  Time to equilibrium: three consecutive blocks of
-       the trace within 3 sigma of it.  Acceptance, the MD as the judge: the
-       warm run's averages over [accept_after, probe) against the equilibrium
-       ones, within 4 sigma of the difference; rejected points keep the
-       fallback.
-    Returns a dict of the measurements; "points" rows are (T, E_z, tau
-    fallback, tau warm, accepted, V/N of the first fallback and warm samples,
-    equilibrium V/N, the same three for |<u>|^2)."""
-    import feram_b200 as fb
+    3. Held-out points (T in 100-450 K, E_z in +-0.001 V/A), off the
+       training grid: n_held visited as a cooling sweep (T descending) and
+       n_shuffled in random order (a scan whose previous point is unrelated).
+       Each point runs from the previous point's final state (fg_chain_point,
+       the reference's .restart chaining: the fallback), from the network's
+       proposal with Maxwell-Boltzmann momenta, and from a cold uni64 start;
+       the fallback continues for the point's equilibrium (block means and
+       their spread).  Time to equilibrium: three consecutive blocks of the
+       trace within 3 sigma of it.  Acceptance, the MD as the judge: the warm
+       run's averages over [accept_after, probe) against the equilibrium,
+       within 4 sigma of the difference; a rejected point keeps the fallback.
+    Returns a dict of the measurements; the "rows" of each pass are (T, E_z,
+    tau fallback, tau warm, tau cold, accepted, V/N of the first fallback
+    and warm samples, equilibrium V/N, the same three for |<u>|^2)."""
     say = log or (lambda *a: None)
     rng = np.random.default_rng(seed)
     if train_chains is None:
@@ -295,62 +361,11 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
                     "loss_first": float(np.mean(hist[:20])), "loss_last": float(np.mean(hist[-50:]))})
         say(f"warm start: trained {train_steps} steps in {t_train:.1f} s, loss {out['loss_first']:.3g} -> "
             f"{out['loss_last']:.3g}")
-        held = sorted(((float(rng.uniform(100.0, 450.0)), float(rng.uniform(-0.001, 0.001))) for _ in range(n_held)),
-                      reverse=True)
-        p0 = make_params(L, held[0][0], held[0][1], -5.0)
-        taus_w, taus_f, accepted, rows = [], [], 0, []
-        t_infer = 0.0
-        with fb.Context(p0, FG_PREC_MIXED) as cf, fb.Context(p0, FG_PREC_MIXED) as cw:
-            cf.build_tables()
-            cw.build_tables()
-            u = A.real_field(p0)
-            q = A.real_field(p0)
-            assert A.lib().fg_init_dipoR_host(C.byref(p0), A.dptr(u), A.dptr(q)) == 0
-            start_point(cf, p0, u, q)
-            cf.run_steps(probe)  # the sweep's first point, thermalised before the held-out ones
-            for i, (T, ez) in enumerate(held):
-                E = [0.0, 0.0, ez]
-                cf.chain_point(T, E)
-                Pf, Vf = equilibration_trace(cf, probe, every)
-                Pe, Ve = equilibration_trace(cf, probe, every)
-                eq = block_stats(Pe, Ve)
-                # warm start from the network
-                t0 = time.perf_counter()
-                net.forward(np.array([[T, 0.0, 0.0, ez, -5.0]] * net.batch), [seed * 1000 + i] * net.batch)
-                pw = make_params(L, T, ez, -5.0)
-                uw = net.field(0, pw)
-                t_infer += time.perf_counter() - t0
-                cw.chain_point(T, E)  # the context's temperature and field (its state is replaced below)
-                start_point(cw, cw.p, uw, maxwell_momenta(cw.p, seed + i))
-                Pw, Vw = equilibration_trace(cw, probe, every)
-                tf = time_to_equilibrium(Pf, Vf, eq, every)
-                tw = time_to_equilibrium(Pw, Vw, eq, every)
-                k0 = accept_after // every
-                a_w = block_stats(Pw[k0:], Vw[k0:])
-                nb_w, nb_e = (len(Pw) - k0) // 5, len(Pe) // 5
-                ok = (abs(a_w[0] - eq[0]) <= 4 * np.hypot(a_w[1] / np.sqrt(nb_w), eq[1] / np.sqrt(nb_e)) + 1e-12 and
-                      abs(a_w[2] - eq[2]) <= 4 * np.hypot(a_w[3] / np.sqrt(nb_w), eq[3] / np.sqrt(nb_e)) + 1e-12)
-                accepted += int(ok)
-                taus_f.append(probe if tf is None else tf)
-                taus_w.append(probe if tw is None else tw)
-                # per site: the first traced potential energy of each start and
-                # the equilibrium one, and |<u>|^2 likewise
-                Nn = cw.p.N
-                rows.append([T, ez, taus_f[-1], taus_w[-1], int(ok), Vf[0] / Nn, Vw[0] / Nn, eq[2] / Nn,
-                             float(Pf[0]), float(Pw[0]), eq[0]])
-                say(f"  point {i}: T {T:.1f} K, E_z {ez:+.5f}: tau fallback {taus_f[-1]}, warm {taus_w[-1]}, "
-                    f"{'accepted' if ok else 'rejected'}")
-        taus_w, taus_f = np.array(taus_w), np.array(taus_f)
-        # the sweep with each point thermalised for its measured time, rejected
-        # warm starts paying both tries
-        eff_w = np.where(np.array([r[4] for r in rows]) == 1, taus_w, taus_w + taus_f)
-        out.update({"held_out": n_held, "probe_steps": probe, "accepted": accepted,
-                    "tau_fallback_median": float(np.median(taus_f)), "tau_warm_median": float(np.median(taus_w)),
-                    "tau_fallback_mean": float(taus_f.mean()), "tau_warm_mean": float(taus_w.mean()),
-                    "warm_faster_points": int(np.sum(taus_w < taus_f)),
-                    "thermalisation_steps_fallback": int(taus_f.sum()),
-                    "thermalisation_steps_warm": int(eff_w.sum()),
-                    "inference_seconds": t_infer, "points": rows})
+        pts = [(float(rng.uniform(100.0, 450.0)), float(rng.uniform(-0.001, 0.001))) for _ in range(n_held + n_shuffled)]
+        out["cooling_sweep"] = _sweep(net, make_params, L, sorted(pts[:n_held], reverse=True), seed, probe, every,
+                                      accept_after, say, "sweep")
+        out["shuffled"] = _sweep(net, make_params, L, pts[n_held:], seed + 7, probe, every, accept_after, say,
+                                 "shuffled")
     finally:
         net.close()
     return out
