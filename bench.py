@@ -320,6 +320,121 @@ def batched_sweep(n_rep=96, steps=200):
             "timing": "wall clock around synchronous calls"}
 
 
+def _block_mean(x, nb=10):
+    """Mean and its standard error from nb block means."""
+    x = np.asarray(x, dtype=np.float64)
+    n = len(x) // nb * nb
+    m = x[:n].reshape(nb, -1).mean(axis=1)
+    return float(m.mean()), float(m.std(ddof=1) / np.sqrt(nb))
+
+
+def _point_obs(rows, N):
+    """Per-site observables of a point's sample rows: V/N, KE/N, |u_bar|
+    (u_bar = sum u / N, the order parameter) and |u_bar|^2."""
+    ub = rows[:, 0:3] / N
+    a = np.sqrt((ub ** 2).sum(axis=1))
+    return {"V": rows[:, 6] / N, "KE": rows[:, 7] / N, "|u|": a, "u2": a * a}
+
+
+def cooling_sweep(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None, log=None):
+    """The batched cooling sweep: n_rep points (supercell 16^3..64^3 by
+    i mod 5, T = 450 - 5 (i mod 71) K), n_therm + n_avg steps each, mixed.
+
+    plain: the reference's sweep, one supercell after another, its points in
+      descending T, each started from the previous point's final state
+      (fg_run_point; cooling.sh:64-69), default plans.
+    batched: every point at once as one replica batch (fg_batch_run_point,
+      plans from fg_batch_tune), each replica from initialize_dipoR's start;
+      with warm_layers also from the warm-start network's proposal.
+    Agreement: per point, V/N, KE/N, |u_bar| and |u_bar|^2 over the n_avg
+    steps (10 block means) against the plain sweep's point, z = difference /
+    combined standard error.  Wall clock around synchronous calls."""
+    import feram_b200 as fb
+    from feram_b200 import _capi as A
+    from feram_b200 import warm_start as W
+    say = log or (lambda *a: None)
+    sizes = [16, 24, 32, 48, 64]
+    Ls = [sizes[i % len(sizes)] for i in range(n_rep)]
+    Ts = [450.0 - 5.0 * (i % 71) for i in range(n_rep)]
+    seeds = [(123456789 + i, 987654321) for i in range(n_rep)]
+    ps = [make_params(Ls[i], kelvin=Ts[i], Ez=0.0, seed=seeds[i]) for i in range(n_rep)]
+    sites = sum(p.N for p in ps)
+    out = {"replicas": n_rep, "sizes": sizes, "kelvin": [450.0, 100.0, -5.0], "sites": sites, "n_therm": n_therm,
+           "n_avg": n_avg, "sample_every": every, "precision": "mixed", "unit": UNIT,
+           "timing": "wall clock around synchronous calls; set-up (tables, initial state) outside"}
+
+    # plain sequential sweep: per size, its points in descending T, chained
+    plain = {}
+    t_plain = 0.0
+    for L in sizes:
+        idx = sorted((i for i in range(n_rep) if Ls[i] == L), key=lambda i: -Ts[i])
+        p0 = make_params(L, kelvin=Ts[idx[0]], Ez=0.0, seed=seeds[idx[0]])
+        with fb.Context(p0, A.FG_PREC_MIXED) as ctx:
+            ctx.build_tables()
+            u, q = initial_state(p0)
+            prepare(ctx, p0, u, q)
+            t0 = time.perf_counter()
+            for i in idx:
+                ctx.run_point(Ts[i], n_therm, n_avg, every)
+                plain[i] = ctx.samples()
+            t_plain += time.perf_counter() - t0
+    out["plain_seconds"] = t_plain
+    out["plain_value"] = sites * (n_therm + n_avg) / t_plain
+    say(f"sweep: plain sequential {t_plain:.1f} s")
+
+    def batched_arm(starts, tag):
+        with fb.Batch(ps, A.FG_PREC_MIXED) as b:
+            for i, r in enumerate(b.replicas):
+                r.build_tables()
+                u, q = starts(i)
+                prepare(r, ps[i], u, q)
+            t0 = time.perf_counter()
+            tb = b.tune(steps=8)
+            t_tune = time.perf_counter() - t0
+            plans = sorted({(ps[i].Lx,) + b.replicas[i].plan[:2] for i in range(n_rep)})
+            t0 = time.perf_counter()
+            b.run_point(Ts, n_therm, n_avg, every)
+            t_run = time.perf_counter() - t0
+            groups = b.groups
+            rows = b.samples()
+        zs = {k: [] for k in ("V", "KE", "|u|", "u2")}
+        worst = []
+        for i in range(n_rep):
+            oa, ob = _point_obs(rows[i], ps[i].N), _point_obs(plain[i], ps[i].N)
+            for k in zs:
+                ma, ea = _block_mean(oa[k])
+                mb, eb = _block_mean(ob[k])
+                z = (ma - mb) / max(np.hypot(ea, eb), 1e-300)
+                zs[k].append(z)
+                if abs(z) > 3.0:
+                    worst.append([Ls[i], Ts[i], k, round(float(z), 2), ma, mb])
+        agree = {k: {"within_3sigma": int(np.sum(np.abs(v) <= 3.0)), "max_abs_z": float(np.max(np.abs(v))),
+                     "chi2_per_point": float(np.mean(np.square(v)))} for k, v in zs.items()}
+        say(f"sweep: batched ({tag}) {t_run:.1f} s, tune {t_tune:.1f} s")
+        worst.sort(key=lambda w: -abs(w[3]))
+        return {"seconds": t_run, "tune_seconds": t_tune, "tune_ms_per_batch_step": list(tb), "plans": plans,
+                "graph_branches": groups, "value": sites * (n_therm + n_avg) / t_run, "speedup_vs_plain": t_plain / t_run,
+                "agreement": agree, "outside_3sigma": worst[:20]}
+
+    out["batched_cold"] = batched_arm(lambda i: initial_state(ps[i]), "cold")
+    if warm_layers is not None:
+        fields = {}
+        t0 = time.perf_counter()
+        for L in sizes:
+            idx = [i for i in range(n_rep) if Ls[i] == L]
+            with W.WarmStartNet((L, L, L), batch=len(idx), seed=7) as net:
+                for l, (w, bb) in enumerate(warm_layers):
+                    net.set_layer(l, w, bb)
+                cond = np.array([[Ts[i], 0.0, 0.0, 0.0, ps[i].GPa[0]] for i in idx])
+                net.forward(cond, [1000 + i for i in idx])
+                for k, i in enumerate(idx):
+                    fields[i] = (net.field(k, ps[i]), W.maxwell_momenta(ps[i], 2000 + i))
+        t_inf = time.perf_counter() - t0
+        out["batched_warm"] = batched_arm(lambda i: fields[i], "warm")
+        out["batched_warm"]["inference_seconds"] = t_inf
+    return out
+
+
 def fft_vs_cufft(L=128, reps=20):
     """The device FFT stage (3-component r2c and c2r: k_xy_fwd + z pass, z
     pass + k_xy_inv; fg_time_fft) against cuFFT on the same GPU, planned as
@@ -421,7 +536,7 @@ def warm_start_leg(L=32, log=None):
         p.E_field_always_zero = 0
         p.N = 0
         return fb.make_param(p)
-    return W.experiment(mp, L=L, log=log)
+    return W.experiment(mp, L=L, log=log, keep_layers=True)
 
 
 def cpu_baseline(p, budget_s=20.0):
@@ -659,6 +774,10 @@ def main():
         fftc = fft_vs_cufft(L)
         epit = epit_hysteresis()
         wstart = warm_start_leg(log=lambda m: print(m, file=sys.stderr, flush=True))
+    sweep = None
+    if rank == 0 and world == 1 and not args.no_batched and not args.mixed_only:
+        sweep = cooling_sweep(warm_layers=wstart.pop("_layers", None) if wstart else None,
+                              log=lambda m: print(m, file=sys.stderr, flush=True))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(p)
@@ -677,7 +796,7 @@ def main():
         "force_err_16_configs": ferr16,
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "batched": batched,
-        "fft_vs_cufft": fftc, "epit_hysteresis": epit, "warm_start": wstart,
+        "fft_vs_cufft": fftc, "epit_hysteresis": epit, "warm_start": wstart, "cooling_sweep": sweep,
         "gpu_launches": A.FG_NPROF * args.steps,  # kernels per bulk NP step graph
     }
     ctxm.close()

@@ -18,12 +18,13 @@ import tempfile
 import numpy as np
 
 from . import _capi
-from ._capi import (FG_PREC_FP64, FG_PREC_MIXED, FG_OK, fg_average, fg_energy, fg_params,
+from ._capi import (FG_PREC_FP64, FG_PREC_MIXED, FG_OK, FG_SAMPLE_COLS, fg_average, fg_energy, fg_params,
                     complex_field, dptr, k_table, physical, real_field)
 
 __all__ = ["Context", "FeramError", "read_param", "make_param", "params_from_text", "default_params",
            "FG_PREC_FP64", "FG_PREC_MIXED", "fg_energy", "fg_average", "fg_params",
-           "real_field", "complex_field", "k_table", "physical", "lib"]
+           "real_field", "complex_field", "k_table", "physical", "lib", "Batch",
+           "wisdom_export", "wisdom_import", "wisdom_forget", "FG_SAMPLE_COLS"]
 
 lib = _capi.lib
 
@@ -253,6 +254,51 @@ class Context:
         self._check(lib().fg_run_steps(self._h, n, C.byref(e)))
         return e
 
+    # -- sweep points and sample series
+    def sample(self):
+        """fg_sample: one row of the device sample series for this state."""
+        self._check(lib().fg_sample(self._h))
+
+    def samples(self) -> np.ndarray:
+        """fg_samples_read: the rows held, (n, FG_SAMPLE_COLS); empties the series."""
+        n = C.c_int()
+        self._check(lib().fg_samples_read(self._h, None, 0, C.byref(n)))
+        out = np.zeros((n.value, FG_SAMPLE_COLS))
+        self._check(lib().fg_samples_read(self._h, dptr(out), n.value, C.byref(n)))
+        return out
+
+    def run_point(self, kelvin: float, n_therm: int, n_avg: int, every: int, E=None) -> fg_energy:
+        """fg_run_point: chain to (kelvin, E), n_therm steps, n_avg steps with a
+        sample row every `every` steps."""
+        e = fg_energy()
+        Ea = None if E is None else np.ascontiguousarray(E, dtype=np.float64)
+        self._check(lib().fg_run_point(self._h, kelvin, dptr(Ea), n_therm, n_avg, every, C.byref(e)))
+        p = fg_params()
+        self._check(lib().fg_get_params(self._h, C.byref(p)))
+        self.p = p
+        return e
+
+    # -- launch plans
+    def tune(self, steps: int = 64):
+        """fg_tune: time the plan candidates, keep the fastest; returns
+        (z tile width, waves, ms per step)."""
+        z, w, ms = C.c_int(), C.c_int(), C.c_double()
+        self._check(lib().fg_tune(self._h, steps, C.byref(z), C.byref(w), C.byref(ms)))
+        return z.value, w.value, ms.value
+
+    def set_plan(self, zcw: int = 0, waves: int = 1):
+        self._check(lib().fg_set_plan(self._h, zcw, waves))
+
+    @property
+    def plan(self):
+        """(z tile width, waves, kick-drift grid, assembly grid)."""
+        v = [C.c_int() for _ in range(4)]
+        self._check(lib().fg_get_plan(self._h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def apply_wisdom(self):
+        self._check(lib().fg_apply_wisdom(self._h))
+
 
 class _Replica(Context):
     """A replica of a Batch: a Context view that the batch owns."""
@@ -304,6 +350,37 @@ class Batch:
         """Branches of the last captured batch graph."""
         return lib().fg_batch_groups(self._b)
 
+    def _bcheck(self, rc):
+        if rc:
+            r = lib().fg_batch_last_error(self._b)
+            raise FeramError(rc, r.decode() if r else "")
+
+    def run_point(self, kelvin, n_therm: int, n_avg: int, every: int, E=None):
+        """fg_batch_run_point: every replica chained to its kelvin[i] (and
+        E[i]), then n_therm + n_avg batch steps with sample rows."""
+        k = np.ascontiguousarray(kelvin, dtype=np.float64)
+        assert k.shape == (len(self.replicas),)
+        Ea = None if E is None else np.ascontiguousarray(E, dtype=np.float64).reshape(len(self.replicas), 3)
+        self._bcheck(lib().fg_batch_run_point(self._b, dptr(k), dptr(Ea), n_therm, n_avg, every))
+        for r in self.replicas:
+            p = fg_params()
+            r._check(lib().fg_get_params(r._h, C.byref(p)))
+            r.p = p
+
+    def samples(self):
+        """Every replica's sample series (emptied)."""
+        return [r.samples() for r in self.replicas]
+
+    def tune(self, steps: int = 16):
+        """fg_batch_tune: per supercell, the fastest plan in whole batch steps;
+        returns (ms per batch step before, after)."""
+        a, b = C.c_double(), C.c_double()
+        self._bcheck(lib().fg_batch_tune(self._b, steps, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def apply_wisdom(self):
+        self._bcheck(lib().fg_batch_apply_wisdom(self._b))
+
     def close(self):
         if getattr(self, "_b", None):
             for r in self.replicas:
@@ -322,6 +399,30 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def wisdom_export() -> str:
+    """fg_wisdom_export: the process's plans as text."""
+    n = C.c_int()
+    lib().fg_wisdom_export(None, 0, C.byref(n))
+    buf = C.create_string_buffer(n.value)
+    rc = lib().fg_wisdom_export(buf, n.value, C.byref(n))
+    if rc:
+        raise FeramError(rc, "fg_wisdom_export")
+    return buf.value.decode()
+
+
+def wisdom_import(text: str) -> int:
+    """fg_wisdom_import: add the plans of `text`; returns how many."""
+    n = C.c_int()
+    rc = lib().fg_wisdom_import(text.encode(), C.byref(n))
+    if rc:
+        raise FeramError(rc, "malformed wisdom")
+    return n.value
+
+
+def wisdom_forget():
+    lib().fg_wisdom_forget()
 
 
 def feram_run(path: str, precision: int = FG_PREC_FP64):

@@ -18,6 +18,7 @@ FILENAME_LEN = 300
 FG_OK, FG_ERR_ARG, FG_ERR_CUDA, FG_ERR_NAN, FG_ERR_TIMEOUT, FG_ERR_UNSUPPORTED, FG_ERR_IO, FG_ERR_STATE = range(8)
 FG_BULK, FG_FILM, FG_EPIT, FG_E110 = range(4)
 FG_NPROF = 5  # kernels of one Nose-Poincare step in fg_profile_step
+FG_SAMPLE_COLS, FG_SAMPLE_CAP = 16, 8192  # sample series rows (fg_sample)
 FG_METHOD_MD, FG_METHOD_VS, FG_METHOD_LF, FG_METHOD_HL = range(4)
 (FG_WAVE_NONE, FG_WAVE_TRIANGULAR_COS, FG_WAVE_TRIANGULAR_SIN,
  FG_WAVE_RAMPING_ON, FG_WAVE_RAMPING_OFF, FG_WAVE_OTHER) = range(6)
@@ -159,6 +160,19 @@ def lib() -> C.CDLL:
         "fg_set_wave": (C.c_int, [vp, C.c_int, C.c_int]),
         "fg_batch_set_grouping": (C.c_int, [vp, C.c_int]),
         "fg_batch_groups": (C.c_int, [vp]),
+        "fg_sample": (C.c_int, [vp]),
+        "fg_samples_read": (C.c_int, [vp, dp, C.c_int, P(C.c_int)]),
+        "fg_run_point": (C.c_int, [vp, C.c_double, dp, C.c_int, C.c_int, C.c_int, C.POINTER(fg_energy)]),
+        "fg_batch_run_point": (C.c_int, [vp, dp, dp, C.c_int, C.c_int, C.c_int]),
+        "fg_tune": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_int), dp]),
+        "fg_batch_tune": (C.c_int, [vp, C.c_int, dp, dp]),
+        "fg_set_plan": (C.c_int, [vp, C.c_int, C.c_int]),
+        "fg_get_plan": (C.c_int, [vp, P(C.c_int), P(C.c_int), P(C.c_int), P(C.c_int)]),
+        "fg_wisdom_export": (C.c_int, [C.c_char_p, C.c_int, P(C.c_int)]),
+        "fg_wisdom_import": (C.c_int, [C.c_char_p, P(C.c_int)]),
+        "fg_wisdom_forget": (None, []),
+        "fg_apply_wisdom": (C.c_int, [vp]),
+        "fg_batch_apply_wisdom": (C.c_int, [vp]),
         "fg_ws_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(vp)]),
         "fg_ws_destroy": (None, [vp]),
         "fg_ws_last_error": (C.c_char_p, [vp]),

@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -183,9 +184,20 @@ struct fg_ctx {
   int NXP = 0, NYP = 0;
   bool bulk_or_film_mirror() const { return P.bulk_or_film == FG_FILM || P.bulk_or_film == FG_EPIT; }
   size_t real_bytes = 0;
+  // launch plan (fg_tune, fg_wisdom_import): the z-tile width asked for
+  // (0: the widest that fits) and the resident waves of the streaming
+  // kernels (0: one block per 256 sites, up to grid_elem)
+  int plan_zcw = 0, plan_waves = 1;
+  // sample series (fg_sample): kSampleCols doubles per row, on the device
+  double* samples = nullptr;
+  int n_samples = 0;
 };
 
 namespace {
+
+// wisdom entries: plans of a context stepped alone, of a replica in a batch
+enum { PLAN_SOLO = 0, PLAN_BATCH = 1 };
+int apply_wisdom(fg_ctx* ctx, int mode);
 
 int fail(fg_ctx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
@@ -606,6 +618,8 @@ bool groupable(const fg_ctx* c) {
 // Replicas a and b step together: same size, precision and site constants.
 bool same_group(const fg_ctx* a, const fg_ctx* b) {
   if (a->prec != b->prec || a->g.Lx != b->g.Lx || a->g.Ly != b->g.Ly || a->g.Lz != b->g.Lz) return false;
+  // one launch covers the group with the first replica's tiles and grids
+  if (a->zt.CW != b->zt.CW || a->grid_kd != b->grid_kd || a->grid_asc != b->grid_asc) return false;
   const AsmConst ka = asm_const(a), kb = asm_const(b);
   return std::memcmp(&ka, &kb, sizeof(AsmConst)) == 0;
 }
@@ -740,6 +754,12 @@ int validate(const fg_params* p, std::string* why) {
   return FG_OK;
 }
 
+// The widest z tile the context's plan allows.
+template <typename T>
+int plan_cw(const fg_ctx* ctx) {
+  return ctx->plan_zcw > 0 ? std::min(ctx->plan_zcw, z_cw_cap<T>()) : z_cw_cap<T>();
+}
+
 // z tiles: CW is the largest power of two <= cwmax dividing Lx/2 whose
 // tile of nc components fits in shared memory
 ZTiles z_tiles(const Geom& g, int nc, size_t esz, int cwmax, int smem_max) {
@@ -751,6 +771,24 @@ ZTiles z_tiles(const Geom& g, int nc, size_t esz, int cwmax, int smem_max) {
   t.nreg = t.ntx * g.Ly;
   t.nnyq = div_up(g.Ly, cw);
   return t;
+}
+
+// Grids of the streaming kernels (grid-stride loops): `waves` resident
+// waves of blocks, or (waves = 0) one block per kThreadsElem sites, never
+// more than grid_elem (the size of the per-block partial-sum buffers).
+template <typename T>
+void plan_grids(fg_ctx* ctx, int waves, int nsm) {
+  const int all = std::max(1, std::min(ctx->grid_elem, div_up(ctx->g.nsite, kThreadsElem)));
+  auto grid = [&](auto kern) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kThreadsElem, 0) != cudaSuccess || nb < 1) nb = 8;
+    return waves <= 0 ? all : std::max(1, std::min(all, waves * nb * nsm));
+  };
+  ctx->grid_kd = grid(k_kick_drift<T>);
+  ctx->grid_kc = std::min(grid(k_kick_close<T, false>), grid(k_kick_close<T, true>));
+  ctx->grid_as = grid(k_assemble<T, false>);
+  ctx->grid_asc = grid(k_assemble<T, true>);
+  ctx->plan_waves = waves;
 }
 
 template <typename T>
@@ -786,7 +824,7 @@ int create_impl(fg_ctx* ctx) {
   auto tiles = [&](int nc, size_t esz, int cwmax) { return z_tiles(g, nc, esz, cwmax, smem_max); };
   ctx->acou = P.mass_acou[0] > 0.0;
   ctx->ncx = ctx->acou ? 12 : 9;
-  ctx->zt = tiles(ctx->ncx, sizeof(cplx<T>), z_cw_cap<T>());
+  ctx->zt = tiles(ctx->ncx, sizeof(cplx<T>), plan_cw<T>(ctx));
   ctx->zt6 = tiles(6, sizeof(cplx<double>), 8);
   ctx->zt1 = tiles(1, sizeof(cplx<double>), 8);
   if ((size_t)ctx->ncx * g.Lz * ctx->zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
@@ -796,17 +834,7 @@ int create_impl(fg_ctx* ctx) {
   ctx->smem_z6 = (int)(6 * (size_t)g.Lz * ctx->zt6.CW * sizeof(cplx<double>));
   ctx->smem_z1 = (int)(1 * (size_t)g.Lz * ctx->zt1.CW * sizeof(cplx<double>));
   ctx->grid_elem = std::max(1, std::min(div_up(g.nsite, kThreadsElem), nsm * 8));
-  {
-    auto wave = [&](auto kern) {
-      int nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kThreadsElem, 0) != cudaSuccess || nb < 1) nb = 8;
-      return std::max(1, std::min(ctx->grid_elem, nb * nsm));
-    };
-    ctx->grid_kd = wave(k_kick_drift<T>);
-    ctx->grid_kc = std::min(wave(k_kick_close<T, false>), wave(k_kick_close<T, true>));
-    ctx->grid_as = wave(k_assemble<T, false>);
-    ctx->grid_asc = wave(k_assemble<T, true>);
-  }
+  plan_grids<T>(ctx, ctx->plan_waves, nsm);
   {
     // The dynamic shared-memory cap is an attribute of the kernel, shared by
     // every context in the process: raise it to what the device allows next
@@ -1354,7 +1382,7 @@ int set_zsite(fg_ctx* ctx, bool on) {
   CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const int smem_max = smem_optin - 8192;
   const int ncx = (ctx->acou ? 12 : 9) + (on ? 3 : 0);
-  const ZTiles zt = z_tiles(g, ncx, sizeof(cplx<T>), z_cw_cap<T>(), smem_max);
+  const ZTiles zt = z_tiles(g, ncx, sizeof(cplx<T>), plan_cw<T>(ctx), smem_max);
   if ((size_t)ncx * g.Lz * zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
     return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
   const int smem_z = (int)(ncx * ((size_t)g.Lz * zt.CW + kZPad<T>) * sizeof(cplx<T>));
@@ -1619,6 +1647,7 @@ int fg_create(const fg_params* p, int precision, fg_ctx** out) {
     return FG_ERR_ARG;
   }
   rc = (precision == FG_PREC_MIXED) ? create_impl<float>(ctx) : create_impl<double>(ctx);
+  if (rc == FG_OK) rc = apply_wisdom(ctx, PLAN_SOLO);
   *out = ctx;
   return rc;
 }
@@ -1637,7 +1666,7 @@ void fg_destroy(fg_ctx* ctx) {
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
                   ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all,
                   ctx->site_minv, ctx->site_macou, ctx->site_sump, ctx->site_species, ctx->site_zstar, ctx->site_E,
-                  ctx->layer_nsum};
+                  ctx->layer_nsum, ctx->samples};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (ctx->sc_host) cudaFreeHost(ctx->sc_host);
@@ -2404,6 +2433,51 @@ int batch_capture(fg_batch* b, cudaGraphExec_t* out) {
   if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   return FG_OK;
 }
+// Ready every replica for a step of the batch graph and (re)capture it:
+// pending force and half step, set-up work on the replica streams finished,
+// a graph whose replicas replaced buffers since its capture dropped.
+int batch_prepare(fg_batch* b) {
+  int rc;
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    fg_ctx* c = b->ctx[i];
+    if ((rc = ensure_ready(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+    if (c->P.method == FG_METHOD_MD && (rc = np_ready_for_step(c)))
+      return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+    // set-up work on the replica's own stream must finish before the batch
+    // stream starts the graph
+    cudaError_t ce = cudaStreamSynchronize(c->stream);
+    if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+  }
+  // a replica whose buffers were replaced (site arrays, plans) invalidates the graph
+  bool stale = b->gen.size() != b->ctx.size();
+  for (size_t i = 0; !stale && i < b->ctx.size(); ++i) stale = b->gen[i] != b->ctx[i]->gen;
+  if (stale) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    b->gen.resize(b->ctx.size());
+    for (size_t i = 0; i < b->ctx.size(); ++i) b->gen[i] = b->ctx[i]->gen;
+  }
+  return batch_capture(b, &b->graph);
+}
+
+// After the launches: wait for the batch stream, then every replica's
+// scalars (status checked) and, with e, its energies.
+int batch_finish(fg_batch* b, fg_energy* e) {
+  cudaError_t ce = cudaStreamSynchronize(b->stream);
+  if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+  int rc;
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    fg_ctx* c = b->ctx[i];
+    c->force_fresh = true;
+    c->flo_valid = false;
+    c->np_ready = c->P.method == FG_METHOD_MD;
+    if ((rc = pull_scalars(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+    if (e) energy_out(c->sc_host, &e[i], false);
+  }
+  return FG_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -2431,6 +2505,7 @@ int fg_batch_create(int n, const fg_params* params, int precision, fg_batch** ou
   }
   *out = nullptr;
   fg_batch* b = new fg_batch();
+  int rc2 = FG_OK;
   for (int i = 0; i < n; ++i) {
     fg_ctx* c = nullptr;
     const int rc = fg_create(&params[i], precision, &c);
@@ -2441,6 +2516,11 @@ int fg_batch_create(int n, const fg_params* params, int precision, fg_batch** ou
       return rc;
     }
     b->ctx.push_back(c);
+    if ((rc2 = apply_wisdom(c, PLAN_BATCH))) {
+      msg("replica " + std::to_string(i) + ": " + c->err);
+      fg_batch_destroy(b);
+      return rc2;
+    }
   }
   b->join.assign((size_t)n, nullptr);
   cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
@@ -2480,43 +2560,529 @@ const char* fg_batch_last_error(const fg_batch* b) { return b ? b->err.c_str() :
 
 int fg_batch_step(fg_batch* b, int n_steps, fg_energy* e) {
   if (!b || n_steps < 0) return FG_ERR_ARG;
-  int rc;
-  for (size_t i = 0; i < b->ctx.size(); ++i) {
-    fg_ctx* c = b->ctx[i];
-    if ((rc = ensure_ready(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
-    if (c->P.method == FG_METHOD_MD && (rc = np_ready_for_step(c)))
-      return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
-    // set-up work on the replica's own stream must finish before the batch
-    // stream starts the graph
-    cudaError_t ce = cudaStreamSynchronize(c->stream);
-    if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
-  }
-  // a replica whose buffers were replaced (site arrays) invalidates the graphs
-  bool stale = b->gen.size() != b->ctx.size();
-  for (size_t i = 0; !stale && i < b->ctx.size(); ++i) stale = b->gen[i] != b->ctx[i]->gen;
-  if (stale) {
-    if (b->graph) {
-      cudaGraphExecDestroy(b->graph);
-      b->graph = nullptr;
-    }
-    b->gen.resize(b->ctx.size());
-    for (size_t i = 0; i < b->ctx.size(); ++i) b->gen[i] = b->ctx[i]->gen;
-  }
-  if ((rc = batch_capture(b, &b->graph))) return rc;
+  int rc = batch_prepare(b);
+  if (rc) return rc;
   for (int k = 0; k < n_steps; ++k) {
     cudaError_t ce = cudaGraphLaunch(b->graph, b->stream);
     if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
   }
-  cudaError_t ce = cudaStreamSynchronize(b->stream);
-  if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+  return batch_finish(b, e);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Launch plans, the autotuner and its wisdom.
+//
+// The reference plans each of its transforms with FFTW_MEASURE when it
+// allocates the coordinates (coord_module.F:155-377), imports plans that
+// were measured before from a "wisdom" file at start-up
+// (feram_common.F:56-69), and ships a program that measures and exports
+// them (feram_fftw_wisdom.F).  Here a plan is the z-pencil tile width (the
+// kx columns one CTA of the z kernel transforms and multiplies) and the
+// grid of the streaming kernels; fg_tune / fg_batch_tune time the candidates
+// on the step itself and keep the fastest, and the wisdom is the table of
+// the plans found, keyed by supercell, precision, components and launch kind
+// (alone, or inside a replica batch), that fg_create and fg_batch_create
+// consult.
+namespace {
+
+struct PlanKey {
+  int mode, prec, Lx, Ly, Lz, ncx;
+  bool operator<(const PlanKey& o) const {
+    const int a[6] = {mode, prec, Lx, Ly, Lz, ncx}, b[6] = {o.mode, o.prec, o.Lx, o.Ly, o.Lz, o.ncx};
+    return std::lexicographical_compare(a, a + 6, b, b + 6);
+  }
+};
+struct PlanVal {
+  int zcw, waves;
+};
+std::mutex g_wisdom_mu;
+std::map<PlanKey, PlanVal> g_wisdom;
+
+PlanKey plan_key(const fg_ctx* c, int mode) { return PlanKey{mode, c->prec, c->g.Lx, c->g.Ly, c->g.Lz, c->ncx}; }
+
+void drop_graphs(fg_ctx* ctx) {
+  for (cudaGraphExec_t* gx : {&ctx->g_np, &ctx->g_np_multi, &ctx->g_lf, &ctx->g_vs, &ctx->g_force})
+    if (*gx) {
+      cudaGraphExecDestroy(*gx);
+      *gx = nullptr;
+    }
+  ++ctx->gen;  // batches holding this replica capture again
+}
+
+// Switch the context to a plan: z tiles (and their per-tile partial sums),
+// the z kernels' shared-memory limit, the streaming grids; the step graphs
+// are captured again at the next step.
+template <typename T>
+int apply_plan_t(fg_ctx* ctx, int zcw, int waves) {
+  const Geom& g = ctx->g;
+  int dev = 0, smem_optin = 0, nsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int smem_max = smem_optin - 8192;
+  const int cwmax = zcw > 0 ? std::min(zcw, z_cw_cap<T>()) : z_cw_cap<T>();
+  const ZTiles zt = z_tiles(g, ctx->ncx, sizeof(cplx<T>), cwmax, smem_max);
+  if ((size_t)ctx->ncx * g.Lz * zt.CW * sizeof(cplx<T>) > (size_t)smem_max)
+    return fail(ctx, FG_ERR_UNSUPPORTED, "a z pencil of the supercell does not fit in shared memory");
+  const int smem_z = (int)(ctx->ncx * ((size_t)g.Lz * zt.CW + kZPad<T>) * sizeof(cplx<T>));
+  const int smem_z3 = (int)(3 * (size_t)g.Lz * zt.CW * sizeof(cplx<T>));
+  cudaError_t ea = cudaSuccess;
+  auto setattr = [&](auto kern, int bytes) {
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    const int cap = smem_optin - (int)fa.sharedSizeBytes;
+    if (e == cudaSuccess && bytes > cap) e = cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, cap);
+    if (e != cudaSuccess) ea = e;
+  };
+  with_z_kspace<T>(g.Lz, zt.CW, ctx->acou, ctx->zsite, [&](auto k) { setattr(k, smem_z); });
+  with_z_pass<T, false>(g.Lz, zt.CW, [&](auto k) { setattr(k, smem_z3); });
+  with_z_pass<T, true>(g.Lz, zt.CW, [&](auto k) { setattr(k, smem_z3); });
+  if (ea != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(ea));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (zt.nreg + zt.nnyq > ctx->zt.nreg + ctx->zt.nnyq) {
+    ctx->broken = true;  // until part_k is allocated again
+    cudaFree(ctx->part_k);
+    ctx->part_k = nullptr;
+    CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)(zt.nreg + zt.nnyq)));
+    ctx->broken = false;
+  }
+  ctx->zt = zt;
+  ctx->smem_z = smem_z;
+  ctx->smem_z3 = smem_z3;
+  ctx->plan_zcw = zcw;
+  plan_grids<T>(ctx, waves, nsm);
+  drop_graphs(ctx);
+  return FG_OK;
+}
+
+int apply_plan(fg_ctx* ctx, int zcw, int waves) {
+  if (ctx->broken) return fail(ctx, FG_ERR_STATE, "an earlier reallocation failed: destroy this context");
+  return ctx->prec == FG_PREC_MIXED ? apply_plan_t<float>(ctx, zcw, waves) : apply_plan_t<double>(ctx, zcw, waves);
+}
+
+int apply_wisdom(fg_ctx* ctx, int mode) {
+  PlanVal v{};
+  {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    auto it = g_wisdom.find(plan_key(ctx, mode));
+    if (it == g_wisdom.end()) return FG_OK;
+    v = it->second;
+  }
+  if (v.zcw == ctx->plan_zcw && v.waves == ctx->plan_waves) return FG_OK;
+  return apply_plan(ctx, v.zcw, v.waves);
+}
+
+void remember_plan(const fg_ctx* ctx, int mode) {
+  std::lock_guard<std::mutex> lk(g_wisdom_mu);
+  g_wisdom[plan_key(ctx, mode)] = PlanVal{ctx->plan_zcw, ctx->plan_waves};
+}
+
+// The candidates: z-tile widths that give distinct tiles (widest first) and
+// the streaming grids (one and two resident waves, every block).
+std::vector<int> zcw_candidates(const fg_ctx* ctx) {
+  const int cap = ctx->prec == FG_PREC_MIXED ? z_cw_cap<float>() : z_cw_cap<double>();
+  std::vector<int> out;
+  int last = -1;
+  for (int w = cap; w >= 1 && (int)out.size() < 3; w /= 2) {
+    int cw = w;
+    while (cw > 1 && ctx->g.m % cw != 0) cw /= 2;
+    if (cw != last) out.push_back(w);
+    last = cw;
+  }
+  return out;
+}
+const int kWaveCandidates[3] = {1, 2, 0};
+
+// The dynamical state a tuning run overwrites: u, p (with the acoustic
+// components) and the device scalars.
+struct Snapshot {
+  void* u = nullptr;
+  void* p = nullptr;
+  DevScalars sc{};
+  size_t bytes = 0;
+};
+void snapshot_free(Snapshot* s) {
+  if (s->u) cudaFree(s->u);
+  if (s->p) cudaFree(s->p);
+  s->u = s->p = nullptr;
+}
+int snapshot_take(fg_ctx* ctx, Snapshot* s) {
+  int rc = pull_scalars(ctx);
+  if (rc) return rc;
+  s->sc = *ctx->sc_host;
+  s->bytes = (ctx->acou ? 6 : 3) * ctx->real_bytes;
+  CK(cudaMalloc(&s->u, s->bytes));
+  CK(cudaMalloc(&s->p, s->bytes));
+  CK(cudaMemcpyAsync(s->u, ctx->u, s->bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(s->p, ctx->p, s->bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FG_OK;
+}
+int snapshot_restore(fg_ctx* ctx, const Snapshot* s) {
+  CK(cudaMemcpyAsync(ctx->u, s->u, s->bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->p, s->p, s->bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  *ctx->sc_host = s->sc;
+  ctx->force_fresh = false;
+  ctx->flo_valid = false;
+  ctx->np_ready = false;
+  return push_scalars(ctx);
+}
+
+// Fastest of `reps` timings of `steps` Nose-Poincare steps (ms per step),
+// after one graph's worth of untimed steps (capture and warm-up).
+int time_solo(fg_ctx* ctx, int steps, int reps, double* ms) {
+  double t = 0.0, best = 1e300;
+  int rc = fg_time_steps(ctx, kNpGraphSteps, &t);
+  for (int r = 0; r < reps && rc == FG_OK; ++r)
+    if ((rc = fg_time_steps(ctx, steps, &t)) == FG_OK) best = std::min(best, t / steps);
+  *ms = best;
+  return rc;
+}
+
+// Steps of every replica of the batch go on the batch stream, followed by
+// one sample row of each replica.
+int sample_enqueue(fg_ctx* ctx, cudaStream_t st);
+
+}  // namespace
+
+extern "C" {
+
+int fg_tune(fg_ctx* ctx, int steps, int* zcw, int* waves, double* ms_per_step) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  if (steps < 1) return FG_ERR_ARG;
+  if (ctx->P.method != FG_METHOD_MD) return fail(ctx, FG_ERR_UNSUPPORTED, "fg_tune times Nose-Poincare ('md') steps");
+  Snapshot snap;
+  if ((rc = snapshot_take(ctx, &snap))) {
+    snapshot_free(&snap);
+    return rc;
+  }
+  double best = 1e300, t = 0.0;
+  int bz = ctx->plan_zcw, bw = ctx->plan_waves;
+  for (int z : zcw_candidates(ctx)) {
+    if ((rc = apply_plan(ctx, z, bw)) || (rc = time_solo(ctx, steps, 3, &t))) break;
+    if (t < best) best = t, bz = z;
+  }
+  for (int w : kWaveCandidates) {
+    if (rc) break;
+    if (w == bw) continue;
+    if ((rc = apply_plan(ctx, bz, w)) || (rc = time_solo(ctx, steps, 3, &t))) break;
+    if (t < best) best = t, bw = w;
+  }
+  if (!rc) rc = apply_plan(ctx, bz, bw);
+  if (!rc) rc = snapshot_restore(ctx, &snap);
+  snapshot_free(&snap);
+  if (rc) return rc;
+  remember_plan(ctx, PLAN_SOLO);
+  if (zcw) *zcw = ctx->zt.CW;
+  if (waves) *waves = ctx->plan_waves;
+  if (ms_per_step) *ms_per_step = best;
+  return FG_OK;
+}
+
+int fg_set_plan(fg_ctx* ctx, int zcw, int waves) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  if (zcw < 0 || waves < 0) return fail(ctx, FG_ERR_ARG, "zcw and waves must be >= 0");
+  return apply_plan(ctx, zcw, waves);
+}
+
+int fg_get_plan(const fg_ctx* ctx, int* zcw, int* waves, int* grid_kd, int* grid_asc) {
+  if (!ctx) return FG_ERR_ARG;
+  if (zcw) *zcw = ctx->zt.CW;
+  if (waves) *waves = ctx->plan_waves;
+  if (grid_kd) *grid_kd = ctx->grid_kd;
+  if (grid_asc) *grid_asc = ctx->grid_asc;
+  return FG_OK;
+}
+
+// Text form: a header line, then one plan per line,
+// "<solo|batch> <fp64|mixed> Lx Ly Lz components zcw waves".
+int fg_wisdom_export(char* buf, int len, int* needed) {
+  std::string out = "feram_b200 wisdom 1\n";
+  {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    for (const auto& kv : g_wisdom) {
+      const PlanKey& k = kv.first;
+      char line[128];
+      std::snprintf(line, sizeof(line), "%s %s %d %d %d %d %d %d\n", k.mode == PLAN_BATCH ? "batch" : "solo",
+                    k.prec == FG_PREC_MIXED ? "mixed" : "fp64", k.Lx, k.Ly, k.Lz, k.ncx, kv.second.zcw,
+                    kv.second.waves);
+      out += line;
+    }
+  }
+  const int n = (int)out.size() + 1;
+  if (needed) *needed = n;
+  if (!buf) return FG_OK;
+  if (len < n) return FG_ERR_ARG;
+  std::memcpy(buf, out.c_str(), (size_t)n);
+  return FG_OK;
+}
+
+int fg_wisdom_import(const char* text, int* n_plans) {
+  if (!text) return FG_ERR_ARG;
+  std::vector<std::pair<PlanKey, PlanVal>> got;
+  const char* s = text;
+  bool header = false;
+  while (*s) {
+    const char* e = std::strchr(s, '\n');
+    std::string line = e ? std::string(s, (size_t)(e - s)) : std::string(s);
+    s = e ? e + 1 : s + line.size();
+    if (line.empty() || line[0] == '#') continue;
+    if (!header) {
+      if (line != "feram_b200 wisdom 1") return FG_ERR_ARG;
+      header = true;
+      continue;
+    }
+    char mode[16], prec[16];
+    int Lx, Ly, Lz, ncx, zcw, waves;
+    char extra;
+    if (std::sscanf(line.c_str(), "%15s %15s %d %d %d %d %d %d %c", mode, prec, &Lx, &Ly, &Lz, &ncx, &zcw, &waves,
+                    &extra) != 8)
+      return FG_ERR_ARG;
+    const std::string ms(mode), ps(prec);
+    if ((ms != "solo" && ms != "batch") || (ps != "mixed" && ps != "fp64") || Lx < 1 || Ly < 1 || Lz < 1 ||
+        ncx < 1 || zcw < 0 || waves < 0)
+      return FG_ERR_ARG;
+    got.push_back({PlanKey{ms == "batch" ? PLAN_BATCH : PLAN_SOLO, ps == "mixed" ? FG_PREC_MIXED : FG_PREC_FP64, Lx,
+                           Ly, Lz, ncx},
+                   PlanVal{zcw, waves}});
+  }
+  if (!header) return FG_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lk(g_wisdom_mu);
+    for (const auto& kv : got) g_wisdom[kv.first] = kv.second;
+  }
+  if (n_plans) *n_plans = (int)got.size();
+  return FG_OK;
+}
+
+void fg_wisdom_forget(void) {
+  std::lock_guard<std::mutex> lk(g_wisdom_mu);
+  g_wisdom.clear();
+}
+
+int fg_apply_wisdom(fg_ctx* ctx) {
+  if (!ctx || !ctx->stream) return FG_ERR_ARG;
+  return apply_wisdom(ctx, PLAN_SOLO);
+}
+
+// ---------------------------------------------------------------------------
+// Sample series and sweep points.
+
+int fg_sample(fg_ctx* ctx) {
+  int rc = ensure_ready(ctx);
+  if (rc) return rc;
+  return sample_enqueue(ctx, ctx->stream);
+}
+
+int fg_samples_read(fg_ctx* ctx, double* out, int max_rows, int* n_rows) {
+  if (!ctx || !ctx->stream || !n_rows) return FG_ERR_ARG;
+  CK(cudaStreamSynchronize(ctx->stream));
+  *n_rows = ctx->n_samples;
+  if (!out) return FG_OK;
+  if (max_rows < ctx->n_samples) return fail(ctx, FG_ERR_ARG, "out holds fewer rows than the series");
+  if (ctx->n_samples > 0)
+    CK(cudaMemcpy(out, ctx->samples, sizeof(double) * kSampleCols * (size_t)ctx->n_samples, cudaMemcpyDeviceToHost));
+  ctx->n_samples = 0;
+  return FG_OK;
+}
+
+// One point of a temperature (field) sweep on one context: chain from the
+// state on the device (fg_chain_point), n_therm steps, then n_avg steps with
+// a sample row every `every` steps, as a point of the reference's cooling
+// scripts runs n_thermalize and n_average steps from the previous .restart
+// (cooling.sh:64-69, molecular-dynamics.F:57-110).
+int fg_run_point(fg_ctx* ctx, double kelvin, const double E[3], int n_therm, int n_avg, int every, fg_energy* e) {
+  if (!ctx || n_therm < 0 || n_avg < 0 || every < 1) return FG_ERR_ARG;
+  if (ctx->n_samples + n_avg / every > kSampleCap)
+    return fail(ctx, FG_ERR_STATE, "the sample series would overflow: read it with fg_samples_read");
+  fg_energy en{};
+  int rc = fg_chain_point(ctx, kelvin, E, &en);
+  if (rc) return rc;
+  if ((rc = np_ready_for_step(ctx))) return rc;
+  int which = 0;
+  cudaGraphExec_t* gx = step_graph(ctx, &which);
+  auto steps = [&](int n) {
+    int i = 0, r = FG_OK;
+    for (; r == FG_OK && i + kNpGraphSteps <= n; i += kNpGraphSteps) r = run_graph(ctx, &ctx->g_np_multi, 4);
+    for (; r == FG_OK && i < n; ++i) r = run_graph(ctx, gx, which);
+    return r;
+  };
+  if ((rc = steps(n_therm))) return rc;
+  for (int k = 0; k + every <= n_avg; k += every)
+    if ((rc = steps(every)) || (rc = sample_enqueue(ctx, ctx->stream))) return rc;
+  ctx->force_fresh = true;
+  ctx->flo_valid = false;
+  ctx->np_ready = true;
+  if ((rc = pull_scalars(ctx))) return rc;
+  if (e) energy_out(ctx->sc_host, e, false);
+  return FG_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int sample_enqueue(fg_ctx* ctx, cudaStream_t st) {
+  if (!ctx->samples) CK(cudaMalloc(&ctx->samples, sizeof(double) * kSampleCols * (size_t)kSampleCap));
+  if (ctx->n_samples >= kSampleCap)
+    return fail(ctx, FG_ERR_STATE, "the sample series is full: read it with fg_samples_read");
+  if (ctx->prec == FG_PREC_MIXED)
+    k_avg_sums<float><<<ctx->grid_elem, kThreadsElem, 0, st>>>(
+        (const float*)ctx->u, ctx->g, ctx->P.Z_star[0], ctx->layer_sump, ctx->part_avg, ctx->site_sump,
+        (const float*)ctx->site_zstar);
+  else
+    k_avg_sums<double><<<ctx->grid_elem, kThreadsElem, 0, st>>>(
+        (const double*)ctx->u, ctx->g, ctx->P.Z_star[0], ctx->layer_sump, ctx->part_avg, ctx->site_sump,
+        (const double*)ctx->site_zstar);
+  CKL();
+  k_sample_row<<<1, RED_THREADS, 0, st>>>(ctx->samples + (size_t)kSampleCols * ctx->n_samples, ctx->part_avg,
+                                          ctx->grid_elem, ctx->sc);
+  CKL();
+  ++ctx->n_samples;
+  return FG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// A sweep point for every replica of the batch at once: each replica chained
+// to its own temperature (kelvin[i]) and field (E[3 i .. 3 i + 2], or none),
+// then n_therm and n_avg steps of the batch graph with a sample row of every
+// replica each `every` steps; the host waits once, at the end.
+int fg_batch_run_point(fg_batch* b, const double* kelvin, const double* E, int n_therm, int n_avg, int every) {
+  if (!b || !kelvin || n_therm < 0 || n_avg < 0 || every < 1) return FG_ERR_ARG;
+  int rc;
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    const fg_ctx* c = b->ctx[i];
+    if (c->P.method != FG_METHOD_MD)
+      return batch_fail(b, FG_ERR_UNSUPPORTED, "replica " + std::to_string(i) + ": sweep points run 'md' replicas");
+    if (c->n_samples + n_avg / every > kSampleCap)
+      return batch_fail(b, FG_ERR_STATE, "replica " + std::to_string(i) + ": the sample series would overflow");
+  }
   for (size_t i = 0; i < b->ctx.size(); ++i) {
     fg_ctx* c = b->ctx[i];
-    c->force_fresh = true;
-    c->flo_valid = false;
-    c->np_ready = c->P.method == FG_METHOD_MD;
-    if ((rc = pull_scalars(c))) return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
-    if (e) energy_out(c->sc_host, &e[i], false);
+    fg_energy en{};
+    if ((rc = fg_chain_point(c, kelvin[i], E ? E + 3 * i : nullptr, &en)))
+      return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
   }
+  if ((rc = batch_prepare(b))) return rc;
+  auto launch = [&](int n) {
+    for (int k = 0; k < n; ++k) {
+      cudaError_t ce = cudaGraphLaunch(b->graph, b->stream);
+      if (ce != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(ce));
+    }
+    return (int)FG_OK;
+  };
+  if ((rc = launch(n_therm))) return rc;
+  for (int k = 0; k + every <= n_avg; k += every) {
+    if ((rc = launch(every))) return rc;
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+      if ((rc = sample_enqueue(b->ctx[i], b->stream)))
+        return batch_fail(b, rc, "replica " + std::to_string(i) + ": " + b->ctx[i]->err);
+  }
+  return batch_finish(b, nullptr);
+}
+
+// The batch autotuner: for each supercell of the batch in turn, the plan
+// candidates applied to all its replicas, each timed as whole batch steps
+// (the other replicas' branches run beside it, as they will), the fastest
+// kept; the states are restored afterwards and the plans remembered as
+// batch wisdom.
+int fg_batch_tune(fg_batch* b, int steps, double* ms_before, double* ms_after) {
+  if (!b || steps < 1) return FG_ERR_ARG;
+  const size_t n = b->ctx.size();
+  std::vector<Snapshot> snap(n);
+  int rc = FG_OK;
+  auto cleanup = [&](int r) {
+    for (Snapshot& s : snap) snapshot_free(&s);
+    return r;
+  };
+  for (size_t i = 0; i < n && rc == FG_OK; ++i) {
+    fg_ctx* c = b->ctx[i];
+    if (c->P.method != FG_METHOD_MD) rc = batch_fail(b, FG_ERR_UNSUPPORTED, "fg_batch_tune times 'md' replicas");
+    else if ((rc = snapshot_take(c, &snap[i]))) rc = batch_fail(b, rc, "replica " + std::to_string(i) + ": " + c->err);
+  }
+  if (rc) return cleanup(rc);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto time_batch = [&](double* ms) {
+    int r = batch_prepare(b);
+    for (int k = 0; r == FG_OK && k < 2; ++k)
+      if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) r = batch_fail(b, FG_ERR_CUDA, "graph launch");
+    double best = 1e300;
+    for (int rep = 0; r == FG_OK && rep < 3; ++rep) {
+      cudaEventRecord(e0, b->stream);
+      for (int k = 0; r == FG_OK && k < steps; ++k)
+        if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) r = batch_fail(b, FG_ERR_CUDA, "graph launch");
+      cudaEventRecord(e1, b->stream);
+      float t = 0.0f;
+      if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+        r = batch_fail(b, FG_ERR_CUDA, "batch timing events");
+      best = std::min(best, (double)t / steps);
+    }
+    if (r == FG_OK) r = batch_finish(b, nullptr);
+    *ms = best;
+    return r;
+  };
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    rc = batch_fail(b, FG_ERR_CUDA, "cudaEventCreate");
+  double best = 0.0, t0 = 0.0;
+  if (!rc) rc = time_batch(&t0);
+  best = t0;
+  // one supercell (key) at a time, every replica of it on the same plan
+  std::vector<bool> done(n, false);
+  for (size_t i = 0; i < n && rc == FG_OK; ++i) {
+    if (done[i]) continue;
+    const PlanKey key = plan_key(b->ctx[i], PLAN_BATCH);
+    std::vector<size_t> members;
+    for (size_t j = i; j < n; ++j)
+      if (!done[j] && !(plan_key(b->ctx[j], PLAN_BATCH) < key) && !(key < plan_key(b->ctx[j], PLAN_BATCH))) {
+        members.push_back(j);
+        done[j] = true;
+      }
+    int bz = b->ctx[i]->plan_zcw, bw = b->ctx[i]->plan_waves;
+    auto try_plan = [&](int z, int w, bool* better) {
+      *better = false;
+      for (size_t j : members)
+        if (int r = apply_plan(b->ctx[j], z, w)) return batch_fail(b, r, b->ctx[j]->err);
+      double t = 0.0;
+      int r = time_batch(&t);
+      if (r == FG_OK && t < best) best = t, *better = true;
+      return r;
+    };
+    bool better = false;
+    for (int z : zcw_candidates(b->ctx[i])) {
+      if (z == bz) continue;
+      if ((rc = try_plan(z, bw, &better))) break;
+      if (better) bz = z;
+    }
+    for (int w : kWaveCandidates) {
+      if (rc || w == bw) continue;
+      if ((rc = try_plan(bz, w, &better))) break;
+      if (better) bw = w;
+    }
+    for (size_t j : members)
+      if (!rc && (rc = apply_plan(b->ctx[j], bz, bw))) rc = batch_fail(b, rc, b->ctx[j]->err);
+    if (!rc) remember_plan(b->ctx[i], PLAN_BATCH);
+  }
+  for (size_t i = 0; i < n && rc == FG_OK; ++i)
+    if ((rc = snapshot_restore(b->ctx[i], &snap[i]))) rc = batch_fail(b, rc, b->ctx[i]->err);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (rc) return cleanup(rc);
+  if (ms_before) *ms_before = t0;
+  if (ms_after) *ms_after = best;
+  return cleanup(FG_OK);
+}
+
+int fg_batch_apply_wisdom(fg_batch* b) {
+  if (!b) return FG_ERR_ARG;
+  for (size_t i = 0; i < b->ctx.size(); ++i)
+    if (int rc = apply_wisdom(b->ctx[i], PLAN_BATCH)) return batch_fail(b, rc, b->ctx[i]->err);
   return FG_OK;
 }
 

@@ -2054,6 +2054,30 @@ __global__ void __launch_bounds__(RED_THREADS) k_avg_finish(double* out6, const 
   }
 }
 
+// One row of a context's sample series (fg_sample): the six masked sums of
+// k_avg_sums (sum u, sum Z* u), then, from the scalars of the last step, the
+// potential energy, the true kinetic energy KE / s^2, s, pi and the six
+// homogeneous strains: the per-step quantities add_to_Average accumulates
+// (average_module.F:75-128), kept as a series so that their block errors
+// can be taken afterwards.
+constexpr int kSampleCols = FG_SAMPLE_COLS;
+constexpr int kSampleCap = FG_SAMPLE_CAP;  // rows a context holds between reads
+__global__ void __launch_bounds__(RED_THREADS) k_sample_row(double* __restrict__ row, const double* __restrict__ part,
+                                                            int nblk, const DevScalars* __restrict__ sc) {
+  for (int q = 0; q < 6; ++q) {
+    double v = reduce_partials(part, nblk, 6, q);
+    if (threadIdx.x == 0) row[q] = v;
+  }
+  if (threadIdx.x == 0) {
+    const double s = sc->s;
+    row[6] = sum_potential(sc->e);
+    row[7] = sc->e[E_DIPO] / (s * s);
+    row[8] = s;
+    row[9] = sc->pi;
+    for (int i = 0; i < 6; ++i) row[10 + i] = sc->strain[i];
+  }
+}
+
 template <typename T>
 __global__ void k_accumulate(double* __restrict__ acc, const T* __restrict__ u, long long n) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)

@@ -322,7 +322,8 @@ def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, t
 
 
 def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40, n_shuffled=20, seed=2024,
-               n_therm=3000, n_snap=14, train_steps=4000, probe=3000, every=20, accept_after=1000, log=None):
+               n_therm=3000, n_snap=14, train_steps=4000, probe=3000, every=20, accept_after=1000, log=None,
+               keep_layers=False):
     """The learned-warm-start protocol on one GPU.
 
     1. Data: MD cooling chains (train_chains of (E_z, GPa), train_temps
@@ -339,7 +340,8 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
        trace within 3 sigma of it.  Acceptance, the MD as the judge: the warm
        run's averages over [accept_after, probe) against the equilibrium,
        within 4 sigma of the difference; a rejected point keeps the fallback.
-    Returns a dict of the measurements; the "rows" of each pass are (T, E_z,
+    Returns a dict of the measurements (with keep_layers, "_layers": the
+    trained [(w, b)] of the four layers); the "rows" of each pass are (T, E_z,
     tau fallback, tau warm, tau cold, accepted, V/N of the first fallback
     and warm samples, equilibrium V/N, the same three for |<u>|^2)."""
     say = log or (lambda *a: None)
@@ -366,6 +368,8 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
                                       accept_after, say, "sweep")
         out["shuffled"] = _sweep(net, make_params, L, pts[n_held:], seed + 7, probe, every, accept_after, say,
                                  "shuffled")
+        if keep_layers:
+            out["_layers"] = [net.layer(l)[:2] for l in range(4)]
     finally:
         net.close()
     return out

@@ -360,6 +360,72 @@ int  fg_batch_set_grouping(fg_batch* b, int on);
 /* Branches of the batch graph last captured (groups and single replicas). */
 int  fg_batch_groups(const fg_batch* b);
 
+/* ---- sweep points and sample series -----------------------------------------
+   A point of a temperature / field sweep as the reference's sweep scripts run
+   it (cooling.sh:64-69: each point a feram run of n_thermalize + n_average
+   steps started from the previous point's .restart; molecular-dynamics.F:57-110),
+   with the state kept on the device.  Every `every` averaging steps a sample
+   row of FG_SAMPLE_COLS doubles goes to a series on the device:
+     0-2   sum_R u(R)       (counted sites, as average_module.F:75-128 sums)
+     3-5   sum_R Z*(R) u(R)
+     6     potential energy (the nine terms of the total)
+     7     dipo_kinetic / s^2
+     8, 9  s, pi
+     10-15 homogeneous strain (xx, yy, zz, yz, zx, xy)
+   so that averages, block errors and susceptibilities are taken afterwards. */
+#define FG_SAMPLE_COLS 16
+#define FG_SAMPLE_CAP 8192   /* rows a context holds between two reads */
+/* Append one row for the present state (no host wait). */
+int  fg_sample(fg_ctx* ctx);
+/* Waits for the context's stream, sets *n_rows to the rows held; with out
+   (room for max_rows rows) copies them and empties the series. */
+int  fg_samples_read(fg_ctx* ctx, double* out, int max_rows, int* n_rows);
+/* fg_chain_point(kelvin, E), n_therm steps, then n_avg steps with a row
+   every `every` steps ('md' only).  e (may be NULL): energies at the end. */
+int  fg_run_point(fg_ctx* ctx, double kelvin, const double E[3], int n_therm, int n_avg, int every,
+                  fg_energy* e);
+/* The same for every replica of a batch at once: replica i chained to
+   kelvin[i] and field E[3i..3i+2] (E may be NULL), then the batch graph; the
+   rows go to each replica's series (read with fg_batch_context +
+   fg_samples_read).  The host waits once, at the end. */
+int  fg_batch_run_point(fg_batch* b, const double* kelvin, const double* E, int n_therm, int n_avg,
+                        int every);
+
+/* ---- launch plans, the autotuner and wisdom ----------------------------------
+   The reference plans its transforms with FFTW_MEASURE (coord_module.F:155-377)
+   and imports saved FFTW wisdom at start-up (feram_common.F:56-69,
+   feram_fftw_wisdom.F).  Here a plan is the z-pencil tile width (kx columns
+   per CTA of the z kernel; the widest that divides Lx/2 and fits shared
+   memory, up to 8 (mixed) / 4 (fp64)) and the grid of the streaming kernels
+   (waves: 1 or 2 resident waves of blocks, 0 = one block per 256 sites).
+   fg_tune times the candidates on the context's own Nose-Poincare steps and
+   keeps the fastest; the state (u, p, strain, s, pi, H0) is restored after
+   it.  The result goes to the process's wisdom, which fg_create (solo) and
+   fg_batch_create (batch) apply to every later context of the same supercell,
+   precision and component count.  Plans change the order of the energies'
+   partial sums only: forces are the same bit for bit. */
+int  fg_tune(fg_ctx* ctx, int steps, int* zcw, int* waves, double* ms_per_step);
+/* Times the plans of each supercell of the batch as whole batch steps
+   (replicas of one supercell share a plan) and keeps the fastest; states
+   restored.  ms_before / ms_after: ms per batch step (may be NULL). */
+int  fg_batch_tune(fg_batch* b, int steps, double* ms_before, double* ms_after);
+/* A plan set by hand (zcw 0: the widest that fits). */
+int  fg_set_plan(fg_ctx* ctx, int zcw, int waves);
+/* The tile width in use, the waves setting and the two main grids. */
+int  fg_get_plan(const fg_ctx* ctx, int* zcw, int* waves, int* grid_kd, int* grid_asc);
+/* Wisdom as text: "feram_b200 wisdom 1", then one line per plan
+   "<solo|batch> <fp64|mixed> Lx Ly Lz components zcw waves".  Export sets
+   *needed (bytes with the NUL) and copies when len is large enough (buf may be
+   NULL to ask the size); import adds the plans (all or, on a malformed line,
+   none: FG_ERR_ARG). */
+int  fg_wisdom_export(char* buf, int len, int* needed);
+int  fg_wisdom_import(const char* text, int* n_plans);
+void fg_wisdom_forget(void);
+/* Apply the wisdom to a context / the replicas of a batch created before the
+   import. */
+int  fg_apply_wisdom(fg_ctx* ctx);
+int  fg_batch_apply_wisdom(fg_batch* b);
+
 /* ---- measurement ----------------------------------------------------------
    CUDA-event timing on the context's own stream (no host work in between). */
 #define FG_NPROF 5

@@ -53,3 +53,44 @@ def test_profile_names_match_header_count(fg):
     names = [L.fg_profile_name(i).decode() for i in range(n + 1)]
     assert all(names[:n]) and names[n] == ""
     assert names[0].startswith("k_kick_drift") and names[-2].startswith("k_assemble")
+
+
+def test_sample_constants_match_header(fg):
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "feram_gpu.h")).read()
+    assert int(hdr.split("#define FG_SAMPLE_COLS")[1].split()[0]) == A.FG_SAMPLE_COLS
+    assert int(hdr.split("#define FG_SAMPLE_CAP")[1].split()[0]) == A.FG_SAMPLE_CAP
+
+
+def test_wisdom_round_trip_needs_no_device(fg):
+    """fg_wisdom_import / fg_wisdom_export: the text form round-trips, later
+    plans replace earlier ones of the same key, and a malformed line imports
+    nothing (as fftw_import_wisdom_from_filename fails as a whole)."""
+    fg.wisdom_forget()
+    try:
+        assert fg.wisdom_export() == "feram_b200 wisdom 1\n"
+        text = ("feram_b200 wisdom 1\n# a comment\nsolo mixed 128 128 128 9 8 1\n"
+                "batch fp64 16 16 16 12 2 0\nbatch mixed 24 24 24 9 4 2\n")
+        assert fg.wisdom_import(text) == 3
+        out = fg.wisdom_export()
+        lines = out.splitlines()
+        assert lines[0] == "feram_b200 wisdom 1" and len(lines) == 4
+        assert sorted(lines[1:]) == sorted(["solo mixed 128 128 128 9 8 1", "batch fp64 16 16 16 12 2 0",
+                                            "batch mixed 24 24 24 9 4 2"])
+        assert fg.wisdom_import("feram_b200 wisdom 1\nsolo mixed 128 128 128 9 4 0\n") == 1
+        assert "solo mixed 128 128 128 9 4 0" in fg.wisdom_export().splitlines()
+        before = fg.wisdom_export()
+        for bad in ("solo mixed 8 8 8 9 4 1\n",                                   # no header
+                    "feram_b200 wisdom 1\nsolo mixed 8 8 8 9 4\n",                # short line
+                    "feram_b200 wisdom 1\nsolo half 8 8 8 9 4 1\n",               # unknown precision
+                    "feram_b200 wisdom 1\nsolo mixed 8 8 8 9 -1 1\n",             # negative width
+                    "feram_b200 wisdom 1\nsolo mixed 8 8 8 9 4 1\nsolo mixed 8 8 8 9 4 1 7\n"):
+            with pytest.raises(fg.FeramError):
+                fg.wisdom_import(bad)
+        assert fg.wisdom_export() == before
+        n = C.c_int()
+        assert A.lib().fg_wisdom_export(None, 0, C.byref(n)) == 0 and n.value == len(before) + 1
+        small = C.create_string_buffer(4)
+        assert A.lib().fg_wisdom_export(small, 4, C.byref(n)) == A.FG_ERR_ARG
+    finally:
+        fg.wisdom_forget()
