@@ -336,34 +336,119 @@ def _point_obs(rows, N):
     return {"V": rows[:, 6] / N, "KE": rows[:, 7] / N, "|u|": a, "u2": a * a}
 
 
-def cooling_sweep(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None, log=None):
-    """The batched cooling sweep: n_rep points (supercell 16^3..64^3 by
-    i mod 5, T = 450 - 5 (i mod 71) K), n_therm + n_avg steps each, mixed.
+def _ensemble_z(means_a, means_b):
+    """z of the difference of two ensemble means (independent replicas)."""
+    a, b = np.asarray(means_a), np.asarray(means_b)
+    se = np.sqrt(a.var(ddof=1) / len(a) + b.var(ddof=1) / len(b))
+    return float((a.mean() - b.mean()) / max(se, 1e-300)), float(a.mean()), float(b.mean()), float(se)
 
-    plain: the reference's sweep, one supercell after another, its points in
-      descending T, each started from the previous point's final state
-      (fg_run_point; cooling.sh:64-69), default plans.
-    batched: every point at once as one replica batch (fg_batch_run_point,
-      plans from fg_batch_tune), each replica from initialize_dipoR's start;
-      with warm_layers also from the warm-start network's proposal.
-    Agreement: per point, V/N, KE/N, |u_bar| and |u_bar|^2 over the n_avg
-    steps (10 block means) against the plain sweep's point, z = difference /
-    combined standard error.  Wall clock around synchronous calls."""
+
+def sweep_replicas(n_rep):
+    """The 96 replicas of the batched sweep: supercell 16^3..64^3 by i mod 5,
+    uni64 seeds (123456789 + i, 987654321)."""
+    sizes = [16, 24, 32, 48, 64]
+    Ls = [sizes[i % len(sizes)] for i in range(n_rep)]
+    seeds = [(123456789 + i, 987654321) for i in range(n_rep)]
+    return sizes, Ls, seeds
+
+
+def chained_sweep(n_rep=96, n_points=4, n_therm=1000, n_avg=1000, every=10, log=None):
+    """The batched cooling sweep as the reference runs a sweep: every replica
+    cools from 450 K in 5 K steps, each point n_therm + n_avg steps started
+    from the previous point's final state (cooling.sh:64-69, fg_chain_point
+    on the device), mixed precision.
+
+    plain: one replica after another (fg_run_point), default plans.
+    batched: all replicas at once, one fg_batch_run_point per temperature
+      (grouped launches, plans from fg_batch_tune).
+    Agreement: per supercell size and point, the ensemble mean over the
+    replicas of that size (independent seeds) of V/N, KE/N, |u_bar| and
+    |u_bar|^2, each replica's value its mean over the n_avg steps; z = the
+    difference over the ensembles' combined standard error.  Wall clock
+    around synchronous calls; set-up (tables, initial state) outside."""
+    import feram_b200 as fb
+    from feram_b200 import _capi as A
+    say = log or (lambda *a: None)
+    sizes, Ls, seeds = sweep_replicas(n_rep)
+    Ts = [450.0 - 5.0 * k for k in range(n_points)]
+    ps = [make_params(Ls[i], kelvin=Ts[0], Ez=0.0, seed=seeds[i]) for i in range(n_rep)]
+    sites = sum(p.N for p in ps)
+    out = {"replicas": n_rep, "sizes": sizes, "kelvin": Ts, "points": n_points, "sites": sites,
+           "n_therm": n_therm, "n_avg": n_avg, "sample_every": every, "precision": "mixed", "unit": UNIT,
+           "site_steps": sites * n_points * (n_therm + n_avg),
+           "timing": "wall clock around synchronous calls; set-up (tables, initial state) outside"}
+    plain = [[None] * n_points for _ in range(n_rep)]
+    t_plain = 0.0
+    for i in range(n_rep):
+        with fb.Context(ps[i], A.FG_PREC_MIXED) as ctx:
+            ctx.build_tables()
+            u, q = initial_state(ps[i])
+            prepare(ctx, ps[i], u, q)
+            t0 = time.perf_counter()
+            for k in range(n_points):
+                ctx.run_point(Ts[k], n_therm, n_avg, every)
+                plain[i][k] = ctx.samples()
+            t_plain += time.perf_counter() - t0
+    say(f"chained sweep: plain sequential {t_plain:.1f} s")
+    batched = [[None] * n_points for _ in range(n_rep)]
+    with fb.Batch(ps, A.FG_PREC_MIXED) as b:
+        for i, r in enumerate(b.replicas):
+            r.build_tables()
+            u, q = initial_state(ps[i])
+            prepare(r, ps[i], u, q)
+        t0 = time.perf_counter()
+        tb = b.tune(steps=8)
+        t_tune = time.perf_counter() - t0
+        plans = sorted({(ps[i].Lx,) + b.replicas[i].plan[:2] for i in range(n_rep)})
+        t0 = time.perf_counter()
+        for k in range(n_points):
+            b.run_point([Ts[k]] * n_rep, n_therm, n_avg, every)
+            for i, rows in enumerate(b.samples()):
+                batched[i][k] = rows
+        t_batch = time.perf_counter() - t0
+        groups = b.groups
+    say(f"chained sweep: batched {t_batch:.1f} s")
+    zs, table = [], []
+    for L in sizes:
+        idx = [i for i in range(n_rep) if Ls[i] == L]
+        for k in range(n_points):
+            for obs in ("V", "KE", "|u|", "u2"):
+                ma = [_point_obs(batched[i][k], ps[i].N)[obs].mean() for i in idx]
+                mb = [_point_obs(plain[i][k], ps[i].N)[obs].mean() for i in idx]
+                z, a_, b_, se = _ensemble_z(ma, mb)
+                zs.append(z)
+                table.append([L, Ts[k], obs, round(z, 3), a_, b_, se])
+    zs = np.abs(np.array(zs))
+    out.update({"plain_seconds": t_plain, "plain_value": out["site_steps"] / t_plain,
+                "batched_seconds": t_batch, "batched_value": out["site_steps"] / t_batch,
+                "speedup": t_plain / t_batch, "tune_seconds": t_tune, "tune_ms_per_batch_step": list(tb),
+                "plans": plans, "graph_branches": groups,
+                "agreement": {"comparisons": int(len(zs)), "within_3sigma": int(np.sum(zs <= 3.0)),
+                              "max_abs_z": float(zs.max()), "chi2_per_comparison": float(np.mean(zs ** 2)),
+                              "rows": table if n_points <= 8 else sorted(table, key=lambda r: -abs(r[3]))[:40]}})
+    return out
+
+
+def parallel_points(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None, log=None):
+    """The points of the sweep run at once instead of one after another: n_rep
+    points (supercell by i mod 5, T = 450 - 5 (i mod 71) K), each started
+    from initialize_dipoR's state (cold) or, with warm_layers, from the
+    warm-start network's proposal, n_therm + n_avg steps in one
+    fg_batch_run_point; against the chained sequential sweep through the same
+    points (per supercell, descending T, fg_run_point).  Agreement per point:
+    V/N, KE/N, |u_bar|, |u_bar|^2 over the n_avg steps (10 block means),
+    z = difference / combined standard error."""
     import feram_b200 as fb
     from feram_b200 import _capi as A
     from feram_b200 import warm_start as W
     say = log or (lambda *a: None)
-    sizes = [16, 24, 32, 48, 64]
-    Ls = [sizes[i % len(sizes)] for i in range(n_rep)]
+    sizes, Ls, seeds = sweep_replicas(n_rep)
     Ts = [450.0 - 5.0 * (i % 71) for i in range(n_rep)]
-    seeds = [(123456789 + i, 987654321) for i in range(n_rep)]
     ps = [make_params(Ls[i], kelvin=Ts[i], Ez=0.0, seed=seeds[i]) for i in range(n_rep)]
     sites = sum(p.N for p in ps)
     out = {"replicas": n_rep, "sizes": sizes, "kelvin": [450.0, 100.0, -5.0], "sites": sites, "n_therm": n_therm,
            "n_avg": n_avg, "sample_every": every, "precision": "mixed", "unit": UNIT,
            "timing": "wall clock around synchronous calls; set-up (tables, initial state) outside"}
-
-    # plain sequential sweep: per size, its points in descending T, chained
     plain = {}
     t_plain = 0.0
     for L in sizes:
@@ -379,8 +464,7 @@ def cooling_sweep(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None
                 plain[i] = ctx.samples()
             t_plain += time.perf_counter() - t0
     out["plain_seconds"] = t_plain
-    out["plain_value"] = sites * (n_therm + n_avg) / t_plain
-    say(f"sweep: plain sequential {t_plain:.1f} s")
+    say(f"parallel points: chained sequential {t_plain:.1f} s")
 
     def batched_arm(starts, tag):
         with fb.Batch(ps, A.FG_PREC_MIXED) as b:
@@ -388,14 +472,10 @@ def cooling_sweep(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None
                 r.build_tables()
                 u, q = starts(i)
                 prepare(r, ps[i], u, q)
-            t0 = time.perf_counter()
-            tb = b.tune(steps=8)
-            t_tune = time.perf_counter() - t0
-            plans = sorted({(ps[i].Lx,) + b.replicas[i].plan[:2] for i in range(n_rep)})
+            b.tune(steps=8)
             t0 = time.perf_counter()
             b.run_point(Ts, n_therm, n_avg, every)
             t_run = time.perf_counter() - t0
-            groups = b.groups
             rows = b.samples()
         zs = {k: [] for k in ("V", "KE", "|u|", "u2")}
         worst = []
@@ -408,15 +488,14 @@ def cooling_sweep(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None
                 zs[k].append(z)
                 if abs(z) > 3.0:
                     worst.append([Ls[i], Ts[i], k, round(float(z), 2), ma, mb])
-        agree = {k: {"within_3sigma": int(np.sum(np.abs(v) <= 3.0)), "max_abs_z": float(np.max(np.abs(v))),
-                     "chi2_per_point": float(np.mean(np.square(v)))} for k, v in zs.items()}
-        say(f"sweep: batched ({tag}) {t_run:.1f} s, tune {t_tune:.1f} s")
+        agree = {k: {"within_3sigma": int(np.sum(np.abs(v) <= 3.0)), "max_abs_z": float(np.max(np.abs(v)))}
+                 for k, v in zs.items()}
+        say(f"parallel points: batched ({tag}) {t_run:.1f} s")
         worst.sort(key=lambda w: -abs(w[3]))
-        return {"seconds": t_run, "tune_seconds": t_tune, "tune_ms_per_batch_step": list(tb), "plans": plans,
-                "graph_branches": groups, "value": sites * (n_therm + n_avg) / t_run, "speedup_vs_plain": t_plain / t_run,
-                "agreement": agree, "outside_3sigma": worst[:20]}
+        return {"seconds": t_run, "speedup_vs_chained_sequential": t_plain / t_run, "agreement": agree,
+                "outside_3sigma": worst[:12]}
 
-    out["batched_cold"] = batched_arm(lambda i: initial_state(ps[i]), "cold")
+    out["cold"] = batched_arm(lambda i: initial_state(ps[i]), "cold")
     if warm_layers is not None:
         fields = {}
         t0 = time.perf_counter()
@@ -429,9 +508,8 @@ def cooling_sweep(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None
                 net.forward(cond, [1000 + i for i in idx])
                 for k, i in enumerate(idx):
                     fields[i] = (net.field(k, ps[i]), W.maxwell_momenta(ps[i], 2000 + i))
-        t_inf = time.perf_counter() - t0
-        out["batched_warm"] = batched_arm(lambda i: fields[i], "warm")
-        out["batched_warm"]["inference_seconds"] = t_inf
+        out["warm"] = batched_arm(lambda i: fields[i], "warm")
+        out["warm"]["inference_seconds"] = time.perf_counter() - t0
     return out
 
 
@@ -622,6 +700,10 @@ def main():
     ap.add_argument("--size", type=int, default=L_DEFAULT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 96-replica batched sweep measurement")
+    ap.add_argument("--sweep-points", type=int, default=4,
+                    help="temperatures of the chained batched sweep from 450 K down in 5 K steps (71: to 100 K)")
+    ap.add_argument("--sweep-only", action="store_true",
+                    help="run the chained batched sweep alone and print its JSON object")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the FFT-vs-cuFFT, thin-film hysteresis and warm-start legs")
     ap.add_argument("--mixed-only", action="store_true",
@@ -630,6 +712,10 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.sweep_only:
+        out = chained_sweep(n_points=args.sweep_points, log=lambda m: print(m, file=sys.stderr, flush=True))
+        print(json.dumps({"cooling_sweep": out}), flush=True)
+        return 0
 
     import torch
     import torch.distributed as dist
@@ -774,10 +860,11 @@ def main():
         fftc = fft_vs_cufft(L)
         epit = epit_hysteresis()
         wstart = warm_start_leg(log=lambda m: print(m, file=sys.stderr, flush=True))
-    sweep = None
+    sweep = points = None
+    say = lambda m: print(m, file=sys.stderr, flush=True)
     if rank == 0 and world == 1 and not args.no_batched and not args.mixed_only:
-        sweep = cooling_sweep(warm_layers=wstart.pop("_layers", None) if wstart else None,
-                              log=lambda m: print(m, file=sys.stderr, flush=True))
+        sweep = chained_sweep(n_points=args.sweep_points, log=say)
+        points = parallel_points(warm_layers=wstart.pop("_layers", None) if wstart else None, log=say)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(p)
@@ -797,6 +884,7 @@ def main():
         "roofline": roofline, "step_roofline": step_roofline, "kernels": per_kernel,
         "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "batched": batched,
         "fft_vs_cufft": fftc, "epit_hysteresis": epit, "warm_start": wstart, "cooling_sweep": sweep,
+        "parallel_points": points,
         "gpu_launches": A.FG_NPROF * args.steps,  # kernels per bulk NP step graph
     }
     ctxm.close()

@@ -24,7 +24,7 @@ from ._capi import (FG_PREC_FP64, FG_PREC_MIXED, FG_OK, FG_SAMPLE_COLS, fg_avera
 __all__ = ["Context", "FeramError", "read_param", "make_param", "params_from_text", "default_params",
            "FG_PREC_FP64", "FG_PREC_MIXED", "fg_energy", "fg_average", "fg_params",
            "real_field", "complex_field", "k_table", "physical", "lib", "Batch",
-           "wisdom_export", "wisdom_import", "wisdom_forget", "FG_SAMPLE_COLS"]
+           "wisdom_export", "wisdom_import", "wisdom_forget", "wisdom_measure", "FG_SAMPLE_COLS"]
 
 lib = _capi.lib
 
@@ -423,6 +423,16 @@ def wisdom_import(text: str) -> int:
 
 def wisdom_forget():
     lib().fg_wisdom_forget()
+
+
+def wisdom_measure(p, n_times: int = 32, precision: int = FG_PREC_MIXED) -> str:
+    """fg_wisdom_measure (feram_fftw_wisdom's role): tune the supercell of the
+    run parameters p; returns the wisdom text afterwards."""
+    eb = C.create_string_buffer(512)
+    rc = lib().fg_wisdom_measure(C.byref(p), n_times, precision, eb, 512)
+    if rc:
+        raise FeramError(rc, _err(eb))
+    return wisdom_export()
 
 
 def feram_run(path: str, precision: int = FG_PREC_FP64):

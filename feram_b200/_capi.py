@@ -171,6 +171,7 @@ def lib() -> C.CDLL:
         "fg_wisdom_export": (C.c_int, [C.c_char_p, C.c_int, P(C.c_int)]),
         "fg_wisdom_import": (C.c_int, [C.c_char_p, P(C.c_int)]),
         "fg_wisdom_forget": (None, []),
+        "fg_wisdom_measure": (C.c_int, [P(fg_params), C.c_int, C.c_int, C.c_char_p, C.c_int]),
         "fg_apply_wisdom": (C.c_int, [vp]),
         "fg_batch_apply_wisdom": (C.c_int, [vp]),
         "fg_ws_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(vp)]),
@@ -178,6 +179,7 @@ def lib() -> C.CDLL:
         "fg_ws_last_error": (C.c_char_p, [vp]),
         "fg_ws_forward": (C.c_int, [vp, fp, C.POINTER(C.c_ulonglong), fp]),
         "fg_ws_backward": (C.c_int, [vp, fp, C.POINTER(C.c_ulonglong), fp, fp, fp]),
+        "fg_ws_backward_du": (C.c_int, [vp, fp, C.POINTER(C.c_ulonglong), fp, fp, fp, fp]),
         "fg_ws_adam": (C.c_int, [vp, C.c_float]),
         "fg_ws_layer_shape": (C.c_int, [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "fg_ws_get_layer": (C.c_int, [vp, C.c_int, fp, fp, fp, fp]),

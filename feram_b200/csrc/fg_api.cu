@@ -2864,6 +2864,32 @@ void fg_wisdom_forget(void) {
   g_wisdom.clear();
 }
 
+// The plans of one supercell measured before the runs, as the reference's
+// feram_fftw_wisdom program measures FFTW plans for a supercell
+// (feram_fftw_wisdom.F): a context with the run's parameters p (made by
+// fg_make_param) and initialize_dipoR's seeded state, tuned over n_times
+// steps; the plan goes to the wisdom (fg_wisdom_export writes it).
+int fg_wisdom_measure(const fg_params* p, int n_times, int precision, char* errbuf, int errlen) {
+  auto msg = [&](const std::string& m) {
+    if (errbuf && errlen > 0) std::snprintf(errbuf, (size_t)errlen, "%s", m.c_str());
+  };
+  if (!p || n_times < 1) {
+    msg("fg_wisdom_measure: parameters and n_times >= 1 are required");
+    return FG_ERR_ARG;
+  }
+  fg_ctx* ctx = nullptr;
+  int rc = fg_create(p, precision, &ctx);
+  const size_t nfield = (size_t)3 * (2 * (p->Lx / 2 + 1)) * (p->Ly + p->padding_y) * p->Lz;
+  std::vector<double> u(nfield, 0.0), q(nfield, 0.0);
+  if (!rc) rc = fg_build_tables(ctx);
+  if (!rc && (rc = fg_init_dipoR_host(p, u.data(), q.data())) != FG_OK) msg("initialize_dipoR failed");
+  if (!rc) rc = fg_set_state(ctx, u.data(), q.data(), 1.0, 0.0, 0.0);
+  if (!rc) rc = fg_tune(ctx, n_times, nullptr, nullptr, nullptr);
+  if (rc && ctx && !ctx->err.empty()) msg(ctx->err);
+  fg_destroy(ctx);
+  return rc;
+}
+
 int fg_apply_wisdom(fg_ctx* ctx) {
   if (!ctx || !ctx->stream) return FG_ERR_ARG;
   return apply_wisdom(ctx, PLAN_SOLO);

@@ -105,23 +105,6 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
 
-// Exact float -> double widening on the integer pipe: the IEEE-754 binary32
-// fields moved into binary64 ones (exponent rebias 127 -> 1023, mantissa
-// shifted by 29 bits).  Zero and subnormal floats give a signed zero (a
-// subnormal float is below 1.2e-38, far under any value the fields hold);
-// infinities and NaNs stay infinities and NaNs.  Used where the conversion
-// unit is the busy pipe (the energy sums of the mixed path), since a widening
-// has no rounding to do.
-__device__ __forceinline__ double widen(float x) {
-  const unsigned b = __float_as_uint(x);
-  const unsigned e = (b >> 23) & 0xffu;
-  const unsigned long long sign = (unsigned long long)(b & 0x80000000u) << 32;
-  const unsigned long long frac = (unsigned long long)(b & 0x7fffffu) << 29;
-  const unsigned long long ex = e == 0u ? 0ull : (e == 0xffu ? 0x7ffull : (unsigned long long)(e + 896u)) << 52;
-  return __longlong_as_double((long long)(sign | (e == 0u ? 0ull : ex | frac)));
-}
-__device__ __forceinline__ double widen(double x) { return x; }
-
 // Device error record (bounds checks, non-finite reductions).  The library
 // is one translation unit, so this __device__ variable has one definition.
 struct DevError {

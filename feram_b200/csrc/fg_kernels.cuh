@@ -1039,10 +1039,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
   }
   const double Ninv = ph->Ninv;
   // Energy sums: the per-k products in T (FP32 in the mixed path, whose
-  // spectra are FP32), accumulated per thread in FP64 (the dipole terms) or
-  // over this thread's few k in T first (the strain terms, acc_t)
+  // spectra are FP32), accumulated per thread in FP64
   double acc[NQ_K] = {0, 0, 0, 0, 0};
-  T acc_t[3] = {(T)0, (T)0, (T)0};
   // constants of the loop, converted to T once per block (kcon, filled
   // before the z stages) and read from shared memory: reading them through
   // ph in the loop repeats the loads and FP64 -> FP32 conversions at every k
@@ -1130,8 +1128,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
       S[5] = sA[5] + sB[5] * tz.x;
       double qd[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) qd[q] = widen(qv[q]);
-      const double w1d = widen(w1);
+      for (int q = 0; q < 6; ++q) qd[q] = (double)qv[q];
+      const double w1d = (double)w1;
       const double es = w1d * (S[0] * qd[0] + S[1] * qd[1] + S[2] * qd[2] + 2.0 * (S[3] * qd[3] + S[4] * qd[4] + S[5] * qd[5]));
       acc[0] += es;
       if constexpr (ZSC) {
@@ -1159,8 +1157,8 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 #pragma unroll
         for (int q = 0; q < 6; ++q) D[q] = (T)(S[q] * Ninv);
       } else {
-        acc[1] += w1d * (widen(D[0]) * qd[0] + widen(D[1]) * qd[1] + widen(D[2]) * qd[2] +
-                         2.0 * (widen(D[3]) * qd[3] + widen(D[4]) * qd[4] + widen(D[5]) * qd[5]));
+        acc[1] += w1d * ((double)D[0] * qd[0] + (double)D[1] * qd[1] + (double)D[2] * qd[2] +
+                         2.0 * ((double)D[3] * qd[3] + (double)D[4] * qd[4] + (double)D[5] * qd[5]));
       }
     }
     cplx<T> F[3];
@@ -1222,9 +1220,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         ec += acou[a].x * cs[a].x + acou[a].y * cs[a].y;
         em += acou[a].x * ck[a].x + acou[a].y * ck[a].y;
       }
-      acc_t[0] += w2 * es;
-      acc_t[1] += w2 * ec;
-      acc_t[2] += w2 * em;
+      acc[2] += (double)(w2 * es);
+      acc[3] += (double)(w2 * ec);
+      acc[4] += (double)(w2 * em);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const cplx<T> v = mk<cplx<T>>(ck[a].x + cs[a].x + KA[a].x, ck[a].y + cs[a].y + KA[a].y);
@@ -1259,9 +1257,9 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
         ec += acou[a].x * cs[a].x + acou[a].y * cs[a].y;
         em += acou[a].x * ck[a].x + acou[a].y * ck[a].y;
       }
-      acc_t[0] -= w2 * (ec + em);
-      acc_t[1] += w2 * ec;
-      acc_t[2] += w2 * em;
+      acc[2] -= (double)(w2 * (ec + em));
+      acc[3] += (double)(w2 * ec);
+      acc[4] += (double)(w2 * em);
     }
     if (acouK_out) {
 #pragma unroll
@@ -1278,9 +1276,6 @@ __global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec,
 #pragma unroll
     for (int i = 0; i < 6; ++i) buf[(3 + i) * ZS + zs * CW + cw] = d[i];
   }
-  acc[2] += (double)acc_t[0];
-  acc[3] += (double)acc_t[1];
-  acc[4] += (double)acc_t[2];
   __syncthreads();
   if constexpr (LZC > 0) {
     ct_inverse_range<T, LZC, ct_nst(LZC) - 1, 0, kZThreads, BZ>(buf, tws_z);
@@ -1333,32 +1328,6 @@ __device__ __forceinline__ V16<T> ldv_first(const T* p, unsigned long long pol) 
 }
 template <typename T>
 __device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V16<T>*>(p) = a; }
-
-// Two consecutive sites of one component (8 bytes FP32, 16 bytes FP64): the
-// assembly's vector width, so that its FP64 site sums stay in registers.
-template <typename T>
-struct alignas(2 * sizeof(T)) V2 {
-  static constexpr int n = 2;
-  T v[2];
-};
-template <typename T>
-__device__ __forceinline__ V2<T> ldv2(const T* p) { return *reinterpret_cast<const V2<T>*>(p); }
-template <typename T>
-__device__ __forceinline__ V2<T> ldv2_first(const T* p, unsigned long long pol) {
-  V2<T> r;
-  if constexpr (sizeof(T) == 4) {
-    const float2 v = ld_first(reinterpret_cast<const float2*>(p), pol);
-    r.v[0] = v.x; r.v[1] = v.y;
-  } else if constexpr (FG_L2_HINT_FP64) {
-    const double2 v = ld_first(reinterpret_cast<const double2*>(p), pol);
-    r.v[0] = v.x; r.v[1] = v.y;
-  } else {
-    r = ldv2(p);
-  }
-  return r;
-}
-template <typename T>
-__device__ __forceinline__ void stv2(T* p, const V2<T>& a) { *reinterpret_cast<V2<T>*>(p) = a; }
 
 // Constants of the site force, in FP64 for both precisions: the mixed path
 // reads FP32 u, the FP32 dipole-dipole force and the FP32 eta, and sums the
@@ -1498,7 +1467,7 @@ __global__ void __launch_bounds__(256, 2)
   for (int i = 0; i < 6; ++i) dy.wh[i] = sc->w_hom[i];
   dy.E0 = sc->E[0]; dy.E1 = sc->E[1]; dy.E2 = sc->E[2];
   double acc[NQ_R] = {0.0, 0.0};
-  constexpr int NV = V2<T>::n;
+  constexpr int NV = V16<T>::n;
   const long long stride = (long long)gridDim.x * blockDim.x;
   const bool sites = site_species != nullptr || site_zstar != nullptr || site_E != nullptr ||
                      (CLOSE && (site_minv != nullptr || site_sump != nullptr));
@@ -1557,21 +1526,19 @@ __global__ void __launch_bounds__(256, 2)
   } else if (g.plane_r % NV == 0) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
-      const V2<T> ux = ldv2(u + i), uy = ldv2(u + ns + i), uz = ldv2(u + 2 * ns + i);
+      const V16<T> ux = ldv(u + i), uy = ldv(u + ns + i), uz = ldv(u + 2 * ns + i);
       // rw is consumed here: evict_first keeps u, p and F in L2
-      const V2<T> a0 = ldv2_first(rw + i, pol_rw), a1 = ldv2_first(rw + ns + i, pol_rw),
-                  a2 = ldv2_first(rw + 2 * ns + i, pol_rw);
-      V2<T> e[6];
+      const V16<T> a0 = ldv_first(rw + i, pol_rw), a1 = ldv_first(rw + ns + i, pol_rw),
+                   a2 = ldv_first(rw + 2 * ns + i, pol_rw);
+      V16<T> e[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) e[q] = ldv2_first(rw + (3 + q) * ns + i, pol_rw);
-      V2<T> o0, o1, o2, l0, l1, l2;
+      for (int q = 0; q < 6; ++q) e[q] = ldv_first(rw + (3 + q) * ns + i, pol_rw);
+      V16<T> o0, o1, o2, l0, l1, l2;
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
-        const double eta[6] = {widen(e[0].v[l]), widen(e[1].v[l]), widen(e[2].v[l]),
-                               widen(e[3].v[l]), widen(e[4].v[l]), widen(e[5].v[l])};
+        const double eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
         double d0, d1, d2;
-        assemble_site(k.pl, k, k.Zs, dy, widen(ux.v[l]), widen(uy.v[l]), widen(uz.v[l]), widen(a0.v[l]), widen(a1.v[l]),
-                      widen(a2.v[l]), eta, d0, d1, d2, acc);
+        assemble_site(k.pl, k, k.Zs, dy, ux.v[l], uy.v[l], uz.v[l], a0.v[l], a1.v[l], a2.v[l], eta, d0, d1, d2, acc);
         o0.v[l] = force_hi<T>(d0);
         o1.v[l] = force_hi<T>(d1);
         o2.v[l] = force_hi<T>(d2);
@@ -1579,17 +1546,17 @@ __global__ void __launch_bounds__(256, 2)
         l1.v[l] = force_lo<T>(d1, o1.v[l]);
         l2.v[l] = force_lo<T>(d2, o2.v[l]);
       }
-      stv2(F + i, o0);
-      stv2(F + ns + i, o1);
-      stv2(F + 2 * ns + i, o2);
+      stv(F + i, o0);
+      stv(F + ns + i, o1);
+      stv(F + 2 * ns + i, o2);
       if (Flo) {
-        stv2(Flo + i, l0);
-        stv2(Flo + ns + i, l1);
-        stv2(Flo + 2 * ns + i, l2);
+        stv(Flo + i, l0);
+        stv(Flo + ns + i, l1);
+        stv(Flo + 2 * ns + i, l2);
       }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
-        V2<T> q[3] = {ldv2(p + i), ldv2(p + ns + i), ldv2(p + 2 * ns + i)};
+        V16<T> q[3] = {ldv(p + i), ldv(p + ns + i), ldv(p + 2 * ns + i)};
         T pp = 0, pf = 0, ff = 0;
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
@@ -1603,7 +1570,7 @@ __global__ void __launch_bounds__(256, 2)
           }
         }
 #pragma unroll
-        for (int a = 0; a < 3; ++a) stv2(p + a * ns + i, q[a]);
+        for (int a = 0; a < 3; ++a) stv(p + a * ns + i, q[a]);
         if (layer_sump[z]) {
           const double mi = layer_minv[z];
           ke[0] += (double)pp * mi;

@@ -395,7 +395,7 @@ __global__ void k_ws_stats_finish(const double* __restrict__ part, int nblk, Geo
 // the chain rule through S(u) at every site.
 __global__ void k_ws_loss_grad(const float* __restrict__ pre, Geo g, const float* __restrict__ cond,
                                const float* __restrict__ coef, const float* __restrict__ mean, float inv_batch,
-                               float* __restrict__ gpre, bf16* __restrict__ gpre16) {
+                               const float* __restrict__ extra, float* __restrict__ gpre, bf16* __restrict__ gpre16) {
   const int total = g.B * g.nsite;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < total; s += gridDim.x * blockDim.x) {
     const int b = s / g.nsite;
@@ -416,6 +416,10 @@ __global__ void k_ws_loss_grad(const float* __restrict__ pre, Geo g, const float
           d += (dd == a ? cf[5] : cf[6]) * nsum;
         }
         gv = d * invN * kUScale * inv_batch;
+        // a gradient on u from outside the statistics (an energy term
+        // evaluated by the MD force: dL/du given per site), chained
+        // through u = kUScale * pre
+        if (extra) gv += extra[(size_t)s * 3 + a] * kUScale;
       }
       gpre[(size_t)s * 16 + a] = gv;
       gpre16[(size_t)s * 16 + a] = __float2bfloat16_rn(gv);
@@ -513,6 +517,7 @@ struct fg_ws {
   float* coef = nullptr;
   float* mean = nullptr;
   float* loss = nullptr;    // [B]
+  float* extra = nullptr;   // caller's dL/du [B][nsite][3] (fg_ws_backward_du), allocated on first use
   int* err = nullptr;
   cudaStream_t stream = nullptr;
   std::string msg;
@@ -579,10 +584,10 @@ int stats(fg_ws* n, bool with_target) {
 }
 
 // Backward through the four layers into each layer's dw, db (accumulated).
-int backward(fg_ws* n) {
+int backward(fg_ws* n, const float* extra) {
   const int tot = total_sites(n);
   ws::k_ws_loss_grad<<<(tot + 255) / 256, 256, 0, n->stream>>>(n->L[3].pre, n->g, n->cond, n->coef, n->mean,
-                                                                1.0f / n->g.B, n->gA, n->gA16);
+                                                                1.0f / n->g.B, extra, n->gA, n->gA16);
   WCK(cudaGetLastError());
   const int grid = tot / ws::kTile;
   const int KS = 2048;  // sites per weight-gradient CTA
@@ -706,7 +711,7 @@ void fg_ws_destroy(fg_ws* n) {
       if (p) cudaFree(p);
   for (void* p : {(void*)n->in16, (void*)n->gA, (void*)n->gB, (void*)n->gA16, (void*)n->gB16, (void*)n->cond,
                   (void*)n->seeds, (void*)n->part, (void*)n->S, (void*)n->target, (void*)n->wts, (void*)n->coef,
-                  (void*)n->mean, (void*)n->loss, (void*)n->err})
+                  (void*)n->mean, (void*)n->loss, (void*)n->extra, (void*)n->err})
     if (p) cudaFree(p);
   if (n->stream) cudaStreamDestroy(n->stream);
   delete n;
@@ -722,15 +727,20 @@ int fg_ws_forward(fg_ws* n, const float* cond, const unsigned long long* seeds, 
   return check_err(n);
 }
 
-int fg_ws_backward(fg_ws* n, const float* cond, const unsigned long long* seeds, const float* target,
-                   const float* weights, float* loss) {
+int fg_ws_backward_du(fg_ws* n, const float* cond, const unsigned long long* seeds, const float* target,
+                      const float* weights, const float* dLdu, float* loss) {
   if (!n || !cond || !seeds || !target || !weights) return FG_ERR_ARG;
   int rc;
   if ((rc = upload_inputs(n, cond, seeds))) return rc;
   WCK(cudaMemcpyAsync(n->target, target, sizeof(float) * ws::kNS * n->g.B, cudaMemcpyHostToDevice, n->stream));
   WCK(cudaMemcpyAsync(n->wts, weights, sizeof(float) * ws::kNS, cudaMemcpyHostToDevice, n->stream));
+  if (dLdu) {
+    const size_t ne = (size_t)total_sites(n) * 3;
+    if (!n->extra && (rc = walloc(n, &n->extra, ne))) return rc;
+    WCK(cudaMemcpyAsync(n->extra, dLdu, sizeof(float) * ne, cudaMemcpyHostToDevice, n->stream));
+  }
   zero_grads(n);
-  if ((rc = forward(n)) || (rc = stats(n, true)) || (rc = backward(n))) return rc;
+  if ((rc = forward(n)) || (rc = stats(n, true)) || (rc = backward(n, dLdu ? n->extra : nullptr))) return rc;
   if (loss) {
     std::vector<float> lb(n->g.B);
     WCK(cudaMemcpyAsync(lb.data(), n->loss, sizeof(float) * n->g.B, cudaMemcpyDeviceToHost, n->stream));
@@ -740,6 +750,11 @@ int fg_ws_backward(fg_ws* n, const float* cond, const unsigned long long* seeds,
     *loss = (float)(s / n->g.B);
   }
   return check_err(n);
+}
+
+int fg_ws_backward(fg_ws* n, const float* cond, const unsigned long long* seeds, const float* target,
+                   const float* weights, float* loss) {
+  return fg_ws_backward_du(n, cond, seeds, target, weights, nullptr, loss);
 }
 
 int fg_ws_adam(fg_ws* n, float lr) {

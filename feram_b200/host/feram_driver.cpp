@@ -204,6 +204,21 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
   if (rc) return rc;
   if ((rc = fg_make_param(&p, errbuf, errlen))) return rc;
   const std::string base = dir_of(path) + p.filename;
+  // saved launch plans next to the input, imported before the context is
+  // made, as feram_common.F:56-69 imports FFTW wisdom at start-up (a file
+  // that fails to parse is reported in the .log and the default plans hold)
+  std::string wisdom_msg = "GPU_WISDOM No gpu_wisdom next to the input: default launch plans.";
+  {
+    std::ifstream wf(dir_of(path) + "gpu_wisdom");
+    if (wf) {
+      std::stringstream ss;
+      ss << wf.rdbuf();
+      int n = 0;
+      wisdom_msg = fg_wisdom_import(ss.str().c_str(), &n) == FG_OK
+                       ? "GPU_WISDOM Successfully imported " + std::to_string(n) + " plans from gpu_wisdom."
+                       : "GPU_WISDOM Failed to import gpu_wisdom (malformed): default launch plans.";
+    }
+  }
   fg_ctx* ctx = nullptr;
   rc = fg_create(&p, precision, &ctx);
   auto bail = [&](int code) {
@@ -389,6 +404,7 @@ extern "C" int fg_feram_run(const char* path, int precision, fg_average* avg_out
     return std::string(p.filename) + step_fn;
   };
   std::ofstream log(base + ".log");
+  log << wisdom_msg << "\n";
   fg_average avg;
   std::memset(&avg, 0, sizeof(avg));
   const int n_steps = p.n_thermalize + p.n_average;

@@ -79,12 +79,19 @@ class WarmStartNet:
         self._check(A.lib().fg_ws_forward(self._h, cp, sd, S.ctypes.data_as(C.POINTER(C.c_float))))
         return S
 
-    def backward(self, cond, seeds, target, weights) -> float:
+    def backward(self, cond, seeds, target, weights, dLdu=None) -> float:
+        """Loss and gradients (fg_ws_backward); with dLdu [batch][N][3] a
+        further gradient on the generated u (fg_ws_backward_du)."""
         keep, cp, sd = self._inputs(cond, seeds)
         t, tp = self._f32(np.asarray(target).reshape(self.batch, NSTAT))
         w, wp = self._f32(weights)
         loss = C.c_float()
-        self._check(A.lib().fg_ws_backward(self._h, cp, sd, tp, wp, C.byref(loss)))
+        if dLdu is None:
+            self._check(A.lib().fg_ws_backward(self._h, cp, sd, tp, wp, C.byref(loss)))
+        else:
+            n = self.batch * self.L[0] * self.L[1] * self.L[2]
+            g, gp = self._f32(np.asarray(dLdu).reshape(n, 3))
+            self._check(A.lib().fg_ws_backward_du(self._h, cp, sd, tp, wp, gp, C.byref(loss)))
         return float(loss.value)
 
     def adam(self, lr: float):
@@ -170,10 +177,11 @@ def generate_training_set(make_params, chains, temps, n_therm=3000, n_snap=14, s
     in `chains`, each through `temps` (descending), every point started from
     the previous one on the device (fg_chain_point), thermalised n_therm
     steps, then n_snap snapshots snap_every steps apart.  All chains step
-    together as one replica batch.  Returns (cond [n][5], stats [n][7])."""
+    together as one replica batch.  Returns (cond [n][5], stats [n][7],
+    potential energy per site [n])."""
     import feram_b200 as fb
     ps = [make_params(temps[0], Ez, gpa) for Ez, gpa in chains]
-    conds, stats = [], []
+    conds, stats, energies = [], [], []
     with fb.Batch(ps, precision) as b:
         for i, (r, p) in enumerate(zip(b.replicas, ps)):
             r.build_tables()
@@ -187,26 +195,83 @@ def generate_training_set(make_params, chains, temps, n_therm=3000, n_snap=14, s
                     r.chain_point(T, [0.0, 0.0, Ez])
             b.step(n_therm)
             for _ in range(n_snap):
-                b.step(snap_every)
-                for r, (Ez, gpa) in zip(b.replicas, chains):
+                es = b.step(snap_every)
+                for r, e, (Ez, gpa) in zip(b.replicas, es, chains):
                     u = A.physical(r.get_state()["dipoR"], r.p)
                     conds.append([T, 0.0, 0.0, Ez, gpa])
                     stats.append(site_stats(u, [0.0, 0.0, Ez]))
-    return np.array(conds, dtype=np.float64), np.array(stats, dtype=np.float64)
+                    energies.append(potential(e) / r.p.N)
+    return (np.array(conds, dtype=np.float64), np.array(stats, dtype=np.float64),
+            np.array(energies, dtype=np.float64))
 
 
-def train(net: WarmStartNet, cond, stats, steps=1500, lr=2e-3, seed=0, log_every=0):
+class EnergyProbe:
+    """The potential energy per site of generated fields and its gradient,
+    from the MD's own force evaluation (mirror_force_mirror: V and dVddi =
+    dV/du): one mixed-precision context per pressure, its uniform field set
+    per sample.  make_params(L, T, E_z, GPa) as experiment takes it."""
+
+    def __init__(self, make_params, L):
+        self.make_params = make_params
+        self.L = L
+        self.ctx = {}
+
+    def _context(self, gpa):
+        import feram_b200 as fb
+        if gpa not in self.ctx:
+            p = self.make_params(self.L, 300.0, 0.0, gpa)
+            c = fb.Context(p, FG_PREC_MIXED)
+            c.build_tables()
+            self.ctx[gpa] = (c, p)
+        return self.ctx[gpa]
+
+    def __call__(self, net, cond):
+        """(V/N [batch], dV/du / N [batch][N][3]) of the last forward's fields."""
+        V, G = [], []
+        for b, c in enumerate(np.asarray(cond)):
+            ctx, p = self._context(float(c[4]))
+            ctx.set_state(net.field(b, p))
+            ctx.set_uniform_E([c[1], c[2], c[3]])
+            e = ctx.mirror_force_mirror()
+            V.append(potential(e) / p.N)
+            G.append(A.physical(ctx.get_state()["dVddi"], p).reshape(-1, 3) / p.N)
+        return np.array(V), np.array(G)
+
+    def close(self):
+        for c, _ in self.ctx.values():
+            c.close()
+        self.ctx = {}
+
+
+def train(net: WarmStartNet, cond, stats, steps=1500, lr=2e-3, seed=0, log_every=0, energies=None, probe=None,
+          energy_from=None):
     """Adam on the moment-matching loss, minibatches of net.batch training
     samples (random order, fresh noise seeds).  Weights: 1 / variance of
-    each statistic over the training set.  Returns the loss history."""
+    each statistic over the training set.  With energies (V/N of each
+    training configuration) and an EnergyProbe, the steps from energy_from
+    (default: half way) on add w_V (V/N - V_target)^2 per sample (w_V: 1 /
+    variance of V/N), whose gradient is the MD force of the generated field:
+    the statistics alone leave the fields smoother than thermal ones (their
+    potential energy too low).  Returns the loss history (statistics, plus
+    the energy term where it is on)."""
     rng = np.random.default_rng(seed)
     w = 1.0 / np.maximum(stats.var(axis=0), 1e-30)
+    use_e = energies is not None and probe is not None
+    wv = 1.0 / max(float(np.var(energies)), 1e-30) if use_e else 0.0
+    e_from = steps // 2 if energy_from is None else energy_from
     hist = []
     for it in range(steps):
         idx = rng.integers(0, len(cond), size=net.batch)
         seeds = rng.integers(1, 2 ** 62, size=net.batch)
         lr_t = lr * (0.1 ** (it / max(steps, 1)))  # exponential decay to lr / 10
-        loss = net.backward(cond[idx], seeds, stats[idx], w)
+        if use_e and it >= e_from:
+            net.forward(cond[idx], seeds)
+            V, G = probe(net, cond[idx])
+            d = V - energies[idx]
+            dLdu = (2.0 * wv / net.batch) * d[:, None, None] * G
+            loss = net.backward(cond[idx], seeds, stats[idx], w, dLdu) + wv * float(np.mean(d * d))
+        else:
+            loss = net.backward(cond[idx], seeds, stats[idx], w)
         net.adam(lr_t)
         hist.append(loss)
         if log_every and it % log_every == 0:
@@ -323,12 +388,14 @@ def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, t
 
 def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40, n_shuffled=20, seed=2024,
                n_therm=3000, n_snap=14, train_steps=4000, probe=3000, every=20, accept_after=1000, log=None,
-               keep_layers=False):
+               keep_layers=False, energy_from=3000):
     """The learned-warm-start protocol on one GPU.
 
     1. Data: MD cooling chains (train_chains of (E_z, GPa), train_temps
        descending) at L^3, snapshots -> (condition, statistics).
-    2. Training: Adam on the moment-matching loss.
+    2. Training: Adam on the moment-matching loss; from step energy_from
+       on (None: never) also on the potential energy per site, with the
+       MD force as its gradient (EnergyProbe).
     3. Held-out points (T in 100-450 K, E_z in +-0.001 V/A), off the
        training grid: n_held visited as a cooling sweep (T descending) and
        n_shuffled in random order (a scan whose previous point is unrelated).
@@ -351,14 +418,21 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
     if train_temps is None:
         train_temps = [450.0 - 25.0 * i for i in range(15)]
     out = {"L": L, "train_chains": len(train_chains), "train_temps": [train_temps[0], train_temps[-1], len(train_temps)]}
-    (cond, stats), t_data = timed(generate_training_set, lambda T, ez, gpa: make_params(L, T, ez, gpa),
+    (cond, stats, energies), t_data = timed(generate_training_set, lambda T, ez, gpa: make_params(L, T, ez, gpa),
                                   train_chains, train_temps, n_therm=n_therm, n_snap=n_snap)
     out["train_configs"] = len(cond)
     out["data_seconds"] = t_data
     say(f"warm start: {len(cond)} training configurations in {t_data:.1f} s")
     net = WarmStartNet((L, L, L), batch=8, seed=seed)
     try:
-        hist, t_train = timed(train, net, cond, stats, steps=train_steps, seed=seed)
+        probe_e = EnergyProbe(make_params, L) if energy_from is not None else None
+        try:
+            hist, t_train = timed(train, net, cond, stats, steps=train_steps, seed=seed, energies=energies,
+                                  probe=probe_e, energy_from=energy_from)
+        finally:
+            if probe_e is not None:
+                probe_e.close()
+        out["energy_matching_from_step"] = energy_from
         out.update({"train_steps": train_steps, "train_seconds": t_train,
                     "loss_first": float(np.mean(hist[:20])), "loss_last": float(np.mean(hist[-50:]))})
         say(f"warm start: trained {train_steps} steps in {t_train:.1f} s, loss {out['loss_first']:.3g} -> "

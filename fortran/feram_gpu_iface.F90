@@ -145,6 +145,49 @@ module feram_gpu_c
        type(c_ptr), value :: ctx
        integer(c_int), value :: on, i_step
      end function fg_set_wave
+     ! a sweep point (cooling.sh:64-69: n_thermalize + n_average steps from
+     ! the previous point's state) with a device sample row every `every`
+     ! averaging steps; rows of FG_SAMPLE_COLS = 16 doubles
+     integer(c_int) function fg_run_point(ctx, kelvin, E, n_therm, n_avg, every, e) &
+          & bind(C, name='fg_run_point')
+       import :: c_int, c_ptr, c_double, fg_energy
+       type(c_ptr), value :: ctx
+       real(c_double), value :: kelvin
+       real(c_double), intent(in) :: E(3)
+       integer(c_int), value :: n_therm, n_avg, every
+       type(fg_energy), intent(out) :: e
+     end function fg_run_point
+     integer(c_int) function fg_sample(ctx) bind(C, name='fg_sample')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+     end function fg_sample
+     integer(c_int) function fg_samples_read(ctx, rows, max_rows, n_rows) bind(C, name='fg_samples_read')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       real(c_double), intent(out) :: rows(16, *)
+       integer(c_int), value :: max_rows
+       integer(c_int), intent(out) :: n_rows
+     end function fg_samples_read
+     ! launch plans: the autotuner (FFTW_MEASURE's role, coord_module.F:155-377)
+     ! and its wisdom as text (feram_common.F:56-69, feram_fftw_wisdom.F)
+     integer(c_int) function fg_tune(ctx, steps, zcw, waves, ms) bind(C, name='fg_tune')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: ctx
+       integer(c_int), value :: steps
+       integer(c_int), intent(out) :: zcw, waves
+       real(c_double), intent(out) :: ms
+     end function fg_tune
+     integer(c_int) function fg_wisdom_import(text, n_plans) bind(C, name='fg_wisdom_import')
+       import :: c_int, c_char
+       character(kind=c_char), intent(in) :: text(*)
+       integer(c_int), intent(out) :: n_plans
+     end function fg_wisdom_import
+     integer(c_int) function fg_wisdom_export(buf, len, needed) bind(C, name='fg_wisdom_export')
+       import :: c_int, c_char
+       character(kind=c_char), intent(out) :: buf(*)
+       integer(c_int), value :: len
+       integer(c_int), intent(out) :: needed
+     end function fg_wisdom_export
   end interface
 end module feram_gpu_c
 

@@ -421,6 +421,12 @@ int  fg_get_plan(const fg_ctx* ctx, int* zcw, int* waves, int* grid_kd, int* gri
 int  fg_wisdom_export(char* buf, int len, int* needed);
 int  fg_wisdom_import(const char* text, int* n_plans);
 void fg_wisdom_forget(void);
+/* feram_fftw_wisdom's measurement for one supercell before the runs: a
+   context with the run's parameters p (after fg_make_param) and
+   initialize_dipoR's seeded state, fg_tune over n_times steps; the plan goes
+   to the wisdom.  fg_feram_run imports a file "gpu_wisdom" next to the
+   .feram input, if there is one, before it creates the context. */
+int  fg_wisdom_measure(const fg_params* p, int n_times, int precision, char* errbuf, int errlen);
 /* Apply the wisdom to a context / the replicas of a batch created before the
    import. */
 int  fg_apply_wisdom(fg_ctx* ctx);
@@ -475,6 +481,12 @@ int  fg_ws_forward(fg_ws* n, const float* cond, const unsigned long long* seeds,
    and its gradients into each layer's dW, db (fg_ws_get_layer). */
 int  fg_ws_backward(fg_ws* n, const float* cond, const unsigned long long* seeds, const float* target,
                     const float* weights, float* loss);
+/* The same with a further gradient dL/du [batch][Lx Ly Lz][3] (sites x
+   fastest) from a loss term outside the statistics, e.g. the potential
+   energy of each generated field, whose gradient is the MD force dVddi
+   (the loss value then covers the statistics only). */
+int  fg_ws_backward_du(fg_ws* n, const float* cond, const unsigned long long* seeds, const float* target,
+                       const float* weights, const float* dLdu, float* loss);
 /* One Adam step (Kingma & Ba) with the gradients of the last fg_ws_backward. */
 int  fg_ws_adam(fg_ws* n, float lr);
 /* Layer l (0..3): [cout][27][cin] weights (tap t = 9 (dz+1) + 3 (dy+1) +

@@ -108,7 +108,7 @@ def test_tune_restores_the_state_and_feeds_wisdom(fg, prec):
     text = fb.wisdom_export()
     mode_prec = "solo " + ("mixed" if prec == A.FG_PREC_MIXED else "fp64")
     assert any(line.startswith(mode_prec + " 16 16 16 9 ") for line in text.splitlines()), text
-    assert e0.total != 0.0
+    assert e0.short_range != 0.0
 
 
 @pytest.mark.parametrize("prec", [A.FG_PREC_FP64, A.FG_PREC_MIXED])
@@ -222,3 +222,28 @@ def test_sample_series_overflow_is_an_error(fg):
         assert "overflow" in str(ei.value)
         ctx.run_point(300.0, 0, 40, 2)
         assert ctx.samples().shape == (20, A.FG_SAMPLE_COLS)
+
+
+def test_wisdom_measure_and_the_driver_reads_gpu_wisdom(fg, tmp_path):
+    """fg_wisdom_measure tunes a supercell as feram_fftw_wisdom measures FFTW
+    plans; fg_feram_run imports a gpu_wisdom file beside its input before it
+    makes the context (feram_common.F:56-69) and says so in the .log; a
+    malformed file leaves the default plans and is reported."""
+    text = fb.wisdom_measure(helpers.params(L="8 8 8"), 8, A.FG_PREC_FP64)
+    lines = [ln for ln in text.splitlines() if ln.startswith("solo fp64 8 8 8 ")]
+    assert len(lines) == 1, text
+    fb.wisdom_forget()
+    deck = helpers.deck(L="8 8 8", n_thermalize="4", n_average="4")
+    (tmp_path / "run.feram").write_text(deck)
+    (tmp_path / "gpu_wisdom").write_text(text)
+    avg_w, _ = fg.feram_run(str(tmp_path / "run.feram"), A.FG_PREC_FP64)
+    log = (tmp_path / "run.log").read_text().splitlines()
+    assert log[0].startswith("GPU_WISDOM Successfully imported"), log[0]
+    assert any(ln.startswith("solo fp64 8 8 8 ") for ln in fb.wisdom_export().splitlines())
+    fb.wisdom_forget()
+    (tmp_path / "gpu_wisdom").write_text("not wisdom\n")
+    avg_d, _ = fg.feram_run(str(tmp_path / "run.feram"), A.FG_PREC_FP64)
+    assert (tmp_path / "run.log").read_text().splitlines()[0].startswith("GPU_WISDOM Failed")
+    assert avg_w.n_steps == avg_d.n_steps
+    # the plan changes the order of the energy sums only
+    assert abs(avg_w.energy.total - avg_d.energy.total) <= 1e-10 * abs(avg_d.energy.total)

@@ -43,7 +43,7 @@ def _torch_stats(u, e):
                         (u ** 4).sum(1).mean(dim=(1, 2, 3)), cl, ct], dim=1)
 
 
-def _reference(layers, B, L, x, cond, target, wts):
+def _reference(layers, B, L, x, cond, target, wts, extra=None):
     Lx, Ly, Lz = L
     h = torch.tensor(x).reshape(B, Lz, Ly, Lx, 16).permute(0, 4, 1, 2, 3).contiguous()
     params = []
@@ -61,12 +61,19 @@ def _reference(layers, B, L, x, cond, target, wts):
     e = torch.tensor(np.asarray(cond)[:, 1:4] / 0.001, dtype=torch.float32)
     S = _torch_stats(u, e)
     loss = ((S - torch.tensor(target, dtype=torch.float32)) ** 2 * torch.tensor(wts, dtype=torch.float32)).sum(1).mean()
-    loss.backward()
+    total = loss
+    if extra is not None:  # a loss term outside the statistics with dL/du = extra
+        Lx, Ly, Lz = L
+        ex = torch.tensor(extra, dtype=torch.float32).reshape(B, Lz, Ly, Lx, 3).permute(0, 4, 1, 2, 3)
+        total = loss + (u * ex).sum()
+    total.backward()
     return u, S, loss, params
 
 
-@pytest.mark.parametrize("L,batch", [((8, 8, 8), 2), ((12, 8, 4), 1)])
-def test_network_forward_and_gradients_match_torch(fg, L, batch):
+@pytest.mark.parametrize("L,batch,extra", [((8, 8, 8), 2, False), ((12, 8, 4), 1, False), ((8, 8, 8), 2, True)])
+def test_network_forward_and_gradients_match_torch(fg, L, batch, extra):
+    """With extra: a further dL/du on the generated field (fg_ws_backward_du,
+    the energy term's MD force in training)."""
     with W.WarmStartNet(L, batch=batch, seed=7) as net:
         rng = np.random.default_rng(3)
         for l in range(4):  # non-zero biases exercise the bias paths
@@ -76,12 +83,15 @@ def test_network_forward_and_gradients_match_torch(fg, L, batch):
         seeds = [11 + i for i in range(batch)]
         target = rng.standard_normal((batch, W.NSTAT)) * 0.01
         wts = np.abs(rng.standard_normal(W.NSTAT)) + 0.5
-        loss_dev = net.backward(cond, seeds, target, wts)
+        nsite = L[0] * L[1] * L[2]
+        dLdu = rng.standard_normal((batch, nsite, 3)).astype(np.float32) * 1e-3 if extra else None
+        loss_dev = net.backward(cond, seeds, target, wts, dLdu)
         x, u_dev = net.io()
         S_dev = net.forward(cond, seeds)
         lay = [net.layer(l) for l in range(4)]
     grads = [(dw, db) for _, _, dw, db in lay]
-    u_ref, S_ref, loss_ref, params = _reference([(w, b) for w, b, _, _ in lay], batch, L, x, cond, target, wts)
+    u_ref, S_ref, loss_ref, params = _reference([(w, b) for w, b, _, _ in lay], batch, L, x, cond, target, wts,
+                                                dLdu)
     Lx, Ly, Lz = L
     u_ref = u_ref.detach().permute(0, 2, 3, 4, 1).reshape(-1, 3).numpy()
     assert np.abs(u_dev - u_ref).max() <= 1e-3 * np.abs(u_ref).max(), np.abs(u_dev - u_ref).max()
