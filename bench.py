@@ -429,12 +429,13 @@ def chained_sweep(n_rep=96, n_points=4, n_therm=1000, n_avg=1000, every=10, log=
     return out
 
 
-def parallel_points(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None, log=None):
+def parallel_points(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=None, n_vs=200, log=None):
     """The points of the sweep run at once instead of one after another: n_rep
     points (supercell by i mod 5, T = 450 - 5 (i mod 71) K), each started
     from initialize_dipoR's state (cold) or, with warm_layers, from the
-    warm-start network's proposal, n_therm + n_avg steps in one
-    fg_batch_run_point; against the chained sequential sweep through the same
+    warm-start network's proposal, settled by n_vs velocity-scaling steps
+    (as warm_start.settle; timed with the run), then n_therm + n_avg steps in
+    one fg_batch_run_point; against the chained sequential sweep through the same
     points (per supercell, descending T, fg_run_point).  Agreement per point:
     V/N, KE/N, |u_bar|, |u_bar|^2 over the n_avg steps (10 block means),
     z = difference / combined standard error."""
@@ -474,6 +475,10 @@ def parallel_points(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=No
                 prepare(r, ps[i], u, q)
             b.tune(steps=8)
             t0 = time.perf_counter()
+            e = fb.fg_energy()
+            for r in b.replicas:
+                for _ in range(n_vs):
+                    r.velocity_scaling(e)
             b.run_point(Ts, n_therm, n_avg, every)
             t_run = time.perf_counter() - t0
             rows = b.samples()
@@ -492,7 +497,8 @@ def parallel_points(n_rep=96, n_therm=1000, n_avg=1000, every=10, warm_layers=No
                  for k, v in zs.items()}
         say(f"parallel points: batched ({tag}) {t_run:.1f} s")
         worst.sort(key=lambda w: -abs(w[3]))
-        return {"seconds": t_run, "speedup_vs_chained_sequential": t_plain / t_run, "agreement": agree,
+        return {"seconds": t_run, "settle_vs_steps": n_vs, "speedup_vs_chained_sequential": t_plain / t_run,
+                "agreement": agree,
                 "outside_3sigma": worst[:12]}
 
     out["cold"] = batched_arm(lambda i: initial_state(ps[i]), "cold")

@@ -273,6 +273,7 @@ void with_z_kspace(int Lz, int cw, bool acou, bool zsite, F f) {
     else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C, true>);
     else f(k_z_kspace<T, 0, 0, true>);
   } else if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C>);
+  else if (sizeof(T) == 4 && cw == 4 && Lz == 128) f(k_z_kspace<T, 128, 4>);
   else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C>);
   else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C>);
   else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C>);

@@ -940,12 +940,17 @@ __global__ void __launch_bounds__(256) k_z_pass(cplx<T>* __restrict__ spec, Geom
 // LZC, CWC > 0 select the compile-time z transforms (launched with exactly
 // kZThreads threads); 0 = runtime plan and tile width.
 constexpr int kZThreads = 256;
+// Resident CTAs per SM the z kernel is compiled for: FP32 tiles of 4 kx
+// columns (37 KB at Lz = 128) leave room for three CTAs, whose 85-register
+// budget the compiler then meets; wider tiles fit two.
+template <typename T>
+constexpr int kZMinBlocks(int cwc) { return (sizeof(T) == 4 && cwc == 4) ? 3 : 2; }
 // Component padding of the compile-time z tile, in complex values (64 bytes).
 template <typename T>
 constexpr int kZPad = 64 / (int)sizeof(cplx<T>);
 
 template <typename T, int LZC = 0, int CWC = 0, bool ACOU = false, bool ZSC = false>
-__global__ void __launch_bounds__(256, 2) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
+__global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* __restrict__ spec, const T* __restrict__ dtab,
                                                      const cplx<T>* __restrict__ ckmod, cplx<T>* __restrict__ acouK_out,
                                                      Geom g, FftPlan pz, const cplx<T>* __restrict__ twz, KMaps km,
                                                      const Phys* __restrict__ ph, double* __restrict__ part,

@@ -315,17 +315,42 @@ def block_stats(P2, V, block: int = 5):
     return (float(bp.mean()), float(bp.std(ddof=1)), float(bv.mean()), float(bv.std(ddof=1)))
 
 
+def accept(Pw, Vw, Pe, Ve, k: float = 4.0, block: int = 5) -> bool:
+    """The MD as the judge of a warm start: the warm run's block-averaged
+    |<u>|^2 and potential energy against the plain run's equilibrium, each
+    within k standard errors of their difference (block means of `block`
+    samples); a rejected warm start keeps the chained fallback."""
+    a, e = block_stats(Pw, Vw, block), block_stats(Pe, Ve, block)
+    na, ne = len(Pw) // block, len(Pe) // block
+    return bool(abs(a[0] - e[0]) <= k * np.hypot(a[1] / np.sqrt(na), e[1] / np.sqrt(ne)) + 1e-12 and
+                abs(a[2] - e[2]) <= k * np.hypot(a[3] / np.sqrt(na), e[3] / np.sqrt(ne)) + 1e-12)
+
+
 def timed(fn, *a, **k):
     t0 = time.perf_counter()
     r = fn(*a, **k)
     return r, time.perf_counter() - t0
 
 
-def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, tag):
+def settle(ctx, T, E, n_vs):
+    """n_vs steps of velocity scaling (velocity_scaling.F:9-103: the kinetic
+    energy held at the target every step) from a proposed state, then the
+    point's Nose-Poincare start (fg_chain_point: force, s = 1, pi = 0, H0).
+    A proposal whose potential energy is off relaxes against the rescaled
+    momenta in a few hundred steps instead of through the slow thermostat."""
+    e = A.fg_energy()
+    for _ in range(n_vs):
+        ctx.velocity_scaling(e)
+    ctx.chain_point(T, E)
+
+
+def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, tag, n_vs=0):
     """One pass over held-out points in the given order: for each, the
     fallback (chained from the previous point), the network's warm start and
-    a cold start (initialize_dipoR's uni64 field, p = 0), `probe` steps
-    each; the fallback continues `probe` more steps for the equilibrium."""
+    a cold start (initialize_dipoR's uni64 field, p = 0), each of the last
+    two settled by n_vs velocity-scaling steps (counted in its time), then
+    `probe` Nose-Poincare steps each; the fallback continues `probe` more
+    steps for the equilibrium."""
     import feram_b200 as fb
     p0 = make_params(L, points[0][0], points[0][1], -5.0)
     rows, t_infer = [], 0.0
@@ -351,6 +376,7 @@ def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, t
             t_infer += time.perf_counter() - t0
             cw.chain_point(T, E)  # the context's temperature and field; its state is replaced
             start_point(cw, cw.p, uw, maxwell_momenta(cw.p, seed + i))
+            settle(cw, T, E, n_vs)
             Pw, Vw = equilibration_trace(cw, probe, every)
             cc.chain_point(T, E)
             pc = A.fg_params.from_buffer_copy(cc.p)
@@ -358,21 +384,19 @@ def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, t
             uc = A.real_field(pc)
             assert A.lib().fg_init_dipoR_host(C.byref(pc), A.dptr(uc), None) == 0
             start_point(cc, cc.p, uc, A.real_field(pc))
+            settle(cc, T, E, n_vs)
             Pc, Vc = equilibration_trace(cc, probe, every)
             tf = time_to_equilibrium(Pf, Vf, eq, every)
             tw = time_to_equilibrium(Pw, Vw, eq, every)
             tc = time_to_equilibrium(Pc, Vc, eq, every)
             k0 = accept_after // every
-            a_w = block_stats(Pw[k0:], Vw[k0:])
-            nb_w, nb_e = (len(Pw) - k0) // 5, len(Pe) // 5
-            ok = (abs(a_w[0] - eq[0]) <= 4 * np.hypot(a_w[1] / np.sqrt(nb_w), eq[1] / np.sqrt(nb_e)) + 1e-12 and
-                  abs(a_w[2] - eq[2]) <= 4 * np.hypot(a_w[3] / np.sqrt(nb_w), eq[3] / np.sqrt(nb_e)) + 1e-12)
-            val = lambda t: probe if t is None else t
+            ok = accept(Pw[k0:], Vw[k0:], Pe, Ve)
+            val = lambda t, extra=0: extra + (probe if t is None else t)
             Nn = cw.p.N
-            rows.append([T, ez, val(tf), val(tw), val(tc), int(ok), Vf[0] / Nn, Vw[0] / Nn, eq[2] / Nn,
+            rows.append([T, ez, val(tf), val(tw, n_vs), val(tc, n_vs), int(ok), Vf[0] / Nn, Vw[0] / Nn, eq[2] / Nn,
                          float(Pf[0]), float(Pw[0]), eq[0]])
-            say(f"  {tag} point {i}: T {T:.1f} K, E_z {ez:+.5f}: tau fallback {val(tf)}, warm {val(tw)}, "
-                f"cold {val(tc)}, {'accepted' if ok else 'rejected'}")
+            say(f"  {tag} point {i}: T {T:.1f} K, E_z {ez:+.5f}: tau fallback {val(tf)}, warm {val(tw, n_vs)}, "
+                f"cold {val(tc, n_vs)}, {'accepted' if ok else 'rejected'}")
     r = np.array(rows)
     tf, tw, tc, acc = r[:, 2], r[:, 3], r[:, 4], r[:, 5]
     eff = np.where(acc == 1, tw, tw + tf)  # a rejected warm start pays both tries
@@ -388,7 +412,7 @@ def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, t
 
 def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40, n_shuffled=20, seed=2024,
                n_therm=3000, n_snap=14, train_steps=4000, probe=3000, every=20, accept_after=1000, log=None,
-               keep_layers=False, energy_from=3000):
+               keep_layers=False, energy_from=3000, n_vs=200):
     """The learned-warm-start protocol on one GPU.
 
     1. Data: MD cooling chains (train_chains of (E_z, GPa), train_temps
@@ -401,7 +425,8 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
        n_shuffled in random order (a scan whose previous point is unrelated).
        Each point runs from the previous point's final state (fg_chain_point,
        the reference's .restart chaining: the fallback), from the network's
-       proposal with Maxwell-Boltzmann momenta, and from a cold uni64 start;
+       proposal with Maxwell-Boltzmann momenta, and from a cold uni64 start
+       (both settled by n_vs velocity-scaling steps, counted in their times);
        the fallback continues for the point's equilibrium (block means and
        their spread).  Time to equilibrium: three consecutive blocks of the
        trace within 3 sigma of it.  Acceptance, the MD as the judge: the warm
@@ -438,10 +463,11 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
         say(f"warm start: trained {train_steps} steps in {t_train:.1f} s, loss {out['loss_first']:.3g} -> "
             f"{out['loss_last']:.3g}")
         pts = [(float(rng.uniform(100.0, 450.0)), float(rng.uniform(-0.001, 0.001))) for _ in range(n_held + n_shuffled)]
+        out["settle_vs_steps"] = n_vs
         out["cooling_sweep"] = _sweep(net, make_params, L, sorted(pts[:n_held], reverse=True), seed, probe, every,
-                                      accept_after, say, "sweep")
+                                      accept_after, say, "sweep", n_vs)
         out["shuffled"] = _sweep(net, make_params, L, pts[n_held:], seed + 7, probe, every, accept_after, say,
-                                 "shuffled")
+                                 "shuffled", n_vs)
         if keep_layers:
             out["_layers"] = [net.layer(l)[:2] for l in range(4)]
     finally:
