@@ -136,7 +136,6 @@ struct fg_ctx {
   double2* trz = nullptr;
   double2* trz_s = nullptr;  // trz and kvz in kz-slot order
   double* kvz_s = nullptr;
-  float* kvz_sf = nullptr;
   double* layer_minv = nullptr;
   unsigned char* layer_sump = nullptr;
   // acoustic-displacement MD (acoustic mass > 0): u, p and F hold three more
@@ -220,7 +219,7 @@ int fail(fg_ctx* c, int code, const std::string& msg) {
 
 template <typename T>
 KMaps kmaps(const fg_ctx* c) {
-  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz, c->trz_s, c->kvz_s, c->kvz_sf};
+  return KMaps{c->revx, c->revy, c->revz, c->kvx, c->kvy, c->kvz, c->trx, c->try_, c->trz, c->trz_s, c->kvz_s};
 }
 
 int check_device_error(fg_ctx* ctx) {
@@ -375,8 +374,10 @@ AsmConst asm_const(const fg_ctx* ctx) {
 // flo: also store the FP32 residual of the force (mixed path)
 template <typename T, bool CLOSE>
 void launch_assemble(fg_ctx* ctx, int tail, bool flo = false) {
-  launch_dep(ctx, k_assemble<T, CLOSE>, CLOSE ? ctx->grid_asc : ctx->grid_as, kThreadsElem, 0,
-             (const T*)ctx->rwork, (const T*)ctx->u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, tail,
+  const bool sites = ctx->site_species || ctx->site_zstar || ctx->site_E ||
+                     (CLOSE && (ctx->site_minv || ctx->site_sump));
+  launch_dep(ctx, sites ? k_assemble<T, CLOSE, true> : k_assemble<T, CLOSE, false>,
+             CLOSE ? ctx->grid_asc : ctx->grid_as, kThreadsElem, 0, (const T*)ctx->rwork, (const T*)ctx->u, (T*)ctx->F, ctx->g, ctx->ph, ctx->sc, ctx->part_r, tail,
              ctx->done + 2, ctx->site_species, (const T*)ctx->site_zstar, (const T*)ctx->site_E,
              ctx->zsite ? zu_comp(ctx) : 0, (T*)ctx->p, ctx->layer_minv, ctx->layer_sump, (const T*)ctx->site_minv,
              ctx->site_sump, ctx->part_ke, (flo && sizeof(T) == 4) ? (T*)ctx->Flo : (T*)nullptr, asm_const(ctx),
@@ -922,8 +923,6 @@ int create_impl(fg_ctx* ctx) {
       }
       if ((rc = upload(ctx, (void**)&ctx->trz_s, tzs))) return rc;
       if ((rc = upload(ctx, (void**)&ctx->kvz_s, kzs))) return rc;
-      std::vector<float> kzf(kzs.begin(), kzs.end());
-      if ((rc = upload(ctx, (void**)&ctx->kvz_sf, kzf))) return rc;
     }
   }
   // per-layer masses and masks (alloc_Coord, read_defects_u.F:52-69)
@@ -1663,7 +1662,7 @@ void fg_destroy(fg_ctx* ctx) {
   if (ctx->g_force) cudaGraphExecDestroy(ctx->g_force);
   void* bufs[] = {ctx->u, ctx->p, ctx->F, ctx->Flo, ctx->spec, ctx->rwork, ctx->dtab, ctx->ckmod, ctx->acouK, ctx->twx,
                   ctx->twm, ctx->twy, ctx->twz, ctx->twx64, ctx->twm64, ctx->twy64, ctx->twz64, ctx->L64, ctx->ltab, ctx->revx,
-                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz, ctx->trz_s, ctx->kvz_s, ctx->kvz_sf,
+                  ctx->revy, ctx->revz, ctx->posm, ctx->kvx, ctx->kvy, ctx->kvz, ctx->trx, ctx->try_, ctx->trz, ctx->trz_s, ctx->kvz_s,
                   ctx->layer_minv, ctx->layer_sump, ctx->ph, ctx->sc, ctx->part_k, ctx->part_r, ctx->part_ke,
                   ctx->part_avg, ctx->avg6, ctx->staging, ctx->dipoRavg, ctx->done, ctx->layer_macou, ctx->layer_all,
                   ctx->site_minv, ctx->site_macou, ctx->site_sump, ctx->site_species, ctx->site_zstar, ctx->site_E,

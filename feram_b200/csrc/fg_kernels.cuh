@@ -896,7 +896,6 @@ struct KMaps {
   const double2* trz;
   const double2* trz_s;  // trz and kvz in kz-slot order (no revz lookup first)
   const double* kvz_s;
-  const float* kvz_sf;   // kvz_s rounded to FP32 (the mixed path's k)
 };
 
 // Plain z pass of nc spectra in place: DIF (INV = false) or DIT (INV = true).
@@ -968,13 +967,6 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
-  __shared__ T kcon[8];  // B11, B12, B44, HC2 xx, xy, yz-yz, 1/N in T
-  if (threadIdx.x < 7) {
-    const int i = threadIdx.x;
-    const double v = i == 0 ? ph->B11 : i == 1 ? ph->B12 : i == 2 ? ph->B44 : i == 3 ? ph->HC2[0][0]
-                   : i == 4 ? ph->HC2[0][1] : i == 5 ? ph->HC2[3][3] : ph->Ninv;
-    kcon[i] = (T)v;
-  }
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
   // ACOU: acoustic-displacement MD, three more components in and out
   // (FFT(acouR) in, dVdacK out; acouFFT.F:9-26, dVdac.F:11-63)
@@ -1046,19 +1038,6 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
   // Energy sums: the per-k products in T (FP32 in the mixed path, whose
   // spectra are FP32), accumulated per thread in FP64
   double acc[NQ_K] = {0, 0, 0, 0, 0};
-  // constants of the loop, converted to T once per block (kcon, filled
-  // before the z stages) and read from shared memory: reading them through
-  // ph in the loop repeats the loads and FP64 -> FP32 conversions at every k
-  // (the loop's store to sc->didiK0 keeps the compiler from hoisting them)
-  const T& B11 = kcon[0];
-  const T& B12 = kcon[1];
-  const T& B44 = kcon[2];
-  const T& hx = kcon[3];
-  const T& hy = kcon[4];
-  const T& h4 = kcon[5];
-  const T& ni = kcon[6];
-  const bool mod_on = ph->modulation_on != 0;
-  const T* __restrict__ kvz_t = reinterpret_cast<const T*>(sizeof(T) == 4 ? km.kvz_sf : (const void*)km.kvz_s);
   // this thread's pencil (fixed cw), decoded once
   const int cw = cwp, col = colp, yslot = ysp;
   const bool pencil_ok = okp;
@@ -1134,8 +1113,7 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
       double qd[6];
 #pragma unroll
       for (int q = 0; q < 6; ++q) qd[q] = (double)qv[q];
-      const double w1d = (double)w1;
-      const double es = w1d * (S[0] * qd[0] + S[1] * qd[1] + S[2] * qd[2] + 2.0 * (S[3] * qd[3] + S[4] * qd[4] + S[5] * qd[5]));
+      const double es = (double)w1 * (S[0] * qd[0] + S[1] * qd[1] + S[2] * qd[2] + 2.0 * (S[3] * qd[3] + S[4] * qd[4] + S[5] * qd[5]));
       acc[0] += es;
       if constexpr (ZSC) {
         // short range on uK, long range on FFT(Z* u): Fl = (L/N) ZuK,
@@ -1162,8 +1140,8 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
 #pragma unroll
         for (int q = 0; q < 6; ++q) D[q] = (T)(S[q] * Ninv);
       } else {
-        acc[1] += w1d * ((double)D[0] * qd[0] + (double)D[1] * qd[1] + (double)D[2] * qd[2] +
-                         2.0 * ((double)D[3] * qd[3] + (double)D[4] * qd[4] + (double)D[5] * qd[5]));
+        acc[1] += (double)w1 * ((double)D[0] * qd[0] + (double)D[1] * qd[1] + (double)D[2] * qd[2] +
+                                2.0 * ((double)D[3] * qd[3] + (double)D[4] * qd[4] + (double)D[5] * qd[5]));
       }
     }
     cplx<T> F[3];
@@ -1171,8 +1149,9 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
     F[1] = mk<cplx<T>>(D[5] * u[0].x + D[1] * u[1].x + D[3] * u[2].x, D[5] * u[0].y + D[1] * u[1].y + D[3] * u[2].y);
     F[2] = mk<cplx<T>>(D[4] * u[0].x + D[3] * u[1].x + D[2] * u[2].x, D[4] * u[0].y + D[3] * u[1].y + D[2] * u[2].y);
     // ---- inhomogeneous strain
-    const T k1 = (T)kv1, k2 = (T)kv2, k3 = __ldg(&kvz_t[zs]);
+    const T k1 = (T)kv1, k2 = (T)kv2, k3 = (T)__ldg(&km.kvz_s[zs]);
     const T kk[4] = {(T)0, k1, k2, k3};
+    const T B11 = (T)ph->B11, B12 = (T)ph->B12, B44 = (T)ph->B44;
     T K[3][3];
 #pragma unroll
     for (int b = 1; b <= 3; ++b) {
@@ -1186,8 +1165,9 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
     // coup2 . didiK with coup2(a, i) of elastic.F:156-180: k_a B1xx/2 on
     // i = a, k_a B1yy/2 on the other two diagonal entries, k_c B4yz on the
     // shear entries (yz: b = y, c = z ...) that involve a, zero on the third
+    const T hx = (T)(ph->HC2[0][0]), hy = (T)(ph->HC2[0][1]), h4 = (T)(ph->HC2[3][3]);
     cplx<T> ck[3] = {mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0), mk<cplx<T>>((T)0, (T)0)};
-    if (mod_on) {
+    if (ph->modulation_on) {
 #pragma unroll
       for (int a = 0; a < 3; ++a) ck[a] = ckmod[tpos * 3 + a];
     }
@@ -1228,6 +1208,7 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
       acc[2] += (double)(w2 * es);
       acc[3] += (double)(w2 * ec);
       acc[4] += (double)(w2 * em);
+      const T ni = (T)Ninv;
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
         const cplx<T> v = mk<cplx<T>>(ck[a].x + cs[a].x + KA[a].x, ck[a].y + cs[a].y + KA[a].y);
@@ -1270,6 +1251,7 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
 #pragma unroll
       for (int a = 0; a < 3; ++a) acouK_out[tpos * 3 + a] = acou[a];
     }
+    const T ni = (T)Ninv;
     d[0] = mk<cplx<T>>(k1 * acou[0].x * ni, k1 * acou[0].y * ni);
     d[1] = mk<cplx<T>>(k2 * acou[1].x * ni, k2 * acou[1].y * ni);
     d[2] = mk<cplx<T>>(k3 * acou[2].x * ni, k3 * acou[2].y * ni);
@@ -1333,6 +1315,41 @@ __device__ __forceinline__ V16<T> ldv_first(const T* p, unsigned long long pol) 
 }
 template <typename T>
 __device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V16<T>*>(p) = a; }
+
+// N consecutive sites of one component, for the assembly's vector path: the
+// sites per thread set its registers (the FP64 site sums of N sites stay
+// live together) against the bytes each thread keeps in flight.
+#ifndef FG_ASM_SITES
+#define FG_ASM_SITES 4  // FP32 sites per thread (FP64: 2)
+#endif
+#ifndef FG_ASM_MINB
+#define FG_ASM_MINB 2   // resident CTAs of 256 threads per SM the assembly is compiled for
+#endif
+template <typename T, int N>
+struct alignas(N * sizeof(T)) VN {
+  static constexpr int n = N;
+  T v[N];
+};
+template <typename T, int N>
+__device__ __forceinline__ VN<T, N> ldn(const T* p) { return *reinterpret_cast<const VN<T, N>*>(p); }
+template <typename T, int N>
+__device__ __forceinline__ VN<T, N> ldn_first(const T* p, unsigned long long pol) {
+  VN<T, N> r;
+  if constexpr (N * sizeof(T) == 16) {
+    const V16<T> a = ldv_first(p, pol);
+#pragma unroll
+    for (int l = 0; l < N; ++l) r.v[l] = a.v[l];
+  } else if constexpr (sizeof(T) == 4 && N == 2) {
+    const float2 a = ld_first(reinterpret_cast<const float2*>(p), pol);
+    r.v[0] = a.x;
+    r.v[1] = a.y;
+  } else {
+    r = ldn<T, N>(p);
+  }
+  return r;
+}
+template <typename T, int N>
+__device__ __forceinline__ void stn(T* p, const VN<T, N>& a) { *reinterpret_cast<VN<T, N>*>(p) = a; }
 
 // Constants of the site force, in FP64 for both precisions: the mixed path
 // reads FP32 u, the FP32 dipole-dipole force and the FP32 eta, and sums the
@@ -1431,8 +1448,8 @@ __device__ __forceinline__ void close_site(T* __restrict__ p, long long ns, long
 // (np_close_tail: KE, H_NP and (38) of the next step).
 // Flo (mixed path, may be null): the FP32 residual of each force component,
 // F + Flo = the FP64 site sum.
-template <typename T, bool CLOSE = false>
-__global__ void __launch_bounds__(256, 2)
+template <typename T, bool CLOSE = false, bool SITES = false>
+__global__ void __launch_bounds__(256, FG_ASM_MINB)
     k_assemble(const T* __restrict__ rw, const T* __restrict__ u, T* __restrict__ F, Geom g,
                const Phys* __restrict__ ph, DevScalars* sc, double* __restrict__ part, int tail, unsigned int* done,
                const unsigned char* __restrict__ site_species, const T* __restrict__ site_zstar,
@@ -1467,16 +1484,22 @@ __global__ void __launch_bounds__(256, 2)
   const unsigned long long pol_rw = l2_evict_first();
   // k: the static constants (kernel parameter, built by asm_const on the
   // host); dy: this step's strain coupling and field
-  AsmDyn dy;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) dy.wh[i] = sc->w_hom[i];
-  dy.E0 = sc->E[0]; dy.E1 = sc->E[1]; dy.E2 = sc->E[2];
+  // (in shared memory: read at each use instead of held in nine FP64
+  // register pairs through the loop)
+  __shared__ AsmDyn dy;
+  if (threadIdx.x < 6) dy.wh[threadIdx.x] = sc->w_hom[threadIdx.x];
+  if (threadIdx.x == 6) dy.E0 = sc->E[0];
+  if (threadIdx.x == 7) dy.E1 = sc->E[1];
+  if (threadIdx.x == 8) dy.E2 = sc->E[2];
+  __syncthreads();
   double acc[NQ_R] = {0.0, 0.0};
-  constexpr int NV = V16<T>::n;
+  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
+  using AV = VN<T, NV>;
   const long long stride = (long long)gridDim.x * blockDim.x;
-  const bool sites = site_species != nullptr || site_zstar != nullptr || site_E != nullptr ||
-                     (CLOSE && (site_minv != nullptr || site_sump != nullptr));
-  if (sites) {
+  // SITES: the per-site loop (any of the site arrays present, chosen on the
+  // host); otherwise the bulk loops, compiled without it so that its FP64
+  // species polynomial does not set their register budget
+  if constexpr (SITES) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += stride) {
       AsmDyn dys = dy;
       double dk2 = 0.0;
@@ -1531,14 +1554,14 @@ __global__ void __launch_bounds__(256, 2)
   } else if (g.plane_r % NV == 0) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
-      const V16<T> ux = ldv(u + i), uy = ldv(u + ns + i), uz = ldv(u + 2 * ns + i);
+      const AV ux = ldn<T, NV>(u + i), uy = ldn<T, NV>(u + ns + i), uz = ldn<T, NV>(u + 2 * ns + i);
       // rw is consumed here: evict_first keeps u, p and F in L2
-      const V16<T> a0 = ldv_first(rw + i, pol_rw), a1 = ldv_first(rw + ns + i, pol_rw),
-                   a2 = ldv_first(rw + 2 * ns + i, pol_rw);
-      V16<T> e[6];
+      const AV a0 = ldn_first<T, NV>(rw + i, pol_rw), a1 = ldn_first<T, NV>(rw + ns + i, pol_rw),
+               a2 = ldn_first<T, NV>(rw + 2 * ns + i, pol_rw);
+      AV e[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) e[q] = ldv_first(rw + (3 + q) * ns + i, pol_rw);
-      V16<T> o0, o1, o2, l0, l1, l2;
+      for (int q = 0; q < 6; ++q) e[q] = ldn_first<T, NV>(rw + (3 + q) * ns + i, pol_rw);
+      AV o0, o1, o2, l0, l1, l2;
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
         const double eta[6] = {e[0].v[l], e[1].v[l], e[2].v[l], e[3].v[l], e[4].v[l], e[5].v[l]};
@@ -1551,17 +1574,17 @@ __global__ void __launch_bounds__(256, 2)
         l1.v[l] = force_lo<T>(d1, o1.v[l]);
         l2.v[l] = force_lo<T>(d2, o2.v[l]);
       }
-      stv(F + i, o0);
-      stv(F + ns + i, o1);
-      stv(F + 2 * ns + i, o2);
+      stn(F + i, o0);
+      stn(F + ns + i, o1);
+      stn(F + 2 * ns + i, o2);
       if (Flo) {
-        stv(Flo + i, l0);
-        stv(Flo + ns + i, l1);
-        stv(Flo + 2 * ns + i, l2);
+        stn(Flo + i, l0);
+        stn(Flo + ns + i, l1);
+        stn(Flo + 2 * ns + i, l2);
       }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
-        V16<T> q[3] = {ldv(p + i), ldv(p + ns + i), ldv(p + 2 * ns + i)};
+        AV q[3] = {ldn<T, NV>(p + i), ldn<T, NV>(p + ns + i), ldn<T, NV>(p + 2 * ns + i)};
         T pp = 0, pf = 0, ff = 0;
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
@@ -1575,7 +1598,7 @@ __global__ void __launch_bounds__(256, 2)
           }
         }
 #pragma unroll
-        for (int a = 0; a < 3; ++a) stv(p + a * ns + i, q[a]);
+        for (int a = 0; a < 3; ++a) stn(p + a * ns + i, q[a]);
         if (layer_sump[z]) {
           const double mi = layer_minv[z];
           ke[0] += (double)pp * mi;
@@ -1635,7 +1658,8 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
-  constexpr int NV = V16<T>::n;
+  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
+  using AV = VN<T, NV>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr && site_sump == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1806,7 +1830,8 @@ __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __rest
   const long long ns = g.nsite;
   const T ck = (T)sc->kick_coef;
   const double cd = sc->pend_drift;
-  constexpr int NV = V16<T>::n;
+  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
+  using AV = VN<T, NV>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1860,7 +1885,8 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
   // pend_kick_f is not changed by block 0's commit
   const T c = PREP ? (T)0 : (T)__ldcg(&sc->pend_kick_f);
   double acc[3] = {0.0, 0.0, 0.0};
-  constexpr int NV = V16<T>::n;
+  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
+  using AV = VN<T, NV>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr && site_sump == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1923,7 +1949,8 @@ __global__ void __launch_bounds__(256) k_drift(T* __restrict__ u, const T* __res
                                                const T* __restrict__ site_minv = nullptr) {
   const long long ns = g.nsite;
   const double c = *coef;
-  constexpr int NV = V16<T>::n;
+  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
+  using AV = VN<T, NV>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
