@@ -1316,41 +1316,6 @@ __device__ __forceinline__ V16<T> ldv_first(const T* p, unsigned long long pol) 
 template <typename T>
 __device__ __forceinline__ void stv(T* p, const V16<T>& a) { *reinterpret_cast<V16<T>*>(p) = a; }
 
-// N consecutive sites of one component, for the assembly's vector path: the
-// sites per thread set its registers (the FP64 site sums of N sites stay
-// live together) against the bytes each thread keeps in flight.
-#ifndef FG_ASM_SITES
-#define FG_ASM_SITES 4  // FP32 sites per thread (FP64: 2)
-#endif
-#ifndef FG_ASM_MINB
-#define FG_ASM_MINB 2   // resident CTAs of 256 threads per SM the assembly is compiled for
-#endif
-template <typename T, int N>
-struct alignas(N * sizeof(T)) VN {
-  static constexpr int n = N;
-  T v[N];
-};
-template <typename T, int N>
-__device__ __forceinline__ VN<T, N> ldn(const T* p) { return *reinterpret_cast<const VN<T, N>*>(p); }
-template <typename T, int N>
-__device__ __forceinline__ VN<T, N> ldn_first(const T* p, unsigned long long pol) {
-  VN<T, N> r;
-  if constexpr (N * sizeof(T) == 16) {
-    const V16<T> a = ldv_first(p, pol);
-#pragma unroll
-    for (int l = 0; l < N; ++l) r.v[l] = a.v[l];
-  } else if constexpr (sizeof(T) == 4 && N == 2) {
-    const float2 a = ld_first(reinterpret_cast<const float2*>(p), pol);
-    r.v[0] = a.x;
-    r.v[1] = a.y;
-  } else {
-    r = ldn<T, N>(p);
-  }
-  return r;
-}
-template <typename T, int N>
-__device__ __forceinline__ void stn(T* p, const VN<T, N>& a) { *reinterpret_cast<VN<T, N>*>(p) = a; }
-
 // Constants of the site force, in FP64 for both precisions: the mixed path
 // reads FP32 u, the FP32 dipole-dipole force and the FP32 eta, and sums the
 // on-site polynomial, the field and both strain couplings in FP64.  Those
@@ -1449,7 +1414,7 @@ __device__ __forceinline__ void close_site(T* __restrict__ p, long long ns, long
 // Flo (mixed path, may be null): the FP32 residual of each force component,
 // F + Flo = the FP64 site sum.
 template <typename T, bool CLOSE = false, bool SITES = false>
-__global__ void __launch_bounds__(256, FG_ASM_MINB)
+__global__ void __launch_bounds__(256, 2)
     k_assemble(const T* __restrict__ rw, const T* __restrict__ u, T* __restrict__ F, Geom g,
                const Phys* __restrict__ ph, DevScalars* sc, double* __restrict__ part, int tail, unsigned int* done,
                const unsigned char* __restrict__ site_species, const T* __restrict__ site_zstar,
@@ -1493,8 +1458,8 @@ __global__ void __launch_bounds__(256, FG_ASM_MINB)
   if (threadIdx.x == 8) dy.E2 = sc->E[2];
   __syncthreads();
   double acc[NQ_R] = {0.0, 0.0};
-  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
-  using AV = VN<T, NV>;
+  constexpr int NV = V16<T>::n;
+  using AV = V16<T>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   // SITES: the per-site loop (any of the site arrays present, chosen on the
   // host); otherwise the bulk loops, compiled without it so that its FP64
@@ -1554,13 +1519,13 @@ __global__ void __launch_bounds__(256, FG_ASM_MINB)
   } else if (g.plane_r % NV == 0) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
       const long long i = iv * NV;
-      const AV ux = ldn<T, NV>(u + i), uy = ldn<T, NV>(u + ns + i), uz = ldn<T, NV>(u + 2 * ns + i);
+      const AV ux = ldv(u + i), uy = ldv(u + ns + i), uz = ldv(u + 2 * ns + i);
       // rw is consumed here: evict_first keeps u, p and F in L2
-      const AV a0 = ldn_first<T, NV>(rw + i, pol_rw), a1 = ldn_first<T, NV>(rw + ns + i, pol_rw),
-               a2 = ldn_first<T, NV>(rw + 2 * ns + i, pol_rw);
+      const AV a0 = ldv_first(rw + i, pol_rw), a1 = ldv_first(rw + ns + i, pol_rw),
+               a2 = ldv_first(rw + 2 * ns + i, pol_rw);
       AV e[6];
 #pragma unroll
-      for (int q = 0; q < 6; ++q) e[q] = ldn_first<T, NV>(rw + (3 + q) * ns + i, pol_rw);
+      for (int q = 0; q < 6; ++q) e[q] = ldv_first(rw + (3 + q) * ns + i, pol_rw);
       AV o0, o1, o2, l0, l1, l2;
 #pragma unroll
       for (int l = 0; l < NV; ++l) {
@@ -1574,17 +1539,17 @@ __global__ void __launch_bounds__(256, FG_ASM_MINB)
         l1.v[l] = force_lo<T>(d1, o1.v[l]);
         l2.v[l] = force_lo<T>(d2, o2.v[l]);
       }
-      stn(F + i, o0);
-      stn(F + ns + i, o1);
-      stn(F + 2 * ns + i, o2);
+      stv(F + i, o0);
+      stv(F + ns + i, o1);
+      stv(F + 2 * ns + i, o2);
       if (Flo) {
-        stn(Flo + i, l0);
-        stn(Flo + ns + i, l1);
-        stn(Flo + 2 * ns + i, l2);
+        stv(Flo + i, l0);
+        stv(Flo + ns + i, l1);
+        stv(Flo + 2 * ns + i, l2);
       }
       if constexpr (CLOSE) {
         const int z = (int)(i / g.plane_r);
-        AV q[3] = {ldn<T, NV>(p + i), ldn<T, NV>(p + ns + i), ldn<T, NV>(p + 2 * ns + i)};
+        AV q[3] = {ldv(p + i), ldv(p + ns + i), ldv(p + 2 * ns + i)};
         T pp = 0, pf = 0, ff = 0;
 #pragma unroll
         for (int l = 0; l < NV; ++l) {
@@ -1598,7 +1563,7 @@ __global__ void __launch_bounds__(256, FG_ASM_MINB)
           }
         }
 #pragma unroll
-        for (int a = 0; a < 3; ++a) stn(p + a * ns + i, q[a]);
+        for (int a = 0; a < 3; ++a) stv(p + a * ns + i, q[a]);
         if (layer_sump[z]) {
           const double mi = layer_minv[z];
           ke[0] += (double)pp * mi;
@@ -1658,8 +1623,8 @@ __global__ void __launch_bounds__(256) k_kick(T* __restrict__ p, const T* __rest
   const long long ns = g.nsite;
   const T c = (T)(*coef);
   double acc[1] = {0.0};
-  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
-  using AV = VN<T, NV>;
+  constexpr int NV = V16<T>::n;
+  using AV = V16<T>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr && site_sump == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1830,8 +1795,8 @@ __global__ void __launch_bounds__(256) k_kick_drift(T* __restrict__ p, T* __rest
   const long long ns = g.nsite;
   const T ck = (T)sc->kick_coef;
   const double cd = sc->pend_drift;
-  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
-  using AV = VN<T, NV>;
+  constexpr int NV = V16<T>::n;
+  using AV = V16<T>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1885,8 +1850,8 @@ __global__ void __launch_bounds__(256) k_kick_close(T* __restrict__ p, const T* 
   // pend_kick_f is not changed by block 0's commit
   const T c = PREP ? (T)0 : (T)__ldcg(&sc->pend_kick_f);
   double acc[3] = {0.0, 0.0, 0.0};
-  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
-  using AV = VN<T, NV>;
+  constexpr int NV = V16<T>::n;
+  using AV = V16<T>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr && site_sump == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
@@ -1949,8 +1914,8 @@ __global__ void __launch_bounds__(256) k_drift(T* __restrict__ u, const T* __res
                                                const T* __restrict__ site_minv = nullptr) {
   const long long ns = g.nsite;
   const double c = *coef;
-  constexpr int NV = sizeof(T) == 4 ? FG_ASM_SITES : 2;
-  using AV = VN<T, NV>;
+  constexpr int NV = V16<T>::n;
+  using AV = V16<T>;
   const long long stride = (long long)gridDim.x * blockDim.x;
   if (g.plane_r % NV == 0 && site_minv == nullptr) {
     for (long long iv = (long long)blockIdx.x * blockDim.x + threadIdx.x; iv < ns / NV; iv += stride) {
