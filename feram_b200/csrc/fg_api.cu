@@ -2088,19 +2088,20 @@ int fg_time_steps(fg_ctx* ctx, int n_steps, double* ms) {
     if ((rc = run_graph(ctx, &ctx->g_np_multi, 4))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
   }
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaEventRecord(e0, ctx->stream));
-  for (int i = 0; i < nmulti; ++i) CK(cudaGraphLaunch(ctx->g_np_multi, ctx->stream));
-  for (int i = 0; i < nsingle; ++i) CK(cudaGraphLaunch(*gx, ctx->stream));
-  CK(cudaEventRecord(e1, ctx->stream));
-  CK(cudaEventSynchronize(e1));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
   float t = 0.0f;
-  CK(cudaEventElapsedTime(&t, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaError_t ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e0, ctx->stream);
+  for (int i = 0; ce == cudaSuccess && i < nmulti; ++i) ce = cudaGraphLaunch(ctx->g_np_multi, ctx->stream);
+  for (int i = 0; ce == cudaSuccess && i < nsingle; ++i) ce = cudaGraphLaunch(*gx, ctx->stream);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e1, ctx->stream);
+  if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+  if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, e0, e1);
+  if (e0) cudaEventDestroy(e0);  // on every path
+  if (e1) cudaEventDestroy(e1);
+  if (ce != cudaSuccess) return fail(ctx, FG_ERR_CUDA, std::string("fg_time_steps: ") + cudaGetErrorString(ce));
   *ms = t;
   ctx->force_fresh = true;
   ctx->flo_valid = false;

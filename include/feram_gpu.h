@@ -436,7 +436,9 @@ int  fg_batch_apply_wisdom(fg_batch* b);
    CUDA-event timing on the context's own stream (no host work in between). */
 #define FG_NPROF 5
 /* Time n_steps steps of p's method launched as fg_run_steps launches them;
-   *ms = total. */
+   *ms = total.  A graph not yet instantiated is first captured and run once
+   untimed (one step, or eight for the eight-step graph), so the state may
+   advance by up to eight steps more than n_steps. */
 int  fg_time_steps(fg_ctx* ctx, int n_steps, double* ms);
 /* One bulk Nose-Poincare step launched kernel by kernel (the same kernels as
    the step's graph) with an event between kernels, averaged over reps steps;
