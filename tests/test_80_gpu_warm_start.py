@@ -116,14 +116,15 @@ def test_site_stats_match_device(fg):
 
 
 def test_training_lowers_the_loss(fg):
-    """Adam on fixed targets: the loss falls by at least 10x in 150 steps."""
+    """Adam on fixed targets: the loss falls by at least 10x in 300 steps."""
     rng = np.random.default_rng(1)
     cond = np.array([[150.0 + 25 * i, 0.0, 0.0, 0.0, -5.0] for i in range(4)])
     target = np.array([[0.0, 0.14 * (i < 2), 0.1 * (i < 2), 0.03, 0.0003, 0.02, 0.005] for i in range(4)])
     wts = 1.0 / np.maximum(target.var(axis=0), 1e-6)
     with W.WarmStartNet((8, 8, 8), batch=4, seed=2) as net:
         hist = []
-        for it in range(150):
+        for it in range(300):
             hist.append(net.backward(cond, rng.integers(1, 2 ** 40, size=4), target, wts))
             net.adam(3e-3)
-    assert np.mean(hist[-10:]) < 0.1 * np.mean(hist[:3]), (hist[:3], hist[-10:])
+    ratio = np.mean(hist[-10:]) / np.mean(hist[:3])
+    assert ratio < 0.1, (ratio, hist[:3], hist[-10:])
