@@ -48,6 +48,7 @@ constexpr int kTile = 128;        // sites (GEMM rows) per CTA
 constexpr int kThreads = 128;     // 4 warps: one TMEM lane quarter each
 constexpr int kTaps = 27;
 constexpr int kNS = 7;            // statistics per sample
+constexpr int kWgradSites = 2048; // sites per weight-gradient CTA (one split)
 constexpr long long kWaitIter = 1LL << 22;  // bounded mbarrier waits (~0.3 s)
 constexpr double kEps2 = 1e-8, kEps4 = 1e-16;  // floors of |m|^2 and sum m_a^4
 
@@ -180,12 +181,16 @@ __global__ void __launch_bounds__(kThreads) k_conv_umma(const bf16* __restrict__
   if (warp == 0) tmem_dealloc(tbase, 32);
 }
 
-// Weight gradient dW[n][t][k] += sum_s gout[s][n] act[nb(s, t)][k] over the
-// sites [blockIdx.y * KS, + KS): rows R = t * KC + k (27 KC of them, tile
-// blockIdx.x), N = NC output channels, K = sites in chunks of 64.
+// Weight gradient of the sites [blockIdx.y * KS, + KS):
+// part[blockIdx.y][n][t][k] = sum_s gout[s][n] act[nb(s, t)][k]; rows
+// R = t * KC + k (27 KC of them, tile blockIdx.x), N = NC output channels,
+// K = sites in chunks of 64.  Each split writes its own slice (no atomics);
+// k_ws_sum_splits adds the slices in a fixed order, so the gradient is the
+// same bit for bit from run to run.
 template <int KC, int NC>
 __global__ void __launch_bounds__(kThreads) k_wgrad_umma(const bf16* __restrict__ act, const bf16* __restrict__ gout,
-                                                         Geo g, int KS, float* __restrict__ dW, int* err) {
+                                                         Geo g, int KS, float* __restrict__ part, int* err) {
+  constexpr size_t kNW = (size_t)NC * kTaps * KC;  // one split's slice
   constexpr int KCH = 64;                   // sites per staged chunk
   constexpr uint32_t SBO = (KCH / 8) * 128;  // 1024 bytes
   __shared__ __align__(128) unsigned char sA[kTile * KCH * 2];
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(kThreads) k_wgrad_umma(const bf16* __restrict_
       if (R < nrows) {
         const int t = R / KC, c = R % KC;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) atomicAdd(&dW[((size_t)(c0 + i) * kTaps + t) * KC + c], v[i]);
+        for (int i = 0; i < 16; ++i) part[(size_t)blockIdx.y * kNW + ((size_t)(c0 + i) * kTaps + t) * KC + c] = v[i];
       }
     }
   } else if (!ok && tid == 0) {
@@ -270,6 +275,15 @@ __global__ void __launch_bounds__(kThreads) k_wgrad_umma(const bf16* __restrict_
   tc_fence_before();
   __syncthreads();
   if (warp == 0) tmem_dealloc(tbase, 32);
+}
+
+// dW[i] += sum over the nsplit slices of part (fixed order)
+__global__ void k_ws_sum_splits(const float* __restrict__ part, int nsplit, int nw, float* __restrict__ dW) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += gridDim.x * blockDim.x) {
+    float acc = 0.0f;
+    for (int sp = 0; sp < nsplit; ++sp) acc += part[(size_t)sp * nw + i];
+    dW[i] += acc;
+  }
 }
 
 // --------------------------------------------------------------- elementwise
@@ -518,6 +532,7 @@ struct fg_ws {
   float* mean = nullptr;
   float* loss = nullptr;    // [B]
   float* extra = nullptr;   // caller's dL/du [B][nsite][3] (fg_ws_backward_du), allocated on first use
+  float* wpart = nullptr;   // weight-gradient slices [split][largest layer]
   int* err = nullptr;
   cudaStream_t stream = nullptr;
   std::string msg;
@@ -590,7 +605,7 @@ int backward(fg_ws* n, const float* extra) {
                                                                 1.0f / n->g.B, extra, n->gA, n->gA16);
   WCK(cudaGetLastError());
   const int grid = tot / ws::kTile;
-  const int KS = 2048;  // sites per weight-gradient CTA
+  const int KS = ws::kWgradSites;
   const int nsplit = (tot + KS - 1) / KS;
   float* g = n->gA;
   bf16* g16 = n->gA16;
@@ -602,9 +617,11 @@ int backward(fg_ws* n, const float* extra) {
     ws::k_ws_bias_grad<<<y.cout, 256, 0, n->stream>>>(g, tot, y.cout, y.db);
     WCK(cudaGetLastError());
     const int mt = (ws::kTaps * y.cin + ws::kTile - 1) / ws::kTile;
-    if (l == 0) ws::k_wgrad_umma<16, 32><<<dim3(mt, nsplit), ws::kThreads, 0, n->stream>>>(act_in, g16, n->g, KS, y.dw, n->err);
-    else if (l < 3) ws::k_wgrad_umma<32, 32><<<dim3(mt, nsplit), ws::kThreads, 0, n->stream>>>(act_in, g16, n->g, KS, y.dw, n->err);
-    else ws::k_wgrad_umma<32, 16><<<dim3(mt, nsplit), ws::kThreads, 0, n->stream>>>(act_in, g16, n->g, KS, y.dw, n->err);
+    if (l == 0) ws::k_wgrad_umma<16, 32><<<dim3(mt, nsplit), ws::kThreads, 0, n->stream>>>(act_in, g16, n->g, KS, n->wpart, n->err);
+    else if (l < 3) ws::k_wgrad_umma<32, 32><<<dim3(mt, nsplit), ws::kThreads, 0, n->stream>>>(act_in, g16, n->g, KS, n->wpart, n->err);
+    else ws::k_wgrad_umma<32, 16><<<dim3(mt, nsplit), ws::kThreads, 0, n->stream>>>(act_in, g16, n->g, KS, n->wpart, n->err);
+    WCK(cudaGetLastError());
+    ws::k_ws_sum_splits<<<(int)((y.nw() + 255) / 256), 256, 0, n->stream>>>(n->wpart, nsplit, (int)y.nw(), y.dw);
     WCK(cudaGetLastError());
     if (l == 0) break;
     // dL/dpre of layer l-1 = (W^T * g) * silu'(pre_{l-1})
@@ -698,6 +715,12 @@ int fg_ws_create(int Lx, int Ly, int Lz, int batch, unsigned long long seed, fg_
       (rc = walloc(n, &n->mean, (size_t)3 * batch)) || (rc = walloc(n, &n->loss, (size_t)batch)) ||
       (rc = walloc(n, &n->err, 1)))
     return rc;
+  {
+    size_t maxnw = 0;
+    for (const Layer& y : n->L) maxnw = std::max(maxnw, y.nw());
+    const size_t nsplit = ((size_t)tot + ws::kWgradSites - 1) / ws::kWgradSites;
+    if ((rc = walloc(n, &n->wpart, nsplit * maxnw))) return rc;
+  }
   WCK(cudaStreamSynchronize(n->stream));
   return FG_OK;
 }
@@ -711,7 +734,7 @@ void fg_ws_destroy(fg_ws* n) {
       if (p) cudaFree(p);
   for (void* p : {(void*)n->in16, (void*)n->gA, (void*)n->gB, (void*)n->gA16, (void*)n->gB16, (void*)n->cond,
                   (void*)n->seeds, (void*)n->part, (void*)n->S, (void*)n->target, (void*)n->wts, (void*)n->coef,
-                  (void*)n->mean, (void*)n->loss, (void*)n->extra, (void*)n->err})
+                  (void*)n->mean, (void*)n->loss, (void*)n->extra, (void*)n->wpart, (void*)n->err})
     if (p) cudaFree(p);
   if (n->stream) cudaStreamDestroy(n->stream);
   delete n;
