@@ -128,3 +128,23 @@ def test_training_lowers_the_loss(fg):
             net.adam(3e-3)
     ratio = np.mean(hist[-10:]) / np.mean(hist[:3])
     assert ratio < 0.1, (ratio, hist[:3], hist[-10:])
+
+
+def test_training_is_reproducible_bit_for_bit(fg):
+    """The weight gradient of several site splits (16^3 x 2 samples: 4
+    splits of 2048 sites) is summed in a fixed order, so two trainings from
+    the same seeds end with the same weights bit for bit."""
+    rng = np.random.default_rng(4)
+    cond = np.array([[200.0, 0.0, 0.0, 0.0, -5.0], [350.0, 0.0, 0.0, 0.0005, -5.0]])
+    target = np.array([[0.0, 0.14, 0.1, 0.03, 0.0003, 0.02, 0.005], [0.0, 0.0, 0.0, 0.02, 0.0002, 0.0, 0.0]])
+    wts = np.ones(W.NSTAT)
+    seeds = [rng.integers(1, 2 ** 40, size=2) for _ in range(3)]
+    out = []
+    for _ in range(2):
+        with W.WarmStartNet((16, 16, 16), batch=2, seed=9) as net:
+            for sd in seeds:
+                net.backward(cond, sd, target, wts)
+                net.adam(1e-3)
+            out.append([net.layer(l)[0] for l in range(4)])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
