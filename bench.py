@@ -36,8 +36,10 @@ sys.path.insert(0, ROOT)
 METRIC = "MD site-steps/s at 128^3: mixed vs FP64 GPU (force err<=1e-6); % HBM peak"
 UNIT = "site-steps/s"
 L_DEFAULT = 128
-# fg_nose_poincare calls in the end-to-end measurement, independent of --steps
-E2E_STEPS = 400
+# fg_nose_poincare calls in the end-to-end measurement, independent of --steps:
+# the run length of the 128^3 workload (1e4 steps), over which the one upload
+# and one download of the whole state are spread
+E2E_STEPS = 10000
 
 # BaTiO3, Zhong-Vanderbilt-Rabe effective-Hamiltonian parameters as used by
 # the reference's BaTiO3 cooling sweep and 64^3 benchmark input decks (eV,
