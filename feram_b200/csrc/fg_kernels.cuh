@@ -522,18 +522,24 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
       }
     };
     // column 0 carries the kx = 0 and kx = Lx/2 columns joined (y_join),
-    // formed by one pass of LYC threads into shared memory first (the stage
-    // below reads it from there and writes its outputs in place)
+    // formed by LYC threads into shared memory while all threads run the
+    // first stage of columns 1 .. MC-1 straight from the spectrum (the join's
+    // loads overlap that stage); column 0's first stage then runs on the
+    // joined column in place
     const int* revy = posm + MC;
     const int* posy = posm + MC + LYC;
     for (int sl = threadIdx.x; sl < LYC; sl += kXYThreads) {
       const int sp = __ldg(&posy[(LYC - __ldg(&revy[sl])) % LYC]);
       buf[sl * (MC + 1)] = y_join(ld(0, sl), ld(0, sp), ld(MC, sl), ld(MC, sp));
     }
-    __syncthreads();
-    auto ldj = [&](int col, int e) { return col == 0 ? buf[e * (MC + 1)] : ld(col, e); };
     auto st = [&](int col, int e, const cplx<T>& v) { buf[col + e * (MC + 1)] = v; };
-    ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, MC, false>(ldj, st, tws_y);
+    auto ld1 = [&](int t, int e) { return ld(t + 1, e); };
+    auto st1 = [&](int t, int e, const cplx<T>& v) { st(t + 1, e, v); };
+    ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, MC - 1, false>(ld1, st1, tws_y);
+    __syncthreads();
+    auto ld0 = [&](int, int e) { return buf[e * (MC + 1)]; };
+    auto st0 = [&](int, int e, const cplx<T>& v) { st(0, e, v); };
+    ct_stage_io<T, LYC, NSY - 1, true, kXYThreads, 1, false>(ld0, st0, tws_y);
     __syncthreads();
     ct_inverse_range<T, LYC, NSY - 2, -1, kXYThreads, BatchCT<MC, MC, 1, 0, MC + 1>>(buf, tws_y);
   } else {
