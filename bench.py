@@ -130,6 +130,42 @@ def loaded_repo_libs():
     return sorted(libs)
 
 
+def rank_layout():
+    """(world size, rank, local rank) from the launcher's environment
+    (torchrun sets them; a plain run is rank 0 of 1)."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def replica_seed(rank):
+    """uni64 seeds of the replica on `rank`: an independent replica per rank,
+    as the reference's feram_mpi task farm runs one input per rank."""
+    return (123456789 + rank, 987654321)
+
+
+def reduce_max(v, world, dist=None, device="cuda"):
+    """The maximum of v over the ranks (all_reduce MAX of one FP64 value)."""
+    if world == 1:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job(sites_per_rank, steps, ms_max, world):
+    """Site-steps per second of the whole job: every rank's sites and steps
+    over the slowest rank's time (weak scaling: work per rank fixed)."""
+    return sites_per_rank * steps * world / (ms_max * 1e-3)
+
+
+def bench_config(L, sites, world):
+    """The workload description both arms print."""
+    return {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm",
+            "sites": sites, "precision": "mixed", "parallelism": f"replicas x{world}",
+            "l2": "working set > 126 MB L2, no flush"}
+
+
 def fp32_config(u):
     """u rounded to FP32: the configuration the mixed path holds."""
     return u.astype(np.float32).astype(np.float64)
@@ -658,7 +694,7 @@ def run_reference(args):
     the Fortran/FFTW binary cannot be built here) on all host cores.  Inputs
     come from the oracle's own read_Param/make_Param/initialize_dipoR, so
     nothing of the product is loaded in this process."""
-    rank = int(os.environ.get("RANK", "0"))
+    world, rank, _ = rank_layout()
     if rank != 0:
         return 0
     L = args.size
@@ -691,7 +727,7 @@ def run_reference(args):
         "steps": n, "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 * (t2 - t0) / n,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic: uni64-seeded dipoles, BaTiO3 ZVR parameters",
-        "config": {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm"},
+        "config": bench_config(L, p.N, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "repo_libs_loaded": loaded_repo_libs(),
@@ -730,9 +766,7 @@ def main():
     import feram_b200 as fb
     from feram_b200 import _capi as A
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_layout()
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -744,14 +778,10 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, world, dist, "cuda")
 
     L = args.size
-    p = make_params(L, seed=(123456789 + rank, 987654321))
+    p = make_params(L, seed=replica_seed(rank))
     u, q = initial_state(p)
 
     ctxm = fb.Context(p, A.FG_PREC_MIXED)
@@ -790,12 +820,12 @@ def main():
         return max_over_ranks(ms.value), clocks
 
     ms_mixed, clocks = timed(ctxm, args.steps, args.warmup, True)
-    value = p.N * args.steps * world / (ms_mixed / 1000.0)
+    value = whole_job(p.N, args.steps, ms_mixed, world)
     steps64 = max(args.steps // 2, 10)
     ms_fp64, value64 = None, None
     if ctx64 is not None:
         ms_fp64, _ = timed(ctx64, steps64, args.warmup, False)
-        value64 = p.N * steps64 * world / (ms_fp64 / 1000.0)
+        value64 = whole_job(p.N, steps64, ms_fp64, world)
 
     # per-kernel times of one step (events between kernels, same stream)
     nprof = A.FG_NPROF
@@ -882,9 +912,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (fields, FFT, forces); f64 thermostat, strain, energy sums",
         "data": "synthetic: uni64-seeded dipoles (sigma 0.03 A), BaTiO3 ZVR parameters",
-        "config": {"workload": f"{L}^3 bulk BaTiO3 Nose-Poincare MD, 300 K, dt 2 fs, E_z 100 kV/cm",
-                   "sites": p.N, "precision": "mixed", "parallelism": f"replicas x{world}",
-                   "l2": "working set > 126 MB L2, no flush"},
+        "config": bench_config(L, p.N, world),
         "fp64": {"value": value64, "ms_per_step": (ms_fp64 / steps64) if ms_fp64 else None, "steps": steps64},
         "mixed_over_fp64": (value / value64) if value64 else None,
         "force_err_mixed_vs_fp64": ferr,
