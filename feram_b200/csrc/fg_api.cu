@@ -1072,6 +1072,10 @@ int create_impl(fg_ctx* ctx) {
   ctx->staging_n = (size_t)3 * ctx->NXP * ctx->NYP * P.Lz;
   CK(cudaMalloc(&ctx->staging, sizeof(double) * ctx->staging_n));
   CK(cudaMemset(ctx->staging, 0, sizeof(double) * ctx->staging_n));
+  // the memsets above run on the legacy default stream, which the context's
+  // non-blocking stream does not wait for: finish them before any kernel of
+  // the context reads the buffers (the done tickets, the zeroed fields)
+  CK(cudaStreamSynchronize(0));
   return FG_OK;
 }
 
@@ -1410,7 +1414,7 @@ int set_zsite(fg_ctx* ctx, bool on) {
   ctx->zsite = on;
   ctx->ltab_ready = false;
   CK(cudaMalloc(&ctx->spec, (size_t)ncx * sizeof(cplx<T>) * (size_t)g.ncplx));
-  CK(cudaMemset(ctx->spec, 0, (size_t)ncx * sizeof(cplx<T>) * (size_t)g.ncplx));
+  CK(cudaMemsetAsync(ctx->spec, 0, (size_t)ncx * sizeof(cplx<T>) * (size_t)g.ncplx, ctx->stream));
   CK(cudaMalloc(&ctx->rwork, (size_t)ncx * ctx->real_bytes));
   CK(cudaMalloc(&ctx->part_k, sizeof(double) * NQ_K * (size_t)(zt.nreg + zt.nnyq)));
   if (on) CK(cudaMalloc(&ctx->ltab, 6 * sizeof(T) * (size_t)g.nkpos));

@@ -553,7 +553,9 @@ int ws_fail(fg_ws* n, int rc, const std::string& m) {
 template <class T>
 int walloc(fg_ws* n, T** p, size_t count) {
   WCK(cudaMalloc((void**)p, count * sizeof(T)));
-  WCK(cudaMemset(*p, 0, count * sizeof(T)));
+  // zeroed on the net's own stream: a plain cudaMemset runs on the legacy
+  // default stream, which the net's non-blocking stream does not wait for
+  WCK(cudaMemsetAsync(*p, 0, count * sizeof(T), n->stream));
   return FG_OK;
 }
 
@@ -702,7 +704,9 @@ int fg_ws_create(int Lx, int Ly, int Lz, int batch, unsigned long long seed, fg_
         (rc = walloc(n, &y.wt16, nw)) || (rc = walloc(n, &y.pre, (size_t)tot * y.cout)))
       return rc;
     if (l < 3 && (rc = walloc(n, &y.act, (size_t)tot * y.cout))) return rc;
-    WCK(cudaMemcpy(y.w, w.data(), nw * sizeof(float), cudaMemcpyHostToDevice));
+    // after its zeroing, in the net's stream order
+    WCK(cudaMemcpyAsync(y.w, w.data(), nw * sizeof(float), cudaMemcpyHostToDevice, n->stream));
+    WCK(cudaStreamSynchronize(n->stream));
     if ((rc = cast_layer(n, l))) return rc;
   }
   n->nblk = std::max(1, std::min(64, n->g.nsite / 1024));
