@@ -349,25 +349,33 @@ def _sweep(net, make_params, L, points, seed, probe, every, accept_after, say, t
     fallback (chained from the previous point), the network's warm start and
     a cold start (initialize_dipoR's uni64 field, p = 0), each of the last
     two settled by n_vs velocity-scaling steps (counted in its time), then
-    `probe` Nose-Poincare steps each; the fallback continues `probe` more
-    steps for the equilibrium."""
+    `probe` Nose-Poincare steps each.  The equilibrium every start is judged
+    against comes from an independent chain through the same points (another
+    uni64 seed), thermalised `probe` steps at each point and then measured
+    over `probe` more: not from the fallback's own continuation, which would
+    share the fallback's slow fluctuations and favour it."""
     import feram_b200 as fb
     p0 = make_params(L, points[0][0], points[0][1], -5.0)
     rows, t_infer = [], 0.0
     with fb.Context(p0, FG_PREC_MIXED) as cf, fb.Context(p0, FG_PREC_MIXED) as cw, \
-            fb.Context(p0, FG_PREC_MIXED) as cc:
-        for c in (cf, cw, cc):
+            fb.Context(p0, FG_PREC_MIXED) as cc, fb.Context(p0, FG_PREC_MIXED) as ce:
+        for c in (cf, cw, cc, ce):
             c.build_tables()
-        u = A.real_field(p0)
-        q = A.real_field(p0)
-        assert A.lib().fg_init_dipoR_host(C.byref(p0), A.dptr(u), A.dptr(q)) == 0
-        start_point(cf, p0, u, q)
-        cf.run_steps(probe)  # the sweep's first point, thermalised before the held-out ones
+        for c, s1 in ((cf, p0.seed[0]), (ce, p0.seed[0] + 1)):
+            pi = A.fg_params.from_buffer_copy(p0)
+            pi.seed[0] = s1
+            u = A.real_field(pi)
+            q = A.real_field(pi)
+            assert A.lib().fg_init_dipoR_host(C.byref(pi), A.dptr(u), A.dptr(q)) == 0
+            start_point(c, p0, u, q)
+            c.run_steps(probe)  # the sweep's first point, thermalised before the held-out ones
         for i, (T, ez) in enumerate(points):
             E = [0.0, 0.0, ez]
             cf.chain_point(T, E)
             Pf, Vf = equilibration_trace(cf, probe, every)
-            Pe, Ve = equilibration_trace(cf, probe, every)
+            ce.chain_point(T, E)
+            ce.run_steps(probe)
+            Pe, Ve = equilibration_trace(ce, probe, every)
             eq = block_stats(Pe, Ve)
             t0 = time.perf_counter()
             net.forward(np.array([[T, 0.0, 0.0, ez, -5.0]] * net.batch), [seed * 1000 + i] * net.batch)
@@ -427,8 +435,8 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
        the reference's .restart chaining: the fallback), from the network's
        proposal with Maxwell-Boltzmann momenta, and from a cold uni64 start
        (both settled by n_vs velocity-scaling steps, counted in their times);
-       the fallback continues for the point's equilibrium (block means and
-       their spread).  Time to equilibrium: three consecutive blocks of the
+       an independent chain through the same points gives the point's
+       equilibrium (block means and their spread).  Time to equilibrium: three consecutive blocks of the
        trace within 3 sigma of it.  Acceptance, the MD as the judge: the warm
        run's averages over [accept_after, probe) against the equilibrium,
        within 4 sigma of the difference; a rejected point keeps the fallback.
