@@ -474,8 +474,9 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
         out["settle_vs_steps"] = n_vs
         out["cooling_sweep"] = _sweep(net, make_params, L, sorted(pts[:n_held], reverse=True), seed, probe, every,
                                       accept_after, say, "sweep", n_vs)
-        out["shuffled"] = _sweep(net, make_params, L, pts[n_held:], seed + 7, probe, every, accept_after, say,
-                                 "shuffled", n_vs)
+        if n_shuffled > 0:
+            out["shuffled"] = _sweep(net, make_params, L, pts[n_held:], seed + 7, probe, every, accept_after, say,
+                                     "shuffled", n_vs)
         if keep_layers:
             out["_layers"] = [net.layer(l)[:2] for l in range(4)]
     finally:
