@@ -316,7 +316,7 @@ def block_stats(P2, V, block: int = 5):
 
 
 def accept(Pw, Vw, Pe, Ve, k: float = 4.0, block: int = 5) -> bool:
-    """The MD as the judge of a warm start: the warm run's block-averaged
+    """The MD as the referee of a warm start: the warm run's block-averaged
     |<u>|^2 and potential energy against the plain run's equilibrium, each
     within k standard errors of their difference (block means of `block`
     samples); a rejected warm start keeps the chained fallback."""
@@ -437,7 +437,7 @@ def experiment(make_params, L=32, train_chains=None, train_temps=None, n_held=40
        (both settled by n_vs velocity-scaling steps, counted in their times);
        an independent chain through the same points gives the point's
        equilibrium (block means and their spread).  Time to equilibrium: three consecutive blocks of the
-       trace within 3 sigma of it.  Acceptance, the MD as the judge: the warm
+       trace within 3 sigma of it.  Acceptance, the MD as the referee: the warm
        run's averages over [accept_after, probe) against the equilibrium,
        within 4 sigma of the difference; a rejected point keeps the fallback.
     Returns a dict of the measurements (with keep_layers, "_layers": the

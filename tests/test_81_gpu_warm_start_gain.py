@@ -1,4 +1,4 @@
-"""What the trained warm-start network gains, and the MD as its judge.
+"""What the trained warm-start network gains, and the MD as its referee.
 
 A small network is trained, as warm_start.experiment trains the large one,
 on configurations that the GPU MD generates along a 16^3 cooling chain
@@ -7,7 +7,7 @@ force).  At a held-out temperature in the ordered phase its proposal, after
 the same velocity-scaling settle as a cold start (initialize_dipoR's field),
 starts closer to the chained run's equilibrium in the order parameter
 |<u>|^2 and in the potential energy than the cold start does.  The
-acceptance judge (warm_start.accept) takes a run of the same equilibrium and
+acceptance test (warm_start.accept) takes a run of the same equilibrium and
 rejects one of another temperature."""
 import ctypes as C
 
@@ -43,7 +43,7 @@ def _equilibrium(T, n_therm=4000, n=3000, every=20):
         return W.equilibration_trace(ctx, n, every), W.equilibration_trace(ctx, n, every)
 
 
-def test_trained_net_starts_closer_to_equilibrium_and_the_judge(fg):
+def test_trained_net_starts_closer_to_equilibrium_and_is_refereed(fg):
     cond, stats, energies = W.generate_training_set(lambda T, ez, gpa: _mp(L, T, ez, gpa), [(0.0, -5.0)],
                                                     [400.0, 350.0, 300.0, 250.0, 200.0, 150.0],
                                                     n_therm=1500, n_snap=8, snap_every=100)
@@ -74,7 +74,7 @@ def test_trained_net_starts_closer_to_equilibrium_and_the_judge(fg):
     dw = (abs(first["warm"][0] - eqP), abs(first["warm"][1] - eqV))
     dc = (abs(first["cold"][0] - eqP), abs(first["cold"][1] - eqV))
     assert dw[0] < dc[0] and dw[1] < dc[1], (first, eqP, eqV)
-    # the judge: the same equilibrium is accepted, another temperature's is
+    # the referee: the same equilibrium is accepted, another temperature's is
     # not (blocks of 300 steps: longer than the order parameter's memory)
     assert W.accept(Pe2, Ve2, Pe, Ve, block=15)
     (Ph, Vh), _ = _equilibrium(300.0, n_therm=2000, n=1500)
