@@ -253,20 +253,31 @@ __device__ __forceinline__ void fft_inverse(cplx<T>* buf, const Batch& B, const 
 }
 
 // ---------------------------------------------------------------------------
-// Compile-time transforms for power-of-two lengths.  Same DIF/DIT algorithm
-// and slot order as above (the host builds its digit-reversal tables from
-// ct_radix), but every index is a compile-time expression, the radices are
-// 16 and 8 (two shared-memory stages for n <= 256), and twiddles come from a
+// Compile-time transforms for power-of-two lengths and for 12, 24 and 48.
+// Same DIF/DIT algorithm and slot order as above (the host builds its
+// digit-reversal tables from ct_radix), but every index is a compile-time
+// expression, the radices are 16 and 8 (two shared-memory stages for
+// n <= 256; 12, 24, 48 add a radix-3 stage), and twiddles come from a
 // shared-memory copy of the table.  Stage plans: 4:[4] 8:[8] 16:[16] 32:[8,4]
-// 64:[4,16] 128:[16,8] 256:[16,16] 512:[16,8,4].  64 starts with radix 4 so
+// 64:[4,16] 128:[16,8] 256:[16,16] 512:[16,8,4] 12:[4,3] 24:[8,3] 48:[16,3].
+// 64 starts with radix 4 so
 // that its first stage (16 butterflies per transform, elements 16 apart) can
 // read a 64-point row straight from global memory in 128-byte runs.
 __host__ __device__ constexpr bool ct_supported(int n) {
-  return n == 4 || n == 8 || n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512;
+  return n == 4 || n == 8 || n == 16 || n == 32 || n == 64 || n == 128 || n == 256 || n == 512 || n == 12 ||
+         n == 24 || n == 48;
 }
-__host__ __device__ constexpr int ct_nst(int n) { return n <= 16 ? 1 : (n <= 256 ? 2 : 3); }
+// 12, 24, 48 (the 24^3 and 48^3 supercells of the batched sweeps): a
+// power-of-two stage, then a radix-3 one (the runtime plan's order for 12
+// and 24)
+__host__ __device__ constexpr int ct_nst(int n) {
+  return (n == 12 || n == 24 || n == 48) ? 2 : (n <= 16 ? 1 : (n <= 256 ? 2 : 3));
+}
 __host__ __device__ constexpr int ct_radix(int n, int st) {
-  return n <= 16 ? n
+  return n == 12 ? (st == 0 ? 4 : 3)
+       : n == 24 ? (st == 0 ? 8 : 3)
+       : n == 48 ? (st == 0 ? 16 : 3)
+       : n <= 16 ? n
        : n == 32 ? (st == 0 ? 8 : 4)
        : n == 64 ? (st == 0 ? 4 : 16)
        : n == 128 ? (st == 0 ? 16 : 8)

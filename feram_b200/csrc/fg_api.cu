@@ -238,15 +238,18 @@ int check_device_error(fg_ctx* ctx) {
 }
 
 // ------------------------------------------------ FFT kernel dispatch
-// Compile-time instances for the cubic power-of-two supercells 16^3..128^3
-// (m = Lx/2, Ly) = (8,16) .. (64,128) and Lz = 16..128; the runtime-plan
-// kernels take every other size.
+// Compile-time instances for the cubic supercells 16^3..128^3 of powers of
+// two and 24^3, 48^3 (the sizes of the batched sweeps): (m = Lx/2, Ly) =
+// (8,16) .. (64,128), (12,24), (24,48) and Lz = 16..128, 24, 48; the
+// runtime-plan kernels take every other size.
 template <typename T, int MODE, class F>
 void with_xy_fwd(int m, int Ly, F f) {
   if (m == 64 && Ly == 128) f(k_xy_fwd<T, MODE, 64, 128>);
   else if (m == 32 && Ly == 64) f(k_xy_fwd<T, MODE, 32, 64>);
   else if (m == 16 && Ly == 32) f(k_xy_fwd<T, MODE, 16, 32>);
   else if (m == 8 && Ly == 16) f(k_xy_fwd<T, MODE, 8, 16>);
+  else if (m == 24 && Ly == 48) f(k_xy_fwd<T, MODE, 24, 48>);
+  else if (m == 12 && Ly == 24) f(k_xy_fwd<T, MODE, 12, 24>);
   else f(k_xy_fwd<T, MODE, 0, 0>);
 }
 template <typename T, class F>
@@ -255,6 +258,8 @@ void with_xy_inv(int m, int Ly, F f) {
   else if (m == 32 && Ly == 64) f(k_xy_inv<T, 32, 64>);
   else if (m == 16 && Ly == 32) f(k_xy_inv<T, 16, 32>);
   else if (m == 8 && Ly == 16) f(k_xy_inv<T, 8, 16>);
+  else if (m == 24 && Ly == 48) f(k_xy_inv<T, 24, 48>);
+  else if (m == 12 && Ly == 24) f(k_xy_inv<T, 12, 24>);
   else f(k_xy_inv<T, 0, 0>);
 }
 template <typename T>
@@ -270,12 +275,16 @@ void with_z_kspace(int Lz, int cw, bool acou, bool zsite, F f) {
     else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C, true>);
     else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C, true>);
     else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C, true>);
+    else if (cw == C && Lz == 48) f(k_z_kspace<T, 48, C, true>);
+    else if (cw == 4 && Lz == 24) f(k_z_kspace<T, 24, 4, true>);
     else f(k_z_kspace<T, 0, 0, true>);
   } else if (cw == C && Lz == 128) f(k_z_kspace<T, 128, C>);
   else if (sizeof(T) == 4 && cw == 4 && Lz == 128) f(k_z_kspace<T, 128, 4>);
   else if (cw == C && Lz == 64) f(k_z_kspace<T, 64, C>);
   else if (cw == C && Lz == 32) f(k_z_kspace<T, 32, C>);
   else if (cw == C && Lz == 16) f(k_z_kspace<T, 16, C>);
+  else if (cw == C && Lz == 48) f(k_z_kspace<T, 48, C>);
+  else if (cw == 4 && Lz == 24) f(k_z_kspace<T, 24, 4>);
   else f(k_z_kspace<T, 0, 0>);
 }
 
@@ -289,6 +298,8 @@ void with_z_pass(int Lz, int cw, F f) {
   else if (cw == C && Lz == 64) f(k_z_pass<T, INV, 64, C, 3>);
   else if (cw == C && Lz == 32) f(k_z_pass<T, INV, 32, C, 3>);
   else if (cw == C && Lz == 16) f(k_z_pass<T, INV, 16, C, 3>);
+  else if (cw == C && Lz == 48) f(k_z_pass<T, INV, 48, C, 3>);
+  else if (cw == 4 && Lz == 24) f(k_z_pass<T, INV, 24, 4, 3>);
   else f(k_z_pass<T, INV>);
 }
 

@@ -8,7 +8,8 @@ from feram_b200 import _capi as A
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(16, 16, 16), (12, 10, 6), (20, 12, 18), (8, 15, 9), (32, 24, 20)]
+# (24, 24, 24), (48, 48, 48): the compile-time transforms with a radix-3 stage
+SHAPES = [(16, 16, 16), (12, 10, 6), (20, 12, 18), (8, 15, 9), (32, 24, 20), (24, 24, 24), (48, 48, 48)]
 TOL = {A.FG_PREC_FP64: 2e-13, A.FG_PREC_MIXED: 2e-6}
 
 
@@ -46,7 +47,7 @@ def test_fft_c2r3_matches_numpy_nonhermitian(fg, shape, prec):
     ctx.close()
 
 
-@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 10, 6), (20, 12, 18)])
+@pytest.mark.parametrize("shape", [(16, 16, 16), (12, 10, 6), (20, 12, 18), (24, 24, 24)])
 def test_device_long_range_table_matches_oracle(fg, shape):
     p, ctx = _ctx(fg, shape, A.FG_PREC_FP64)
     ctx.build_tables()
