@@ -343,6 +343,13 @@ def batched_sweep(n_rep=96, steps=200):
         b.step(steps)
         t_batch = time.perf_counter() - t0
         groups = b.groups
+        # the same grouped graph without branch launch priorities
+        b.set_priorities(False)
+        b.step(3)
+        t0 = time.perf_counter()
+        b.step(steps)
+        t_noprio = time.perf_counter() - t0
+        b.set_priorities(True)
         # the same replicas, one after another (warm-up captures both the
         # eight-step and the one-step graph of fg_run_steps)
         for r in b.replicas:
@@ -354,6 +361,7 @@ def batched_sweep(n_rep=96, steps=200):
     return {"replicas": n_rep, "sizes": sizes, "kelvin_grid": [450.0, 100.0, -5.0], "sites": sites, "steps": steps, "precision": "mixed",
             "value": sites * steps / t_batch, "unit": UNIT, "graph_branches": groups,
             "branch_per_replica_value": sites * steps / t_branch,
+            "no_branch_priority_value": sites * steps / t_noprio,
             "sequential_value": sites * steps / t_seq, "speedup": t_seq / t_batch,
             "timing": "wall clock around synchronous calls"}
 
@@ -445,6 +453,13 @@ def chained_sweep(n_rep=96, n_points=4, n_therm=1000, n_avg=1000, every=10, log=
                 batched[i][k] = rows
         t_batch = time.perf_counter() - t0
         groups = b.groups
+        # the same grouped graph without branch launch priorities
+        b.set_priorities(False)
+        b.step(3)
+        t0 = time.perf_counter()
+        b.step(steps)
+        t_noprio = time.perf_counter() - t0
+        b.set_priorities(True)
     say(f"chained sweep: batched {t_batch:.1f} s")
     zs, table = [], []
     for L in sizes:

@@ -345,6 +345,10 @@ class Batch:
         """Replicas of one size step as one launch per kernel (default)."""
         lib().fg_batch_set_grouping(self._b, 1 if on else 0)
 
+    def set_priorities(self, on: bool = True):
+        """Branches of small supercells at a higher launch priority (default)."""
+        lib().fg_batch_set_priorities(self._b, 1 if on else 0)
+
     @property
     def groups(self) -> int:
         """Branches of the last captured batch graph."""

@@ -160,6 +160,7 @@ def lib() -> C.CDLL:
         "fg_set_wave": (C.c_int, [vp, C.c_int, C.c_int]),
         "fg_batch_set_grouping": (C.c_int, [vp, C.c_int]),
         "fg_batch_groups": (C.c_int, [vp]),
+        "fg_batch_set_priorities": (C.c_int, [vp, C.c_int]),
         "fg_sample": (C.c_int, [vp]),
         "fg_samples_read": (C.c_int, [vp, dp, C.c_int, P(C.c_int)]),
         "fg_run_point": (C.c_int, [vp, C.c_double, dp, C.c_int, C.c_int, C.c_int, C.POINTER(fg_energy)]),

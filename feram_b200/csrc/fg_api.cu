@@ -187,6 +187,10 @@ struct fg_ctx {
   // (0: the widest that fits) and the resident waves of the streaming
   // kernels (0: one block per 256 sites, up to grid_elem)
   int plan_zcw = 0, plan_waves = 1;
+  // launch priority of the kernels this context enqueues while use_prio is
+  // set (a replica batch's capture: small supercells ahead of large ones)
+  bool use_prio = false;
+  int launch_prio = 0;
   // sample series (fg_sample): kSampleCols doubles per row, on the device
   double* samples = nullptr;
   int n_samples = 0;
@@ -317,11 +321,20 @@ void launch_dep(fg_ctx* ctx, void (*kern)(KArgs...), dim3 grid, dim3 block, size
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = ctx->stream;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute at[2];
+  unsigned n = 0;
+  if (ctx->pdl) {
+    at[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[n].val.programmaticStreamSerializationAllowed = 1;
+    ++n;
+  }
+  if (ctx->use_prio) {
+    at[n].id = cudaLaunchAttributePriority;
+    at[n].val.priority = ctx->launch_prio;
+    ++n;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = ctx->pdl ? 1 : 0;
+  cfg.numAttrs = n;
   cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
@@ -2363,6 +2376,7 @@ struct fg_batch {
   cudaGraphExec_t graph = nullptr;   // one step of every replica
   std::vector<unsigned> gen;         // the replicas' gen when the graphs were captured
   bool grouping = true;              // replicas of one size step as one launch per kernel
+  bool priorities = true;            // branches of small supercells at a higher launch priority
   std::vector<std::vector<int>> groups;  // of the captured graph: replica indices per branch
   std::vector<RepArgs*> grp_dev;     // device tables of the grouped branches
   std::string err;
@@ -2424,15 +2438,35 @@ int batch_capture(fg_batch* b, cudaGraphExec_t* out) {
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, cudaGetErrorString(e));
   if ((e = cudaEventRecord(b->fork, b->stream)) != cudaSuccess) rc = FG_ERR_CUDA;
+  // branch priorities: the branches of the most sites at the lowest
+  // priority, each smaller one a step higher (down to the device's
+  // greatest), so that the short kernels of small supercells are scheduled
+  // into the waves of the large ones instead of after them
+  std::vector<int> prio(b->groups.size(), 0);
+  if (b->priorities && b->groups.size() > 1) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    std::vector<std::pair<long long, size_t>> by_sites;
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+      long long sites = 0;
+      for (int k : b->groups[gi]) sites += b->ctx[(size_t)k]->g.nsite;
+      by_sites.push_back({-sites, gi});
+    }
+    std::sort(by_sites.begin(), by_sites.end());
+    for (size_t r = 0; r < by_sites.size(); ++r) prio[by_sites[r].second] = std::max(greatest, least - (int)r);
+  }
   for (size_t gi = 0; gi < b->groups.size() && rc == FG_OK; ++gi) {
     const std::vector<int>& grp = b->groups[gi];
     fg_ctx* c = b->ctx[(size_t)grp[0]];
+    c->use_prio = b->priorities && b->groups.size() > 1;
+    c->launch_prio = prio[gi];
     if ((e = cudaStreamWaitEvent(c->stream, b->fork, 0)) != cudaSuccess) { rc = FG_ERR_CUDA; break; }
     if (grp.size() > 1)
       rc = c->prec == FG_PREC_MIXED ? enqueue_np_group<float>(c, b->grp_dev[gi], (int)grp.size())
                                     : enqueue_np_group<double>(c, b->grp_dev[gi], (int)grp.size());
     else
       rc = enqueue_step(c);
+    c->use_prio = false;
     if (rc) {
       b->err = "replica " + std::to_string(grp[0]) + ": " + c->err;
       break;
@@ -2444,7 +2478,7 @@ int batch_capture(fg_batch* b, cudaGraphExec_t* out) {
   cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
   if (rc) return rc == FG_ERR_CUDA && b->err.empty() ? batch_fail(b, rc, cudaGetErrorString(e)) : rc;
   if (ee != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ee));
-  e = cudaGraphInstantiate(out, graph, 0);
+  e = cudaGraphInstantiateWithFlags(out, graph, b->priorities ? cudaGraphInstantiateFlagUseNodePriority : 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return batch_fail(b, FG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   return FG_OK;
@@ -2567,6 +2601,19 @@ int fg_batch_set_grouping(fg_batch* b, int on) {
 }
 
 int fg_batch_groups(const fg_batch* b) { return b ? (int)b->groups.size() : 0; }
+
+int fg_batch_set_priorities(fg_batch* b, int on) {
+  if (!b) return FG_ERR_ARG;
+  if ((on != 0) != b->priorities) {
+    b->priorities = on != 0;
+    if (b->graph) {
+      cudaStreamSynchronize(b->stream);
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+  }
+  return FG_OK;
+}
 
 fg_ctx* fg_batch_context(fg_batch* b, int i) {
   return (b && i >= 0 && i < (int)b->ctx.size()) ? b->ctx[(size_t)i] : nullptr;

@@ -359,6 +359,12 @@ int  fg_batch_step(fg_batch* b, int n_steps, fg_energy* e);
 int  fg_batch_set_grouping(fg_batch* b, int on);
 /* Branches of the batch graph last captured (groups and single replicas). */
 int  fg_batch_groups(const fg_batch* b);
+/* Launch priorities for the branches of the batch graph on (default) or off:
+   the branch of the most sites at the device's lowest priority, each smaller
+   one a step higher, so that the short kernels of small supercells fill the
+   waves of the large ones.  Scheduling only; the results are the same bit
+   for bit. */
+int  fg_batch_set_priorities(fg_batch* b, int on);
 
 /* ---- sweep points and sample series -----------------------------------------
    A point of a temperature / field sweep as the reference's sweep scripts run

@@ -167,3 +167,30 @@ def test_grouped_replicas_equal_branches(fg, prec):
         assert a["s"] == c["s"] and a["pi"] == c["pi"]
         for f in A.POTENTIAL_FIELDS + ["dipo_kinetic", "total", "H_Nose_Poincare"]:
             assert getattr(out[False][1][i], f) == getattr(out[True][1][i], f), (i, f)
+
+
+def test_branch_priorities_change_no_bit(fg):
+    """Launch priorities on the batch graph's branches (small supercells
+    ahead of large ones) only reorder independent kernels: every replica's
+    state and energies are the same bit for bit with and without them."""
+    ps = [helpers.params(L=f"{n} {n} {n}", kelvin=str(300 - 20 * i)) for i, n in enumerate((8, 16, 16, 24))]
+    states = [(helpers.seeded_u(p, 90 + i, sigma=0.05), helpers.seeded_p(p, 90 + i, sigma=0.01))
+              for i, p in enumerate(ps)]
+    out = {}
+    for prio in (False, True):
+        with fb.Batch(ps, A.FG_PREC_MIXED) as b:
+            b.set_priorities(prio)
+            for r, (u, q) in zip(b.replicas, states):
+                r.build_tables()
+                r.set_state(u, q)
+                r.mirror_force_mirror()
+            es = b.step(9)
+            out[prio] = ([r.get_state() for r in b.replicas], es, b.groups)
+    assert out[False][2] == out[True][2] == 3
+    for i, p in enumerate(ps):
+        a, c = out[False][0][i], out[True][0][i]
+        for k in ("dipoR", "dipoP", "dVddi"):
+            assert np.array_equal(A.physical(a[k], p), A.physical(c[k], p)), (i, k)
+        assert a["s"] == c["s"] and a["pi"] == c["pi"]
+        for f in A.POTENTIAL_FIELDS + ["dipo_kinetic", "total", "H_Nose_Poincare"]:
+            assert getattr(out[False][1][i], f) == getattr(out[True][1][i], f), (i, f)
