@@ -453,13 +453,6 @@ def chained_sweep(n_rep=96, n_points=4, n_therm=1000, n_avg=1000, every=10, log=
                 batched[i][k] = rows
         t_batch = time.perf_counter() - t0
         groups = b.groups
-        # the same grouped graph without branch launch priorities
-        b.set_priorities(False)
-        b.step(3)
-        t0 = time.perf_counter()
-        b.step(steps)
-        t_noprio = time.perf_counter() - t0
-        b.set_priorities(True)
     say(f"chained sweep: batched {t_batch:.1f} s")
     zs, table = [], []
     for L in sizes:
