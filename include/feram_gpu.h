@@ -529,7 +529,7 @@ int  fg_ws_field(fg_ws* n, int b, int padding_y, double* dipoR);
    should come before any stream capture; a set-up that fails is not kept,
    and the next call tries it again.  The two host tables are copied from
    ordinary (pageable) host memory, so the call may wait until the stream
-   has taken them.  All calls on one device share the array: calls that
+   has taken them, and no call can be captured into a CUDA graph.  All calls on one device share the array: calls that
    overlap in time (different streams or host threads) race, and the caller
    must order them. */
 #define FG_NOALLOC_MAX_LZ 1024
