@@ -43,6 +43,14 @@ template <typename C, bool INV> __device__ __forceinline__ C mul_mi(C a) {
   return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
 }
 
+// Dynamic shared memory of a kernel, 16-byte aligned.  The host emulation
+// of the kernels (tests/host_emu) defines it, and the inline-PTX helpers
+// below (FG_HOST_EMU), as plain host code.
+#ifndef FG_DYN_SMEM
+#define FG_DYN_SMEM(name) extern __shared__ __align__(16) unsigned char name[]
+#endif
+
+#ifndef FG_HOST_EMU
 // Asynchronous global -> shared copies (cp.async, sm_80+): many copies in
 // flight per thread without register staging; complete with cp_async_wait().
 template <int BYTES>
@@ -53,6 +61,7 @@ __device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
   else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+#endif  // FG_HOST_EMU
 
 // L2 eviction priority for data read once and not needed again before it is
 // rewritten (a spectrum the next pass consumes, rwork read by the assembly):
@@ -63,6 +72,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_al
 #ifndef FG_L2_HINT_FP64
 #define FG_L2_HINT_FP64 0
 #endif
+#ifndef FG_HOST_EMU
 __device__ __forceinline__ unsigned long long l2_evict_first() {
   unsigned long long p;
   asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
@@ -104,6 +114,7 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
   asm volatile("griddepcontrol.wait;\n" ::: "memory");
 }
+#endif  // FG_HOST_EMU
 
 // Device error record (bounds checks, non-finite reductions).  The library
 // is one translation unit, so this __device__ variable has one definition.

@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_fwd(const T*
     src = (const T*)grp[blockIdx.z].u;
     spec = (cplx<T>*)grp[blockIdx.z].spec;
   }
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FG_DYN_SMEM(smem_raw);
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
   using T2 = typename RT2<T>::type;
@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_xy_inv(const cp
   // energies and the homogeneous strain, from k_z_kspace's block partials
   // (nothing in this kernel needs them; k_assemble does).
   if (ph != nullptr && blockIdx.x == 0 && blockIdx.y == 0) homo_strain_tail(ph, sc, part_k, nblk_k);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FG_DYN_SMEM(smem_raw);
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_m[MC > 0 ? MC : 1], tws_y[LYC > 0 ? LYC : 1], tws_x[MC > 0 ? MC + 1 : 1];
   using T2 = typename RT2<T>::type;
@@ -910,7 +910,7 @@ struct KMaps {
 template <typename T, bool INV, int LZC = 0, int CWC = 0, int NCC = 0>
 __global__ void __launch_bounds__(256) k_z_pass(cplx<T>* __restrict__ spec, Geom g, FftPlan pz,
                                                 const cplx<T>* __restrict__ twz, int nc, ZTiles zt) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FG_DYN_SMEM(smem_raw);
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   if constexpr (LZC > 0) {
     __shared__ cplx<T> tws[LZC];
@@ -970,7 +970,7 @@ __global__ void __launch_bounds__(256, kZMinBlocks<T>(CWC)) k_z_kspace(cplx<T>* 
     part = a.part_k;
     sc = a.sc;
   }
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FG_DYN_SMEM(smem_raw);
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   __shared__ cplx<T> tws_z[LZC > 0 ? LZC : 1];
   const int Lz = LZC > 0 ? LZC : g.Lz, CW = CWC > 0 ? CWC : zt.CW;
@@ -2144,7 +2144,7 @@ __global__ void __launch_bounds__(256) k_z_ewald_pack(const cplx<double>* __rest
                                                       const cplx<double>* __restrict__ twz, KMaps km,
                                                       const Phys* __restrict__ ph, double a0, double kappa,
                                                       double eps_inf, int max_x, int max_y, int max_z, ZTiles zt) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FG_DYN_SMEM(smem_raw);
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem_raw);
   const int Lz = g.Lz, CW = zt.CW;
   z_tile_load<double>(buf, spec, g, zt, 6);
@@ -2215,7 +2215,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_z_modulation_pack(const cplx<double>* __restrict__ spec, cplx<T>* __restrict__ ck,
                                                            Geom g, FftPlan pz, const cplx<double>* __restrict__ twz,
                                                            KMaps km, double mod_const, ZTiles zt) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  FG_DYN_SMEM(smem_raw);
   cplx<double>* buf = reinterpret_cast<cplx<double>*>(smem_raw);
   const int Lz = g.Lz, CW = zt.CW;
   z_tile_load<double>(buf, spec, g, zt, 1);
