@@ -98,8 +98,11 @@ long double field(const std::vector<T>& u, long long ns, int c, long long i) {
   }
 }
 
+// extra: 0 the 9 components; 1 acoustic MD (components 9..11 are src
+// components 3..5, the acoustic displacement stored after u); 2 per-site Z*
+// (components 9..11 are Z*(R) u, dipoFFT.F:36-44)
 template <typename T, int MC, int LYC>
-void xy_case(int Lx, int Ly, int Lz) {
+void xy_case(int Lx, int Ly, int Lz, int extra = 0) {
   Geom g{};
   g.Lx = Lx;
   g.Ly = Ly;
@@ -127,29 +130,40 @@ void xy_case(int Lx, int Ly, int Lz) {
   const std::vector<cplx<T>> twx = twiddles<T>(Lx), twm = twiddles<T>(g.m), twy = twiddles<T>(Ly);
 
   const long long ns = g.nsite;
-  std::vector<T> u((size_t)(3 * ns));
-  std::mt19937_64 gen(77u + (unsigned)(Lx * 1000 + Ly * 10 + Lz));
-  std::uniform_real_distribution<double> dist(-0.2, 0.2);
+  const int nc = extra ? 12 : 9, zu0 = extra == 2 ? 9 : 0;
+  std::vector<T> u((size_t)((extra == 1 ? 6 : 3) * ns)), zs;
+  std::mt19937_64 gen(77u + (unsigned)(Lx * 1000 + Ly * 10 + Lz + extra));
+  std::uniform_real_distribution<double> dist(-0.2, 0.2), zdist(0.5, 1.5);
   for (auto& v : u) v = (T)dist(gen);
+  if (extra == 2) {
+    zs.resize((size_t)ns);
+    for (auto& v : zs) v = (T)zdist(gen);
+  }
+  auto fld = [&](int c, long long i) -> long double {
+    if (c < 9) return field(u, ns, c, i);
+    if (extra == 1) return u[(size_t)((c - 6) * ns + i)];
+    return (long double)zs[(size_t)i] * u[(size_t)((c - 9) * ns + i)];
+  };
   const T nan = std::nan("");
-  std::vector<cplx<T>> spec((size_t)(9 * g.ncplx), mk<cplx<T>>(nan, nan));
+  std::vector<cplx<T>> spec((size_t)(nc * g.ncplx), mk<cplx<T>>(nan, nan));
   const size_t smem = sizeof(cplx<T>) * (size_t)Ly * (size_t)(g.m + 1);
 
-  emu::launch(k_xy_fwd<T, SRC_U9, MC, LYC>, dim3((unsigned)Lz, 9), dim3(512), smem, (const T*)u.data(),
+  emu::launch(k_xy_fwd<T, SRC_U9, MC, LYC>, dim3((unsigned)Lz, (unsigned)nc), dim3(512), smem, (const T*)u.data(),
               spec.data(), g, px, py, (const cplx<T>*)twx.data(), (const cplx<T>*)twm.data(),
-              (const cplx<T>*)twy.data(), (const int*)posm.data(), 0, (const T*)nullptr, 0, (const RepArgs*)nullptr);
+              (const cplx<T>*)twy.data(), (const int*)posm.data(), 0, (const T*)(extra == 2 ? zs.data() : nullptr), zu0,
+              (const RepArgs*)nullptr);
 
   // direct transform: along x for kx = 0..m, then along y
   const std::vector<cld> wx = unit_roots(Lx), wy = unit_roots(Ly);
   double ef = 0, xmax = 0, fmax = 0;
   std::vector<cld> rowx((size_t)Ly * (g.m + 1));
-  for (int c = 0; c < 9; ++c)
+  for (int c = 0; c < nc; ++c)
     for (int z = 0; z < Lz; ++z) {
       for (int y = 0; y < Ly; ++y)
         for (int kx = 0; kx <= g.m; ++kx) {
           cld s = 0;
           for (int x = 0; x < Lx; ++x) {
-            const long double f = field(u, ns, c, (long long)z * g.plane_r + (long long)y * Lx + x);
+            const long double f = fld(c, (long long)z * g.plane_r + (long long)y * Lx + x);
             fmax = std::max(fmax, (double)std::fabs(f));
             s += f * wx[(size_t)((kx * x) % Lx)];
           }
@@ -169,20 +183,20 @@ void xy_case(int Lx, int Ly, int Lz) {
       }
     }
 
-  std::vector<T> out((size_t)(9 * ns), nan);
-  emu::launch(k_xy_inv<T, MC, LYC>, dim3((unsigned)Lz, 9), dim3(512), smem, (const cplx<T>*)spec.data(), out.data(),
+  std::vector<T> out((size_t)(nc * ns), nan);
+  emu::launch(k_xy_inv<T, MC, LYC>, dim3((unsigned)Lz, (unsigned)nc), dim3(512), smem, (const cplx<T>*)spec.data(), out.data(),
               g, px, py, (const cplx<T>*)twx.data(), (const cplx<T>*)twm.data(), (const cplx<T>*)twy.data(),
               (const int*)posm.data(), 0, (const Phys*)nullptr, (DevScalars*)nullptr, (const double*)nullptr, 0,
               (const RepArgs*)nullptr);
   double eb = 0;
   const long double scale = (long double)Lx * Ly;
-  for (int c = 0; c < 9; ++c)
+  for (int c = 0; c < nc; ++c)
     for (long long i = 0; i < ns; ++i) {
-      const double d = (double)std::fabs((long double)out[(size_t)(c * ns + i)] - scale * field(u, ns, c, i));
+      const double d = (double)std::fabs((long double)out[(size_t)(c * ns + i)] - scale * fld(c, i));
       eb = std::max(eb, std::isfinite(d) ? d : 1e300);
     }
-  std::printf("xy_%s_%s_%dx%dx%d %.3e %.3e\n", sizeof(T) == 4 ? "f32" : "f64", MC > 0 ? "ct" : "rt", Lx, Ly, Lz,
-              ef / xmax, eb / ((double)scale * fmax));
+  std::printf("xy_%s_%s_%dx%dx%d%s %.3e %.3e\n", sizeof(T) == 4 ? "f32" : "f64", MC > 0 ? "ct" : "rt", Lx, Ly, Lz,
+              extra == 1 ? "_acou" : extra == 2 ? "_zstar" : "", ef / xmax, eb / ((double)scale * fmax));
   std::fflush(stdout);
 }
 
@@ -315,6 +329,10 @@ void all_cases() {
   xy_case<T, 0, 0>(20, 12, 2);
   xy_case<T, 0, 0>(30, 18, 1);
   xy_case<T, 0, 0>(16, 16, 2);
+  xy_case<T, 8, 16>(16, 16, 2, 1);
+  xy_case<T, 8, 16>(16, 16, 2, 2);
+  xy_case<T, 0, 0>(12, 10, 2, 1);
+  xy_case<T, 0, 0>(12, 10, 2, 2);
   // 3D transforms with the z pass instances of the library's dispatch
   constexpr int C = sizeof(T) == 4 ? 8 : 4;
   fft3_case<T, 8, 16, 16, C>(16, 16, 16);

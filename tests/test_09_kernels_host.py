@@ -5,9 +5,11 @@ g++ behind `tests/host_emu/kernel_emu.h` (the threads of a block as fibers
 switched at __syncthreads() and warp shuffles, blocks in grid order) and runs
 the library's own kernels on small supercells:
 
-* `k_xy_fwd` (SRC_U9: u and u⊗u formed on load, dipoFFT.F:19-44) against a
-  direct 2D DFT per z plane and component, in the slot orders of the x and y
-  plans; `k_xy_inv` must return Lx*Ly times each plane;
+* `k_xy_fwd` (SRC_U9: u and u⊗u formed on load, dipoFFT.F:19-44; with the
+  acoustic displacement as components 9..11, or Z*(R) u for per-site Z*,
+  dipoFFT.F:36-44) against a direct 2D DFT per z plane and component, in the
+  slot orders of the x and y plans; `k_xy_inv` must return Lx*Ly times each
+  plane;
 * the 3-component r2c / c2r of `fg_fft_r2c3` / `fg_fft_c2r3` (`k_xy_fwd`
   SRC_FIELD + `k_z_pass`, coord_module.F:155-157,310-312) against a direct 3D
   DFT, and back to Lx*Ly*Lz times the fields;
@@ -54,7 +56,9 @@ def test_every_instance_ran(emu_lines):
         for name in ("fft3_{p}_ct_16x16x16", "fft3_{p}_ct_16x16x128", "fft3_{p}_ct_24x24x24", "fft3_{p}_ct_16x16x48",
                      "fft3_{p}_rt_20x6x15", "xy_{p}_rt_10x6x2"):
             assert name.format(p=prec) in emu_lines
-    assert len(emu_lines) == 2 * (11 + 8)
+        for name in ("xy_{p}_ct_16x16x2_acou", "xy_{p}_ct_16x16x2_zstar", "xy_{p}_rt_12x10x2_zstar"):
+            assert name.format(p=prec) in emu_lines
+    assert len(emu_lines) == 2 * (15 + 8)
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])
